@@ -1,0 +1,20 @@
+"""aperture3_b200: the Aperture3 particle update for NVIDIA B200 (sm_100a).
+
+The Vay push fused with charge-conserving (Esirkepov) current deposition,
+the per-step tile counting sort and the Yee FDTD field update, as
+hand-written CUDA kernels in libaperture_b200.so behind a C ABI
+(include/aperture_b200.h). This package is the host-side mirror of the
+reference's lab-facing classes (ptc_updater, field_solver, sim_environment,
+sim_data) over that ABI. There is no CPU fallback: importing the classes
+loads the library and fails if it is missing.
+"""
+from . import _lib  # noqa: F401
+from .sim import (FLAG_IGNORE_CURRENT, FLAG_IGNORE_EM, ELECTRON, ION, POSITRON, FieldSolver,
+                  PtcUpdater, SimData, SimEnvironment, SimParams, field_solver, ptc_updater,
+                  species_flag)
+
+__all__ = [
+    "SimParams", "SimEnvironment", "SimData", "ptc_updater", "field_solver", "PtcUpdater",
+    "FieldSolver", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
+    "FLAG_IGNORE_CURRENT",
+]

@@ -1,0 +1,144 @@
+"""ctypes binding of libaperture_b200.so (the C ABI in include/aperture_b200.h).
+
+The library is the only compute path: importing this module fails loudly if
+the shared object is missing or does not export the declared symbols.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaperture_b200.so")
+
+AP_MAX_SPECIES = 8
+AP_MAX_CELL = 0xFFFFFFFF
+
+STATUS = {
+    0: "AP_OK", 1: "AP_ERR_INVALID", 2: "AP_ERR_CUDA", 3: "AP_ERR_NAN",
+    4: "AP_ERR_MOVED_FAR", 5: "AP_ERR_CAPACITY", 6: "AP_ERR_TIMEOUT",
+    7: "AP_ERR_UNSUPPORTED", 8: "AP_ERR_NOMEM", 9: "AP_ERR_TILE",
+}
+
+
+class ApError(RuntimeError):
+    """A nonzero ap_status. The reference reports these conditions by
+    throwing from CudaSafeCall or trapping in the kernel
+    (src/cuda/cudaUtility.h:34-74, ptc_updater.cu:102-109)."""
+
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+
+
+class ApMesh(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int * 3), ("guard", C.c_int * 3),
+        ("delta", C.c_float * 3), ("inv_delta", C.c_float * 3),
+        ("lower", C.c_float * 3), ("sizes", C.c_float * 3),
+        ("dimension", C.c_int),
+    ]
+
+
+class ApParams(C.Structure):
+    _fields_ = [
+        ("num_species", C.c_int), ("data_interval", C.c_int),
+        ("current_smoothing", C.c_int), ("periodic", C.c_int * 3),
+        ("charges", C.c_float * AP_MAX_SPECIES), ("masses", C.c_float * AP_MAX_SPECIES),
+        ("tile", C.c_int * 2),
+    ]
+
+
+class ApArray(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("pitch", C.c_size_t)]
+
+
+class ApFields(C.Structure):
+    _fields_ = [
+        ("E", ApArray * 3), ("B", ApArray * 3), ("Ebg", ApArray * 3), ("Bbg", ApArray * 3),
+        ("J", ApArray * 3), ("Rho", ApArray * AP_MAX_SPECIES), ("divE", ApArray),
+        ("divB", ApArray),
+    ]
+
+
+class ApParticles(C.Structure):
+    _fields_ = [
+        ("x1", C.c_void_p), ("x2", C.c_void_p), ("x3", C.c_void_p),
+        ("p1", C.c_void_p), ("p2", C.c_void_p), ("p3", C.c_void_p),
+        ("E", C.c_void_p), ("weight", C.c_void_p), ("cell", C.c_void_p),
+        ("id", C.c_void_p), ("flag", C.c_void_p),
+    ]
+
+
+class ApStepStats(C.Structure):
+    _fields_ = [("nan_momenta", C.c_uint64), ("moved_far", C.c_uint64),
+                ("lost", C.c_uint64), ("tile_faults", C.c_uint64), ("live", C.c_uint64)]
+
+
+class ApDiag(C.Structure):
+    _fields_ = [("kinetic", C.c_double), ("charge", C.c_double),
+                ("field_energy", C.c_double), ("max_abs_rho", C.c_double),
+                ("gauss_residual", C.c_double), ("max_abs_j", C.c_double)]
+
+
+_vp = C.c_void_p
+_i = C.c_int
+# name -> (restype, argtypes); every function declared in aperture_b200.h
+SIGNATURES = {
+    "ap_version": (C.c_char_p, []),
+    "ap_status_string": (C.c_char_p, [_i]),
+    "ap_ctx_create": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams), C.POINTER(_vp)]),
+    "ap_ctx_destroy": (_i, [_vp]),
+    "ap_set_stream": (_i, [_vp, _vp]),
+    "ap_set_sync": (_i, [_vp, _i]),
+    "ap_sync": (_i, [_vp]),
+    "ap_bind_fields": (_i, [_vp, C.POINTER(ApFields)]),
+    "ap_bind_particles": (_i, [_vp, C.POINTER(ApParticles), C.c_size_t, C.c_size_t]),
+    "ap_particles_modified": (_i, [_vp, C.c_size_t]),
+    "ap_get_number": (_i, [_vp, C.POINTER(C.c_size_t)]),
+    "ap_update_particles": (_i, [_vp, C.c_double, C.c_uint32]),
+    "ap_smooth_current": (_i, [_vp, C.c_uint32]),
+    "ap_smooth_array": (_i, [_vp, ApArray]),
+    "ap_update_fields": (_i, [_vp, C.c_double, C.c_uint32]),
+    "ap_update_e_field": (_i, [_vp, C.c_double]),
+    "ap_update_b_field": (_i, [_vp, C.c_double]),
+    "ap_compute_divs": (_i, [_vp]),
+    "ap_send_guard_cells": (_i, [_vp, ApArray]),
+    "ap_send_add_guard_cells": (_i, [_vp, ApArray]),
+    "ap_sort_by_cell": (_i, [_vp]),
+    "ap_get_tile_order": (_i, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_uint32),
+                               C.POINTER(C.c_size_t)]),
+    "ap_get_stats": (_i, [_vp, C.POINTER(ApStepStats)]),
+    "ap_diagnostics": (_i, [_vp, C.POINTER(ApDiag)]),
+    "ap_last_error": (_i, [_vp]),
+    "ap_launch_count": (C.c_uint64, [_vp]),
+}
+
+
+def load(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python aperture3_b200/build.py` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)  # AttributeError if the symbol is not exported
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = load()
+    return _LIB
+
+
+def check(status, what):
+    if status != 0:
+        raise ApError(status, what)
+    return status

@@ -1,0 +1,554 @@
+// C ABI of libaperture_b200.so: context management, binding of the
+// caller's arrays, and the orchestration of ptc_updater::update_particles /
+// field_solver::update_fields for one rank.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+
+#include "ap_internal.h"
+
+using namespace apb;
+
+struct ap_ctx : public apb::Ctx {};
+
+namespace apb {
+
+MeshK make_meshk(const ap_mesh &m) {
+  MeshK k;
+  for (int i = 0; i < 3; ++i) {
+    k.dims[i] = m.dims[i];
+    k.guard[i] = m.guard[i];
+    k.red[i] = m.dims[i] - 2 * m.guard[i];
+    k.delta[i] = m.delta[i];
+    k.inv_delta[i] = m.inv_delta[i];
+  }
+  if (m.dims[1] <= 1 && m.dims[2] <= 1)
+    k.dim = 1;
+  else if (m.dims[2] <= 1)
+    k.dim = 2;
+  else
+    k.dim = 3;
+  return k;
+}
+
+}  // namespace apb
+
+namespace {
+
+int fail(Ctx *c, int st) {
+  if (c) c->last_error = st;
+  return st;
+}
+
+int cuda_fail(Ctx *c, cudaError_t e) {
+  if (e == cudaSuccess) return AP_OK;
+  if (e == cudaErrorMemoryAllocation) return fail(c, AP_ERR_NOMEM);
+  return fail(c, AP_ERR_CUDA);
+}
+
+#define AP_TRY(expr)                              \
+  do {                                            \
+    cudaError_t _e = (expr);                      \
+    if (_e != cudaSuccess) return cuda_fail(c, _e); \
+  } while (0)
+
+#define AP_TRY_ST(expr)              \
+  do {                               \
+    int _s = (expr);                 \
+    if (_s != AP_OK) return fail(c, _s); \
+  } while (0)
+
+bool is_supported_tile(int tx, int ty) {
+  return (tx == 16 && ty == 16) || (tx == 32 && ty == 16) || (tx == 32 && ty == 32) ||
+         (tx == 8 && ty == 8) || (tx == 16 && ty == 8) || (tx == 4 && ty == 4);
+}
+
+void choose_tiles(Ctx &c) {
+  const int r0 = c.mk.red[0], r1 = c.mk.dim > 1 ? c.mk.red[1] : 1;
+  int tx = c.params.tile[0], ty = c.params.tile[1];
+  if (c.mk.dim == 1) {
+    tx = 1;
+    ty = 1;
+  } else if (!is_supported_tile(tx, ty)) {
+    const int cand[4][2] = {{16, 16}, {8, 8}, {4, 4}, {4, 4}};
+    tx = 4;
+    ty = 4;
+    for (auto &t : cand)
+      if ((r0 + t[0] - 1) / t[0] >= 3 && (r1 + t[1] - 1) / t[1] >= 3) {
+        tx = t[0];
+        ty = t[1];
+        break;
+      }
+  }
+  c.tiles.tx = tx;
+  c.tiles.ty = ty;
+  c.tiles.ntx = (r0 + tx - 1) / tx;
+  c.tiles.nty = c.mk.dim > 1 ? (r1 + ty - 1) / ty : 1;
+  c.tiles.ntiles = c.tiles.ntx * c.tiles.nty;
+}
+
+// The per-step order update needs at least three tiles per dim so that the
+// eight neighbours of a tile are distinct; smaller grids rebuild the order
+// with the full sort every step.
+bool incremental_order(const Ctx &c) { return c.tiles.ntx >= 3 && c.tiles.nty >= 3; }
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor maps for the E/B tiles: a box of (tx + 8) x (ty + 2) floats whose
+// x start is rounded down to a multiple of four floats (16 bytes).
+bool setup_tensor_maps(Ctx &c) {
+  if (c.mk.dim != 2) return false;
+  auto enc = encode_fn();
+  if (!enc) return false;
+  const ap_array *src[6] = {&c.fields.E[0], &c.fields.E[1], &c.fields.E[2],
+                            &c.fields.B[0], &c.fields.B[1], &c.fields.B[2]};
+  for (int k = 0; k < 6; ++k) {
+    const ap_array &a = *src[k];
+    if ((reinterpret_cast<uintptr_t>(a.ptr) & 15u) || (a.pitch & 15u)) return false;
+    cuuint64_t gdim[2] = {(cuuint64_t)c.mesh.dims[0], (cuuint64_t)c.mesh.dims[1]};
+    cuuint64_t gstride[1] = {(cuuint64_t)a.pitch};
+    cuuint32_t box[2] = {(cuuint32_t)(c.tiles.tx + 8), (cuuint32_t)(c.tiles.ty + 2)};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult r = enc(&c.maps.m[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, a.ptr, gdim, gstride, box,
+                     estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+  }
+  return true;
+}
+
+bool valid_array(const ap_array &a, const ap_mesh &m) {
+  return a.ptr != nullptr && a.pitch >= sizeof(float) * (size_t)m.dims[0] &&
+         (a.pitch % sizeof(float)) == 0;
+}
+
+int finish(Ctx *c) {
+  if (!c->sync) return AP_OK;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e);
+  return AP_OK;
+}
+
+int check_status(Ctx *c) {
+  cudaError_t e = cudaMemcpyAsync(c->status_host, c->status, sizeof(DevStatus),
+                                  cudaMemcpyDeviceToHost, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e);
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e);
+  const DevStatus &s = *c->status_host;
+  if (s.tile_faults) c->order_valid = false;
+  if (s.timeouts) return fail(c, AP_ERR_TIMEOUT);
+  if (s.tile_faults) return fail(c, AP_ERR_TILE);
+  if (s.nan_momenta) return fail(c, AP_ERR_NAN);
+  if (s.moved_far) return fail(c, AP_ERR_MOVED_FAR);
+  return AP_OK;
+}
+
+int alloc_particle_state(Ctx *c, size_t cap) {
+  if (cap <= c->order_cap && c->order[0]) return AP_OK;
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(c->order[i]);
+    c->order[i] = nullptr;
+  }
+  cudaFree(c->dir);
+  c->dir = nullptr;
+  size_t n = cap < 1 ? 1 : cap;
+  for (int i = 0; i < 2; ++i)
+    if (cudaMalloc(&c->order[i], n * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
+  if (cudaMalloc(&c->dir, n) != cudaSuccess) return AP_ERR_NOMEM;
+  c->order_cap = n;
+  return ensure_scratch(*c, n);
+}
+
+}  // namespace
+
+extern "C" {
+
+AP_API const char *ap_version(void) { return "aperture_b200 0.1 (sm_100a)"; }
+
+AP_API const char *ap_status_string(int s) {
+  switch (s) {
+    case AP_OK: return "ok";
+    case AP_ERR_INVALID: return "invalid argument or state";
+    case AP_ERR_CUDA: return "CUDA runtime error";
+    case AP_ERR_NAN: return "NaN momentum in push";
+    case AP_ERR_MOVED_FAR: return "particle moved more than one cell";
+    case AP_ERR_CAPACITY: return "size exceeds a fixed limit";
+    case AP_ERR_TIMEOUT: return "bounded device wait timed out";
+    case AP_ERR_UNSUPPORTED: return "unsupported grid or option";
+    case AP_ERR_NOMEM: return "device allocation failed";
+    case AP_ERR_TILE: return "particle outside its sort tile";
+    default: return "unknown status";
+  }
+}
+
+AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params, ap_ctx **out) {
+  if (!mesh || !params || !out) return AP_ERR_INVALID;
+  *out = nullptr;
+  MeshK mk = make_meshk(*mesh);
+  if (mk.dim == 3) return AP_ERR_UNSUPPORTED;
+  for (int d = 0; d < mk.dim; ++d) {
+    if (mesh->guard[d] < 2) return AP_ERR_INVALID;  // the deposit reaches two cells out
+    if (mk.red[d] < 1) return AP_ERR_INVALID;
+    if (params->periodic[d] && mk.red[d] < 2 * mesh->guard[d]) return AP_ERR_INVALID;
+  }
+  if (params->num_species < 1 || params->num_species > AP_MAX_SPECIES) return AP_ERR_INVALID;
+  if (params->data_interval < 1 || params->current_smoothing < 0) return AP_ERR_INVALID;
+  if ((uint64_t)mesh->dims[0] * mesh->dims[1] * mesh->dims[2] >= AP_MAX_CELL - 1ull)
+    return AP_ERR_CAPACITY;
+  ap_ctx *c = new (std::nothrow) ap_ctx();
+  if (!c) return AP_ERR_NOMEM;
+  c->mesh = *mesh;
+  c->params = *params;
+  c->mk = mk;
+  choose_tiles(*c);
+  cudaGetDevice(&c->device);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return AP_ERR_CUDA;
+  }
+  c->own_stream = true;
+  const int nt = c->tiles.ntiles;
+  bool ok = cudaMalloc(&c->status, sizeof(DevStatus)) == cudaSuccess &&
+            cudaMallocHost(&c->status_host, sizeof(DevStatus)) == cudaSuccess &&
+            cudaMalloc(&c->dir_count, sizeof(uint32_t) * ((size_t)nt * 10 + 16)) == cudaSuccess &&
+            cudaMalloc(&c->grp_off, sizeof(uint32_t) * ((size_t)nt * 9 + 16)) == cudaSuccess &&
+            cudaMalloc(&c->tile_start[0], sizeof(uint32_t) * (nt + 1)) == cudaSuccess &&
+            cudaMalloc(&c->tile_start[1], sizeof(uint32_t) * (nt + 1)) == cudaSuccess &&
+            cudaMalloc(&c->queue, sizeof(uint32_t) * 4) == cudaSuccess &&
+            cudaMalloc(&c->diag_dev, sizeof(double) * 16) == cudaSuccess &&
+            cudaMallocHost(&c->diag_host, sizeof(double) * 16) == cudaSuccess;
+  if (!ok) {
+    ap_ctx_destroy(c);
+    return AP_ERR_NOMEM;
+  }
+  cudaMemset(c->status, 0, sizeof(DevStatus));
+  std::memset(c->status_host, 0, sizeof(DevStatus));
+  *out = c;
+  return AP_OK;
+}
+
+AP_API int ap_ctx_destroy(ap_ctx *c) {
+  if (!c) return AP_ERR_INVALID;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(c->order[i]);
+    cudaFree(c->tile_start[i]);
+    cudaFree(c->keys[i]);
+    cudaFree(c->vals[i]);
+  }
+  cudaFree(c->dir);
+  cudaFree(c->dir_count);
+  cudaFree(c->grp_off);
+  cudaFree(c->queue);
+  cudaFree(c->cub_tmp);
+  cudaFree(c->gather_tmp);
+  cudaFree(c->tmp_j);
+  cudaFree(c->acc);
+  cudaFree(c->status);
+  cudaFree(c->diag_dev);
+  if (c->status_host) cudaFreeHost(c->status_host);
+  if (c->diag_host) cudaFreeHost(c->diag_host);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return AP_OK;
+}
+
+AP_API int ap_set_stream(ap_ctx *c, void *stream) {
+  if (!c) return AP_ERR_INVALID;
+  if (c->own_stream && c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  c->own_stream = false;
+  c->stream = static_cast<cudaStream_t>(stream);
+  return AP_OK;
+}
+
+AP_API int ap_set_sync(ap_ctx *c, int sync) {
+  if (!c) return AP_ERR_INVALID;
+  c->sync = sync != 0;
+  return AP_OK;
+}
+
+AP_API int ap_sync(ap_ctx *c) {
+  if (!c) return AP_ERR_INVALID;
+  return check_status(c);
+}
+
+AP_API int ap_bind_fields(ap_ctx *c, const ap_fields *f) {
+  if (!c || !f) return AP_ERR_INVALID;
+  const ap_mesh &m = c->mesh;
+  for (int k = 0; k < 3; ++k)
+    if (!valid_array(f->E[k], m) || !valid_array(f->B[k], m) || !valid_array(f->Ebg[k], m) ||
+        !valid_array(f->Bbg[k], m) || !valid_array(f->J[k], m))
+      return fail(c, AP_ERR_INVALID);
+  for (int s = 0; s < c->params.num_species; ++s)
+    if (!valid_array(f->Rho[s], m)) return fail(c, AP_ERR_INVALID);
+  c->fields = *f;
+  c->fields_bound = true;
+  c->use_tma = setup_tensor_maps(*c);
+  if (!c->acc) {
+    c->acc_comp = (size_t)m.dims[0] * m.dims[1] * m.dims[2];
+    AP_TRY(cudaMalloc(&c->acc, sizeof(double) * c->acc_comp * (3 + c->params.num_species)));
+  }
+  if (!c->tmp_j) {
+    size_t pitch = sizeof(float) * (size_t)m.dims[0];
+    AP_TRY(cudaMalloc(&c->tmp_j, pitch * (size_t)m.dims[1] * m.dims[2]));
+    AP_TRY(cudaMemset(c->tmp_j, 0, pitch * (size_t)m.dims[1] * m.dims[2]));
+    c->tmp_pitch = m.dims[0];
+  }
+  return AP_OK;
+}
+
+AP_API int ap_bind_particles(ap_ctx *c, const ap_particles *p, size_t number, size_t capacity) {
+  if (!c || !p) return AP_ERR_INVALID;
+  if (number > capacity || capacity >= (size_t)UINT32_MAX) return fail(c, AP_ERR_CAPACITY);
+  if (!p->x1 || !p->x2 || !p->x3 || !p->p1 || !p->p2 || !p->p3 || !p->E || !p->weight ||
+      !p->cell || !p->id || !p->flag)
+    return fail(c, AP_ERR_INVALID);
+  c->ptc = *p;
+  c->number = number;
+  c->capacity = capacity;
+  c->ptc_bound = true;
+  c->order_valid = false;
+  AP_TRY_ST(alloc_particle_state(c, capacity));
+  return AP_OK;
+}
+
+AP_API int ap_particles_modified(ap_ctx *c, size_t number) {
+  if (!c || !c->ptc_bound) return AP_ERR_INVALID;
+  if (number > c->capacity) return fail(c, AP_ERR_CAPACITY);
+  c->number = number;
+  c->order_valid = false;
+  return AP_OK;
+}
+
+AP_API int ap_get_number(const ap_ctx *c, size_t *n) {
+  if (!c || !n) return AP_ERR_INVALID;
+  *n = c->number;
+  return AP_OK;
+}
+
+AP_API int ap_smooth_array(ap_ctx *c, ap_array a) {
+  if (!c || !c->fields_bound || !valid_array(a, c->mesh)) return AP_ERR_INVALID;
+  int bnd[4] = {!c->params.periodic[0], !c->params.periodic[0], !c->params.periodic[1],
+                !c->params.periodic[1]};
+  AP_TRY(launch_filter(*c, a, bnd));
+  return finish(c);
+}
+
+static int smooth_current_async(ap_ctx *c, uint32_t step) {
+  int bnd[4] = {!c->params.periodic[0], !c->params.periodic[0], !c->params.periodic[1],
+                !c->params.periodic[1]};
+  const bool out = ((step + 1) % (uint32_t)c->params.data_interval) == 0;
+  for (int it = 0; it < c->params.current_smoothing; ++it) {
+    for (int k = 0; k < 3; ++k) AP_TRY(launch_filter(*c, c->fields.J[k], bnd));
+    for (int k = 0; k < 3; ++k) AP_TRY(launch_copy_guards(*c, c->fields.J[k]));
+    if (out)
+      for (int s = 0; s < c->params.num_species; ++s) {
+        AP_TRY(launch_filter(*c, c->fields.Rho[s], bnd));
+        AP_TRY(launch_copy_guards(*c, c->fields.Rho[s]));
+      }
+  }
+  return AP_OK;
+}
+
+AP_API int ap_smooth_current(ap_ctx *c, uint32_t step) {
+  if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  AP_TRY_ST(smooth_current_async(c, step));
+  return finish(c);
+}
+
+AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
+  if (!c || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  const ap_params &pr = c->params;
+  const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
+  // data.J.initialize(); data.Rho[i].initialize() (ptc_updater.cu:752-755):
+  // the FP64 accumulators start at zero; J (and Rho on output steps) are
+  // overwritten by the finalize pass, Rho is zeroed on other steps.
+  const int ncomp = 3 + (do_rho ? pr.num_species : 0);
+  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(double) * c->acc_comp * ncomp, c->stream));
+  if (!do_rho)
+    for (int s = 0; s < pr.num_species; ++s) AP_TRY(launch_zero(*c, c->fields.Rho[s]));
+  AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+
+  if (c->number > 0) {
+    PushDepositParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.m = c->mk;
+    P.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
+               c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
+    const ap_array *fa[6] = {&c->fields.E[0], &c->fields.E[1], &c->fields.E[2],
+                             &c->fields.B[0], &c->fields.B[1], &c->fields.B[2]};
+    for (int k = 0; k < 6; ++k) P.F[k] = FieldArr{fa[k]->ptr, (int)(fa[k]->pitch / 4)};
+    for (int k = 0; k < 3; ++k)
+      P.J[k] = FieldArr{c->fields.J[k].ptr, (int)(c->fields.J[k].pitch / 4)};
+    for (int s = 0; s < pr.num_species; ++s)
+      P.Rho[s] = FieldArr{c->fields.Rho[s].ptr, (int)(c->fields.Rho[s].pitch / 4)};
+    P.acc = c->acc;
+    P.acc_pitch = c->mesh.dims[0];
+    P.acc_comp = c->acc_comp;
+    // The kernel receives dt as float (Scalar dt); q_over_m is evaluated as
+    // dt * 0.5f * q / m (ptc_updater.cu:42, 101).
+    const float dtf = (float)dt;
+    P.dt = dtf;
+    for (int s = 0; s < AP_MAX_SPECIES; ++s) {
+      volatile float a = dtf * 0.5f;
+      volatile float b = a * pr.charges[s];
+      P.qm[s] = pr.masses[s] != 0.0f ? b / pr.masses[s] : 0.0f;
+      P.charge[s] = pr.charges[s];
+    }
+    P.num_species = pr.num_species;
+    P.do_rho = do_rho ? 1 : 0;
+    for (int d = 0; d < 3; ++d) P.periodic[d] = pr.periodic[d];
+    P.status = c->status;
+    P.number = c->number;
+    if (c->mk.dim == 1) {
+      AP_TRY(launch_push_deposit_1d(*c, P));
+    } else {
+      if (!c->order_valid) AP_TRY(rebuild_tile_order(*c));
+      P.t = c->tiles;
+      P.order = c->order[c->cur];
+      P.tile_start = c->tile_start[c->cur];
+      P.dir = c->dir;
+      P.dir_count = c->dir_count;
+      P.queue = c->queue;
+      AP_TRY(launch_push_deposit_2d(*c, P));
+      if (incremental_order(*c)) {
+        const int nxt = c->cur ^ 1;
+        AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
+        AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur], c->order[c->cur], c->dir,
+                                    c->grp_off, c->order[nxt]));
+        c->cur = nxt;
+      } else {
+        c->order_valid = false;
+      }
+    }
+  }
+  // send_add_guard_cells(J), and Rho on output steps (ptc_updater.cu:800-805),
+  // fused with the FP64 -> FP32 rounding
+  AP_TRY(launch_finalize_current(*c, ncomp));
+  AP_TRY_ST(smooth_current_async(c, step));
+  if (!c->sync) return AP_OK;
+  return check_status(c);
+}
+
+AP_API int ap_update_e_field(ap_ctx *c, double dt) {
+  if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  AP_TRY(launch_update_e(*c, (float)dt));
+  return finish(c);
+}
+
+AP_API int ap_update_b_field(ap_ctx *c, double dt) {
+  if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  AP_TRY(launch_update_b(*c, (float)dt));
+  return finish(c);
+}
+
+AP_API int ap_compute_divs(ap_ctx *c) {
+  if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  AP_TRY(launch_divs(*c));
+  return finish(c);
+}
+
+AP_API int ap_update_fields(ap_ctx *c, double dt, uint32_t step) {
+  if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  // field_solver::update_fields (field_solver.cu:334-358)
+  if (step == 0) AP_TRY(launch_update_e(*c, (float)(0.5 * dt)));
+  AP_TRY(launch_update_b(*c, (float)dt));
+  AP_TRY(launch_update_e(*c, (float)dt));
+  AP_TRY(launch_divs(*c));
+  return finish(c);
+}
+
+AP_API int ap_send_guard_cells(ap_ctx *c, ap_array a) {
+  if (!c || !valid_array(a, c->mesh)) return AP_ERR_INVALID;
+  AP_TRY(launch_copy_guards(*c, a));
+  return finish(c);
+}
+
+AP_API int ap_send_add_guard_cells(ap_ctx *c, ap_array a) {
+  if (!c || !valid_array(a, c->mesh)) return AP_ERR_INVALID;
+  AP_TRY(launch_fold_guards(*c, a));
+  return finish(c);
+}
+
+AP_API int ap_sort_by_cell(ap_ctx *c) {
+  if (!c || !c->ptc_bound) return AP_ERR_INVALID;
+  size_t n = 0;
+  AP_TRY(sort_by_cell(*c, &n));
+  c->number = n;
+  c->order_valid = false;
+  return AP_OK;
+}
+
+AP_API int ap_get_tile_order(ap_ctx *c, const uint32_t **order, const uint32_t **tile_start,
+                             uint32_t *ntiles, size_t *live) {
+  if (!c || !c->ptc_bound || c->mk.dim != 2) return AP_ERR_INVALID;
+  if (!c->order_valid) AP_TRY(rebuild_tile_order(*c));
+  uint32_t n = 0;
+  AP_TRY(cudaMemcpyAsync(&n, c->tile_start[c->cur] + c->tiles.ntiles, sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, c->stream));
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  if (order) *order = c->order[c->cur];
+  if (tile_start) *tile_start = c->tile_start[c->cur];
+  if (ntiles) *ntiles = (uint32_t)c->tiles.ntiles;
+  if (live) *live = n;
+  return AP_OK;
+}
+
+AP_API int ap_get_stats(ap_ctx *c, ap_step_stats *s) {
+  if (!c || !s) return AP_ERR_INVALID;
+  AP_TRY(cudaMemcpyAsync(c->status_host, c->status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                         c->stream));
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  s->nan_momenta = c->status_host->nan_momenta;
+  s->moved_far = c->status_host->moved_far;
+  s->lost = c->status_host->lost;
+  s->tile_faults = c->status_host->tile_faults;
+  s->live = 0;
+  if (c->mk.dim == 2 && c->order_valid) {
+    uint32_t n = 0;
+    AP_TRY(cudaMemcpy(&n, c->tile_start[c->cur] + c->tiles.ntiles, sizeof(uint32_t),
+                      cudaMemcpyDeviceToHost));
+    s->live = n;
+  }
+  return AP_OK;
+}
+
+AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
+  if (!c || !out || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  AP_TRY(launch_diagnostics(*c, c->diag_dev));
+  AP_TRY(cudaMemcpyAsync(c->diag_host, c->diag_dev, sizeof(double) * 6, cudaMemcpyDeviceToHost,
+                         c->stream));
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  out->kinetic = c->diag_host[0];
+  out->charge = c->diag_host[1];
+  out->field_energy = c->diag_host[2];
+  out->max_abs_rho = c->diag_host[3];
+  out->gauss_residual = c->diag_host[4];
+  out->max_abs_j = c->diag_host[5];
+  return AP_OK;
+}
+
+AP_API int ap_last_error(const ap_ctx *c) { return c ? c->last_error : AP_ERR_INVALID; }
+
+AP_API uint64_t ap_launch_count(const ap_ctx *c) { return c ? c->launches : 0; }
+
+}  // extern "C"

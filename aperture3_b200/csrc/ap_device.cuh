@@ -1,0 +1,113 @@
+// Device-side arithmetic of the particle update.
+//
+// Every expression keeps the operation order of the reference kernels and
+// the library is compiled with -fmad=false and IEEE division / square root,
+// so each FP32 result is the correctly rounded value of the same sequence
+// of operations the reference writes down: momenta, positions and cell
+// indices match an FP32 CPU evaluation of the reference bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace apb {
+
+// ParticleFlag bits (src/core/enum_types.h:76-87); species in the top three
+// bits of the flag (src/utils/util_functions.h:66-69).
+constexpr uint32_t kFlagIgnoreCurrent = 1u << 3;
+constexpr uint32_t kFlagIgnoreEM = 1u << 4;
+__device__ __forceinline__ int ptc_type(uint32_t flag) { return (int)(flag >> 29); }
+
+// spline_t<1> (src/cuda/utils/interpolation.cuh:28-37): max(1 - |dx|, 0).
+__device__ __forceinline__ float cic(float dx) {
+  float w = 1.0f - fabsf(dx);
+  return w > 0.0f ? w : 0.0f;
+}
+
+// Interpolation weights of one dimension for a particle at cell c with
+// offset rel (interp_cell, interpolation.cuh:79-87). The reference visits
+// the three nodes c-1, c, c+1; for an offset in [0, 1] at most two of them
+// carry a nonzero weight, and which two is decided exactly:
+//  - stagger 1 (node at t + 1): nodes c-1 and c; node c+1 sits at distance
+//    (c + 2) - (c + rel) >= 1.
+//  - stagger 0 (node at t + 0.5): nodes c-1, c when c + rel < c + 0.5,
+//    otherwise c, c+1; the skipped node is at distance >= 1.
+// Skipping a node whose weight is exactly zero leaves the accumulated sum
+// bit-identical (the running sum starts at +0 and x + (+-0) == x).
+struct Weights1D {
+  int base0;       // first node for stagger 0 (c-1 or c)
+  float w0[2];     // stagger-0 weights of nodes base0, base0 + 1
+  float w1[2];     // stagger-1 weights of nodes c-1, c
+};
+
+__device__ __forceinline__ Weights1D weights_1d(float rel, int c) {
+  Weights1D W;
+  float xc = rel + (float)c;
+  float fc = (float)c;
+  float fcm = (float)(c - 1);
+  W.w1[0] = cic((fcm + 1.0f) - xc);
+  W.w1[1] = cic((fc + 1.0f) - xc);
+  if (xc < fc + 0.5f) {
+    W.base0 = c - 1;
+    W.w0[0] = cic((fcm + 0.5f) - xc);
+    W.w0[1] = cic((fc + 0.5f) - xc);
+  } else {
+    W.base0 = c;
+    W.w0[0] = cic((fc + 0.5f) - xc);
+    W.w0[1] = cic(((float)(c + 1) + 0.5f) - xc);
+  }
+  return W;
+}
+
+// vay_push (src/cuda/algorithms/vay_push.cuh:8-30). E and B are already
+// scaled by q dt / (2 m).
+__device__ __forceinline__ void vay_push(float &p1, float &p2, float &p3, float &gamma,
+                                         float E1, float E2, float E3, float B1,
+                                         float B2, float B3) {
+  float up1 = p1 + 2.0f * E1 + (p2 * B3 - p3 * B2) / gamma;
+  float up2 = p2 + 2.0f * E2 + (p3 * B1 - p1 * B3) / gamma;
+  float up3 = p3 + 2.0f * E3 + (p1 * B2 - p2 * B1) / gamma;
+  float tt = B1 * B1 + B2 * B2 + B3 * B3;
+  float ut = up1 * B1 + up2 * B2 + up3 * B3;
+  float sigma = 1.0f + up1 * up1 + up2 * up2 + up3 * up3 - tt;
+  float inv_gamma2 = 2.0f / (sigma + sqrtf(sigma * sigma + 4.0f * (tt + ut * ut)));
+  float s = 1.0f / (1.0f + inv_gamma2 * tt);
+  gamma = 1.0f / sqrtf(inv_gamma2);
+  p1 = (up1 + B1 * ut * inv_gamma2 + (up2 * B3 - up3 * B2) / gamma) * s;
+  p2 = (up2 + B2 * ut * inv_gamma2 + (up3 * B1 - up1 * B3) / gamma) * s;
+  p3 = (up3 + B3 * ut * inv_gamma2 + (up1 * B2 - up2 * B1) / gamma) * s;
+}
+
+// movement2d / center2d (src/cuda/algorithms/ptc_updater_helper.cuh:26-41).
+__device__ __forceinline__ float movement2d(float sx0, float sx1, float sy0, float sy1) {
+  return (sy1 - sy0) * 0.5f * (sx0 + sx1);
+}
+__device__ __forceinline__ float center2d(float sx0, float sx1, float sy0, float sy1) {
+  return (2.0f * sx1 * sy1 + sx0 * sy1 + sx1 * sy0 + 2.0f * sx0 * sy0) * 0.1666667f;
+}
+
+// Staggers of E1..B3 (ptc_updater.cu:55-60): bit 0 = x stagger, bit 1 = y.
+// E1 0b110, E2 0b101, E3 0b011, B1 0b001, B2 0b010, B3 0b100.
+__host__ __device__ constexpr int stag_x(int k) {
+  return (k == 0) ? 0 : (k == 1) ? 1 : (k == 2) ? 1 : (k == 3) ? 1 : (k == 4) ? 0 : 0;
+}
+__host__ __device__ constexpr int stag_y(int k) {
+  return (k == 0) ? 1 : (k == 1) ? 0 : (k == 2) ? 1 : (k == 3) ? 0 : (k == 4) ? 1 : 0;
+}
+
+// Zone-based wrap of one coordinate after a move of at most one cell
+// (find_zone, quadmesh.h:264-273; cell shift of copy_component_to_buffer,
+// kernels.cu:134-142). Returns false when the particle leaves through a
+// non-periodic side.
+__device__ __forceinline__ bool wrap_coord(int &c, int g, int n, int red, int periodic) {
+  if (c < g) {
+    if (!periodic) return false;
+    c += red;
+  } else if (c >= n - g) {
+    if (!periodic) return false;
+    c -= red;
+  }
+  return true;
+}
+
+}  // namespace apb

@@ -1,0 +1,166 @@
+// Internal declarations shared by the CUDA translation units of
+// libaperture_b200.so. Nothing here is part of the public ABI.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/aperture_b200.h"
+
+namespace apb {
+
+// Status-word bits written by kernels (device side, atomicOr) and counters
+// (atomicAdd) in DevStatus.
+struct DevStatus {
+  unsigned long long nan_momenta;
+  unsigned long long moved_far;
+  unsigned long long lost;
+  unsigned long long tile_faults;
+  unsigned long long timeouts;
+};
+
+// Grid constants a kernel needs (a copy of the host ap_mesh, in the
+// forms the kernels use).
+struct MeshK {
+  int dims[3];
+  int guard[3];
+  int red[3];
+  float delta[3];
+  float inv_delta[3];
+  int dim;
+};
+
+struct PtcK {
+  float *x1, *x2, *x3, *p1, *p2, *p3, *E, *w;
+  uint32_t *cell;
+  uint32_t *flag;
+};
+
+struct FieldArr {
+  float *ptr;
+  int pitch;  // in floats
+};
+
+// Six tensor maps for the E/B tiles (E1, E2, E3, B1, B2, B3).
+struct alignas(64) FieldMaps {
+  CUtensorMap m[6];
+};
+
+// Tile geometry of the 2D sort.
+struct TilesK {
+  int tx, ty;    // tile size in cells
+  int ntx, nty;  // tiles per dim
+  int ntiles;
+};
+
+struct PushDepositParams {
+  MeshK m;
+  PtcK p;
+  FieldArr F[6];     // E1..E3, B1..B3 (used when tensor maps are off)
+  FieldArr J[3];
+  FieldArr Rho[AP_MAX_SPECIES];
+  // FP64 accumulators of J1..J3 then Rho[0..num_species): component k at
+  // acc + k * acc_comp, row-major with row length acc_pitch.
+  double *acc;
+  int acc_pitch;
+  size_t acc_comp;
+  float dt;
+  float qm[AP_MAX_SPECIES];      // dt * 0.5f * q / m, evaluated as the reference does
+  float charge[AP_MAX_SPECIES];
+  int num_species;
+  int do_rho;
+  int periodic[3];
+  // 2D tile order
+  TilesK t;
+  const uint32_t *order;
+  const uint32_t *tile_start;
+  uint8_t *dir;
+  uint32_t *dir_count;   // ntiles * 10
+  uint32_t *queue;
+  DevStatus *status;
+  size_t number;         // 1D: particle slots
+};
+
+// Per-context state.
+struct Ctx {
+  int device = 0;
+  ap_mesh mesh{};
+  ap_params params{};
+  MeshK mk{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool sync = true;
+  int last_error = AP_OK;
+  uint64_t launches = 0;
+  int num_sms = 148;
+
+  bool fields_bound = false;
+  ap_fields fields{};
+  bool use_tma = false;
+  FieldMaps maps{};
+
+  bool ptc_bound = false;
+  ap_particles ptc{};
+  size_t number = 0;
+  size_t capacity = 0;
+
+  // 2D tile order (ping-pong)
+  TilesK tiles{};
+  uint32_t *order[2] = {nullptr, nullptr};
+  uint32_t *tile_start[2] = {nullptr, nullptr};
+  int cur = 0;
+  bool order_valid = false;
+  uint8_t *dir = nullptr;
+  uint32_t *dir_count = nullptr;
+  uint32_t *grp_off = nullptr;
+  uint32_t *queue = nullptr;
+  size_t order_cap = 0;
+
+  // rebuild / sort scratch
+  uint32_t *keys[2] = {nullptr, nullptr};
+  uint32_t *vals[2] = {nullptr, nullptr};
+  void *cub_tmp = nullptr;
+  size_t cub_tmp_bytes = 0;
+  void *gather_tmp = nullptr;
+  size_t scratch_cap = 0;
+
+  // FP64 current / charge accumulators (3 + num_species components)
+  double *acc = nullptr;
+  size_t acc_comp = 0;
+
+  // filter scratch
+  float *tmp_j = nullptr;
+  int tmp_pitch = 0;
+
+  DevStatus *status = nullptr;     // device
+  DevStatus *status_host = nullptr;  // pinned
+  double *diag_dev = nullptr;
+  double *diag_host = nullptr;
+};
+
+// --- launchers (defined in the .cu files) ---
+cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P);
+cudaError_t launch_push_deposit_1d(Ctx &c, const PushDepositParams &P);
+cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count,
+                             uint32_t *new_start, uint32_t *grp_off);
+cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start,
+                                 const uint32_t *old_order, const uint8_t *dir,
+                                 const uint32_t *grp_off, uint32_t *new_order);
+cudaError_t rebuild_tile_order(Ctx &c);
+cudaError_t sort_by_cell(Ctx &c, size_t *new_number);
+
+cudaError_t launch_fold_guards(Ctx &c, ap_array a);
+cudaError_t launch_copy_guards(Ctx &c, ap_array a);
+cudaError_t launch_update_e(Ctx &c, float dt);
+cudaError_t launch_update_b(Ctx &c, float dt);
+cudaError_t launch_divs(Ctx &c);
+cudaError_t launch_filter(Ctx &c, ap_array a, int bnd[4]);
+cudaError_t launch_zero(Ctx &c, ap_array a);
+cudaError_t launch_finalize_current(Ctx &c, int ncomp);
+cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
+
+MeshK make_meshk(const ap_mesh &m);
+int ensure_scratch(Ctx &c, size_t n);
+
+}  // namespace apb

@@ -1,0 +1,155 @@
+// FP64 diagnostics of the particle update, reduced on the device.
+// The reference has only per-particle gamma (cuda/core/particles.cu:10-22)
+// and EdotB averages; these reductions are new. Values are accumulated in
+// double in registers, per block in shared memory, and across blocks with
+// double atomics; maxima of non-negative doubles use the integer order of
+// their bit patterns.
+#include <cuda_runtime.h>
+
+#include "ap_device.cuh"
+#include "ap_internal.h"
+
+namespace apb {
+
+namespace {
+
+constexpr int kDiagThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+  return r;
+}
+
+__device__ __forceinline__ double block_max(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sh[w]);
+  return r;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long *>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+
+struct DiagParams {
+  PtcK p;
+  size_t number;
+  double mass[AP_MAX_SPECIES];
+  double charge[AP_MAX_SPECIES];
+  int n0, n1, g0, g1, dim, num_species;
+  double cell_volume;
+  FieldArr E[3], B[3], J[3], Rho[AP_MAX_SPECIES], divE;
+  double *out;  // kinetic, charge, field energy, max|rho|, max|divE - rho|, max|J|
+};
+
+__global__ void __launch_bounds__(kDiagThreads) k_diag_particles(const DiagParams P) {
+  __shared__ double sh[kDiagThreads / 32];
+  double kin = 0.0, q = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P.number;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (P.p.cell[i] == AP_MAX_CELL) continue;
+    const int sp = ptc_type(P.p.flag[i]);
+    const double p1 = P.p.p1[i], p2 = P.p.p2[i], p3 = P.p.p3[i];
+    const double pp = p1 * p1 + p2 * p2 + p3 * p3;
+    const double gm1 = pp / (sqrt(1.0 + pp) + 1.0);  // gamma - 1 without cancellation
+    const double w = P.p.w[i];
+    kin += w * P.mass[sp] * gm1;
+    q += w * P.charge[sp];
+  }
+  const double sk = block_sum(kin, sh);
+  const double sq = block_sum(q, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(P.out + 0, sk);
+    atomicAdd(P.out + 1, sq);
+  }
+}
+
+__global__ void __launch_bounds__(kDiagThreads) k_diag_fields(const DiagParams P) {
+  __shared__ double sh[kDiagThreads / 32];
+  const int r0 = P.n0 - 2 * P.g0;
+  const int r1 = P.dim > 1 ? P.n1 - 2 * P.g1 : 1;
+  const int g1 = P.dim > 1 ? P.g1 : 0;
+  const size_t total = (size_t)r0 * r1;
+  double en = 0.0, mrho = 0.0, mres = 0.0, mj = 0.0;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = P.g0 + (int)(t % r0), j = g1 + (int)(t / r0);
+    double s = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double e = P.E[k].ptr[(size_t)j * P.E[k].pitch + i];
+      const double b = P.B[k].ptr[(size_t)j * P.B[k].pitch + i];
+      s += e * e + b * b;
+      mj = fmax(mj, fabs((double)P.J[k].ptr[(size_t)j * P.J[k].pitch + i]));
+    }
+    en += 0.5 * s * P.cell_volume;
+    double rho = 0.0;
+    for (int sp = 0; sp < P.num_species; ++sp)
+      rho += P.Rho[sp].ptr[(size_t)j * P.Rho[sp].pitch + i];
+    mrho = fmax(mrho, fabs(rho));
+    if (P.divE.ptr) mres = fmax(mres, fabs((double)P.divE.ptr[(size_t)j * P.divE.pitch + i] - rho));
+  }
+  const double se = block_sum(en, sh);
+  const double a = block_max(mrho, sh);
+  const double b = block_max(mres, sh);
+  const double cj = block_max(mj, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(P.out + 2, se);
+    atomic_max_nonneg(P.out + 3, a);
+    atomic_max_nonneg(P.out + 4, b);
+    atomic_max_nonneg(P.out + 5, cj);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_diagnostics(Ctx &c, double *out) {
+  DiagParams P;
+  P.p = PtcK{c.ptc.x1, c.ptc.x2, c.ptc.x3, c.ptc.p1, c.ptc.p2,
+             c.ptc.p3, c.ptc.E,  c.ptc.weight, c.ptc.cell, c.ptc.flag};
+  P.number = c.number;
+  for (int s = 0; s < AP_MAX_SPECIES; ++s) {
+    P.mass[s] = c.params.masses[s];
+    P.charge[s] = c.params.charges[s];
+  }
+  P.n0 = c.mesh.dims[0];
+  P.n1 = c.mesh.dims[1];
+  P.g0 = c.mesh.guard[0];
+  P.g1 = c.mesh.guard[1];
+  P.dim = c.mk.dim;
+  P.num_species = c.params.num_species;
+  P.cell_volume = (double)c.mesh.delta[0] * (c.mk.dim > 1 ? (double)c.mesh.delta[1] : 1.0);
+  auto fa = [](const ap_array &a) { return FieldArr{a.ptr, (int)(a.pitch / 4)}; };
+  for (int k = 0; k < 3; ++k) {
+    P.E[k] = fa(c.fields.E[k]);
+    P.B[k] = fa(c.fields.B[k]);
+    P.J[k] = fa(c.fields.J[k]);
+  }
+  for (int s = 0; s < c.params.num_species; ++s) P.Rho[s] = fa(c.fields.Rho[s]);
+  P.divE = c.fields.divE.ptr ? fa(c.fields.divE) : FieldArr{nullptr, 0};
+  P.out = out;
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * 6, c.stream);
+  if (e != cudaSuccess) return e;
+  int grid = c.num_sms * 4;
+  if (c.number > 0) {
+    k_diag_particles<<<grid, kDiagThreads, 0, c.stream>>>(P);
+    c.launches++;
+  }
+  k_diag_fields<<<grid, kDiagThreads, 0, c.stream>>>(P);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace apb

@@ -1,0 +1,539 @@
+// Fused Vay push + Esirkepov deposition + move for Cartesian 1D and 2D.
+//
+// Replaces Kernels::ptc_push_cart_{1,2}d and deposit_current_cart_{1,2}d
+// (src/cuda/algorithms/ptc_updater.cu:21-141, 220-386), which the
+// reference runs as two grid-stride launches with global float atomics.
+//
+// 2D design: the particles are kept in a stable tile order (one list of
+// slot indices per tile of TX x TY cells, maintained by a counting sort each
+// step). A persistent CTA takes tiles from a queue; for each tile it
+//   1. stages the E/B tile plus a one-cell halo into shared memory with six
+//      TMA 2D tiled loads (no multicast) completing on an mbarrier,
+//   2. zeroes a shared-memory J (and Rho) tile with a two-cell halo,
+//   3. pushes and deposits its particles, one particle per thread, reading
+//      fields from shared memory and adding current with shared FP64
+//      atomics (each contribution is the reference's FP32 value),
+//   4. flushes the J tile once into the FP64 accumulators in global memory
+//      (red.global.add.f64); a finalize pass folds the periodic guards and
+//      rounds each cell once to FP32, and
+//   5. records, per particle, the direction of its new tile (0..8, 9 = gone)
+//      plus per-direction counts, which the order update consumes.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "ap_device.cuh"
+#include "ap_internal.h"
+
+namespace apb {
+
+namespace {
+
+constexpr int kThreads2D = 256;
+constexpr uint32_t kDirGone = 9;
+constexpr uint32_t kMbarSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// Bounded wait on an mbarrier phase; returns false when the limit is hit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < kMbarSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(float *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int TX, int TY>
+struct TileGeom {
+  static constexpr int BX = TX + 8;   // field box width: x start rounded down to 4 floats
+  static constexpr int BY = TY + 2;   // one halo row on each side
+  static constexpr int FSZ = ((BX * BY + 31) / 32) * 32;  // 128-byte aligned stride
+  static constexpr int JX = TX + 4;   // J tile: two halo cells on each side
+  static constexpr int JY = TY + 4;
+  static constexpr int JSZ = JX * JY;
+  static constexpr int HDR = 128;     // mbarrier, tile id, abort flag, counters
+  static size_t smem_bytes(int nrho) {
+    return HDR + sizeof(float) * 6 * FSZ + sizeof(double) * (3 + nrho) * JSZ;
+  }
+};
+
+template <int TX, int TY, bool kTMA, bool kRho>
+__global__ void __launch_bounds__(kThreads2D)
+    k_push_deposit_2d(const __grid_constant__ PushDepositParams P,
+                      const __grid_constant__ FieldMaps maps) {
+  using G = TileGeom<TX, TY>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
+  int *s_tile = reinterpret_cast<int *>(smem + 8);
+  int *s_abort = reinterpret_cast<int *>(smem + 12);
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(smem + 16);
+  float *sF = reinterpret_cast<float *>(smem + G::HDR);
+  double *sJ = reinterpret_cast<double *>(sF + 6 * G::FSZ);
+  double *sR = sJ + 3 * G::JSZ;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
+  const int g0 = P.m.guard[0], g1 = P.m.guard[1];
+  const int nzero = (3 + (kRho ? P.num_species : 0)) * G::JSZ;
+
+  if (tid == 0) {
+    if (kTMA) mbar_init(mbar, 1);
+    *s_abort = 0;
+  }
+  __syncthreads();
+
+  uint32_t phase = 0;
+  for (;;) {
+    if (tid == 0) *s_tile = (int)atomicAdd(P.queue, 1u);
+    if (tid < 10) s_cnt[tid] = 0;
+    __syncthreads();
+    const int t = *s_tile;
+    if (t >= P.t.ntiles) break;
+    const int tix = t % P.t.ntx, tiy = t / P.t.ntx;
+    const int x0 = g0 + tix * TX, y0 = g1 + tiy * TY;
+    const int xs = (x0 - 1) & ~3, ys = y0 - 1;
+    const int jx0 = x0 - 2, jy0 = y0 - 2;
+
+    // 1. field tile
+    if (kTMA) {
+      if (tid == 0) {
+        fence_proxy_async_smem();
+        mbar_expect_tx(mbar, 6u * G::BX * G::BY * 4u);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tma_load_2d(sF + k * G::FSZ, &maps.m[k], xs, ys, mbar);
+      }
+    } else {
+      for (int i = tid; i < 6 * G::BX * G::BY; i += blockDim.x) {
+        int k = i / (G::BX * G::BY), rem = i % (G::BX * G::BY);
+        int yy = ys + rem / G::BX, xx = xs + rem % G::BX;
+        float v = 0.0f;
+        if (xx < dims0 && yy < dims1) v = P.F[k].ptr[(size_t)yy * P.F[k].pitch + xx];
+        sF[k * G::FSZ + rem] = v;
+      }
+    }
+    // 2. zero the current (and charge) tile
+    for (int i = tid; i < nzero; i += blockDim.x) sJ[i] = 0.0;
+    if (kTMA) {
+      if (!mbar_wait(mbar, phase)) atomicExch(s_abort, 1);
+    }
+    __syncthreads();
+    if (*s_abort) {
+      if (tid == 0) {
+        atomicAdd(&P.status->timeouts, 1ull);
+        mbar_wait(mbar, phase);  // give copies in flight one more bounded wait
+      }
+      break;
+    }
+
+    // 3. particles of this tile
+    const uint32_t base = P.tile_start[t];
+    const int n_t = (int)(P.tile_start[t + 1] - base);
+    for (int r = tid; r < n_t; r += blockDim.x) {
+      const uint32_t pos = base + (uint32_t)r;
+      const uint32_t idx = __ldg(P.order + pos);
+      const uint32_t c = __ldcs(P.p.cell + idx);
+      const uint32_t flag = __ldcs(P.p.flag + idx);
+      float x1 = __ldcs(P.p.x1 + idx), x2 = __ldcs(P.p.x2 + idx), x3 = __ldcs(P.p.x3 + idx);
+      float p1 = __ldcs(P.p.p1 + idx), p2 = __ldcs(P.p.p2 + idx), p3 = __ldcs(P.p.p3 + idx);
+      const float w = __ldcs(P.p.w + idx);
+      const int c1 = (int)(c % (uint32_t)dims0);
+      const int c2 = (int)(c / (uint32_t)dims0);
+      uint32_t dir = 4;
+      const bool in_tile = (c != AP_MAX_CELL) && c1 >= x0 && c1 < x0 + TX && c2 >= y0 &&
+                           c2 < y0 + TY;
+      if (!in_tile) {
+        atomicAdd(&P.status->tile_faults, 1ull);
+        dir = kDirGone;
+      } else if (p1 != p1 || p2 != p2 || p3 != p3) {
+        // The reference traps here (ptc_updater.cu:102-109); the particle is
+        // left untouched and reported instead.
+        atomicAdd(&P.status->nan_momenta, 1ull);
+      } else {
+        const int sp = ptc_type(flag);
+        float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
+        const bool em = !(flag & kFlagIgnoreEM);
+        if (em) {
+          const float qm = P.qm[sp];
+          const Weights1D Wx = weights_1d(x1, c1);
+          const Weights1D Wy = weights_1d(x2, c2);
+          float fe[6];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const float *f = sF + k * G::FSZ;
+            const int ib = (stag_x(k) ? c1 - 1 : Wx.base0) - xs;
+            const int jb = (stag_y(k) ? c2 - 1 : Wy.base0) - ys;
+            const float wx0 = stag_x(k) ? Wx.w1[0] : Wx.w0[0];
+            const float wx1 = stag_x(k) ? Wx.w1[1] : Wx.w0[1];
+            const float wy0 = stag_y(k) ? Wy.w1[0] : Wy.w0[0];
+            const float wy1 = stag_y(k) ? Wy.w1[1] : Wy.w0[1];
+            const float *row0 = f + jb * G::BX + ib;
+            const float *row1 = row0 + G::BX;
+            float acc = 0.0f;
+            acc += row0[0] * wx0 * wy0;
+            acc += row0[1] * wx1 * wy0;
+            acc += row1[0] * wx0 * wy1;
+            acc += row1[1] * wx1 * wy1;
+            fe[k] = acc * qm;
+          }
+          vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
+        } else {
+          gamma = P.p.E[idx];  // the deposit reads the stored gamma
+        }
+        // deposit_current_cart_2d (ptc_updater.cu:295-386)
+        const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
+        float nx1 = x1 + (v1 * P.dt) * P.m.inv_delta[0];
+        float nx2 = x2 + (v2 * P.dt) * P.m.inv_delta[1];
+        const int dc1 = (int)floorf(nx1);
+        const int dc2 = (int)floorf(nx2);
+        nx1 -= (float)dc1;
+        nx2 -= (float)dc2;
+        const float nx3 = x3 + v3 * P.dt;
+        const bool far = dc1 > 1 || dc1 < -1 || dc2 > 1 || dc2 < -1;
+
+        if (!far && !(flag & kFlagIgnoreCurrent)) {
+          const float weight = -P.charge[sp] * w;
+          const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
+          const int j0 = (dc2 == -1 ? -2 : -1), j1 = (dc2 == 1 ? 1 : 0);
+          float sx0[4], sx1[4];
+#pragma unroll
+          for (int i = -2; i <= 1; ++i) {
+            sx0[i + 2] = cic(-x1 + i + 1);
+            sx1[i + 2] = cic(-nx1 + (i + 1 - dc1));
+          }
+          float djy[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+          double *sJ1 = sJ, *sJ2 = sJ + G::JSZ, *sJ3 = sJ + 2 * G::JSZ;
+          double *sRho = sR + sp * G::JSZ;
+#pragma unroll
+          for (int j = -2; j <= 1; ++j) {
+            if (j < j0 || j > j1) continue;
+            const float sy0 = cic(-x2 + j + 1);
+            const float sy1 = cic(-nx2 + (j + 1 - dc2));
+            const int row = (c2 + j - jy0) * G::JX;
+            float djx = 0.0f;
+#pragma unroll
+            for (int i = -2; i <= 1; ++i) {
+              if (i < i0 || i > i1) continue;
+              const int o = row + (c1 + i - jx0);
+              djx += movement2d(sy0, sy1, sx0[i + 2], sx1[i + 2]);
+              atomicAdd(sJ1 + o + 1, (double)(weight * djx));
+              djy[i + 2] += movement2d(sx0[i + 2], sx1[i + 2], sy0, sy1);
+              atomicAdd(sJ2 + o + G::JX, (double)(weight * djy[i + 2]));
+              const float val2 = center2d(sx0[i + 2], sx1[i + 2], sy0, sy1);
+              atomicAdd(sJ3 + o, (double)(-weight * v3 * val2));
+              if (kRho && sp < P.num_species) {
+                const float s1 = sx1[i + 2] * sy1;
+                atomicAdd(sRho + o, (double)(-weight * s1));
+              }
+            }
+          }
+        }
+        // move + wrap through periodic sides (send_particles semantics)
+        int c1n = c1 + dc1, c2n = c2 + dc2;
+        bool keep = !far;
+        keep = keep && wrap_coord(c1n, g0, dims0, P.m.red[0], P.periodic[0]);
+        keep = keep && wrap_coord(c2n, g1, dims1, P.m.red[1], P.periodic[1]);
+        uint32_t ncell = AP_MAX_CELL;
+        if (keep) {
+          ncell = (uint32_t)(c1n + c2n * dims0);
+          int dtx = (c1n - g0) / TX - tix;
+          int dty = (c2n - g1) / TY - tiy;
+          if (dtx > 1) dtx = -1;
+          if (dtx < -1) dtx = 1;
+          if (dty > 1) dty = -1;
+          if (dty < -1) dty = 1;
+          dir = (uint32_t)((dty + 1) * 3 + (dtx + 1));
+        } else {
+          dir = kDirGone;
+          if (far)
+            atomicAdd(&P.status->moved_far, 1ull);
+          else
+            atomicAdd(&P.status->lost, 1ull);
+        }
+        __stcs(P.p.x1 + idx, nx1);
+        __stcs(P.p.x2 + idx, nx2);
+        __stcs(P.p.x3 + idx, nx3);
+        if (em) {
+          __stcs(P.p.p1 + idx, p1);
+          __stcs(P.p.p2 + idx, p2);
+          __stcs(P.p.p3 + idx, p3);
+          __stcs(P.p.E + idx, gamma);
+        }
+        __stcs(P.p.cell + idx, ncell);
+      }
+      P.dir[pos] = (uint8_t)dir;
+      const unsigned peers = __match_any_sync(__activemask(), dir);
+      if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[dir], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+
+    // 4. flush the current (and charge) tile once
+    for (int i = tid; i < nzero; i += blockDim.x) {
+      const double v = sJ[i];
+      if (v == 0.0) continue;
+      const int comp = i / G::JSZ, rem = i % G::JSZ;
+      const int gx = jx0 + rem % G::JX, gy = jy0 + rem / G::JX;
+      if (gx >= dims0 || gy >= dims1) continue;
+      atomicAdd(P.acc + comp * P.acc_comp + (size_t)gy * P.acc_pitch + gx, v);
+    }
+    if (tid < 10) P.dir_count[t * 10 + tid] = s_cnt[tid];
+    phase ^= 1u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1D: the whole line is small, so each CTA takes a contiguous chunk of
+// particle slots, finds the cell range it touches, and deposits into a
+// shared-memory window over that range (or straight to global memory when
+// the window would not fit). Fields are read through the read-only cache.
+
+constexpr int kThreads1D = 256;
+constexpr int kItems1D = 8;
+constexpr int kChunk1D = kThreads1D * kItems1D;
+constexpr int kWinDoubles1D = 6000;  // shared window, all components
+
+__device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weights1D &W, int c1,
+                                                  int stag) {
+  const int b = stag ? c1 - 1 : W.base0;
+  const float w0 = stag ? W.w1[0] : W.w0[0];
+  const float w1 = stag ? W.w1[1] : W.w0[1];
+  float acc = 0.0f;
+  acc += __ldg(f.ptr + b) * w0;
+  acc += __ldg(f.ptr + b + 1) * w1;
+  return acc;
+}
+
+template <bool kRho>
+__global__ void __launch_bounds__(kThreads1D)
+    k_push_deposit_1d(const __grid_constant__ PushDepositParams P) {
+  __shared__ double sW[kWinDoubles1D];
+  __shared__ int s_lo, s_hi;
+  const int tid = threadIdx.x;
+  const int n0 = P.m.dims[0], g0 = P.m.guard[0];
+  const int ncomp = 3 + (kRho ? P.num_species : 0);
+  const int win_comp = kWinDoubles1D / ncomp;
+  const size_t nchunks = (P.number + kChunk1D - 1) / kChunk1D;
+
+  for (size_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const size_t first = ch * kChunk1D;
+    if (tid == 0) {
+      s_lo = INT_MAX;
+      s_hi = INT_MIN;
+    }
+    __syncthreads();
+    uint32_t cells[kItems1D];
+    int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+    for (int k = 0; k < kItems1D; ++k) {
+      const size_t idx = first + (size_t)k * kThreads1D + tid;
+      cells[k] = idx < P.number ? P.p.cell[idx] : AP_MAX_CELL;
+      if (cells[k] != AP_MAX_CELL) {
+        lo = min(lo, (int)cells[k]);
+        hi = max(hi, (int)cells[k]);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((tid & 31) == 0 && lo <= hi) {
+      atomicMin(&s_lo, lo);
+      atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    const int wlo = s_lo - 2;
+    const int wlen = s_hi - s_lo + 5;
+    const bool use_smem = (s_lo <= s_hi) && wlen <= win_comp;
+    if (use_smem)
+      for (int i = tid; i < ncomp * win_comp; i += kThreads1D) sW[i] = 0.0;
+    __syncthreads();
+
+#pragma unroll 1
+    for (int k = 0; k < kItems1D; ++k) {
+      const size_t idx = first + (size_t)k * kThreads1D + tid;
+      uint32_t c = cells[k];
+      if (c == AP_MAX_CELL) continue;
+      if ((int)c < g0 || (int)c >= n0 - g0) {  // ptc_updater.cu:30-33
+        P.p.cell[idx] = AP_MAX_CELL;
+        continue;
+      }
+      const uint32_t flag = P.p.flag[idx];
+      float x1 = P.p.x1[idx];
+      float p1 = P.p.p1[idx], p2 = P.p.p2[idx], p3 = P.p.p3[idx];
+      if (p1 != p1 || p2 != p2 || p3 != p3) {
+        atomicAdd(&P.status->nan_momenta, 1ull);
+        continue;
+      }
+      const int sp = ptc_type(flag);
+      const int c1 = (int)c;
+      float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
+      const bool em = !(flag & kFlagIgnoreEM);
+      if (em) {
+        // ptc_push_cart_1d (ptc_updater.cu:21-76): only the x stagger bit
+        // matters in 1D.
+        const float qm = P.qm[sp];
+        const Weights1D W = weights_1d(x1, c1);
+        float fe[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) fe[q] = interp_1d_global(P.F[q], W, c1, stag_x(q)) * qm;
+        vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
+        P.p.p1[idx] = p1;
+        P.p.p2[idx] = p2;
+        P.p.p3[idx] = p3;
+        P.p.E[idx] = gamma;
+      } else {
+        gamma = P.p.E[idx];
+      }
+      // deposit_current_cart_1d (ptc_updater.cu:220-293)
+      const float w = P.p.w[idx];
+      const float x2 = P.p.x2[idx], x3 = P.p.x3[idx];
+      const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
+      float nx1 = x1 + (v1 * P.dt) / P.m.delta[0];
+      const int dc1 = (int)floorf(nx1);
+      nx1 -= (float)dc1;
+      const bool far = dc1 > 1 || dc1 < -1;
+      P.p.x1[idx] = nx1;
+      P.p.x2[idx] = x2 + v2 * P.dt;
+      P.p.x3[idx] = x3 + v3 * P.dt;
+      if (!far && !(flag & kFlagIgnoreCurrent)) {
+        const float weight = P.charge[sp] * w;
+        const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
+        float djx = 0.0f;
+#pragma unroll
+        for (int i = -2; i <= 1; ++i) {
+          if (i < i0 || i > i1) continue;
+          const float sx0 = cic(-x1 + i + 1);
+          const float sx1 = cic(-nx1 + (i + 1 - dc1));
+          const int off = i + c1;
+          djx += sx1 - sx0;
+          const float a1 = -weight * djx;
+          const float val1 = 0.5f * (sx0 + sx1);
+          const float a2 = weight * v2 * val1;
+          const float a3 = weight * v3 * val1;
+          if (use_smem) {
+            atomicAdd(&sW[off + 1 - wlo], (double)a1);
+            atomicAdd(&sW[win_comp + off - wlo], (double)a2);
+            atomicAdd(&sW[2 * win_comp + off - wlo], (double)a3);
+            if (kRho && sp < P.num_species)
+              atomicAdd(&sW[(3 + sp) * win_comp + off - wlo], (double)(weight * sx1));
+          } else {
+            atomicAdd(P.acc + off + 1, (double)a1);
+            atomicAdd(P.acc + P.acc_comp + off, (double)a2);
+            atomicAdd(P.acc + 2 * P.acc_comp + off, (double)a3);
+            if (kRho && sp < P.num_species)
+              atomicAdd(P.acc + (3 + sp) * P.acc_comp + off, (double)(weight * sx1));
+          }
+        }
+      }
+      int cn = c1 + dc1;
+      bool keep = !far && wrap_coord(cn, g0, n0, P.m.red[0], P.periodic[0]);
+      if (!keep) atomicAdd(far ? &P.status->moved_far : &P.status->lost, 1ull);
+      P.p.cell[idx] = keep ? (uint32_t)cn : AP_MAX_CELL;
+    }
+    __syncthreads();
+    if (use_smem) {
+      for (int i = tid; i < ncomp * wlen; i += kThreads1D) {
+        const int comp = i / wlen, o = i % wlen;
+        const double v = sW[comp * win_comp + o];
+        if (v == 0.0) continue;
+        const int gx = wlo + o;
+        if (gx < 0 || gx >= n0) continue;
+        atomicAdd(P.acc + comp * P.acc_comp + gx, v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int TX, int TY>
+cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
+  using G = TileGeom<TX, TY>;
+  const int nrho = P.do_rho ? P.num_species : 0;
+  const size_t smem = G::smem_bytes(nrho);
+  cudaError_t e = cudaMemsetAsync(P.queue, 0, sizeof(uint32_t), c.stream);
+  if (e != cudaSuccess) return e;
+  auto run = [&](auto kern) -> cudaError_t {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads2D, smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    int grid = c.num_sms * per_sm;
+    if (grid > P.t.ntiles) grid = P.t.ntiles;
+    if (grid < 1) grid = 1;
+    kern<<<grid, kThreads2D, smem, c.stream>>>(P, c.maps);
+    c.launches++;
+    return cudaGetLastError();
+  };
+  if (c.use_tma) {
+    return P.do_rho ? run(k_push_deposit_2d<TX, TY, true, true>)
+                    : run(k_push_deposit_2d<TX, TY, true, false>);
+  }
+  return P.do_rho ? run(k_push_deposit_2d<TX, TY, false, true>)
+                  : run(k_push_deposit_2d<TX, TY, false, false>);
+}
+
+}  // namespace
+
+cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P) {
+  const int tx = P.t.tx, ty = P.t.ty;
+  if (tx == 16 && ty == 16) return launch_2d_tiles<16, 16>(c, P);
+  if (tx == 32 && ty == 16) return launch_2d_tiles<32, 16>(c, P);
+  if (tx == 32 && ty == 32) return launch_2d_tiles<32, 32>(c, P);
+  if (tx == 8 && ty == 8) return launch_2d_tiles<8, 8>(c, P);
+  if (tx == 16 && ty == 8) return launch_2d_tiles<16, 8>(c, P);
+  if (tx == 4 && ty == 4) return launch_2d_tiles<4, 4>(c, P);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_push_deposit_1d(Ctx &c, const PushDepositParams &P) {
+  size_t nchunks = (P.number + kChunk1D - 1) / kChunk1D;
+  if (nchunks == 0) return cudaSuccess;
+  int grid = (int)(nchunks < (size_t)c.num_sms * 8 ? nchunks : (size_t)c.num_sms * 8);
+  if (P.do_rho)
+    k_push_deposit_1d<true><<<grid, kThreads1D, 0, c.stream>>>(P);
+  else
+    k_push_deposit_1d<false><<<grid, kThreads1D, 0, c.stream>>>(P);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace apb

@@ -1,0 +1,410 @@
+// Particle ordering on the device.
+//
+// Per-step tile counting sort. The push/deposit kernel walks each tile's
+// particles in the current (stable) tile order and records, per particle,
+// the direction d in 0..8 of the tile it moved to (9 = gone) and per-tile
+// direction counts. Because the input is grouped by tile and a particle
+// only moves to one of its tile's eight neighbours, the stable counting
+// sort by new tile reduces to:
+//   k_tile_scan     for each destination tile, sum the counts from its (up
+//                   to nine) source tiles, scan to get tile offsets, and
+//                   give each (source, direction) group its offset, sources
+//                   taken in ascending tile index;
+//   k_order_scatter for each source tile, rank particles within their
+//                   direction group in order and write them to
+//                   group offset + rank.
+// The result equals a stable counting sort of the previous order by the new
+// tile key (core/particle_base_impl.hpp:250-305 applied to tile keys).
+//
+// Full rebuild (after binding or external changes) and sort_by_cell
+// (cuda/core/particle_base_impl.cu:435-487) use a stable LSD radix sort.
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include "ap_device.cuh"
+#include "ap_internal.h"
+
+namespace apb {
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScatterThreads = 256;
+
+struct TileTopo {
+  int ntx, nty, ntiles, per0, per1;
+};
+
+// Source tile of destination (ux, uy) for direction (dx, dy) in -1..1, or
+// -1 when it falls outside a non-periodic edge.
+__device__ __forceinline__ int source_tile(const TileTopo &T, int ux, int uy, int dx, int dy) {
+  int sx = ux - dx, sy = uy - dy;
+  if (sx < 0) {
+    if (!T.per0) return -1;
+    sx += T.ntx;
+  } else if (sx >= T.ntx) {
+    if (!T.per0) return -1;
+    sx -= T.ntx;
+  }
+  if (sy < 0) {
+    if (!T.per1) return -1;
+    sy += T.nty;
+  } else if (sy >= T.nty) {
+    if (!T.per1) return -1;
+    sy -= T.nty;
+  }
+  return sx + sy * T.ntx;
+}
+
+// Gathers the (source tile, direction, count) triples of destination u,
+// sorted by source tile index. Returns how many there are.
+__device__ __forceinline__ int gather_sources(const TileTopo &T, const uint32_t *cnt, int u,
+                                              int src[9], int dirv[9], uint32_t num[9]) {
+  const int ux = u % T.ntx, uy = u / T.ntx;
+  int n = 0;
+  for (int dy = -1; dy <= 1; ++dy)
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int s = source_tile(T, ux, uy, dx, dy);
+      if (s < 0) continue;
+      const int d = (dy + 1) * 3 + (dx + 1);
+      // insertion by source index
+      int k = n++;
+      while (k > 0 && src[k - 1] > s) {
+        src[k] = src[k - 1];
+        dirv[k] = dirv[k - 1];
+        num[k] = num[k - 1];
+        --k;
+      }
+      src[k] = s;
+      dirv[k] = d;
+      num[k] = cnt[s * 10 + d];
+    }
+  return n;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_tile_scan(TileTopo T, const uint32_t *__restrict__ cnt, uint32_t *__restrict__ new_start,
+                uint32_t *__restrict__ grp_off) {
+  __shared__ uint32_t s_part[kScanThreads];
+  const int tid = threadIdx.x;
+  const int per = (T.ntiles + kScanThreads - 1) / kScanThreads;
+  const int u0 = tid * per, u1 = min(T.ntiles, u0 + per);
+  int src[9], dirv[9];
+  uint32_t num[9];
+  uint32_t local = 0;
+  for (int u = u0; u < u1; ++u) {
+    const int n = gather_sources(T, cnt, u, src, dirv, num);
+    for (int k = 0; k < n; ++k) local += num[k];
+  }
+  s_part[tid] = local;
+  __syncthreads();
+  // inclusive Hillis-Steele scan over the per-thread sums
+  for (int off = 1; off < kScanThreads; off <<= 1) {
+    uint32_t v = tid >= off ? s_part[tid - off] : 0u;
+    __syncthreads();
+    s_part[tid] += v;
+    __syncthreads();
+  }
+  uint32_t run = s_part[tid] - local;
+  for (int u = u0; u < u1; ++u) {
+    new_start[u] = run;
+    const int n = gather_sources(T, cnt, u, src, dirv, num);
+    for (int k = 0; k < n; ++k) {
+      grp_off[src[k] * 9 + dirv[k]] = run;
+      run += num[k];
+    }
+  }
+  if (tid == kScanThreads - 1) new_start[T.ntiles] = s_part[tid];
+}
+
+// One CTA per source tile: stable rank within each direction group.
+__global__ void __launch_bounds__(kScatterThreads)
+    k_order_scatter(int ntiles, const uint32_t *__restrict__ old_start,
+                    const uint32_t *__restrict__ old_order, const uint8_t *__restrict__ dir,
+                    const uint32_t *__restrict__ grp_off, uint32_t *__restrict__ new_order,
+                    uint32_t capacity, DevStatus *status) {
+  constexpr int kWarps = kScatterThreads / 32;
+  __shared__ uint32_t s_wcnt[kWarps][10];
+  __shared__ uint32_t s_base[10];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int s = blockIdx.x; s < ntiles; s += gridDim.x) {
+    const uint32_t b = old_start[s], e = old_start[s + 1];
+    if (tid < 10) s_base[tid] = (tid < 9) ? grp_off[s * 9 + tid] : 0u;
+    __syncthreads();
+    for (uint32_t c0 = b; c0 < e; c0 += kScatterThreads) {
+      const uint32_t pos = c0 + tid;
+      const bool valid = pos < e;
+      const uint32_t d = valid ? dir[pos] : 9u;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+      if (tid < kWarps * 10) (&s_wcnt[0][0])[tid] = 0u;
+      __syncthreads();
+      if (lane == __ffs(peers) - 1) s_wcnt[warp][d] = __popc(peers);
+      __syncthreads();
+      uint32_t before = 0;
+      if (valid && d < 9) {
+        for (int w = 0; w < warp; ++w) before += s_wcnt[w][d];
+        const uint32_t dst = s_base[d] + before + rank;
+        if (dst < capacity)
+          new_order[dst] = old_order[pos];
+        else
+          atomicAdd(&status->tile_faults, 1ull);
+      }
+      __syncthreads();
+      if (tid < 9) {
+        uint32_t tot = 0;
+        for (int w = 0; w < kWarps; ++w) tot += s_wcnt[w][tid];
+        s_base[tid] += tot;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Keys for the full rebuild: tile of a bulk cell, ntiles otherwise; cells
+// outside the bulk are emptied as the reference push does (ptc_updater.cu:
+// 87-90).
+__global__ void k_tile_keys(MeshK m, TilesK T, uint32_t *cell, size_t n, uint32_t *keys,
+                            uint32_t *vals) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t c = cell[i];
+    uint32_t key = (uint32_t)T.ntiles;
+    if (c != AP_MAX_CELL) {
+      int c1 = (int)(c % (uint32_t)m.dims[0]);
+      int c2 = (int)((c / (uint32_t)m.dims[0]) % (uint32_t)m.dims[1]);
+      int c3 = (int)(c / ((uint32_t)m.dims[0] * (uint32_t)m.dims[1]));
+      bool bulk = c1 >= m.guard[0] && c1 < m.dims[0] - m.guard[0] && c2 >= m.guard[1] &&
+                  c2 < m.dims[1] - m.guard[1] && c3 >= m.guard[2] && c3 < m.dims[2] - m.guard[2];
+      if (bulk) {
+        int tx = (c1 - m.guard[0]) / T.tx;
+        int ty = (m.dim > 1) ? (c2 - m.guard[1]) / T.ty : 0;
+        key = (uint32_t)(tx + ty * T.ntx);
+      } else {
+        cell[i] = AP_MAX_CELL;
+      }
+    }
+    keys[i] = key;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+__global__ void k_histogram(const uint32_t *keys, size_t n, uint32_t nbins, uint32_t *hist) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t k = keys[i];
+    if (k < nbins) atomicAdd(hist + k, 1u);
+  }
+}
+
+// Exclusive scan of nbins counters into start[0..nbins] with one CTA.
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_counts(const uint32_t *counts, int nbins, uint32_t *start) {
+  __shared__ uint32_t s_part[kScanThreads];
+  const int tid = threadIdx.x;
+  const int per = (nbins + kScanThreads - 1) / kScanThreads;
+  const int b0 = tid * per, b1 = min(nbins, b0 + per);
+  uint32_t local = 0;
+  for (int b = b0; b < b1; ++b) local += counts[b];
+  s_part[tid] = local;
+  __syncthreads();
+  for (int off = 1; off < kScanThreads; off <<= 1) {
+    uint32_t v = tid >= off ? s_part[tid - off] : 0u;
+    __syncthreads();
+    s_part[tid] += v;
+    __syncthreads();
+  }
+  uint32_t run = s_part[tid] - local;
+  for (int b = b0; b < b1; ++b) {
+    start[b] = run;
+    run += counts[b];
+  }
+  if (tid == kScanThreads - 1) start[nbins] = s_part[tid];
+}
+
+__global__ void k_count_below(const uint32_t *keys, size_t n, uint32_t bound, uint32_t *count) {
+  uint32_t local = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    local += keys[i] < bound;
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+__global__ void k_cell_keys(const uint32_t *cell, size_t n, uint32_t ncells, uint32_t *keys,
+                            uint32_t *vals) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t c = cell[i];
+    keys[i] = (c == AP_MAX_CELL) ? ncells : c;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+template <typename T>
+__global__ void k_gather(const T *src, const uint32_t *perm, size_t n, T *dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = src[perm[i]];
+}
+
+int bits_for(uint32_t maxkey) {
+  int b = 1;
+  while (b < 32 && (maxkey >> b) != 0) ++b;
+  return b;
+}
+
+int grid_for(Ctx &c, size_t n, int threads) {
+  size_t g = (n + threads - 1) / threads;
+  size_t cap = (size_t)c.num_sms * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// Stable radix sort of (keys[0], vals[0]) -> result pointers.
+cudaError_t radix_pairs(Ctx &c, size_t n, int end_bit, uint32_t **keys_out,
+                        uint32_t **vals_out) {
+  cub::DoubleBuffer<uint32_t> k(c.keys[0], c.keys[1]);
+  cub::DoubleBuffer<uint32_t> v(c.vals[0], c.vals[1]);
+  size_t bytes = c.cub_tmp_bytes;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(c.cub_tmp, bytes, k, v, (int64_t)n, 0,
+                                                   end_bit, c.stream);
+  if (e != cudaSuccess) return e;
+  *keys_out = k.Current();
+  *vals_out = v.Current();
+  c.launches += (uint64_t)((end_bit + 7) / 8) * 3;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count, uint32_t *new_start,
+                             uint32_t *grp_off) {
+  TileTopo T{c.tiles.ntx, c.tiles.nty, c.tiles.ntiles, c.params.periodic[0],
+             c.params.periodic[1]};
+  k_tile_scan<<<1, kScanThreads, 0, c.stream>>>(T, dir_count, new_start, grp_off);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start, const uint32_t *old_order,
+                                 const uint8_t *dir, const uint32_t *grp_off,
+                                 uint32_t *new_order) {
+  int grid = c.tiles.ntiles < c.num_sms * 8 ? c.tiles.ntiles : c.num_sms * 8;
+  k_order_scatter<<<grid, kScatterThreads, 0, c.stream>>>(c.tiles.ntiles, old_start, old_order,
+                                                          dir, grp_off, new_order,
+                                                          (uint32_t)c.order_cap, c.status);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+// Scratch for the radix sorts: two key and two value buffers of n entries,
+// CUB's temporary storage, and an 8-byte-per-slot gather buffer.
+int ensure_scratch(Ctx &c, size_t n) {
+  if (n <= c.scratch_cap && c.keys[0]) return AP_OK;
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(c.keys[i]);
+    cudaFree(c.vals[i]);
+    c.keys[i] = c.vals[i] = nullptr;
+  }
+  cudaFree(c.cub_tmp);
+  cudaFree(c.gather_tmp);
+  c.cub_tmp = c.gather_tmp = nullptr;
+  size_t cap = n < 1024 ? 1024 : n;
+  for (int i = 0; i < 2; ++i) {
+    if (cudaMalloc(&c.keys[i], cap * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
+    if (cudaMalloc(&c.vals[i], cap * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
+  }
+  cub::DoubleBuffer<uint32_t> k(c.keys[0], c.keys[1]);
+  cub::DoubleBuffer<uint32_t> v(c.vals[0], c.vals[1]);
+  size_t bytes = 0;
+  if (cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int64_t)cap, 0, 32) != cudaSuccess)
+    return AP_ERR_CUDA;
+  if (cudaMalloc(&c.cub_tmp, bytes) != cudaSuccess) return AP_ERR_NOMEM;
+  c.cub_tmp_bytes = bytes;
+  if (cudaMalloc(&c.gather_tmp, cap * sizeof(uint64_t)) != cudaSuccess) return AP_ERR_NOMEM;
+  c.scratch_cap = cap;
+  return AP_OK;
+}
+
+// Builds the tile order from scratch: stable sort of slots [0, number) by
+// tile key, then tile offsets from a histogram.
+cudaError_t rebuild_tile_order(Ctx &c) {
+  const size_t n = c.number;
+  const uint32_t nt = (uint32_t)c.tiles.ntiles;
+  uint32_t *start = c.tile_start[c.cur];
+  cudaError_t e;
+  e = cudaMemsetAsync(c.dir_count, 0, sizeof(uint32_t) * (nt + 1), c.stream);
+  if (e != cudaSuccess) return e;
+  if (n > 0) {
+    k_tile_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.mk, c.tiles, c.ptc.cell, n,
+                                                          c.keys[0], c.vals[0]);
+    c.launches++;
+    uint32_t *ko, *vo;
+    e = radix_pairs(c, n, bits_for(nt), &ko, &vo);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(c.order[c.cur], vo, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                        c.stream);
+    if (e != cudaSuccess) return e;
+    k_histogram<<<grid_for(c, n, 256), 256, 0, c.stream>>>(ko, n, nt, c.dir_count);
+    c.launches++;
+  }
+  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, (int)nt, start);
+  c.launches++;
+  c.order_valid = true;
+  return cudaGetLastError();
+}
+
+cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
+  const size_t n = c.number;
+  *new_number = 0;
+  if (n == 0) return cudaSuccess;
+  const uint32_t ncells =
+      (uint32_t)c.mesh.dims[0] * (uint32_t)c.mesh.dims[1] * (uint32_t)c.mesh.dims[2];
+  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.ptc.cell, n, ncells, c.keys[0],
+                                                        c.vals[0]);
+  c.launches++;
+  uint32_t *ko, *vo;
+  cudaError_t e = radix_pairs(c, n, bits_for(ncells), &ko, &vo);
+  if (e != cudaSuccess) return e;
+  const int g = grid_for(c, n, 256);
+  // rearrange every SoA member through the gather buffer
+  // (cuda/core/particle_base_impl.cu:466-487)
+#define AP_GATHER(FIELD, T)                                                                \
+  do {                                                                                      \
+    k_gather<T><<<g, 256, 0, c.stream>>>(c.ptc.FIELD, vo, n, (T *)c.gather_tmp);           \
+    c.launches++;                                                                           \
+    e = cudaMemcpyAsync(c.ptc.FIELD, c.gather_tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, \
+                        c.stream);                                                          \
+    if (e != cudaSuccess) return e;                                                         \
+  } while (0)
+  AP_GATHER(x1, float);
+  AP_GATHER(x2, float);
+  AP_GATHER(x3, float);
+  AP_GATHER(p1, float);
+  AP_GATHER(p2, float);
+  AP_GATHER(p3, float);
+  AP_GATHER(E, float);
+  AP_GATHER(weight, float);
+  AP_GATHER(cell, uint32_t);
+  AP_GATHER(id, uint64_t);
+  AP_GATHER(flag, uint32_t);
+#undef AP_GATHER
+  // number of non-empty slots = position of the first key == ncells
+  // (upper_bound of MAX_CELL - 1, particle_base_impl.cu:454-458)
+  uint32_t *cnt = c.dir_count;
+  e = cudaMemsetAsync(cnt, 0, sizeof(uint32_t), c.stream);
+  if (e != cudaSuccess) return e;
+  k_count_below<<<g, 256, 0, c.stream>>>(ko, n, ncells, cnt);
+  c.launches++;
+  uint32_t live = 0;
+  e = cudaMemcpyAsync(&live, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return e;
+  *new_number = live;
+  return cudaSuccess;
+}
+
+}  // namespace apb

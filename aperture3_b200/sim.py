@@ -1,0 +1,383 @@
+"""Host-side mirror of the reference's lab-facing interface.
+
+Same class and method names as the reference's algorithm classes and the
+parts of sim_environment / sim_data they use (src/algorithms/ptc_updater.h,
+field_solver.h, src/sim_environment.h, src/sim_data.h), without MPI: one
+rank, one GPU, periodic exchange done by device kernels. Every operation
+goes through libaperture_b200.so; device memory comes from torch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import (AP_MAX_CELL, AP_MAX_SPECIES, ApArray, ApDiag, ApFields, ApMesh, ApParams,
+                   ApParticles, ApStepStats, check)
+
+PTC_FIELDS = (
+    ("x1", torch.float32), ("x2", torch.float32), ("x3", torch.float32),
+    ("p1", torch.float32), ("p2", torch.float32), ("p3", torch.float32),
+    ("E", torch.float32), ("weight", torch.float32),
+    ("cell", torch.int32), ("id", torch.int64), ("flag", torch.int32),
+)
+NP_DTYPES = {"cell": np.uint32, "id": np.uint64, "flag": np.uint32}
+
+ELECTRON, POSITRON, ION = 0, 1, 2
+FLAG_IGNORE_CURRENT = 1 << 3
+FLAG_IGNORE_EM = 1 << 4
+
+
+def species_flag(sp: int) -> int:
+    """gen_ptc_type_flag (src/utils/util_functions.h:71-74)."""
+    return (sp & 7) << 29
+
+
+@dataclasses.dataclass
+class SimParams:
+    """The SimParams fields the particle update uses (src/sim_params.h:17-123),
+    with the reference's key names."""
+    N: Sequence[int] = (1, 1, 1)
+    guard: Sequence[int] = (0, 0, 0)
+    lower: Sequence[float] = (0.0, 0.0, 0.0)
+    size: Sequence[float] = (1.0, 1.0, 1.0)
+    delta_t: float = 0.01
+    q_e: float = 1.0
+    ion_mass: float = 1.0
+    num_species: int = 2
+    periodic_boundary: Sequence[bool] = (False, False, False)
+    data_interval: int = 100
+    current_smoothing: int = 0
+    sort_interval: int = 20
+    max_ptc_number: int = 100
+    B0: float = 1.0
+    max_steps: int = 0
+    tile_size: Sequence[int] = (0, 0, 0)
+
+    @classmethod
+    def from_toml(cls, path: str) -> "SimParams":
+        """parse_config (src/sim_params.cpp:34-219) for the keys above."""
+        import tomllib
+        with open(path, "rb") as f:
+            d = tomllib.load(f)
+        p = cls()
+        flat = dict(d)
+        flat.update(d.get("Grid", {}))
+        flat.update(d.get("Simulation", {}))
+        for k in dataclasses.fields(cls):
+            if k.name in flat:
+                setattr(p, k.name, flat[k.name])
+        return p
+
+
+def _pad3(v, fill):
+    v = list(v) + [fill] * (3 - len(v))
+    return v[:3]
+
+
+class SimEnvironment:
+    """sim_environment (src/sim_environment.h) for one rank."""
+
+    def __init__(self, params: SimParams, device: Optional[int] = None):
+        self.params = params
+        if device is not None:
+            torch.cuda.set_device(device)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.mesh = self._make_mesh(params)
+        # setup_env (sim_environment_impl.hpp:90-101)
+        q = np.float32(params.q_e)
+        self.charges = [float(q)] * AP_MAX_SPECIES
+        self.masses = [float(q)] * AP_MAX_SPECIES
+        self.charges[ELECTRON] = float(-q)
+        self.masses[ION] = float(np.float32(q * np.float32(params.ion_mass)))
+        self.periodic = [int(bool(x)) for x in _pad3(params.periodic_boundary, False)]
+        ap = ApParams()
+        ap.num_species = int(params.num_species)
+        ap.data_interval = int(params.data_interval)
+        ap.current_smoothing = int(params.current_smoothing)
+        for i in range(3):
+            ap.periodic[i] = self.periodic[i]
+        for i in range(AP_MAX_SPECIES):
+            ap.charges[i] = self.charges[i]
+            ap.masses[i] = self.masses[i]
+        ts = _pad3(params.tile_size, 0)
+        ap.tile[0], ap.tile[1] = int(ts[0]), int(ts[1])
+        self.ap_params = ap
+        self._lib = _lib.lib()
+        ctx = C.c_void_p()
+        check(self._lib.ap_ctx_create(C.byref(self.mesh), C.byref(ap), C.byref(ctx)),
+              "ap_ctx_create")
+        self.ctx = ctx
+
+    @staticmethod
+    def _make_mesh(p: SimParams) -> ApMesh:
+        """Grid::init (src/core/grid.cpp:31-48)."""
+        N = _pad3(p.N, 1)
+        g = _pad3(p.guard, 0)
+        lo = _pad3(p.lower, 0.0)
+        sz = _pad3(p.size, 1.0)
+        m = ApMesh()
+        for i in range(3):
+            m.guard[i] = int(g[i])
+            m.dims[i] = int(N[i]) + 2 * int(g[i])
+            m.lower[i] = float(np.float32(lo[i]))
+            m.sizes[i] = float(np.float32(sz[i]))
+            d = np.float32(np.float32(sz[i]) / np.float32(N[i]))
+            m.delta[i] = float(d)
+            m.inv_delta[i] = float(np.float32(1.0 / np.float64(d)))
+        if m.dims[1] <= 1 and m.dims[2] <= 1:
+            m.dimension = 1
+        elif m.dims[2] <= 1:
+            m.dimension = 2
+        else:
+            m.dimension = 3
+        return m
+
+    @property
+    def dims(self):
+        return [self.mesh.dims[i] for i in range(3)]
+
+    def dim(self):
+        return self.mesh.dimension
+
+    def set_stream(self, stream: torch.cuda.Stream):
+        check(self._lib.ap_set_stream(self.ctx, C.c_void_p(stream.cuda_stream)), "ap_set_stream")
+
+    def set_sync(self, sync: bool):
+        check(self._lib.ap_set_sync(self.ctx, int(sync)), "ap_set_sync")
+
+    def sync(self):
+        check(self._lib.ap_sync(self.ctx), "ap_sync")
+
+    def send_guard_cells(self, field):
+        """send_guard_cells for a scalar array or a list of components."""
+        for a in (field if isinstance(field, (list, tuple)) else [field]):
+            check(self._lib.ap_send_guard_cells(self.ctx, array_view(a)), "ap_send_guard_cells")
+
+    def send_add_guard_cells(self, field):
+        for a in (field if isinstance(field, (list, tuple)) else [field]):
+            check(self._lib.ap_send_add_guard_cells(self.ctx, array_view(a)),
+                  "ap_send_add_guard_cells")
+
+    def launch_count(self) -> int:
+        return int(self._lib.ap_launch_count(self.ctx))
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self._lib.ap_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def array_view(t: torch.Tensor) -> ApArray:
+    """ApArray of a pitched field tensor (rows x padded row)."""
+    pitch = t.stride(0) * t.element_size()
+    return ApArray(t.data_ptr(), pitch)
+
+
+def _alloc_field(dims, device, row_align=4):
+    rows = dims[1] * dims[2]
+    padded = (dims[0] + row_align - 1) // row_align * row_align
+    full = torch.zeros((rows, padded), dtype=torch.float32, device=device)
+    return full[:, : dims[0]]
+
+
+class SimData:
+    """sim_data (src/sim_data.h:14-70): fields and the particle store."""
+
+    def __init__(self, env: SimEnvironment, capacity: Optional[int] = None, row_align: int = 4):
+        """row_align: field rows are padded to a multiple of this many floats
+        (4 gives the 16-byte row pitch the TMA field loads need; 1 packs the
+        rows, which makes the kernels read the field tiles with plain loads
+        when dims[0] is not a multiple of 4)."""
+        self.env = env
+        dims = env.dims
+        dev = env.device
+        mk = lambda: _alloc_field(dims, dev, row_align)  # noqa: E731
+        self.E = [mk() for _ in range(3)]
+        self.B = [mk() for _ in range(3)]
+        self.Ebg = [mk() for _ in range(3)]
+        self.Bbg = [mk() for _ in range(3)]
+        self.J = [mk() for _ in range(3)]
+        self.Rho = [mk() for _ in range(env.params.num_species)]
+        self.divE = mk()
+        self.divB = mk()
+        cap = int(capacity if capacity is not None else env.params.max_ptc_number)
+        self.capacity = cap
+        self.particles: Dict[str, torch.Tensor] = {
+            name: torch.zeros(max(cap, 1), dtype=dt, device=dev) for name, dt in PTC_FIELDS}
+        self.particles["cell"].fill_(-1)  # MAX_CELL
+        self.number = 0
+        self._bind()
+
+    def _bind(self):
+        f = ApFields()
+        for key in ("E", "B", "Ebg", "Bbg", "J"):
+            arr = getattr(f, key)
+            for c in range(3):
+                arr[c] = array_view(getattr(self, key)[c])
+        for s, r in enumerate(self.Rho):
+            f.Rho[s] = array_view(r)
+        f.divE = array_view(self.divE)
+        f.divB = array_view(self.divB)
+        lib = self.env._lib
+        check(lib.ap_bind_fields(self.env.ctx, C.byref(f)), "ap_bind_fields")
+        p = ApParticles()
+        for name, _ in PTC_FIELDS:
+            setattr(p, name, self.particles[name].data_ptr())
+        check(lib.ap_bind_particles(self.env.ctx, C.byref(p), self.number, self.capacity),
+              "ap_bind_particles")
+
+    # -- particles -------------------------------------------------------
+    def set_particles(self, host: Dict[str, np.ndarray]):
+        """Copies host SoA arrays into slots [0, n) and marks the tile order
+        for rebuild."""
+        n = len(host["x1"])
+        if n > self.capacity:
+            raise _lib.ApError(5, "set_particles")
+        for name, dt in PTC_FIELDS:
+            a = np.ascontiguousarray(host[name])
+            t = torch.from_numpy(a.view(np.int32) if dt == torch.int32 else
+                                 (a.view(np.int64) if dt == torch.int64 else a))
+            self.particles[name][:n].copy_(t)
+        self.number = n
+        self.particles_modified()
+
+    def particles_modified(self, number: Optional[int] = None):
+        if number is not None:
+            self.number = int(number)
+        check(self.env._lib.ap_particles_modified(self.env.ctx, self.number),
+              "ap_particles_modified")
+
+    def particles_host(self) -> Dict[str, np.ndarray]:
+        torch.cuda.synchronize()
+        out = {}
+        for name, _ in PTC_FIELDS:
+            a = self.particles[name][: self.number].cpu().numpy()
+            out[name] = a.view(NP_DTYPES[name]) if name in NP_DTYPES else a
+        return out
+
+    def sort_particles(self):
+        """sim_data::sort_particles (sim_data_impl.hpp:78-89)."""
+        lib = self.env._lib
+        check(lib.ap_sort_by_cell(self.env.ctx), "ap_sort_by_cell")
+        n = C.c_size_t()
+        check(lib.ap_get_number(self.env.ctx, C.byref(n)), "ap_get_number")
+        self.number = int(n.value)
+
+    def tile_order(self):
+        """(order, tile_start) of the per-step tile counting sort, as host arrays."""
+        lib = self.env._lib
+        o, ts = C.c_void_p(), C.c_void_p()
+        nt, live = C.c_uint32(), C.c_size_t()
+        check(lib.ap_get_tile_order(self.env.ctx, C.byref(o), C.byref(ts), C.byref(nt),
+                                    C.byref(live)), "ap_get_tile_order")
+        order = device_to_host(o.value, live.value * 4).view(np.uint32)
+        start = device_to_host(ts.value, (nt.value + 1) * 4).view(np.uint32)
+        return order, start
+
+    def stats(self) -> ApStepStats:
+        s = ApStepStats()
+        check(self.env._lib.ap_get_stats(self.env.ctx, C.byref(s)), "ap_get_stats")
+        return s
+
+    def diagnostics(self) -> ApDiag:
+        d = ApDiag()
+        check(self.env._lib.ap_diagnostics(self.env.ctx, C.byref(d)), "ap_diagnostics")
+        return d
+
+    # -- fields ----------------------------------------------------------
+    def fields_host(self):
+        torch.cuda.synchronize()
+        g = lambda t: t.contiguous().cpu().numpy()  # noqa: E731
+        return {
+            "E": [g(a) for a in self.E], "B": [g(a) for a in self.B],
+            "Ebg": [g(a) for a in self.Ebg], "Bbg": [g(a) for a in self.Bbg],
+            "J": [g(a) for a in self.J], "Rho": [g(a) for a in self.Rho],
+            "divE": g(self.divE), "divB": g(self.divB),
+        }
+
+    def set_fields(self, host):
+        for key in ("E", "B", "Ebg", "Bbg", "J"):
+            if key in host:
+                for c in range(3):
+                    getattr(self, key)[c].copy_(torch.from_numpy(np.ascontiguousarray(host[key][c])))
+        if "Rho" in host:
+            for s, a in enumerate(host["Rho"]):
+                self.Rho[s].copy_(torch.from_numpy(np.ascontiguousarray(a)))
+
+
+def _wrap_device_ptr(ptr: int, n: int) -> torch.Tensor:
+    """Non-owning uint8 tensor over device memory [ptr, ptr + n)."""
+    class _Holder:
+        __cuda_array_interface__ = {
+            "shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Holder(), device="cuda")
+
+
+def device_to_host(ptr: int, nbytes: int) -> np.ndarray:
+    """Copy of nbytes of device memory at ptr, as a uint8 numpy array."""
+    if nbytes == 0:
+        return np.empty(0, np.uint8)
+    torch.cuda.synchronize()
+    return _wrap_device_ptr(ptr, nbytes).cpu().numpy().copy()
+
+
+class ptc_updater:
+    """ptc_updater (src/algorithms/ptc_updater.h:11-24)."""
+
+    def __init__(self, env: SimEnvironment):
+        self.env = env
+
+    def update_particles(self, data: SimData, dt: float, step: int = 0):
+        """ptc_updater::update_particles (ptc_updater.cu:748-841)."""
+        check(self.env._lib.ap_update_particles(self.env.ctx, float(dt), int(step)),
+              "ap_update_particles")
+
+    def apply_boundary(self, data: SimData, dt: float, step: int = 0):
+        """No-op, as in the reference (ptc_updater.cu:843-850)."""
+
+    def smooth_current(self, data_or_array, step: int = 0):
+        """smooth_current(sim_data&, step) or smooth_current(multi_array&)."""
+        if isinstance(data_or_array, SimData):
+            check(self.env._lib.ap_smooth_current(self.env.ctx, int(step)), "ap_smooth_current")
+        else:
+            check(self.env._lib.ap_smooth_array(self.env.ctx, array_view(data_or_array)),
+                  "ap_smooth_array")
+
+
+class field_solver:
+    """field_solver (src/algorithms/field_solver.h:11-25)."""
+
+    def __init__(self, env: SimEnvironment):
+        self.env = env
+
+    def update_fields(self, data: SimData, dt: float, step: int = 0):
+        check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), int(step)),
+              "ap_update_fields")
+
+    def apply_outflow_boundary(self, data: SimData, time: float = 0.0):
+        """No-op, as in the reference (field_solver.cu:451-452)."""
+
+    def compute_divs(self, data: SimData):
+        check(self.env._lib.ap_compute_divs(self.env.ctx), "ap_compute_divs")
+
+    def update_e_field(self, data: SimData, dt: float):
+        check(self.env._lib.ap_update_e_field(self.env.ctx, float(dt)), "ap_update_e_field")
+
+    def update_b_field(self, data: SimData, dt: float):
+        check(self.env._lib.ap_update_b_field(self.env.ctx, float(dt)), "ap_update_b_field")
+
+
+# Python-style aliases
+PtcUpdater = ptc_updater
+FieldSolver = field_solver

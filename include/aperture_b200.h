@@ -1,0 +1,209 @@
+/*
+ * aperture_b200.h -- C ABI of the B200 particle update for Aperture3 labs.
+ *
+ * Replaces the CUDA implementations behind the reference's algorithm
+ * classes (src/algorithms/ptc_updater.h, field_solver.h) for Cartesian 1D
+ * and 2D grids: the Vay push fused with charge-conserving (Esirkepov)
+ * current deposition, the periodic guard exchange of a single rank, and
+ * the Yee FDTD field update. All arrays are device memory owned by the
+ * caller (sim_data in the reference); the library owns only its scratch.
+ *
+ * Conventions
+ *  - Every function returns an ap_status (0 == AP_OK).
+ *  - Field arrays are pitched like cudaMalloc3D arrays (pitch in bytes,
+ *    dims[1] * dims[2] rows of dims[0] floats), as multi_array
+ *    (src/core/multi_array.h) stores them.
+ *  - Particles use the reference SoA members (src/data/particle_data.h:50-61).
+ *    cell == AP_MAX_CELL marks an empty slot.
+ *  - By default each call synchronises its stream before returning, as the
+ *    reference calls cudaDeviceSynchronize after each kernel
+ *    (ptc_updater.cu:776-777); ap_set_sync(ctx, 0) makes calls asynchronous.
+ */
+#ifndef APERTURE_B200_H_
+#define APERTURE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define AP_API __attribute__((visibility("default")))
+#else
+#define AP_API
+#endif
+
+#define AP_MAX_CELL 0xFFFFFFFFu
+#define AP_MAX_SPECIES 8
+
+typedef enum {
+  AP_OK = 0,
+  AP_ERR_INVALID = 1,      /* bad argument, or a call made in the wrong state */
+  AP_ERR_CUDA = 2,         /* a CUDA runtime call failed                       */
+  AP_ERR_NAN = 3,          /* NaN momentum met by the push (reference: trap)   */
+  AP_ERR_MOVED_FAR = 4,    /* a particle moved more than one cell in a step    */
+  AP_ERR_CAPACITY = 5,     /* a size exceeds a fixed limit                     */
+  AP_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up               */
+  AP_ERR_UNSUPPORTED = 7,  /* grid dimension / option not implemented          */
+  AP_ERR_NOMEM = 8,        /* device allocation failed                         */
+  AP_ERR_TILE = 9          /* a particle was found outside its sort tile       */
+} ap_status;
+
+/* Same members and layout as Quadmesh (src/core/quadmesh.h:16-29). */
+typedef struct {
+  int dims[3];
+  int guard[3];
+  float delta[3];
+  float inv_delta[3];
+  float lower[3];
+  float sizes[3];
+  int dimension;
+} ap_mesh;
+
+/* The SimParams fields the particle update and field solver read
+ * (src/sim_params.h:17-123) plus the per-species charges and masses
+ * (sim_environment_impl.hpp:90-101), and the device tile shape. */
+typedef struct {
+  int num_species;           /* Rho arrays present (1..8)                   */
+  int data_interval;         /* Rho is deposited when (step+1) % it == 0   */
+  int current_smoothing;     /* binomial filter passes over J per step     */
+  int periodic[3];           /* periodic_boundary                          */
+  float charges[AP_MAX_SPECIES];
+  float masses[AP_MAX_SPECIES];
+  int tile[2];               /* sort tile in cells; 0 picks a default       */
+} ap_params;
+
+typedef struct {
+  float *ptr;
+  size_t pitch; /* bytes between rows */
+} ap_array;
+
+/* The sim_data members used by the update (src/sim_data.h:14-70). */
+typedef struct {
+  ap_array E[3], B[3], Ebg[3], Bbg[3], J[3];
+  ap_array Rho[AP_MAX_SPECIES];
+  ap_array divE, divB;
+} ap_fields;
+
+/* particle_data (src/data/particle_data.h:50-61). */
+typedef struct {
+  float *x1, *x2, *x3;
+  float *p1, *p2, *p3;
+  float *E, *weight;
+  uint32_t *cell;
+  uint64_t *id;
+  uint32_t *flag;
+} ap_particles;
+
+/* Counters of the last update, read back from the device status word. */
+typedef struct {
+  uint64_t nan_momenta;  /* particles skipped for NaN momentum            */
+  uint64_t moved_far;    /* particles with |dc| > 1 (deposit skipped)     */
+  uint64_t lost;         /* particles that left through a non-periodic side */
+  uint64_t tile_faults;  /* particles found outside their tile            */
+  uint64_t live;         /* particles in the tile order after the update  */
+} ap_step_stats;
+
+/* FP64 diagnostics: the reductions are done on the device in double. */
+typedef struct {
+  double kinetic;        /* sum w * m * (gamma - 1) over live particles      */
+  double charge;         /* sum q * w over live particles                    */
+  double field_energy;   /* 0.5 * sum (E^2 + B^2) * cell volume over the bulk */
+  double max_abs_rho;    /* max |rho_total| over the bulk                    */
+  double gauss_residual; /* max |divE - sum rho| over the bulk               */
+  double max_abs_j;      /* max |J| over the bulk, all components            */
+} ap_diag;
+
+typedef struct ap_ctx ap_ctx;
+
+/* Library version string. */
+AP_API const char *ap_version(void);
+/* Human-readable name of an ap_status. */
+AP_API const char *ap_status_string(int status);
+
+/* Creates a context for one rank's grid. Replaces the constructors
+ * ptc_updater(sim_environment&) (ptc_updater.cu:742-744) and
+ * field_solver(sim_environment&) (field_solver.cu:330), and the
+ * __constant__ mesh/params upload of setup_env_extra
+ * (cuda/sim_environment.cpp:129-157). Uses the current CUDA device. */
+AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params,
+                         ap_ctx **out);
+AP_API int ap_ctx_destroy(ap_ctx *ctx);
+
+/* Stream used by every launch of this context (default: a private
+ * non-blocking stream). */
+AP_API int ap_set_stream(ap_ctx *ctx, void *cuda_stream);
+/* 1 (default): every call synchronises before returning and reports device
+ * status; 0: calls only enqueue work, ap_sync() reports status. */
+AP_API int ap_set_sync(ap_ctx *ctx, int sync);
+AP_API int ap_sync(ap_ctx *ctx);
+
+/* Binds the field arrays (get_data_ptrs, cuda/sim_data.cu:295). */
+AP_API int ap_bind_fields(ap_ctx *ctx, const ap_fields *fields);
+/* Binds the particle arrays: slots [0, number) are in use, capacity is the
+ * allocated length (particles_t, core/particle_base.h). */
+AP_API int ap_bind_particles(ap_ctx *ctx, const ap_particles *ptc,
+                             size_t number, size_t capacity);
+/* Tells the context that the caller changed particle slots (cells, counts)
+ * since the last update; the tile order is rebuilt at the next update. */
+AP_API int ap_particles_modified(ap_ctx *ctx, size_t number);
+AP_API int ap_get_number(const ap_ctx *ctx, size_t *number);
+
+/* ptc_updater::update_particles(sim_data&, double dt, uint32_t step)
+ * (ptc_updater.cu:748-841): zero J (and Rho), push, deposit + move, fold
+ * the guard current, smooth, and wrap particles through periodic sides. */
+AP_API int ap_update_particles(ap_ctx *ctx, double dt, uint32_t step);
+/* ptc_updater::smooth_current(sim_data&, uint32_t) (ptc_updater.cu:852-873). */
+AP_API int ap_smooth_current(ap_ctx *ctx, uint32_t step);
+/* ptc_updater::smooth_current(multi_array<Scalar>&) (ptc_updater.cu:875-912):
+ * one filter pass over one array (no guard refresh). */
+AP_API int ap_smooth_array(ap_ctx *ctx, ap_array a);
+
+/* field_solver::update_fields(sim_data&, double dt, uint32_t step)
+ * (field_solver.cu:334-358). */
+AP_API int ap_update_fields(ap_ctx *ctx, double dt, uint32_t step);
+/* field_solver::update_e_field / update_b_field / compute_divs
+ * (field_solver.cu:404-449, 360-402, 454-504). These write the bulk and,
+ * in periodic dims, the guard images of the updated cells. */
+AP_API int ap_update_e_field(ap_ctx *ctx, double dt);
+AP_API int ap_update_b_field(ap_ctx *ctx, double dt);
+AP_API int ap_compute_divs(ap_ctx *ctx);
+
+/* sim_environment::send_guard_cells / send_add_guard_cells for one array on
+ * one rank (sim_environment_impl.hpp:274-317, cuda/sim_environment.cpp:
+ * 9-127): periodic copy / fold of the guard strips. */
+AP_API int ap_send_guard_cells(ap_ctx *ctx, ap_array a);
+AP_API int ap_send_add_guard_cells(ap_ctx *ctx, ap_array a);
+
+/* sim_data::sort_particles -> particle_base::sort_by_cell
+ * (sim_data_impl.hpp:78-89, cuda/core/particle_base_impl.cu:435-487):
+ * stable sort of all SoA members by cell, empty slots last and trimmed. */
+AP_API int ap_sort_by_cell(ap_ctx *ctx);
+
+/* The device tile order maintained by the per-step counting sort: order has
+ * `live` entries (particle slot indices grouped by tile, stable), and
+ * tile_start has ntiles + 1 entries. Pointers stay valid until the next
+ * update. */
+AP_API int ap_get_tile_order(ap_ctx *ctx, const uint32_t **order,
+                             const uint32_t **tile_start, uint32_t *ntiles,
+                             size_t *live);
+
+/* Counters of the last update (waits for the stream). */
+AP_API int ap_get_stats(ap_ctx *ctx, ap_step_stats *stats);
+/* FP64 energy / charge / Gauss-law diagnostics (new; the reference only
+ * computes per-particle gamma, cuda/core/particles.cu:10-22). */
+AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
+
+/* Status of the last failing call on this context. */
+AP_API int ap_last_error(const ap_ctx *ctx);
+
+/* Number of kernels this context has launched (for launch accounting). */
+AP_API uint64_t ap_launch_count(const ap_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APERTURE_B200_H_ */

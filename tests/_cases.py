@@ -1,0 +1,73 @@
+"""Seeded random particle/field cases shared by the CPU and GPU tests."""
+import numpy as np
+
+import oracle
+
+STAG = [(0, 1), (1, 0), (1, 1), (1, 0), (0, 1), (0, 0)]  # E1..E3, B1..B3 (x, y)
+
+
+def empty_ptc(n):
+    return {name: np.zeros(n, dt) for name, dt in oracle.PTC_FIELDS}
+
+
+def random_particles(m, n, rng, gamma_max=20.0, edge_frac=0.2, species=(0, 1), ncells=None):
+    """n particles in random bulk cells; a fraction sits exactly on or next to
+    cell edges; momenta isotropic with gamma log-uniform in [1, gamma_max]."""
+    p = empty_ptc(n)
+    g0, g1 = m.guard[0], m.guard[1]
+    c1 = rng.integers(g0, m.dims[0] - g0, n)
+    if m.dimension > 1:
+        c2 = rng.integers(g1, m.dims[1] - g1, n)
+    else:
+        c2 = np.zeros(n, np.int64)
+    p["cell"][:] = (c1 + c2 * m.dims[0]).astype(np.uint32)
+    for k in ("x1", "x2"):
+        x = rng.random(n, dtype=np.float32)
+        e = rng.random(n) < edge_frac
+        choice = rng.integers(0, 4, n)
+        edge_vals = np.array([0.0, np.nextafter(np.float32(1), np.float32(0)), 0.5,
+                              np.float32(1e-7)], np.float32)
+        x[e] = edge_vals[choice[e]]
+        p[k][:] = x
+    if m.dimension == 1:
+        p["x2"][:] = rng.standard_normal(n).astype(np.float32)
+    p["x3"][:] = rng.standard_normal(n).astype(np.float32)
+    gamma = np.exp(rng.random(n) * np.log(gamma_max))
+    pm = np.sqrt(np.maximum(gamma * gamma - 1.0, 0.0))
+    ct = 2 * rng.random(n) - 1
+    st = np.sqrt(1 - ct * ct)
+    ph = 2 * np.pi * rng.random(n)
+    p["p1"][:] = (pm * st * np.cos(ph)).astype(np.float32)
+    p["p2"][:] = (pm * st * np.sin(ph)).astype(np.float32)
+    p["p3"][:] = (pm * ct).astype(np.float32)
+    p["E"][:] = np.sqrt(1 + p["p1"].astype(np.float64) ** 2 + p["p2"].astype(np.float64) ** 2
+                        + p["p3"].astype(np.float64) ** 2).astype(np.float32)
+    p["weight"][:] = (0.5 + rng.random(n)).astype(np.float32)
+    sp = rng.choice(np.array(species), n)
+    p["flag"][:] = (sp.astype(np.uint32) << np.uint32(29))
+    p["id"][:] = np.arange(n, dtype=np.uint64)
+    return p
+
+
+def random_fields(m, rng, amp=0.5, num_species=2, bg=True):
+    f = oracle.new_fields(m, num_species)
+    for key in ("E", "B"):
+        for c in range(3):
+            f[key][c][:] = (amp * rng.standard_normal(f[key][c].shape)).astype(np.float32)
+    if bg:
+        for key in ("Ebg", "Bbg"):
+            for c in range(3):
+                f[key][c][:] = (0.1 * amp * rng.standard_normal(f[key][c].shape)).astype(np.float32)
+    return f
+
+
+def mesh_1d(N, guard=2, size=1.0):
+    return oracle.make_mesh((N, 1, 1), (guard, 0, 0), size=(size, 1, 1))
+
+
+def mesh_2d(N0, N1, guard=2, size=(1.0, 1.0)):
+    return oracle.make_mesh((N0, N1, 1), (guard, guard, 0), size=(size[0], size[1], 1))
+
+
+CHARGES = [-1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+MASSES = [1.0] * 8

@@ -1,0 +1,243 @@
+"""GPU parity of the C ABI against the CPU oracle (run on a B200).
+
+Bar: particle momenta, gamma, positions and cell indices bit-exact; the
+tile order and sort_by_cell bit-exact; J and Rho within 1e-6 of their
+maximum magnitude against the oracle's FP64-accumulated deposit; the field
+solver and guard exchange bit-exact on identical inputs.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from _cases import mesh_1d, random_fields, random_particles
+from _gpu_helpers import Pair, assert_bits, make_params
+
+pytestmark = pytest.mark.gpu
+
+J_TOL = 1e-6  # of max |J| (and max |rho|)
+
+
+def _fields(m, rng, amp=0.3):
+    f = random_fields(m, rng, amp=amp)
+    for key in ("E", "B", "Ebg", "Bbg"):
+        for c in range(3):
+            oracle.send_guard_cells(m, f[key][c], (1, 1, 0))
+    return f
+
+
+def _setup(N, nptc, seed, tile=(0, 0), periodic=(True, True), data_interval=1, row_align=4,
+           gamma_max=50.0):
+    params = make_params(N, periodic=periodic, data_interval=data_interval, tile=tile,
+                         capacity=nptc)
+    m = oracle.make_mesh(params.N, params.guard, size=params.size)
+    rng = np.random.default_rng(seed)
+    f = _fields(m, rng)
+    p = random_particles(m, nptc, rng, gamma_max=gamma_max)
+    return Pair(params, f, p, row_align=row_align)
+
+
+@pytest.mark.parametrize("tile", [(4, 4), (8, 8), (16, 16), (16, 8)])
+def test_2d_push_deposit_bitexact(tile):
+    pr = _setup((64, 48), 6000, seed=1, tile=tile)
+    for step in range(4):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL, rho=True)
+
+
+def test_2d_tile_order_is_stable_counting_sort():
+    pr = _setup((64, 64), 8000, seed=2, tile=(8, 8))
+    tile = (8, 8)
+    cells0 = pr.data.particles_host()["cell"]
+    keys = np.array([oracle.tile_key(pr.m, tile, int(c)) for c in cells0], np.uint32)
+    nt = oracle.tile_key(pr.m, tile, oracle.MAX_CELL)
+    order = oracle.stable_counting_sort(keys, nt + 1)
+    order = order[keys[order] < nt]
+    for step in range(5):
+        pr.both_update_particles(step)
+        cells = pr.p["cell"]
+        order_ref, start_ref = oracle.tile_order(pr.m, tile, cells, order)
+        order_gpu, start_gpu = pr.data.tile_order()
+        assert_bits(start_gpu, start_ref, f"tile_start step {step}")
+        assert_bits(order_gpu, order_ref, f"tile order step {step}")
+        order = order_ref
+
+
+def test_1d_push_deposit_bitexact():
+    params = make_params((512,), periodic=(True,), capacity=4096)
+    m = oracle.make_mesh(params.N, params.guard, size=params.size)
+    rng = np.random.default_rng(3)
+    f = random_fields(m, rng, amp=0.3)
+    for key in ("E", "B"):
+        for c in range(3):
+            oracle.send_guard_cells(m, f[key][c], (1, 0, 0))
+    p = random_particles(m, 4096, rng, gamma_max=50.0)
+    pr = Pair(params, f, p)
+    for step in range(4):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL, rho=True)
+
+
+@pytest.mark.parametrize("N", [(64, 48), (512,)])
+def test_update_fields_bitexact(N):
+    params = make_params(N, capacity=1)
+    m = oracle.make_mesh(params.N, params.guard, size=params.size)
+    rng = np.random.default_rng(4)
+    per = (1, 1 if m.dimension > 1 else 0, 0)
+    f = random_fields(m, rng)
+    for c in range(3):
+        f["J"][c][:] = (0.1 * rng.standard_normal(f["J"][c].shape)).astype(np.float32)
+    for key in ("E", "B", "Ebg", "Bbg"):
+        for c in range(3):
+            oracle.send_guard_cells(m, f[key][c], per)
+    pr = Pair(params, f, random_particles(m, 0, rng))
+    for step in range(3):
+        pr.both_update_fields(step)
+        g = pr.data.fields_host()
+        for key in ("E", "B"):
+            for c in range(3):
+                assert_bits(g[key][c], pr.f[key][c], f"{key}{c + 1} step {step}")
+        g0, g1 = m.guard[0], m.guard[1]
+        sl = ((slice(g1, m.dims[1] - g1) if m.dimension > 1 else slice(0, 1)),
+              slice(g0, m.dims[0] - g0))
+        assert_bits(g["divE"][sl], pr.f["divE"][sl], "divE")
+        assert_bits(g["divB"][sl], pr.f["divB"][sl], "divB")
+
+
+@pytest.mark.parametrize("N", [(40, 24), (64,)])
+def test_guard_exchange_bitexact(N):
+    params = make_params(N, capacity=1)
+    m = oracle.make_mesh(params.N, params.guard, size=params.size)
+    rng = np.random.default_rng(5)
+    pr = Pair(params, {}, random_particles(m, 0, rng))
+    per = (1, 1 if m.dimension > 1 else 0, 0)
+    a = rng.standard_normal(pr.f["J"][0].shape).astype(np.float32)
+    pr.data.set_fields({"J": [a, a, a]})
+    pr.env.send_guard_cells(pr.data.J[0])
+    pr.env.send_add_guard_cells(pr.data.J[1])
+    ref_copy, ref_add = a.copy(), a.copy()
+    oracle.send_guard_cells(m, ref_copy, per)
+    oracle.send_add_guard_cells(m, ref_add, per)
+    g = pr.data.fields_host()
+    assert_bits(g["J"][0], ref_copy, "send_guard_cells")
+    assert_bits(g["J"][1], ref_add, "send_add_guard_cells")
+
+
+def test_sort_by_cell_bitexact():
+    params = make_params((32, 32), capacity=5000)
+    m = oracle.make_mesh(params.N, params.guard, size=params.size)
+    rng = np.random.default_rng(6)
+    p = random_particles(m, 5000, rng)
+    holes = rng.random(5000) < 0.1
+    p["cell"][holes] = oracle.MAX_CELL
+    pr = Pair(params, {}, p)
+    pr.data.sort_particles()
+    n_ref = oracle.sort_by_cell(m, pr.p, 5000)
+    assert pr.data.number == n_ref
+    got = pr.data.particles_host()
+    for k, _ in oracle.PTC_FIELDS:
+        assert_bits(got[k], pr.p[k][:n_ref], f"sorted {k}")
+
+
+def test_no_tensor_map_path_bitexact():
+    """Rows packed to an odd length make the field tiles load without TMA."""
+    pr = _setup((61, 45), 4000, seed=7, row_align=1)
+    for step in range(3):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL)
+
+
+def test_empty_and_single_particle():
+    pr = _setup((32, 32), 0, seed=8)
+    pr.both_update_particles(0)
+    assert all(np.abs(j).max() == 0 for j in pr.data.fields_host()["J"])
+    pr = _setup((32, 32), 1, seed=9)
+    for step in range(3):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL)
+
+
+def test_lost_through_non_periodic_sides():
+    pr = _setup((32, 32), 6000, seed=10, periodic=(False, False), gamma_max=200.0)
+    lost = 0
+    for step in range(4):
+        lost += pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL)
+    assert lost > 0
+    assert int(pr.data.stats().live) == int(np.sum(pr.p["cell"] != oracle.MAX_CELL))
+
+
+def test_ignore_flags_bitexact():
+    pr = _setup((32, 32), 3000, seed=11)
+    rng = np.random.default_rng(12)
+    fl = pr.p["flag"]
+    fl[rng.random(3000) < 0.2] |= np.uint32(1 << 4)   # ignore_EM
+    fl[rng.random(3000) < 0.2] |= np.uint32(1 << 3)   # ignore_current
+    pr.data.set_particles(pr.p)
+    for step in range(3):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL)
+
+
+def test_nan_momentum_is_reported_not_trapped():
+    from aperture3_b200._lib import ApError
+    pr = _setup((32, 32), 500, seed=13)
+    pr.p["p1"][7] = np.float32("nan")
+    pr.data.set_particles(pr.p)
+    with pytest.raises(ApError) as e:
+        pr.pusher.update_particles(pr.data, pr.dt, 0)
+    assert e.value.status == 3
+    assert pr.data.stats().nan_momenta == 1
+
+
+def test_moved_far_is_reported():
+    from aperture3_b200._lib import ApError
+    pr = _setup((32, 32), 500, seed=14, gamma_max=1000.0)
+    with pytest.raises(ApError) as e:
+        pr.pusher.update_particles(pr.data, pr.dt * 8, 0)
+    assert e.value.status == 4
+
+
+def test_continuity_residual():
+    """Esirkepov charge conservation through the ABI: rho(t+1) - rho(t) +
+    div J = 0 on the bulk, within 1e-6 of max|rho|."""
+    pr = _setup((48, 48), 8000, seed=15, tile=(8, 8))
+    pr.pusher.update_particles(pr.data, pr.dt, 0)
+    rho0 = sum(r.cpu().double() for r in pr.data.Rho).numpy()
+    pr.pusher.update_particles(pr.data, pr.dt, 1)
+    g = pr.data.fields_host()
+    rho1 = sum(r.astype(np.float64) for r in g["Rho"])
+    J1, J2 = g["J"][0].astype(np.float64), g["J"][1].astype(np.float64)
+    m = pr.m
+    g0, g1, n0, n1 = m.guard[0], m.guard[1], m.dims[0], m.dims[1]
+    xs, xs1 = slice(g0, n0 - g0), slice(g0 + 1, n0 - g0 + 1)
+    ys, ys1 = slice(g1, n1 - g1), slice(g1 + 1, n1 - g1 + 1)
+    div = (J1[ys, xs1] - J1[ys, xs]) + (J2[ys1, xs] - J2[ys, xs])
+    res = np.abs(rho1[ys, xs] - rho0[ys, xs] + div).max()
+    assert res <= 1e-6 * np.abs(rho1).max(), res
+
+
+def test_coupled_steps_within_tolerance():
+    """Particles + fields for several steps: the GPU's J is not summed in the
+    oracle's order, so coupled runs are compared within the stated
+    tolerances (momenta 1e-5 relative)."""
+    pr = _setup((48, 48), 6000, seed=16, tile=(8, 8))
+    for step in range(5):
+        pr.pusher.update_particles(pr.data, pr.dt, step)
+        pr.solver.update_fields(pr.data, pr.dt, step)
+        pr.step = step
+        oracle.update_particles(pr.m, pr.p, len(pr.p["x1"]), pr.f, pr.dt, step, 1, 2, 0,
+                                pr.env.charges, pr.env.masses, pr.periodic)
+        oracle.update_fields(pr.m, pr.f, pr.dt, step, pr.periodic)
+    got = pr.data.particles_host()
+    same_cell = got["cell"] == pr.p["cell"]
+    assert same_cell.mean() > 0.999
+    for k in ("p1", "p2", "p3"):
+        a, b = got[k].astype(np.float64), pr.p[k].astype(np.float64)
+        scale = np.maximum(np.abs(b), 1e-3)
+        assert (np.abs(a - b) / scale).max() <= 1e-5, k
