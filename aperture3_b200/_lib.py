@@ -45,7 +45,7 @@ class ApParams(C.Structure):
         ("num_species", C.c_int), ("data_interval", C.c_int),
         ("current_smoothing", C.c_int), ("periodic", C.c_int * 3),
         ("charges", C.c_float * AP_MAX_SPECIES), ("masses", C.c_float * AP_MAX_SPECIES),
-        ("tile", C.c_int * 2),
+        ("tile", C.c_int * 2), ("chunk", C.c_int),
     ]
 
 
@@ -81,6 +81,13 @@ class ApDiag(C.Structure):
                 ("gauss_residual", C.c_double), ("max_abs_j", C.c_double)]
 
 
+class ApPhaseTimes(C.Structure):
+    _fields_ = [("push_deposit_ms", C.c_double), ("order_ms", C.c_double),
+                ("rebuild_ms", C.c_double), ("finalize_ms", C.c_double),
+                ("fields_ms", C.c_double), ("sort_ms", C.c_double),
+                ("push_deposit_launches", C.c_uint64)]
+
+
 _vp = C.c_void_p
 _i = C.c_int
 # name -> (restype, argtypes); every function declared in aperture_b200.h
@@ -110,6 +117,8 @@ SIGNATURES = {
                                C.POINTER(C.c_size_t)]),
     "ap_get_stats": (_i, [_vp, C.POINTER(ApStepStats)]),
     "ap_diagnostics": (_i, [_vp, C.POINTER(ApDiag)]),
+    "ap_set_profiling": (_i, [_vp, _i]),
+    "ap_get_phase_times": (_i, [_vp, C.POINTER(ApPhaseTimes), _i]),
     "ap_last_error": (_i, [_vp]),
     "ap_launch_count": (C.c_uint64, [_vp]),
 }

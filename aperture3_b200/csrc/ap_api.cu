@@ -25,6 +25,7 @@ MeshK make_meshk(const ap_mesh &m) {
     k.delta[i] = m.delta[i];
     k.inv_delta[i] = m.inv_delta[i];
   }
+  k.div0 = (m.dims[0] > 1) ? (~0ull / (unsigned long long)m.dims[0]) + 1ull : 0ull;
   if (m.dims[1] <= 1 && m.dims[2] <= 1)
     k.dim = 1;
   else if (m.dims[2] <= 1)
@@ -62,8 +63,8 @@ int cuda_fail(Ctx *c, cudaError_t e) {
   } while (0)
 
 bool is_supported_tile(int tx, int ty) {
-  return (tx == 16 && ty == 16) || (tx == 32 && ty == 16) || (tx == 32 && ty == 32) ||
-         (tx == 8 && ty == 8) || (tx == 16 && ty == 8) || (tx == 4 && ty == 4);
+  return (tx == 16 && ty == 16) || (tx == 32 && ty == 16) || (tx == 8 && ty == 8) ||
+         (tx == 16 && ty == 8) || (tx == 4 && ty == 4);
 }
 
 void choose_tiles(Ctx &c) {
@@ -174,6 +175,34 @@ int alloc_particle_state(Ctx *c, size_t cap) {
   return ensure_scratch(*c, n);
 }
 
+enum Phase { kPhPushDeposit = 0, kPhOrder, kPhRebuild, kPhFinalize, kPhFields, kPhSort, kPhN };
+
+// Starts a timed phase; returns the slot to close with phase_end, or -1.
+int phase_begin(Ctx *c, int phase) {
+  if (!c->profiling) return -1;
+  if (c->ev_used == c->ev_cap) {
+    int cap = c->ev_cap ? 2 * c->ev_cap : 256;
+    auto *nv = new (std::nothrow) Ctx::EventPair[cap];
+    if (!nv) return -1;
+    for (int i = 0; i < c->ev_used; ++i) nv[i] = c->ev[i];
+    for (int i = c->ev_used; i < cap; ++i) {
+      cudaEventCreate(&nv[i].a);
+      cudaEventCreate(&nv[i].b);
+    }
+    delete[] c->ev;
+    c->ev = nv;
+    c->ev_cap = cap;
+  }
+  int k = c->ev_used++;
+  c->ev[k].phase = phase;
+  cudaEventRecord(c->ev[k].a, c->stream);
+  return k;
+}
+
+void phase_end(Ctx *c, int k) {
+  if (k >= 0) cudaEventRecord(c->ev[k].b, c->stream);
+}
+
 }  // namespace
 
 extern "C" {
@@ -232,6 +261,9 @@ AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params, ap_ctx **
             cudaMalloc(&c->tile_start[1], sizeof(uint32_t) * (nt + 1)) == cudaSuccess &&
             cudaMalloc(&c->queue, sizeof(uint32_t) * 4) == cudaSuccess &&
             cudaMalloc(&c->diag_dev, sizeof(double) * 16) == cudaSuccess &&
+            cudaMalloc(&c->fx_used, sizeof(FixedFmt)) == cudaSuccess &&
+            cudaMalloc(&c->n_max, sizeof(uint32_t)) == cudaSuccess &&
+            cudaMalloc(&c->wmax, sizeof(float)) == cudaSuccess &&
             cudaMallocHost(&c->diag_host, sizeof(double) * 16) == cudaSuccess;
   if (!ok) {
     ap_ctx_destroy(c);
@@ -239,6 +271,9 @@ AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params, ap_ctx **
   }
   cudaMemset(c->status, 0, sizeof(DevStatus));
   std::memset(c->status_host, 0, sizeof(DevStatus));
+  cudaMemset(c->fx_used, 0, sizeof(FixedFmt));
+  cudaMemset(c->n_max, 0, sizeof(uint32_t));
+  cudaMemset(c->wmax, 0, sizeof(float));
   *out = c;
   return AP_OK;
 }
@@ -260,10 +295,18 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->gather_tmp);
   cudaFree(c->tmp_j);
   cudaFree(c->acc);
+  cudaFree(c->fx_used);
+  cudaFree(c->n_max);
+  cudaFree(c->wmax);
   cudaFree(c->status);
   cudaFree(c->diag_dev);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->diag_host) cudaFreeHost(c->diag_host);
+  for (int i = 0; i < c->ev_cap; ++i) {
+    cudaEventDestroy(c->ev[i].a);
+    cudaEventDestroy(c->ev[i].b);
+  }
+  delete[] c->ev;
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return AP_OK;
@@ -305,7 +348,8 @@ AP_API int ap_bind_fields(ap_ctx *c, const ap_fields *f) {
   c->use_tma = setup_tensor_maps(*c);
   if (!c->acc) {
     c->acc_comp = (size_t)m.dims[0] * m.dims[1] * m.dims[2];
-    AP_TRY(cudaMalloc(&c->acc, sizeof(double) * c->acc_comp * (3 + c->params.num_species)));
+    AP_TRY(cudaMalloc(&c->acc, sizeof(unsigned long long) * c->acc_comp *
+                                   (3 + c->params.num_species)));
   }
   if (!c->tmp_j) {
     size_t pitch = sizeof(float) * (size_t)m.dims[0];
@@ -327,6 +371,7 @@ AP_API int ap_bind_particles(ap_ctx *c, const ap_particles *p, size_t number, si
   c->capacity = capacity;
   c->ptc_bound = true;
   c->order_valid = false;
+  c->scale_valid = false;
   AP_TRY_ST(alloc_particle_state(c, capacity));
   return AP_OK;
 }
@@ -336,6 +381,7 @@ AP_API int ap_particles_modified(ap_ctx *c, size_t number) {
   if (number > c->capacity) return fail(c, AP_ERR_CAPACITY);
   c->number = number;
   c->order_valid = false;
+  c->scale_valid = false;
   return AP_OK;
 }
 
@@ -383,10 +429,14 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   // the FP64 accumulators start at zero; J (and Rho on output steps) are
   // overwritten by the finalize pass, Rho is zeroed on other steps.
   const int ncomp = 3 + (do_rho ? pr.num_species : 0);
-  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(double) * c->acc_comp * ncomp, c->stream));
+  int ph = phase_begin(c, kPhFinalize);
+  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
+                         c->stream));
+  if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
   if (!do_rho)
     for (int s = 0; s < pr.num_species; ++s) AP_TRY(launch_zero(*c, c->fields.Rho[s]));
   AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  phase_end(c, ph);
 
   if (c->number > 0) {
     PushDepositParams P;
@@ -404,6 +454,11 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
     P.acc = c->acc;
     P.acc_pitch = c->mesh.dims[0];
     P.acc_comp = c->acc_comp;
+    P.fx_used = c->fx_used;
+    P.n_max = c->n_max;
+    P.wmax = c->wmax;
+    P.qmax = 0.0f;
+    for (int s = 0; s < AP_MAX_SPECIES; ++s) P.qmax = fmaxf(P.qmax, fabsf(pr.charges[s]));
     // The kernel receives dt as float (Scalar dt); q_over_m is evaluated as
     // dt * 0.5f * q / m (ptc_updater.cu:42, 101).
     const float dtf = (float)dt;
@@ -420,21 +475,33 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
     P.status = c->status;
     P.number = c->number;
     if (c->mk.dim == 1) {
+      ph = phase_begin(c, kPhPushDeposit);
       AP_TRY(launch_push_deposit_1d(*c, P));
+      phase_end(c, ph);
+      c->pd_launches++;
     } else {
-      if (!c->order_valid) AP_TRY(rebuild_tile_order(*c));
+      if (!c->order_valid) {
+        ph = phase_begin(c, kPhRebuild);
+        AP_TRY(rebuild_tile_order(*c));
+        phase_end(c, ph);
+      }
       P.t = c->tiles;
       P.order = c->order[c->cur];
       P.tile_start = c->tile_start[c->cur];
       P.dir = c->dir;
       P.dir_count = c->dir_count;
       P.queue = c->queue;
+      ph = phase_begin(c, kPhPushDeposit);
       AP_TRY(launch_push_deposit_2d(*c, P));
+      phase_end(c, ph);
+      c->pd_launches++;
       if (incremental_order(*c)) {
         const int nxt = c->cur ^ 1;
+        ph = phase_begin(c, kPhOrder);
         AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
         AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur], c->order[c->cur], c->dir,
                                     c->grp_off, c->order[nxt]));
+        phase_end(c, ph);
         c->cur = nxt;
       } else {
         c->order_valid = false;
@@ -443,7 +510,9 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   }
   // send_add_guard_cells(J), and Rho on output steps (ptc_updater.cu:800-805),
   // fused with the FP64 -> FP32 rounding
+  ph = phase_begin(c, kPhFinalize);
   AP_TRY(launch_finalize_current(*c, ncomp));
+  phase_end(c, ph);
   AP_TRY_ST(smooth_current_async(c, step));
   if (!c->sync) return AP_OK;
   return check_status(c);
@@ -470,10 +539,12 @@ AP_API int ap_compute_divs(ap_ctx *c) {
 AP_API int ap_update_fields(ap_ctx *c, double dt, uint32_t step) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
   // field_solver::update_fields (field_solver.cu:334-358)
+  const int ph = phase_begin(c, kPhFields);
   if (step == 0) AP_TRY(launch_update_e(*c, (float)(0.5 * dt)));
   AP_TRY(launch_update_b(*c, (float)dt));
   AP_TRY(launch_update_e(*c, (float)dt));
   AP_TRY(launch_divs(*c));
+  phase_end(c, ph);
   return finish(c);
 }
 
@@ -492,7 +563,9 @@ AP_API int ap_send_add_guard_cells(ap_ctx *c, ap_array a) {
 AP_API int ap_sort_by_cell(ap_ctx *c) {
   if (!c || !c->ptc_bound) return AP_ERR_INVALID;
   size_t n = 0;
+  const int ph = phase_begin(c, kPhSort);
   AP_TRY(sort_by_cell(*c, &n));
+  phase_end(c, ph);
   c->number = n;
   c->order_valid = false;
   return AP_OK;
@@ -544,6 +617,35 @@ AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
   out->max_abs_rho = c->diag_host[3];
   out->gauss_residual = c->diag_host[4];
   out->max_abs_j = c->diag_host[5];
+  return AP_OK;
+}
+
+AP_API int ap_set_profiling(ap_ctx *c, int on) {
+  if (!c) return AP_ERR_INVALID;
+  c->profiling = on != 0;
+  return AP_OK;
+}
+
+AP_API int ap_get_phase_times(ap_ctx *c, ap_phase_times *out, int reset) {
+  if (!c || !out) return AP_ERR_INVALID;
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  double t[kPhN] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < c->ev_used; ++i) {
+    float ms = 0.0f;
+    AP_TRY(cudaEventElapsedTime(&ms, c->ev[i].a, c->ev[i].b));
+    t[c->ev[i].phase] += ms;
+  }
+  out->push_deposit_ms = t[kPhPushDeposit];
+  out->order_ms = t[kPhOrder];
+  out->rebuild_ms = t[kPhRebuild];
+  out->finalize_ms = t[kPhFinalize];
+  out->fields_ms = t[kPhFields];
+  out->sort_ms = t[kPhSort];
+  out->push_deposit_launches = c->pd_launches;
+  if (reset) {
+    c->ev_used = 0;
+    c->pd_launches = 0;
+  }
   return AP_OK;
 }
 

@@ -29,6 +29,15 @@ struct MeshK {
   float delta[3];
   float inv_delta[3];
   int dim;
+  unsigned long long div0;  // floor(2^64 / dims[0]) + 1: c / dims[0] = umul64hi(c, div0)
+};
+
+// Fixed-point format of the current/charge accumulators (see
+// k_push_deposit.cu): a contribution v becomes X = rint(v * 2^S), split into
+// hi = X >> L (int32) and lo = X mod 2^L (uint32) in shared memory.
+struct FixedFmt {
+  int S;
+  int L;
 };
 
 struct PtcK {
@@ -60,11 +69,17 @@ struct PushDepositParams {
   FieldArr F[6];     // E1..E3, B1..B3 (used when tensor maps are off)
   FieldArr J[3];
   FieldArr Rho[AP_MAX_SPECIES];
-  // FP64 accumulators of J1..J3 then Rho[0..num_species): component k at
-  // acc + k * acc_comp, row-major with row length acc_pitch.
-  double *acc;
+  // Fixed-point accumulators of J1..J3 then Rho[0..num_species): component k
+  // at acc + k * acc_comp, row-major with row length acc_pitch. A value v is
+  // stored as the 64-bit integer rint(v * 2^S) (two's complement), S from
+  // the FixedFmt the kernel writes to fx_used.
+  unsigned long long *acc;
   int acc_pitch;
   size_t acc_comp;
+  FixedFmt *fx_used;      // device: format used by this update (read by finalize)
+  const uint32_t *n_max;  // device: largest tile population (2D)
+  const float *wmax;      // device: largest |weight|
+  float qmax;             // largest |charge|
   float dt;
   float qm[AP_MAX_SPECIES];      // dt * 0.5f * q / m, evaluated as the reference does
   float charge[AP_MAX_SPECIES];
@@ -125,13 +140,27 @@ struct Ctx {
   void *gather_tmp = nullptr;
   size_t scratch_cap = 0;
 
-  // FP64 current / charge accumulators (3 + num_species components)
-  double *acc = nullptr;
+  // fixed-point current / charge accumulators (3 + num_species components)
+  unsigned long long *acc = nullptr;
   size_t acc_comp = 0;
+  FixedFmt *fx_used = nullptr;  // device: format of the last deposit
+  uint32_t *n_max = nullptr;    // device: largest tile population
+  float *wmax = nullptr;        // device: max |weight| over the bound particles
+  bool scale_valid = false;
 
   // filter scratch
   float *tmp_j = nullptr;
   int tmp_pitch = 0;
+
+  // per-phase event timing (ap_set_profiling)
+  bool profiling = false;
+  struct EventPair {
+    cudaEvent_t a, b;
+    int phase;
+  };
+  EventPair *ev = nullptr;
+  int ev_used = 0, ev_cap = 0;
+  uint64_t pd_launches = 0;
 
   DevStatus *status = nullptr;     // device
   DevStatus *status_host = nullptr;  // pinned
@@ -158,6 +187,7 @@ cudaError_t launch_divs(Ctx &c);
 cudaError_t launch_filter(Ctx &c, ap_array a, int bnd[4]);
 cudaError_t launch_zero(Ctx &c, ap_array a);
 cudaError_t launch_finalize_current(Ctx &c, int ncomp);
+cudaError_t launch_fixed_scale(Ctx &c);
 cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
 
 MeshK make_meshk(const ap_mesh &m);

@@ -200,22 +200,27 @@ __global__ void k_copy_bulk(Geo G, Arr src, Arr dst) {
   dst(a, b) = src(a, b);
 }
 
-// Folds the periodic guard layers of the FP64 accumulators into the bulk
-// and rounds once to FP32. For one rank, send_add_guard_cells
+// Folds the periodic guard layers of the fixed-point accumulators into the
+// bulk and rounds once to FP32. For one rank, send_add_guard_cells
 // (cuda/sim_environment.cpp:71-127) adds the lower guard strip of a dim into
 // the upper interior strip and the upper guard strip into the lower interior
 // strip, dim 0 (all rows) before dim 1 (all columns), leaving the guard
-// values in place; per cell that is the gather below.
-__global__ void k_finalize(Geo G, const double *__restrict__ acc, int acc_pitch,
-                           size_t acc_comp, int ncomp, Arr o0, Arr o1, Arr o2, Arr o3, Arr o4,
-                           Arr o5, Arr o6, Arr o7, Arr o8, Arr o9, Arr o10) {
+// values in place; per cell that is the gather below. The integer sums are
+// exact, so the order of the adds does not matter; the only rounding is the
+// final conversion (int64 -> double is exact below 2^53, then one rounding
+// to FP32).
+__global__ void k_finalize(Geo G, const unsigned long long *__restrict__ acc, int acc_pitch,
+                           size_t acc_comp, const FixedFmt *fmt, int ncomp, Arr o0, Arr o1,
+                           Arr o2, Arr o3, Arr o4, Arr o5, Arr o6, Arr o7, Arr o8, Arr o9,
+                           Arr o10) {
   const int rows = G.dim > 1 ? G.n1 : 1;
   const size_t total = (size_t)G.n0 * rows;
   const int comp = blockIdx.y;
   if (comp >= ncomp) return;
   Arr outs[11] = {o0, o1, o2, o3, o4, o5, o6, o7, o8, o9, o10};
   const Arr out = outs[comp];
-  const double *a = acc + comp * acc_comp;
+  const unsigned long long *a = acc + comp * acc_comp;
+  const double inv = ldexp(1.0, -fmt->S);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
     const int x = (int)(t % G.n0), y = (int)(t / G.n0);
@@ -228,14 +233,13 @@ __global__ void k_finalize(Geo G, const double *__restrict__ acc, int acc_pitch,
       if (y >= G.g1 && y < 2 * G.g1) yi = y + G.r1;
       else if (y >= G.n1 - 2 * G.g1 && y < G.n1 - G.g1) yi = y - G.r1;
     }
-    double v = a[(size_t)y * acc_pitch + x];
+    unsigned long long v = a[(size_t)y * acc_pitch + x];
     if (xi >= 0) v += a[(size_t)y * acc_pitch + xi];
     if (yi >= 0) {
-      double w = a[(size_t)yi * acc_pitch + x];
-      if (xi >= 0) w += a[(size_t)yi * acc_pitch + xi];
-      v += w;
+      v += a[(size_t)yi * acc_pitch + x];
+      if (xi >= 0) v += a[(size_t)yi * acc_pitch + xi];
     }
-    out(x, y) = (float)v;
+    out(x, y) = (float)((double)(long long)v * inv);
   }
 }
 
@@ -348,7 +352,8 @@ cudaError_t launch_finalize_current(Ctx &c, int ncomp) {
   int gx = (int)((total + 255) / 256);
   if (gx > c.num_sms * 8) gx = c.num_sms * 8;
   dim3 grid(gx, ncomp);
-  k_finalize<<<grid, 256, 0, c.stream>>>(G, c.acc, c.mesh.dims[0], c.acc_comp, ncomp, o[0], o[1],
+  k_finalize<<<grid, 256, 0, c.stream>>>(G, c.acc, c.mesh.dims[0], c.acc_comp, c.fx_used, ncomp,
+                                         o[0], o[1],
                                          o[2], o[3], o[4], o[5], o[6], o[7], o[8], o[9], o[10]);
   c.launches++;
   return cudaGetLastError();

@@ -10,14 +10,24 @@
 //   1. stages the E/B tile plus a one-cell halo into shared memory with six
 //      TMA 2D tiled loads (no multicast) completing on an mbarrier,
 //   2. zeroes a shared-memory J (and Rho) tile with a two-cell halo,
-//   3. pushes and deposits its particles, one particle per thread, reading
-//      fields from shared memory and adding current with shared FP64
-//      atomics (each contribution is the reference's FP32 value),
-//   4. flushes the J tile once into the FP64 accumulators in global memory
-//      (red.global.add.f64); a finalize pass folds the periodic guards and
-//      rounds each cell once to FP32, and
+//   3. walks the tile's list in chunks of CH particles: a coalesced load
+//      stages the chunk's records in shared memory, each warp then pushes
+//      and deposits 32 particles that sit CH/32 places apart in the list
+//      (in a cell-sorted list that puts the lanes of a warp in different
+//      cells, so their current updates do not collide), and a coalesced
+//      store writes the chunk back,
+//   4. flushes the J tile once into 64-bit accumulators in global memory; a
+//      finalize pass folds the periodic guards and rounds each cell once to
+//      FP32, and
 //   5. records, per particle, the direction of its new tile (0..8, 9 = gone)
 //      plus per-direction counts, which the order update consumes.
+//
+// Current and charge are accumulated exactly in fixed point: each FP32
+// contribution (the reference's value) becomes X = rint(v * 2^S), added as a
+// high word X >> L (int32) and a low word X mod 2^L (uint32) with native
+// 32-bit shared atomics. S and L are chosen from the largest tile population
+// n so that neither word can overflow over n contributions; the sums are
+// exact, so the result does not depend on the order of the atomics.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -79,7 +89,33 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <int TX, int TY>
+// Bits needed to represent n (ceil(log2(n + 1))).
+__device__ __forceinline__ int bits_of(uint32_t n) { return 32 - __clz(n); }
+
+// Fixed-point format for sums of at most 2^lg contributions of magnitude at
+// most qw: |X| < 2^(B-1), hi = X >> L with L = 32 - lg. With B = 63 - 2 lg,
+// |sum hi| < 2^30 and sum lo < 2^32 over 2^lg contributions.
+__device__ __forceinline__ FixedFmt fixed_format(int lg, int B, float qw) {
+  FixedFmt f;
+  f.L = 32 - lg;
+  int S = B - 2;
+  if (qw > 0.0f) S -= ilogbf(qw);
+  f.S = max(-100, min(100, S));
+  return f;
+}
+
+struct Acc32 {
+  int *hi;
+  unsigned *lo;
+};
+
+__device__ __forceinline__ void add_fixed(const Acc32 &a, int o, float v, float scale, int L) {
+  const long long X = __float2ll_rn(v * scale);  // exact scaling by a power of two
+  atomicAdd(a.hi + o, (int)(X >> L));
+  atomicAdd(a.lo + o, (unsigned)X & ((1u << L) - 1u));
+}
+
+template <int TX, int TY, int CH>
 struct TileGeom {
   static constexpr int BX = TX + 8;   // field box width: x start rounded down to 4 floats
   static constexpr int BY = TY + 2;   // one halo row on each side
@@ -87,31 +123,57 @@ struct TileGeom {
   static constexpr int JX = TX + 4;   // J tile: two halo cells on each side
   static constexpr int JY = TY + 4;
   static constexpr int JSZ = JX * JY;
+  static constexpr int SP = CH + CH / 64;  // staged chunk, one pad word per 64
   static constexpr int HDR = 128;     // mbarrier, tile id, abort flag, counters
+  static constexpr size_t stage_bytes() { return 10 * 4 * SP + 2 * SP; }
   static size_t smem_bytes(int nrho) {
-    return HDR + sizeof(float) * 6 * FSZ + sizeof(double) * (3 + nrho) * JSZ;
+    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + stage_bytes();
   }
 };
 
-template <int TX, int TY, bool kTMA, bool kRho>
-__global__ void __launch_bounds__(kThreads2D)
+__device__ __forceinline__ int spos(int e) { return e + (e >> 6); }
+
+// Write-back modes of a staged particle.
+constexpr uint8_t kWritePos = 1;  // x1, x2, x3, cell
+constexpr uint8_t kWriteMom = 2;  // p1, p2, p3, E
+
+template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho>
+__global__ void __launch_bounds__(kThreads2D, MINB)
     k_push_deposit_2d(const __grid_constant__ PushDepositParams P,
                       const __grid_constant__ FieldMaps maps) {
-  using G = TileGeom<TX, TY>;
+  using G = TileGeom<TX, TY, CH>;
+  constexpr int SP = G::SP;
+  constexpr int PER_THREAD = CH / kThreads2D;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
   int *s_tile = reinterpret_cast<int *>(smem + 8);
   int *s_abort = reinterpret_cast<int *>(smem + 12);
   uint32_t *s_cnt = reinterpret_cast<uint32_t *>(smem + 16);
   float *sF = reinterpret_cast<float *>(smem + G::HDR);
-  double *sJ = reinterpret_cast<double *>(sF + 6 * G::FSZ);
-  double *sR = sJ + 3 * G::JSZ;
+  const int ncomp = 3 + (kRho ? P.num_species : 0);
+  int *sJhi = reinterpret_cast<int *>(sF + 6 * G::FSZ);
+  unsigned *sJlo = reinterpret_cast<unsigned *>(sJhi + ncomp * G::JSZ);
+  float *st = reinterpret_cast<float *>(sJlo + ncomp * G::JSZ);
+  float *s_x1 = st, *s_x2 = st + SP, *s_x3 = st + 2 * SP;
+  float *s_p1 = st + 3 * SP, *s_p2 = st + 4 * SP, *s_p3 = st + 5 * SP;
+  float *s_w = st + 6 * SP;  // weight in, gamma out
+  uint32_t *s_cell = reinterpret_cast<uint32_t *>(st + 7 * SP);
+  uint32_t *s_flag = reinterpret_cast<uint32_t *>(st + 8 * SP);
+  uint32_t *s_idx = reinterpret_cast<uint32_t *>(st + 9 * SP);
+  uint8_t *s_dir = reinterpret_cast<uint8_t *>(st + 10 * SP);
+  uint8_t *s_mode = s_dir + SP;
 
   const int tid = threadIdx.x;
-  const int lane = tid & 31;
+  const int lane = tid & 31, warp = tid >> 5;
   const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
   const int g0 = P.m.guard[0], g1 = P.m.guard[1];
-  const int nzero = (3 + (kRho ? P.num_species : 0)) * G::JSZ;
+  const int nacc = ncomp * G::JSZ;
+
+  // fixed-point format of this update, from the largest tile population
+  const int lg = max(4, bits_of(*P.n_max));
+  const FixedFmt fx = fixed_format(lg, 63 - 2 * lg, P.qmax * *P.wmax);
+  const float fscale = ldexpf(1.0f, fx.S);
+  if (blockIdx.x == 0 && tid == 0) *P.fx_used = fx;
 
   if (tid == 0) {
     if (kTMA) mbar_init(mbar, 1);
@@ -140,7 +202,7 @@ __global__ void __launch_bounds__(kThreads2D)
         for (int k = 0; k < 6; ++k) tma_load_2d(sF + k * G::FSZ, &maps.m[k], xs, ys, mbar);
       }
     } else {
-      for (int i = tid; i < 6 * G::BX * G::BY; i += blockDim.x) {
+      for (int i = tid; i < 6 * G::BX * G::BY; i += kThreads2D) {
         int k = i / (G::BX * G::BY), rem = i % (G::BX * G::BY);
         int yy = ys + rem / G::BX, xx = xs + rem % G::BX;
         float v = 0.0f;
@@ -149,7 +211,10 @@ __global__ void __launch_bounds__(kThreads2D)
       }
     }
     // 2. zero the current (and charge) tile
-    for (int i = tid; i < nzero; i += blockDim.x) sJ[i] = 0.0;
+    for (int i = tid; i < nacc; i += kThreads2D) {
+      sJhi[i] = 0;
+      sJlo[i] = 0u;
+    }
     if (kTMA) {
       if (!mbar_wait(mbar, phase)) atomicExch(s_abort, 1);
     }
@@ -162,155 +227,219 @@ __global__ void __launch_bounds__(kThreads2D)
       break;
     }
 
-    // 3. particles of this tile
+    // 3. particles of this tile, CH at a time
     const uint32_t base = P.tile_start[t];
     const int n_t = (int)(P.tile_start[t + 1] - base);
-    for (int r = tid; r < n_t; r += blockDim.x) {
-      const uint32_t pos = base + (uint32_t)r;
-      const uint32_t idx = __ldg(P.order + pos);
-      const uint32_t c = __ldcs(P.p.cell + idx);
-      const uint32_t flag = __ldcs(P.p.flag + idx);
-      float x1 = __ldcs(P.p.x1 + idx), x2 = __ldcs(P.p.x2 + idx), x3 = __ldcs(P.p.x3 + idx);
-      float p1 = __ldcs(P.p.p1 + idx), p2 = __ldcs(P.p.p2 + idx), p3 = __ldcs(P.p.p3 + idx);
-      const float w = __ldcs(P.p.w + idx);
-      const int c1 = (int)(c % (uint32_t)dims0);
-      const int c2 = (int)(c / (uint32_t)dims0);
-      uint32_t dir = 4;
-      const bool in_tile = (c != AP_MAX_CELL) && c1 >= x0 && c1 < x0 + TX && c2 >= y0 &&
-                           c2 < y0 + TY;
-      if (!in_tile) {
-        atomicAdd(&P.status->tile_faults, 1ull);
-        dir = kDirGone;
-      } else if (p1 != p1 || p2 != p2 || p3 != p3) {
-        // The reference traps here (ptc_updater.cu:102-109); the particle is
-        // left untouched and reported instead.
-        atomicAdd(&P.status->nan_momenta, 1ull);
-      } else {
-        const int sp = ptc_type(flag);
-        float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
-        const bool em = !(flag & kFlagIgnoreEM);
-        if (em) {
-          const float qm = P.qm[sp];
-          const Weights1D Wx = weights_1d(x1, c1);
-          const Weights1D Wy = weights_1d(x2, c2);
-          float fe[6];
+    for (int c0 = 0; c0 < n_t; c0 += CH) {
+      const int nch = min(CH, n_t - c0);
+      // 3a. coalesced load of the chunk
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            const float *f = sF + k * G::FSZ;
-            const int ib = (stag_x(k) ? c1 - 1 : Wx.base0) - xs;
-            const int jb = (stag_y(k) ? c2 - 1 : Wy.base0) - ys;
-            const float wx0 = stag_x(k) ? Wx.w1[0] : Wx.w0[0];
-            const float wx1 = stag_x(k) ? Wx.w1[1] : Wx.w0[1];
-            const float wy0 = stag_y(k) ? Wy.w1[0] : Wy.w0[0];
-            const float wy1 = stag_y(k) ? Wy.w1[1] : Wy.w0[1];
-            const float *row0 = f + jb * G::BX + ib;
-            const float *row1 = row0 + G::BX;
-            float acc = 0.0f;
-            acc += row0[0] * wx0 * wy0;
-            acc += row0[1] * wx1 * wy0;
-            acc += row1[0] * wx0 * wy1;
-            acc += row1[1] * wx1 * wy1;
-            fe[k] = acc * qm;
-          }
-          vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
-        } else {
-          gamma = P.p.E[idx];  // the deposit reads the stored gamma
+      for (int k = 0; k < PER_THREAD; ++k) {
+        const int e = tid + k * kThreads2D;
+        if (e < nch) {
+          const int s = spos(e);
+          const uint32_t idx = P.order[base + c0 + e];
+          s_idx[s] = idx;
+          s_cell[s] = P.p.cell[idx];
+          s_flag[s] = P.p.flag[idx];
+          s_x1[s] = P.p.x1[idx];
+          s_x2[s] = P.p.x2[idx];
+          s_x3[s] = P.p.x3[idx];
+          s_p1[s] = P.p.p1[idx];
+          s_p2[s] = P.p.p2[idx];
+          s_p3[s] = P.p.p3[idx];
+          s_w[s] = P.p.w[idx];
         }
-        // deposit_current_cart_2d (ptc_updater.cu:295-386)
-        const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
-        float nx1 = x1 + (v1 * P.dt) * P.m.inv_delta[0];
-        float nx2 = x2 + (v2 * P.dt) * P.m.inv_delta[1];
-        const int dc1 = (int)floorf(nx1);
-        const int dc2 = (int)floorf(nx2);
-        nx1 -= (float)dc1;
-        nx2 -= (float)dc2;
-        const float nx3 = x3 + v3 * P.dt;
-        const bool far = dc1 > 1 || dc1 < -1 || dc2 > 1 || dc2 < -1;
-
-        if (!far && !(flag & kFlagIgnoreCurrent)) {
-          const float weight = -P.charge[sp] * w;
-          const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
-          const int j0 = (dc2 == -1 ? -2 : -1), j1 = (dc2 == 1 ? 1 : 0);
-          float sx0[4], sx1[4];
+      }
+      __syncthreads();
+      // 3b. push + deposit: lane l of warp w takes element l*CH/32 + w*PER_THREAD + k
+      for (int k = 0; k < PER_THREAD; ++k) {
+        const int e = lane * (CH / 32) + warp * PER_THREAD + k;
+        if (e >= nch) continue;
+        const int s = spos(e);
+        const uint32_t c = s_cell[s];
+        const uint32_t flag = s_flag[s];
+        const float x1 = s_x1[s], x2 = s_x2[s], x3 = s_x3[s];
+        float p1 = s_p1[s], p2 = s_p2[s], p3 = s_p3[s];
+        const float w = s_w[s];
+        const int c2 = (int)__umul64hi((unsigned long long)c, P.m.div0);
+        const int c1 = (int)c - c2 * dims0;
+        uint32_t dir = 4;
+        uint8_t mode = 0;
+        const bool in_tile = (c != AP_MAX_CELL) && c1 >= x0 && c1 < x0 + TX && c2 >= y0 &&
+                             c2 < y0 + TY;
+        if (!in_tile) {
+          atomicAdd(&P.status->tile_faults, 1ull);
+          dir = kDirGone;
+        } else if (p1 != p1 || p2 != p2 || p3 != p3) {
+          // The reference traps here (ptc_updater.cu:102-109); the particle is
+          // left untouched and reported instead.
+          atomicAdd(&P.status->nan_momenta, 1ull);
+        } else {
+          const int sp = ptc_type(flag);
+          float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
+          const bool em = !(flag & kFlagIgnoreEM);
+          if (em) {
+            const float qm = P.qm[sp];
+            const Weights1D Wx = weights_1d(x1, c1);
+            const Weights1D Wy = weights_1d(x2, c2);
+            float fe[6];
 #pragma unroll
-          for (int i = -2; i <= 1; ++i) {
-            sx0[i + 2] = cic(-x1 + i + 1);
-            sx1[i + 2] = cic(-nx1 + (i + 1 - dc1));
+            for (int q = 0; q < 6; ++q) {
+              const float *f = sF + q * G::FSZ;
+              const int ib = (stag_x(q) ? c1 - 1 : Wx.base0) - xs;
+              const int jb = (stag_y(q) ? c2 - 1 : Wy.base0) - ys;
+              const float wx0 = stag_x(q) ? Wx.w1[0] : Wx.w0[0];
+              const float wx1 = stag_x(q) ? Wx.w1[1] : Wx.w0[1];
+              const float wy0 = stag_y(q) ? Wy.w1[0] : Wy.w0[0];
+              const float wy1 = stag_y(q) ? Wy.w1[1] : Wy.w0[1];
+              const float *row0 = f + jb * G::BX + ib;
+              const float *row1 = row0 + G::BX;
+              float acc = 0.0f;
+              acc += row0[0] * wx0 * wy0;
+              acc += row0[1] * wx1 * wy0;
+              acc += row1[0] * wx0 * wy1;
+              acc += row1[1] * wx1 * wy1;
+              fe[q] = acc * qm;
+            }
+            vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
+          } else {
+            gamma = P.p.E[s_idx[s]];  // the deposit reads the stored gamma
           }
-          float djy[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-          double *sJ1 = sJ, *sJ2 = sJ + G::JSZ, *sJ3 = sJ + 2 * G::JSZ;
-          double *sRho = sR + sp * G::JSZ;
+          // deposit_current_cart_2d (ptc_updater.cu:295-386)
+          const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
+          float nx1 = x1 + (v1 * P.dt) * P.m.inv_delta[0];
+          float nx2 = x2 + (v2 * P.dt) * P.m.inv_delta[1];
+          const int dc1 = (int)floorf(nx1);
+          const int dc2 = (int)floorf(nx2);
+          nx1 -= (float)dc1;
+          nx2 -= (float)dc2;
+          const float nx3 = x3 + v3 * P.dt;
+          const bool far = dc1 > 1 || dc1 < -1 || dc2 > 1 || dc2 < -1;
+
+          if (!far && !(flag & kFlagIgnoreCurrent)) {
+            // Esirkepov over the reference's ranges i in [i0, i1], j in [j0, j1]
+            // (2 or 3 nodes per dim). Every lane walks the same 3 x 3 window
+            // starting at (ib, jb) so the warp does not diverge; the third
+            // node of a 2-node range is predicated off. Cumulative sums run
+            // in the reference's order, so each contribution keeps its value.
+            const float weight = -P.charge[sp] * w;
+            const int ib = (dc1 == -1 ? -2 : -1), nib = (dc1 == 0 ? 2 : 3);
+            const int jb = (dc2 == -1 ? -2 : -1), njb = (dc2 == 0 ? 2 : 3);
+            float sx0[3], sx1[3];
 #pragma unroll
-          for (int j = -2; j <= 1; ++j) {
-            if (j < j0 || j > j1) continue;
-            const float sy0 = cic(-x2 + j + 1);
-            const float sy1 = cic(-nx2 + (j + 1 - dc2));
-            const int row = (c2 + j - jy0) * G::JX;
-            float djx = 0.0f;
+            for (int a = 0; a < 3; ++a) {
+              const int i = ib + a;
+              sx0[a] = cic(-x1 + i + 1);
+              sx1[a] = cic(-nx1 + (i + 1 - dc1));
+            }
+            float djy[3] = {0.0f, 0.0f, 0.0f};
+            const Acc32 J1{sJhi, sJlo}, J2{sJhi + G::JSZ, sJlo + G::JSZ},
+                J3{sJhi + 2 * G::JSZ, sJlo + 2 * G::JSZ};
+            const Acc32 R{sJhi + (3 + sp) * G::JSZ, sJlo + (3 + sp) * G::JSZ};
+            const bool rho = kRho && sp < P.num_species;
+            const int obase = (c2 + jb - jy0) * G::JX + (c1 + ib - jx0);
 #pragma unroll
-            for (int i = -2; i <= 1; ++i) {
-              if (i < i0 || i > i1) continue;
-              const int o = row + (c1 + i - jx0);
-              djx += movement2d(sy0, sy1, sx0[i + 2], sx1[i + 2]);
-              atomicAdd(sJ1 + o + 1, (double)(weight * djx));
-              djy[i + 2] += movement2d(sx0[i + 2], sx1[i + 2], sy0, sy1);
-              atomicAdd(sJ2 + o + G::JX, (double)(weight * djy[i + 2]));
-              const float val2 = center2d(sx0[i + 2], sx1[i + 2], sy0, sy1);
-              atomicAdd(sJ3 + o, (double)(-weight * v3 * val2));
-              if (kRho && sp < P.num_species) {
-                const float s1 = sx1[i + 2] * sy1;
-                atomicAdd(sRho + o, (double)(-weight * s1));
+            for (int b = 0; b < 3; ++b) {
+              const int j = jb + b;
+              const bool jv = b < njb;
+              const float sy0 = cic(-x2 + j + 1);
+              const float sy1 = cic(-nx2 + (j + 1 - dc2));
+              float djx = 0.0f;
+#pragma unroll
+              for (int a = 0; a < 3; ++a) {
+                if (jv && a < nib) {
+                  const int o = obase + b * G::JX + a;
+                  djx += movement2d(sy0, sy1, sx0[a], sx1[a]);
+                  add_fixed(J1, o + 1, weight * djx, fscale, fx.L);
+                  djy[a] += movement2d(sx0[a], sx1[a], sy0, sy1);
+                  add_fixed(J2, o + G::JX, weight * djy[a], fscale, fx.L);
+                  const float val2 = center2d(sx0[a], sx1[a], sy0, sy1);
+                  add_fixed(J3, o, -weight * v3 * val2, fscale, fx.L);
+                  if (rho) {
+                    const float s1 = sx1[a] * sy1;
+                    add_fixed(R, o, -weight * s1, fscale, fx.L);
+                  }
+                }
               }
             }
           }
+          // move + wrap through periodic sides (send_particles semantics)
+          int c1n = c1 + dc1, c2n = c2 + dc2;
+          bool keep = !far;
+          keep = keep && wrap_coord(c1n, g0, dims0, P.m.red[0], P.periodic[0]);
+          keep = keep && wrap_coord(c2n, g1, dims1, P.m.red[1], P.periodic[1]);
+          uint32_t ncell = AP_MAX_CELL;
+          if (keep) {
+            ncell = (uint32_t)(c1n + c2n * dims0);
+            int dtx = (c1n - g0) / TX - tix;
+            int dty = (c2n - g1) / TY - tiy;
+            if (dtx > 1) dtx = -1;
+            if (dtx < -1) dtx = 1;
+            if (dty > 1) dty = -1;
+            if (dty < -1) dty = 1;
+            dir = (uint32_t)((dty + 1) * 3 + (dtx + 1));
+          } else {
+            dir = kDirGone;
+            if (far)
+              atomicAdd(&P.status->moved_far, 1ull);
+            else
+              atomicAdd(&P.status->lost, 1ull);
+          }
+          s_x1[s] = nx1;
+          s_x2[s] = nx2;
+          s_x3[s] = nx3;
+          s_cell[s] = ncell;
+          mode = kWritePos;
+          if (em) {
+            s_p1[s] = p1;
+            s_p2[s] = p2;
+            s_p3[s] = p3;
+            s_w[s] = gamma;
+            mode |= kWriteMom;
+          }
         }
-        // move + wrap through periodic sides (send_particles semantics)
-        int c1n = c1 + dc1, c2n = c2 + dc2;
-        bool keep = !far;
-        keep = keep && wrap_coord(c1n, g0, dims0, P.m.red[0], P.periodic[0]);
-        keep = keep && wrap_coord(c2n, g1, dims1, P.m.red[1], P.periodic[1]);
-        uint32_t ncell = AP_MAX_CELL;
-        if (keep) {
-          ncell = (uint32_t)(c1n + c2n * dims0);
-          int dtx = (c1n - g0) / TX - tix;
-          int dty = (c2n - g1) / TY - tiy;
-          if (dtx > 1) dtx = -1;
-          if (dtx < -1) dtx = 1;
-          if (dty > 1) dty = -1;
-          if (dty < -1) dty = 1;
-          dir = (uint32_t)((dty + 1) * 3 + (dtx + 1));
-        } else {
-          dir = kDirGone;
-          if (far)
-            atomicAdd(&P.status->moved_far, 1ull);
-          else
-            atomicAdd(&P.status->lost, 1ull);
-        }
-        __stcs(P.p.x1 + idx, nx1);
-        __stcs(P.p.x2 + idx, nx2);
-        __stcs(P.p.x3 + idx, nx3);
-        if (em) {
-          __stcs(P.p.p1 + idx, p1);
-          __stcs(P.p.p2 + idx, p2);
-          __stcs(P.p.p3 + idx, p3);
-          __stcs(P.p.E + idx, gamma);
-        }
-        __stcs(P.p.cell + idx, ncell);
+        s_dir[s] = (uint8_t)dir;
+        s_mode[s] = mode;
+        const unsigned peers = __match_any_sync(__activemask(), dir);
+        if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[dir], (uint32_t)__popc(peers));
       }
-      P.dir[pos] = (uint8_t)dir;
-      const unsigned peers = __match_any_sync(__activemask(), dir);
-      if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[dir], (uint32_t)__popc(peers));
+      __syncthreads();
+      // 3c. coalesced write-back of the chunk
+#pragma unroll
+      for (int k = 0; k < PER_THREAD; ++k) {
+        const int e = tid + k * kThreads2D;
+        if (e < nch) {
+          const int s = spos(e);
+          const uint8_t mode = s_mode[s];
+          const uint32_t idx = s_idx[s];
+          if (mode & kWritePos) {
+            P.p.x1[idx] = s_x1[s];
+            P.p.x2[idx] = s_x2[s];
+            P.p.x3[idx] = s_x3[s];
+            P.p.cell[idx] = s_cell[s];
+          }
+          if (mode & kWriteMom) {
+            P.p.p1[idx] = s_p1[s];
+            P.p.p2[idx] = s_p2[s];
+            P.p.p3[idx] = s_p3[s];
+            P.p.E[idx] = s_w[s];
+          }
+          P.dir[base + c0 + e] = s_dir[s];
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
 
     // 4. flush the current (and charge) tile once
-    for (int i = tid; i < nzero; i += blockDim.x) {
-      const double v = sJ[i];
-      if (v == 0.0) continue;
+    for (int i = tid; i < nacc; i += kThreads2D) {
+      const long long v = (long long)sJhi[i] * (1ll << fx.L) + (long long)sJlo[i];
+      if (v == 0) continue;
       const int comp = i / G::JSZ, rem = i % G::JSZ;
       const int gx = jx0 + rem % G::JX, gy = jy0 + rem / G::JX;
       if (gx >= dims0 || gy >= dims1) continue;
-      atomicAdd(P.acc + comp * P.acc_comp + (size_t)gy * P.acc_pitch + gx, v);
+      atomicAdd(P.acc + comp * P.acc_comp + (size_t)gy * P.acc_pitch + gx,
+                (unsigned long long)v);
     }
     if (tid < 10) P.dir_count[t * 10 + tid] = s_cnt[tid];
     phase ^= 1u;
@@ -320,13 +449,14 @@ __global__ void __launch_bounds__(kThreads2D)
 // ---------------------------------------------------------------------------
 // 1D: the whole line is small, so each CTA takes a contiguous chunk of
 // particle slots, finds the cell range it touches, and deposits into a
-// shared-memory window over that range (or straight to global memory when
-// the window would not fit). Fields are read through the read-only cache.
+// shared-memory window over that range (or straight to the global
+// accumulators when the window would not fit). Fields are read through the
+// read-only cache.
 
 constexpr int kThreads1D = 256;
 constexpr int kItems1D = 8;
-constexpr int kChunk1D = kThreads1D * kItems1D;
-constexpr int kWinDoubles1D = 6000;  // shared window, all components
+constexpr int kChunk1D = kThreads1D * kItems1D;  // 2048 particles
+constexpr int kWin1D = 6000;                     // cell-components per window
 
 __device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weights1D &W, int c1,
                                                   int stag) {
@@ -342,13 +472,21 @@ __device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weigh
 template <bool kRho>
 __global__ void __launch_bounds__(kThreads1D)
     k_push_deposit_1d(const __grid_constant__ PushDepositParams P) {
-  __shared__ double sW[kWinDoubles1D];
+  __shared__ int sWhi[kWin1D];
+  __shared__ unsigned sWlo[kWin1D];
   __shared__ int s_lo, s_hi;
   const int tid = threadIdx.x;
   const int n0 = P.m.dims[0], g0 = P.m.guard[0];
   const int ncomp = 3 + (kRho ? P.num_species : 0);
-  const int win_comp = kWinDoubles1D / ncomp;
+  const int win_comp = kWin1D / ncomp;
   const size_t nchunks = (P.number + kChunk1D - 1) / kChunk1D;
+  // A window sums at most kChunk1D contributions per cell; the global
+  // accumulators at most `number`.
+  const int lgw = bits_of(kChunk1D);
+  const int lgn = bits_of((uint32_t)min(P.number, (size_t)0x7fffffff));
+  const FixedFmt fx = fixed_format(lgw, min(63 - 2 * lgw, 62 - lgn), P.qmax * *P.wmax);
+  const float fscale = ldexpf(1.0f, fx.S);
+  if (blockIdx.x == 0 && tid == 0) *P.fx_used = fx;
 
   for (size_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const size_t first = ch * kChunk1D;
@@ -381,7 +519,10 @@ __global__ void __launch_bounds__(kThreads1D)
     const int wlen = s_hi - s_lo + 5;
     const bool use_smem = (s_lo <= s_hi) && wlen <= win_comp;
     if (use_smem)
-      for (int i = tid; i < ncomp * win_comp; i += kThreads1D) sW[i] = 0.0;
+      for (int i = tid; i < ncomp * win_comp; i += kThreads1D) {
+        sWhi[i] = 0;
+        sWlo[i] = 0u;
+      }
     __syncthreads();
 
 #pragma unroll 1
@@ -447,17 +588,21 @@ __global__ void __launch_bounds__(kThreads1D)
           const float a2 = weight * v2 * val1;
           const float a3 = weight * v3 * val1;
           if (use_smem) {
-            atomicAdd(&sW[off + 1 - wlo], (double)a1);
-            atomicAdd(&sW[win_comp + off - wlo], (double)a2);
-            atomicAdd(&sW[2 * win_comp + off - wlo], (double)a3);
+            const Acc32 W{sWhi, sWlo};
+            add_fixed(W, off + 1 - wlo, a1, fscale, fx.L);
+            add_fixed(W, win_comp + off - wlo, a2, fscale, fx.L);
+            add_fixed(W, 2 * win_comp + off - wlo, a3, fscale, fx.L);
             if (kRho && sp < P.num_species)
-              atomicAdd(&sW[(3 + sp) * win_comp + off - wlo], (double)(weight * sx1));
+              add_fixed(W, (3 + sp) * win_comp + off - wlo, weight * sx1, fscale, fx.L);
           } else {
-            atomicAdd(P.acc + off + 1, (double)a1);
-            atomicAdd(P.acc + P.acc_comp + off, (double)a2);
-            atomicAdd(P.acc + 2 * P.acc_comp + off, (double)a3);
-            if (kRho && sp < P.num_species)
-              atomicAdd(P.acc + (3 + sp) * P.acc_comp + off, (double)(weight * sx1));
+            auto gadd = [&](int k2, int x, float v) {
+              atomicAdd(P.acc + k2 * P.acc_comp + x,
+                        (unsigned long long)__float2ll_rn(v * fscale));
+            };
+            gadd(0, off + 1, a1);
+            gadd(1, off, a2);
+            gadd(2, off, a3);
+            if (kRho && sp < P.num_species) gadd(3 + sp, off, weight * sx1);
           }
         }
       }
@@ -470,20 +615,21 @@ __global__ void __launch_bounds__(kThreads1D)
     if (use_smem) {
       for (int i = tid; i < ncomp * wlen; i += kThreads1D) {
         const int comp = i / wlen, o = i % wlen;
-        const double v = sW[comp * win_comp + o];
-        if (v == 0.0) continue;
+        const int si = comp * win_comp + o;
+        const long long v = (long long)sWhi[si] * (1ll << fx.L) + (long long)sWlo[si];
+        if (v == 0) continue;
         const int gx = wlo + o;
         if (gx < 0 || gx >= n0) continue;
-        atomicAdd(P.acc + comp * P.acc_comp + gx, v);
+        atomicAdd(P.acc + comp * P.acc_comp + gx, (unsigned long long)v);
       }
     }
     __syncthreads();
   }
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int CH, int MINB>
 cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
-  using G = TileGeom<TX, TY>;
+  using G = TileGeom<TX, TY, CH>;
   const int nrho = P.do_rho ? P.num_species : 0;
   const size_t smem = G::smem_bytes(nrho);
   cudaError_t e = cudaMemsetAsync(P.queue, 0, sizeof(uint32_t), c.stream);
@@ -495,7 +641,7 @@ cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
     int per_sm = 0;
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads2D, smem);
     if (err != cudaSuccess) return err;
-    if (per_sm < 1) per_sm = 1;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = c.num_sms * per_sm;
     if (grid > P.t.ntiles) grid = P.t.ntiles;
     if (grid < 1) grid = 1;
@@ -504,23 +650,55 @@ cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
     return cudaGetLastError();
   };
   if (c.use_tma) {
-    return P.do_rho ? run(k_push_deposit_2d<TX, TY, true, true>)
-                    : run(k_push_deposit_2d<TX, TY, true, false>);
+    return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, true, true>)
+                    : run(k_push_deposit_2d<TX, TY, CH, MINB, true, false>);
   }
-  return P.do_rho ? run(k_push_deposit_2d<TX, TY, false, true>)
-                  : run(k_push_deposit_2d<TX, TY, false, false>);
+  return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, false, true>)
+                  : run(k_push_deposit_2d<TX, TY, CH, MINB, false, false>);
+}
+
+// Staged chunk of 2048 particles with two CTAs per SM, or 1024 with three.
+template <int TX, int TY>
+cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
+  if (c.params.chunk == 1024) return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
+  return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
+}
+
+// Largest |weight| over slots [0, n) (non-negative floats order like their
+// bit patterns).
+__global__ void k_weight_max(const float *w, const uint32_t *cell, size_t n, float *out) {
+  float mx = 0.0f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (cell[i] != AP_MAX_CELL) mx = fmaxf(mx, fabsf(w[i]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(reinterpret_cast<unsigned int *>(out), __float_as_uint(mx));
 }
 
 }  // namespace
 
+// Recomputes the largest particle weight (after the caller changed particles).
+cudaError_t launch_fixed_scale(Ctx &c) {
+  cudaError_t e = cudaMemsetAsync(c.wmax, 0, sizeof(float), c.stream);
+  if (e != cudaSuccess) return e;
+  if (c.number > 0) {
+    size_t g = (c.number + 255) / 256;
+    if (g > (size_t)c.num_sms * 8) g = (size_t)c.num_sms * 8;
+    k_weight_max<<<(int)g, 256, 0, c.stream>>>(c.ptc.weight, c.ptc.cell, c.number, c.wmax);
+    c.launches++;
+  }
+  c.scale_valid = true;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P) {
   const int tx = P.t.tx, ty = P.t.ty;
-  if (tx == 16 && ty == 16) return launch_2d_tiles<16, 16>(c, P);
-  if (tx == 32 && ty == 16) return launch_2d_tiles<32, 16>(c, P);
-  if (tx == 32 && ty == 32) return launch_2d_tiles<32, 32>(c, P);
-  if (tx == 8 && ty == 8) return launch_2d_tiles<8, 8>(c, P);
-  if (tx == 16 && ty == 8) return launch_2d_tiles<16, 8>(c, P);
-  if (tx == 4 && ty == 4) return launch_2d_tiles<4, 4>(c, P);
+  if (tx == 16 && ty == 16) return launch_2d_chunk<16, 16>(c, P);
+  if (tx == 32 && ty == 16) return launch_2d_chunk<32, 16>(c, P);
+  if (tx == 8 && ty == 8) return launch_2d_chunk<8, 8>(c, P);
+  if (tx == 16 && ty == 8) return launch_2d_chunk<16, 8>(c, P);
+  if (tx == 4 && ty == 4) return launch_2d_chunk<4, 4>(c, P);
   return cudaErrorInvalidValue;
 }
 

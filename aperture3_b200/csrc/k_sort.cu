@@ -84,20 +84,26 @@ __device__ __forceinline__ int gather_sources(const TileTopo &T, const uint32_t 
 
 __global__ void __launch_bounds__(kScanThreads)
     k_tile_scan(TileTopo T, const uint32_t *__restrict__ cnt, uint32_t *__restrict__ new_start,
-                uint32_t *__restrict__ grp_off) {
+                uint32_t *__restrict__ grp_off, uint32_t *__restrict__ n_max) {
   __shared__ uint32_t s_part[kScanThreads];
+  __shared__ uint32_t s_max;
+  if (threadIdx.x == 0) s_max = 0;
   const int tid = threadIdx.x;
   const int per = (T.ntiles + kScanThreads - 1) / kScanThreads;
   const int u0 = tid * per, u1 = min(T.ntiles, u0 + per);
   int src[9], dirv[9];
   uint32_t num[9];
-  uint32_t local = 0;
+  uint32_t local = 0, mx = 0;
   for (int u = u0; u < u1; ++u) {
     const int n = gather_sources(T, cnt, u, src, dirv, num);
-    for (int k = 0; k < n; ++k) local += num[k];
+    uint32_t nu = 0;
+    for (int k = 0; k < n; ++k) nu += num[k];
+    local += nu;
+    mx = max(mx, nu);
   }
   s_part[tid] = local;
   __syncthreads();
+  atomicMax(&s_max, mx);
   // inclusive Hillis-Steele scan over the per-thread sums
   for (int off = 1; off < kScanThreads; off <<= 1) {
     uint32_t v = tid >= off ? s_part[tid - off] : 0u;
@@ -115,6 +121,8 @@ __global__ void __launch_bounds__(kScanThreads)
     }
   }
   if (tid == kScanThreads - 1) new_start[T.ntiles] = s_part[tid];
+  __syncthreads();
+  if (tid == 0) *n_max = s_max;
 }
 
 // One CTA per source tile: stable rank within each direction group.
@@ -199,15 +207,21 @@ __global__ void k_histogram(const uint32_t *keys, size_t n, uint32_t nbins, uint
 
 // Exclusive scan of nbins counters into start[0..nbins] with one CTA.
 __global__ void __launch_bounds__(kScanThreads)
-    k_scan_counts(const uint32_t *counts, int nbins, uint32_t *start) {
+    k_scan_counts(const uint32_t *counts, int nbins, uint32_t *start, uint32_t *n_max) {
   __shared__ uint32_t s_part[kScanThreads];
+  __shared__ uint32_t s_max;
   const int tid = threadIdx.x;
+  if (tid == 0) s_max = 0;
   const int per = (nbins + kScanThreads - 1) / kScanThreads;
   const int b0 = tid * per, b1 = min(nbins, b0 + per);
-  uint32_t local = 0;
-  for (int b = b0; b < b1; ++b) local += counts[b];
+  uint32_t local = 0, mx = 0;
+  for (int b = b0; b < b1; ++b) {
+    local += counts[b];
+    mx = max(mx, counts[b]);
+  }
   s_part[tid] = local;
   __syncthreads();
+  atomicMax(&s_max, mx);
   for (int off = 1; off < kScanThreads; off <<= 1) {
     uint32_t v = tid >= off ? s_part[tid - off] : 0u;
     __syncthreads();
@@ -220,6 +234,8 @@ __global__ void __launch_bounds__(kScanThreads)
     run += counts[b];
   }
   if (tid == kScanThreads - 1) start[nbins] = s_part[tid];
+  __syncthreads();
+  if (tid == 0 && n_max) *n_max = s_max;
 }
 
 __global__ void k_count_below(const uint32_t *keys, size_t n, uint32_t bound, uint32_t *count) {
@@ -283,7 +299,7 @@ cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count, uint32_t *new_st
                              uint32_t *grp_off) {
   TileTopo T{c.tiles.ntx, c.tiles.nty, c.tiles.ntiles, c.params.periodic[0],
              c.params.periodic[1]};
-  k_tile_scan<<<1, kScanThreads, 0, c.stream>>>(T, dir_count, new_start, grp_off);
+  k_tile_scan<<<1, kScanThreads, 0, c.stream>>>(T, dir_count, new_start, grp_off, c.n_max);
   c.launches++;
   return cudaGetLastError();
 }
@@ -350,7 +366,7 @@ cudaError_t rebuild_tile_order(Ctx &c) {
     k_histogram<<<grid_for(c, n, 256), 256, 0, c.stream>>>(ko, n, nt, c.dir_count);
     c.launches++;
   }
-  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, (int)nt, start);
+  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, (int)nt, start, c.n_max);
   c.launches++;
   c.order_valid = true;
   return cudaGetLastError();

@@ -57,6 +57,7 @@ class SimParams:
     B0: float = 1.0
     max_steps: int = 0
     tile_size: Sequence[int] = (0, 0, 0)
+    chunk: int = 0
 
     @classmethod
     def from_toml(cls, path: str) -> "SimParams":
@@ -106,6 +107,7 @@ class SimEnvironment:
             ap.masses[i] = self.masses[i]
         ts = _pad3(params.tile_size, 0)
         ap.tile[0], ap.tile[1] = int(ts[0]), int(ts[1])
+        ap.chunk = int(params.chunk)
         self.ap_params = ap
         self._lib = _lib.lib()
         ctx = C.c_void_p()
@@ -251,6 +253,27 @@ class SimData:
             self.particles[name][:n].copy_(t)
         self.number = n
         self.particles_modified()
+
+    def set_particles_device(self, ptc: Dict[str, torch.Tensor]):
+        """Copies device SoA tensors (any integer dtype for cell/id/flag) into
+        slots [0, n) and marks the tile order for rebuild."""
+        n = ptc["x1"].numel()
+        if n > self.capacity:
+            raise _lib.ApError(5, "set_particles_device")
+        for name, dt in PTC_FIELDS:
+            src = ptc[name]
+            if dt == torch.int32 and src.dtype != torch.int32:
+                src = (src.to(torch.int64) & 0xFFFFFFFF)
+                src = torch.where(src >= 2 ** 31, src - 2 ** 32, src).to(torch.int32)
+            self.particles[name][:n].copy_(src)
+        self.number = n
+        self.particles_modified()
+
+    def set_fields_device(self, fields: Dict[str, List[torch.Tensor]]):
+        for key in ("E", "B", "Ebg", "Bbg", "J"):
+            if key in fields:
+                for c in range(3):
+                    getattr(self, key)[c].copy_(fields[key][c])
 
     def particles_modified(self, number: Optional[int] = None):
         if number is not None:

@@ -1,0 +1,485 @@
+#!/usr/bin/env python
+"""Benchmark of the Aperture3 particle update on B200.
+
+Workload (one step = the reference lab's loop body, labs/box/src/main.cpp:
+81-91): ptc_updater::update_particles (Vay push + Esirkepov deposit + move,
+tile counting sort, current fold) and field_solver::update_fields (Yee
+FDTD), plus sort_particles every sort_interval (20) steps, on the 2D
+Cartesian box: 1024 x 1024 cells, 64 particles per cell (67,108,864), seeded
+synthetic initial state (aperture3_b200.ic.box2d). The particle SoA
+(3.2 GB) is far larger than L2 (126 MB), so no L2 flush is needed between
+steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (launched with torch.distributed.run): every rank runs its own box
+(replicas: the single-GPU path has no cross-GPU exchange); value is the
+particle-steps of all ranks over the slowest rank's device time.
+--impl reference times the CPU path (the reference's own kernels compiled
+for the host when available, else the C restatement) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (push+deposit)"
+UNIT = "particle-steps/s"
+ALG_BYTES_PER_PARTICLE = 68  # 36 B read + 32 B written per particle-step
+ALG_BYTES_PER_CELL = 36      # 6 field reads + 3 current writes, 4 B each
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=1024)
+    ap.add_argument("--ppc", type=int, default=64)
+    ap.add_argument("--tile", type=int, nargs=2, default=(16, 16))
+    ap.add_argument("--sort-interval", type=int, default=20)
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds of CPU work for the cpu_baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds for the whole --impl reference run")
+    return ap.parse_args()
+
+
+def workload_config(args, tile):
+    n = args.N * args.N * args.ppc
+    return {
+        "workload": (f"2D Cartesian periodic box {args.N}x{args.N}, {args.ppc} ppc "
+                     f"({n} particles, e-/e+ pairs, gamma log-uniform in [1,1e3]), "
+                     "B3=1 + 8 Fourier modes in E and B; per step Vay push + Esirkepov "
+                     "deposit + tile counting sort + Yee FDTD, sort_by_cell every "
+                     f"{args.sort_interval} steps"),
+        "grid": [args.N, args.N], "ppc": args.ppc, "particles": n,
+        "tile": list(tile), "sort_interval": args.sort_interval,
+        "l2": "inputs larger than L2 (particle SoA 48 B x N_p)",
+    }
+
+
+# --------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.proc = None
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            sel = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", sel, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self, t0, t1):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        ts = time.mktime(time.strptime(parts[0].split(".")[0],
+                                                       "%Y/%m/%d %H:%M:%S"))
+                        frac = float("0." + parts[0].split(".")[1]) if "." in parts[0] else 0.0
+                        rows.append((ts + frac, float(parts[1]), float(parts[2]), parts[5:9]))
+                    except Exception:
+                        continue
+        except Exception:
+            return None
+        if not rows:
+            return None
+        inside = [r for r in rows if t0 - 0.15 <= r[0] <= t1 + 0.15]
+        if not inside:
+            inside = sorted(rows, key=lambda r: abs(r[0] - 0.5 * (t0 + t1)))[:3]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in inside for i, v in enumerate(r[3])
+                          if v.lower() in ("active", "1")})
+        return {"sm_mhz": statistics.median(r[1] for r in inside),
+                "sm_max_mhz": max(r[2] for r in inside), "reasons": reasons,
+                "samples": len(inside)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per particle of the fused kernel from the committed ncu
+    summary (line 'dram_bytes_per_particle: X'), or None."""
+    path = os.path.join(ROOT, "profiles", "k_push_deposit_2d_box.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_particle:"):
+                    return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------
+# CPU path (baseline leg and reference arm)
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class CpuBox:
+    """The same step on the host: the reference's own push/deposit/FDTD
+    kernels compiled for the host (oracle/_ref) when present, else the C
+    restatement (oracle/liboracle.so), with all host threads."""
+
+    def __init__(self, params, fields_np, ptc_np, threads):
+        import numpy as np
+        import oracle
+        self.o = oracle
+        self.np = np
+        self.m = oracle.make_mesh(params.N, params.guard, params.lower, params.size)
+        self.f = oracle.new_fields(self.m, params.num_species)
+        for c in range(3):
+            self.f["E"][c][:] = fields_np["E"][c]
+            self.f["B"][c][:] = fields_np["B"][c]
+        self.p = ptc_np
+        self.n = len(ptc_np["x1"])
+        self.params = params
+        self.threads = threads
+        q = 1.0
+        self.charges = [-q] + [q] * 7
+        self.masses = [q] * 8
+        self.periodic = [1, 1, 0]
+        self.kind = "port"
+
+    def step(self, step):
+        self.o.update_particles(self.m, self.p, self.n, self.f, self.params.delta_t, step,
+                                self.params.data_interval, 2, 0, self.charges, self.masses,
+                                self.periodic, self.threads)
+        self.o.update_fields(self.m, self.f, self.params.delta_t, step, self.periodic)
+        if step % 20 == 0 and step != 0:
+            self.n = self.o.sort_by_cell(self.m, self.p, self.n)
+
+
+def cpu_sample(args, ppc_sample, seed=1):
+    from aperture3_b200 import ic
+    params, fields, ptc = ic.box2d(seed=seed, N=args.N, ppc=ppc_sample, device="cpu")
+    fields_np = {"E": [f.numpy() for f in fields["E"]], "B": [f.numpy() for f in fields["B"]]}
+    return params, fields_np, ic.to_numpy_ptc(ptc)
+
+
+def time_cpu(args, budget_s, min_steps=1, max_steps=None):
+    """Runs the CPU step on a sample of the workload sized to budget_s.
+    Returns (particle-steps/s, threads, sample description, steps)."""
+    threads = cpu_threads()
+    # calibrate on 1 ppc
+    params, f, p = cpu_sample(args, 2)
+    box = CpuBox(params, f, p, threads)
+    t = time.perf_counter()
+    box.step(1)
+    dt1 = time.perf_counter() - t
+    per_particle = dt1 / box.n
+    steps = max(min_steps, 1)
+    ppc = 2
+    while ppc * 2 <= args.ppc and per_particle * args.N * args.N * ppc * 2 * steps <= budget_s:
+        ppc *= 2
+    params, f, p = cpu_sample(args, ppc)
+    box = CpuBox(params, f, p, threads)
+    nsteps = steps if max_steps is None else max_steps
+    box.step(0)  # warm-up (includes the half step of E)
+    t = time.perf_counter()
+    for s in range(1, nsteps + 1):
+        box.step(s)
+    el = time.perf_counter() - t
+    rate = box.n * nsteps / el
+    desc = (f"{args.N}x{args.N} grid, {ppc} ppc ({box.n} particles), {nsteps} step(s) after "
+            f"1 warm-up, {threads} threads ({box.kind})")
+    return rate, threads, desc, box.kind
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = cpu_threads()
+    params, f, p = cpu_sample(args, 2)
+    box = CpuBox(params, f, p, threads)
+    t = time.perf_counter()
+    box.step(1)
+    per_particle = (time.perf_counter() - t) / box.n
+    total_steps = args.steps + args.warmup
+    ppc = 2
+    while ppc * 2 <= args.ppc and per_particle * args.N * args.N * ppc * 2 * total_steps <= args.ref_budget:
+        ppc *= 2
+    params, f, p = cpu_sample(args, ppc)
+    box = CpuBox(params, f, p, threads)
+    for s in range(args.warmup):
+        box.step(s)
+    t = time.perf_counter()
+    for s in range(args.warmup, args.warmup + args.steps):
+        box.step(s)
+    el = time.perf_counter() - t
+    value = box.n * args.steps / el
+    sample = (f"{args.N}x{args.N} grid, {ppc} ppc ({box.n} particles) of the {args.ppc}-ppc "
+              f"workload, {args.steps} timed steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)", "config": workload_config(args, (0, 0)),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": box.kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU path
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from aperture3_b200 import SimData, SimEnvironment, field_solver, ic, ptc_updater
+    from aperture3_b200._lib import ApPhaseTimes, check
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    params, fields, ptc = ic.box2d(seed=1000 + rank, N=args.N, ppc=args.ppc, device=dev,
+                                   tile=tuple(args.tile))
+    params.chunk = args.chunk
+    n = ptc["x1"].numel()
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=n)
+    data.set_fields_device(fields)
+    data.set_particles_device(ptc)
+    del ptc
+    torch.cuda.empty_cache()
+    stream = torch.cuda.Stream()
+    env.set_stream(stream)
+    env.set_sync(False)
+    pusher, solver = ptc_updater(env), field_solver(env)
+    dt = params.delta_t
+    lib = env._lib
+
+    def one_step(s):
+        pusher.update_particles(data, dt, s)
+        solver.update_fields(data, dt, s)
+        if s % args.sort_interval == 0 and s != 0:
+            data.sort_particles()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sampler = ClockSampler(local_rank)
+    with torch.cuda.stream(stream):
+        for s in range(args.warmup):
+            one_step(s)
+        env.sync()
+        check(lib.ap_set_profiling(env.ctx, 1), "profiling")
+        check(lib.ap_get_phase_times(env.ctx, ApPhaseTimes(), 1), "reset")
+        launches0 = env.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        t_wall0 = time.time()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(args.warmup, args.warmup + args.steps):
+            one_step(s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_wall1 = time.time()
+        barrier()
+        env.sync()  # raises on a device-reported error
+    ms = e0.elapsed_time(e1)
+    launches = env.launch_count() - launches0
+    pt = ApPhaseTimes()
+    check(lib.ap_get_phase_times(env.ctx, pt, 1), "phase times")
+    check(lib.ap_set_profiling(env.ctx, 0), "profiling off")
+    sampler.stop()
+    clocks = sampler.summary(t_wall0, t_wall1)
+
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = n * args.steps * world / (ms_max / 1e3)
+
+    # roofline of the fused push/deposit kernel
+    G = (args.N + 4) * (args.N + 4)
+    alg_bytes = ALG_BYTES_PER_PARTICLE * n + ALG_BYTES_PER_CELL * G
+    k_ms = pt.push_deposit_ms / max(pt.push_deposit_launches, 1)
+    achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    tpp = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tpp * n if tpp is not None else None),
+                "kernel": "k_push_deposit_2d", "kernel_ms": k_ms,
+                "phases_ms_per_step": {
+                    "push_deposit": pt.push_deposit_ms / args.steps,
+                    "tile_sort": pt.order_ms / args.steps,
+                    "rebuild": pt.rebuild_ms / args.steps,
+                    "finalize": pt.finalize_ms / args.steps,
+                    "fields": pt.fields_ms / args.steps,
+                    "sort_by_cell": pt.sort_ms / args.steps}}
+
+    # e2e through the C ABI with host buffers: upload the run's initial state
+    # from pinned host memory, run the steps, read the FP64 diagnostics back
+    # every step, download the final particles and fields.
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, env, data, pusher, solver, dt, stream, n)
+    if world > 1 and e2e is not None:
+        t = torch.tensor([e2e["ms"]], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = n * args.steps * world / (float(t.item()) / 1e3)
+    if e2e is not None:
+        e2e.pop("ms")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, threads, desc, kind = time_cpu(args, args.cpu_budget)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded initial state, aperture3_b200.ic.box2d)",
+        "config": dict(workload_config(args, (env.ap_params.tile[0] or 16,
+                                              env.ap_params.tile[1] or 16)),
+                       parallelism=("replicas" if world > 1 else "single")),
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    env.close()
+
+
+def run_e2e(args, env, data, pusher, solver, dt, stream, n):
+    import torch
+    from aperture3_b200._lib import ApDiag, check
+    from aperture3_b200.sim import PTC_FIELDS
+
+    names = [k for k, _ in PTC_FIELDS]
+    host = {k: torch.empty_like(data.particles[k][:n], device="cpu").pin_memory() for k in names}
+    fhost = {k: [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in getattr(data, k)]
+             for k in ("E", "B", "J")}
+    with torch.cuda.stream(stream):
+        for k in names:
+            host[k].copy_(data.particles[k][:n], non_blocking=True)
+        for k in fhost:
+            for h, a in zip(fhost[k], getattr(data, k)):
+                h.copy_(a, non_blocking=True)
+    torch.cuda.synchronize()
+    h2d = sum(t.numel() * t.element_size() for t in host.values()) + \
+        sum(t.numel() * t.element_size() for k in ("E", "B") for t in fhost[k])
+    d2h = sum(t.numel() * t.element_size() for t in host.values()) + \
+        sum(t.numel() * t.element_size() for v in fhost.values() for t in v)
+    diag = ApDiag()
+    d2h_diag = 48
+    lib = env._lib
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for k in names:
+            data.particles[k][:n].copy_(host[k], non_blocking=True)
+        for k in ("E", "B"):
+            for h, a in zip(fhost[k], getattr(data, k)):
+                a.copy_(h, non_blocking=True)
+        data.particles_modified(n)
+        for s in range(args.steps):
+            pusher.update_particles(data, dt, s)
+            solver.update_fields(data, dt, s)
+            if s % args.sort_interval == 0 and s != 0:
+                data.sort_particles()
+            check(lib.ap_diagnostics(env.ctx, diag), "ap_diagnostics")
+        for k in names:
+            host[k].copy_(data.particles[k][:n], non_blocking=True)
+        for k in fhost:
+            for h, a in zip(fhost[k], getattr(data, k)):
+                h.copy_(a, non_blocking=True)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    env.sync()
+    ms = e0.elapsed_time(e1)
+    return {"value": n * args.steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps,
+            "d2h_bytes_per_step": d2h / args.steps + d2h_diag, "ms": ms,
+            "includes": "initial-state upload, all steps with a per-step FP64 diagnostics "
+                        "readback, final particle and field download"}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -73,6 +73,8 @@ typedef struct {
   float charges[AP_MAX_SPECIES];
   float masses[AP_MAX_SPECIES];
   int tile[2];               /* sort tile in cells; 0 picks a default       */
+  int chunk;                 /* particles staged per pass in the 2D kernel:
+                                1024 or 2048; 0 picks a default             */
 } ap_params;
 
 typedef struct {
@@ -195,6 +197,24 @@ AP_API int ap_get_stats(ap_ctx *ctx, ap_step_stats *stats);
 /* FP64 energy / charge / Gauss-law diagnostics (new; the reference only
  * computes per-particle gamma, cuda/core/particles.cu:10-22). */
 AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
+
+/* Device time per phase of the update, from CUDA events recorded on the
+ * context's stream around each phase while profiling is on. */
+typedef struct {
+  double push_deposit_ms; /* fused push + deposit kernel                  */
+  double order_ms;        /* per-step tile counting sort (scan + scatter) */
+  double rebuild_ms;      /* full tile-order rebuild                      */
+  double finalize_ms;     /* current/charge zeroing, fold and rounding    */
+  double fields_ms;       /* Yee update of E and B and divergences        */
+  double sort_ms;         /* sort_by_cell                                 */
+  uint64_t push_deposit_launches;
+} ap_phase_times;
+
+/* Turns per-phase event timing on (1) or off (0); new for measurement. */
+AP_API int ap_set_profiling(ap_ctx *ctx, int on);
+/* Sums the recorded phase times (waits for the stream); reset != 0 clears
+ * them afterwards. */
+AP_API int ap_get_phase_times(ap_ctx *ctx, ap_phase_times *out, int reset);
 
 /* Status of the last failing call on this context. */
 AP_API int ap_last_error(const ap_ctx *ctx);

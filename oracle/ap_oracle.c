@@ -550,6 +550,7 @@ void or_update_e_2d(const or_mesh *m, or_fields *f, float dt) {
   const float *b01 = f->Bbg[0], *b02 = f->Bbg[1], *b03 = f->Bbg[2];
   const float *j1 = f->J[0], *j2 = f->J[1], *j3 = f->J[2];
   const float id0 = m->inv_delta[0], id1 = m->inv_delta[1];
+#pragma omp parallel for schedule(static)
   for (int n2 = m->guard[1]; n2 < m->dims[1] - m->guard[1]; n2++)
     for (int n1 = m->guard[0]; n1 < m->dims[0] - m->guard[0]; n1++) {
       AT(e1, n1, n2) +=
@@ -580,6 +581,7 @@ void or_update_b_2d(const or_mesh *m, or_fields *f, float dt) {
   const float *e01 = f->Ebg[0], *e02 = f->Ebg[1], *e03 = f->Ebg[2];
   float *b1 = f->B[0], *b2 = f->B[1], *b3 = f->B[2];
   const float id0 = m->inv_delta[0], id1 = m->inv_delta[1];
+#pragma omp parallel for schedule(static)
   for (int n2 = m->guard[1]; n2 < m->dims[1] - m->guard[1]; n2++)
     for (int n1 = m->guard[0]; n1 < m->dims[0] - m->guard[0]; n1++) {
       AT(b1, n1, n2) -= dt *
@@ -608,6 +610,7 @@ void or_compute_divs_2d(const or_mesh *m, or_fields *f) {
   const float *b1 = f->B[0], *b2 = f->B[1];
   const float *b01 = f->Bbg[0], *b02 = f->Bbg[1];
   const float id0 = m->inv_delta[0], id1 = m->inv_delta[1];
+#pragma omp parallel for schedule(static)
   for (int n2 = m->guard[1]; n2 < m->dims[1] - m->guard[1]; n2++)
     for (int n1 = m->guard[0]; n1 < m->dims[0] - m->guard[0]; n1++) {
       AT(f->divE, n1, n2) =
