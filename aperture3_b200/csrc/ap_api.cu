@@ -257,6 +257,7 @@ AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params, ap_ctx **
             cudaMallocHost(&c->status_host, sizeof(DevStatus)) == cudaSuccess &&
             cudaMalloc(&c->dir_count, sizeof(uint32_t) * ((size_t)nt * 10 + 16)) == cudaSuccess &&
             cudaMalloc(&c->grp_off, sizeof(uint32_t) * ((size_t)nt * 9 + 16)) == cudaSuccess &&
+            cudaMalloc(&c->newcount, sizeof(uint32_t) * ((size_t)nt + 16)) == cudaSuccess &&
             cudaMalloc(&c->tile_start[0], sizeof(uint32_t) * (nt + 1)) == cudaSuccess &&
             cudaMalloc(&c->tile_start[1], sizeof(uint32_t) * (nt + 1)) == cudaSuccess &&
             cudaMalloc(&c->queue, sizeof(uint32_t) * 4) == cudaSuccess &&
@@ -290,9 +291,11 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->dir);
   cudaFree(c->dir_count);
   cudaFree(c->grp_off);
+  cudaFree(c->newcount);
   cudaFree(c->queue);
   cudaFree(c->cub_tmp);
   cudaFree(c->gather_tmp);
+  cudaFree(c->cell_start);
   cudaFree(c->tmp_j);
   cudaFree(c->acc);
   cudaFree(c->fx_used);
@@ -564,10 +567,10 @@ AP_API int ap_sort_by_cell(ap_ctx *c) {
   if (!c || !c->ptc_bound) return AP_ERR_INVALID;
   size_t n = 0;
   const int ph = phase_begin(c, kPhSort);
+  c->order_valid = false;  // sort_by_cell rebuilds the 2D tile order
   AP_TRY(sort_by_cell(*c, &n));
   phase_end(c, ph);
   c->number = n;
-  c->order_valid = false;
   return AP_OK;
 }
 

@@ -129,6 +129,7 @@ struct Ctx {
   uint8_t *dir = nullptr;
   uint32_t *dir_count = nullptr;
   uint32_t *grp_off = nullptr;
+  uint32_t *newcount = nullptr;  // per-tile population after the step
   uint32_t *queue = nullptr;
   size_t order_cap = 0;
 
@@ -139,6 +140,7 @@ struct Ctx {
   size_t cub_tmp_bytes = 0;
   void *gather_tmp = nullptr;
   size_t scratch_cap = 0;
+  uint32_t *cell_start = nullptr;  // ncells + 1 entries, set by sort_by_cell
 
   // fixed-point current / charge accumulators (3 + num_species components)
   unsigned long long *acc = nullptr;

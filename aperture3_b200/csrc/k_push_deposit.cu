@@ -89,6 +89,17 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// 4-byte asynchronous global -> shared copy (no register round trip).
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)),
+               "l"(gmem_src)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Bits needed to represent n (ceil(log2(n + 1))).
 __device__ __forceinline__ int bits_of(uint32_t n) { return 32 - __clz(n); }
 
@@ -232,7 +243,7 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
     const int n_t = (int)(P.tile_start[t + 1] - base);
     for (int c0 = 0; c0 < n_t; c0 += CH) {
       const int nch = min(CH, n_t - c0);
-      // 3a. coalesced load of the chunk
+      // 3a. coalesced asynchronous load of the chunk
 #pragma unroll
       for (int k = 0; k < PER_THREAD; ++k) {
         const int e = tid + k * kThreads2D;
@@ -240,17 +251,18 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
           const int s = spos(e);
           const uint32_t idx = P.order[base + c0 + e];
           s_idx[s] = idx;
-          s_cell[s] = P.p.cell[idx];
-          s_flag[s] = P.p.flag[idx];
-          s_x1[s] = P.p.x1[idx];
-          s_x2[s] = P.p.x2[idx];
-          s_x3[s] = P.p.x3[idx];
-          s_p1[s] = P.p.p1[idx];
-          s_p2[s] = P.p.p2[idx];
-          s_p3[s] = P.p.p3[idx];
-          s_w[s] = P.p.w[idx];
+          cp_async4(s_cell + s, P.p.cell + idx);
+          cp_async4(s_flag + s, P.p.flag + idx);
+          cp_async4(s_x1 + s, P.p.x1 + idx);
+          cp_async4(s_x2 + s, P.p.x2 + idx);
+          cp_async4(s_x3 + s, P.p.x3 + idx);
+          cp_async4(s_p1 + s, P.p.p1 + idx);
+          cp_async4(s_p2 + s, P.p.p2 + idx);
+          cp_async4(s_p3 + s, P.p.p3 + idx);
+          cp_async4(s_w + s, P.p.w + idx);
         }
       }
+      cp_async_wait_all();
       __syncthreads();
       // 3b. push + deposit: lane l of warp w takes element l*CH/32 + w*PER_THREAD + k
       for (int k = 0; k < PER_THREAD; ++k) {
@@ -323,6 +335,11 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
             // starting at (ib, jb) so the warp does not diverge; the third
             // node of a 2-node range is predicated off. Cumulative sums run
             // in the reference's order, so each contribution keeps its value.
+            // The third column of J1 and the third row of J2 are only ever the
+            // last node of a 3-node range, where the cumulative sum covers the
+            // whole support (sum of new weights minus sum of old weights,
+            // zero up to rounding); the reference adds that rounding residue,
+            // these sites are skipped.
             const float weight = -P.charge[sp] * w;
             const int ib = (dc1 == -1 ? -2 : -1), nib = (dc1 == 0 ? 2 : 3);
             const int jb = (dc2 == -1 ? -2 : -1), njb = (dc2 == 0 ? 2 : 3);
@@ -351,9 +368,9 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
                 if (jv && a < nib) {
                   const int o = obase + b * G::JX + a;
                   djx += movement2d(sy0, sy1, sx0[a], sx1[a]);
-                  add_fixed(J1, o + 1, weight * djx, fscale, fx.L);
+                  if (a < 2) add_fixed(J1, o + 1, weight * djx, fscale, fx.L);
                   djy[a] += movement2d(sx0[a], sx1[a], sy0, sy1);
-                  add_fixed(J2, o + G::JX, weight * djy[a], fscale, fx.L);
+                  if (b < 2) add_fixed(J2, o + G::JX, weight * djy[a], fscale, fx.L);
                   const float val2 = center2d(sx0[a], sx1[a], sy0, sy1);
                   add_fixed(J3, o, -weight * v3 * val2, fscale, fx.L);
                   if (rho) {
@@ -657,11 +674,12 @@ cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
                   : run(k_push_deposit_2d<TX, TY, CH, MINB, false, false>);
 }
 
-// Staged chunk of 2048 particles with two CTAs per SM, or 1024 with three.
+// Staged chunk of 1024 particles with three CTAs per SM (default), or 2048
+// with two.
 template <int TX, int TY>
 cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
-  if (c.params.chunk == 1024) return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
-  return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
+  if (c.params.chunk == 2048) return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
+  return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
 }
 
 // Largest |weight| over slots [0, n) (non-negative floats order like their

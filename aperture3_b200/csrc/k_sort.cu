@@ -6,7 +6,8 @@
 // direction counts. Because the input is grouped by tile and a particle
 // only moves to one of its tile's eight neighbours, the stable counting
 // sort by new tile reduces to:
-//   k_tile_scan     for each destination tile, sum the counts from its (up
+//   k_tile_newcount / k_scan_counts / k_tile_groups: for each destination
+//                   tile, sum the counts from its (up
 //                   to nine) source tiles, scan to get tile offsets, and
 //                   give each (source, direction) group its offset, sources
 //                   taken in ascending tile index;
@@ -82,89 +83,168 @@ __device__ __forceinline__ int gather_sources(const TileTopo &T, const uint32_t 
   return n;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-    k_tile_scan(TileTopo T, const uint32_t *__restrict__ cnt, uint32_t *__restrict__ new_start,
-                uint32_t *__restrict__ grp_off, uint32_t *__restrict__ n_max) {
-  __shared__ uint32_t s_part[kScanThreads];
-  __shared__ uint32_t s_max;
-  if (threadIdx.x == 0) s_max = 0;
-  const int tid = threadIdx.x;
-  const int per = (T.ntiles + kScanThreads - 1) / kScanThreads;
-  const int u0 = tid * per, u1 = min(T.ntiles, u0 + per);
-  int src[9], dirv[9];
-  uint32_t num[9];
-  uint32_t local = 0, mx = 0;
-  for (int u = u0; u < u1; ++u) {
+// New population of every destination tile: the counts its (up to nine)
+// source tiles recorded for the direction that leads to it.
+__global__ void k_tile_newcount(TileTopo T, const uint32_t *__restrict__ cnt,
+                                uint32_t *__restrict__ newcount) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < T.ntiles; u += gridDim.x * blockDim.x) {
+    int src[9], dirv[9];
+    uint32_t num[9];
     const int n = gather_sources(T, cnt, u, src, dirv, num);
     uint32_t nu = 0;
     for (int k = 0; k < n; ++k) nu += num[k];
-    local += nu;
-    mx = max(mx, nu);
+    newcount[u] = nu;
   }
-  s_part[tid] = local;
-  __syncthreads();
-  atomicMax(&s_max, mx);
-  // inclusive Hillis-Steele scan over the per-thread sums
-  for (int off = 1; off < kScanThreads; off <<= 1) {
-    uint32_t v = tid >= off ? s_part[tid - off] : 0u;
-    __syncthreads();
-    s_part[tid] += v;
-    __syncthreads();
-  }
-  uint32_t run = s_part[tid] - local;
-  for (int u = u0; u < u1; ++u) {
-    new_start[u] = run;
+}
+
+// Offsets of the (source, direction) groups inside each destination tile:
+// sources in ascending tile index, so the concatenation is the stable order.
+__global__ void k_tile_groups(TileTopo T, const uint32_t *__restrict__ cnt,
+                              const uint32_t *__restrict__ new_start,
+                              uint32_t *__restrict__ grp_off) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < T.ntiles; u += gridDim.x * blockDim.x) {
+    int src[9], dirv[9];
+    uint32_t num[9];
     const int n = gather_sources(T, cnt, u, src, dirv, num);
+    uint32_t run = new_start[u];
     for (int k = 0; k < n; ++k) {
       grp_off[src[k] * 9 + dirv[k]] = run;
       run += num[k];
     }
   }
-  if (tid == kScanThreads - 1) new_start[T.ntiles] = s_part[tid];
-  __syncthreads();
-  if (tid == 0) *n_max = s_max;
 }
 
-// One CTA per source tile: stable rank within each direction group.
+// One CTA per source tile: stable rank within each direction group. The
+// tile's list is cut into one contiguous segment per warp; pass 1 counts the
+// directions of each segment with warp ballots, one barrier turns the counts
+// into per-warp offsets, and pass 2 walks the segment again, ranking lanes
+// that share a direction with __match_any_sync, so every entry lands at
+// group offset + entries of that direction before it.
 __global__ void __launch_bounds__(kScatterThreads)
     k_order_scatter(int ntiles, const uint32_t *__restrict__ old_start,
                     const uint32_t *__restrict__ old_order, const uint8_t *__restrict__ dir,
                     const uint32_t *__restrict__ grp_off, uint32_t *__restrict__ new_order,
                     uint32_t capacity, DevStatus *status) {
   constexpr int kWarps = kScatterThreads / 32;
-  __shared__ uint32_t s_wcnt[kWarps][10];
-  __shared__ uint32_t s_base[10];
+  __shared__ uint32_t s_cnt[kWarps][10];
+  __shared__ uint32_t s_base[kWarps][10];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   for (int s = blockIdx.x; s < ntiles; s += gridDim.x) {
     const uint32_t b = old_start[s], e = old_start[s + 1];
-    if (tid < 10) s_base[tid] = (tid < 9) ? grp_off[s * 9 + tid] : 0u;
+    const uint32_t n = e - b;
+    const uint32_t seg = ((n + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+    const uint32_t w0 = b + min(n, warp * seg), w1 = b + min(n, (warp + 1) * seg);
+    // pass 1: direction counts of this warp's segment
+    uint32_t mycnt = 0;  // lane f < 10 holds the count of direction f
+    for (uint32_t p = w0 + lane; p < w1 + 31; p += 32) {
+      if (p - lane >= w1) break;
+      const uint32_t d = p < w1 ? dir[p] : 10u;
+#pragma unroll
+      for (uint32_t f = 0; f < 10; ++f) {
+        const uint32_t m = __ballot_sync(0xffffffffu, d == f);
+        if (lane == (int)f) mycnt += __popc(m);
+      }
+    }
+    if (lane < 10) s_cnt[warp][lane] = mycnt;
     __syncthreads();
-    for (uint32_t c0 = b; c0 < e; c0 += kScatterThreads) {
-      const uint32_t pos = c0 + tid;
-      const bool valid = pos < e;
-      const uint32_t d = valid ? dir[pos] : 9u;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-      if (tid < kWarps * 10) (&s_wcnt[0][0])[tid] = 0u;
-      __syncthreads();
-      if (lane == __ffs(peers) - 1) s_wcnt[warp][d] = __popc(peers);
-      __syncthreads();
-      uint32_t before = 0;
-      if (valid && d < 9) {
-        for (int w = 0; w < warp; ++w) before += s_wcnt[w][d];
-        const uint32_t dst = s_base[d] + before + rank;
+    if (lane < 9) {
+      uint32_t off = grp_off[s * 9 + lane];
+      for (int w = 0; w < warp; ++w) off += s_cnt[w][lane];
+      s_base[warp][lane] = off;
+    }
+    __syncwarp();
+    // pass 2: stable placement; entries that stay in the tile (direction 4,
+    // nearly all of them) are ranked with one ballot, the rest with
+    // __match_any_sync
+    uint32_t base4 = s_base[warp][4];
+    for (uint32_t p = w0 + lane; p < w1 + 31; p += 32) {
+      if (p - lane >= w1) break;
+      const bool valid = p < w1;
+      const uint32_t d = valid ? dir[p] : 10u;
+      const uint32_t stay = __ballot_sync(0xffffffffu, d == 4u);
+      const uint32_t other = __ballot_sync(0xffffffffu, d < 9u && d != 4u);
+      uint32_t dst = 0xffffffffu;
+      if (d == 4u) dst = base4 + __popc(stay & lt);
+      base4 += __popc(stay);
+      if (other) {
+        if ((other >> lane) & 1u) {
+          const uint32_t peers = __match_any_sync(other, d);
+          const uint32_t bs = s_base[warp][d];
+          dst = bs + __popc(peers & lt);
+          __syncwarp(other);
+          if ((peers & lt) == 0u) s_base[warp][d] = bs + __popc(peers);
+        }
+        __syncwarp();
+      }
+      if (dst != 0xffffffffu) {
         if (dst < capacity)
-          new_order[dst] = old_order[pos];
+          new_order[dst] = old_order[p];
         else
           atomicAdd(&status->tile_faults, 1ull);
       }
-      __syncthreads();
-      if (tid < 9) {
-        uint32_t tot = 0;
-        for (int w = 0; w < kWarps; ++w) tot += s_wcnt[w][tid];
-        s_base[tid] += tot;
-      }
-      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// start[k] = first position of key k in the sorted keys[0, n), for
+// k = 0..nbins (start[nbins] = position of the first key >= nbins); also the
+// largest segment length over keys < nbins.
+__global__ void k_segment_starts(const uint32_t *__restrict__ keys, size_t n, uint32_t nbins,
+                                 uint32_t *__restrict__ start) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i <= n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t prev = (i == 0) ? 0u : min(keys[i - 1], nbins) + 1u;  // first key not yet started
+    const uint32_t cur = (i == n) ? nbins : min(keys[i], nbins);
+    for (uint32_t k = prev; k <= cur; ++k) start[k] = (uint32_t)i;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_segment_max(const uint32_t *__restrict__ start, uint32_t nbins, uint32_t *n_max) {
+  __shared__ uint32_t s_max;
+  if (threadIdx.x == 0) s_max = 0;
+  __syncthreads();
+  uint32_t mx = 0;
+  for (uint32_t k = threadIdx.x; k < nbins; k += blockDim.x) mx = max(mx, start[k + 1] - start[k]);
+  atomicMax(&s_max, mx);
+  __syncthreads();
+  if (threadIdx.x == 0) *n_max = s_max;
+}
+
+// Tile order of particles sorted by cell: the particles of tile t are, row
+// by row, the contiguous runs [cell_start[first cell of the row], cell_start
+// [one past the last cell]) -- which is the stable counting sort by tile of
+// the cell-sorted array.
+__global__ void k_tile_counts_from_cells(MeshK m, TilesK T, const uint32_t *__restrict__ cs,
+                                         uint32_t *__restrict__ counts) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T.ntiles; t += gridDim.x * blockDim.x) {
+    const int tx = t % T.ntx, ty = t / T.ntx;
+    const int x0 = m.guard[0] + tx * T.tx;
+    const int x1 = min(x0 + T.tx, m.dims[0] - m.guard[0]);
+    const int y0 = m.guard[1] + ty * T.ty;
+    const int y1 = min(y0 + T.ty, m.dims[1] - m.guard[1]);
+    uint32_t n = 0;
+    for (int y = y0; y < y1; ++y) n += cs[y * m.dims[0] + x1] - cs[y * m.dims[0] + x0];
+    counts[t] = n;
+  }
+}
+
+__global__ void k_tile_fill_from_cells(MeshK m, TilesK T, const uint32_t *__restrict__ cs,
+                                       const uint32_t *__restrict__ tile_start,
+                                       uint32_t *__restrict__ order) {
+  for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+    const int tx = t % T.ntx, ty = t / T.ntx;
+    const int x0 = m.guard[0] + tx * T.tx;
+    const int x1 = min(x0 + T.tx, m.dims[0] - m.guard[0]);
+    const int y0 = m.guard[1] + ty * T.ty;
+    const int y1 = min(y0 + T.ty, m.dims[1] - m.guard[1]);
+    uint32_t out = tile_start[t];
+    for (int y = y0; y < y1; ++y) {
+      const uint32_t a = cs[y * m.dims[0] + x0], b = cs[y * m.dims[0] + x1];
+      for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) order[out + (i - a)] = i;
+      out += b - a;
     }
   }
 }
@@ -194,14 +274,6 @@ __global__ void k_tile_keys(MeshK m, TilesK T, uint32_t *cell, size_t n, uint32_
     }
     keys[i] = key;
     vals[i] = (uint32_t)i;
-  }
-}
-
-__global__ void k_histogram(const uint32_t *keys, size_t n, uint32_t nbins, uint32_t *hist) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t k = keys[i];
-    if (k < nbins) atomicAdd(hist + k, 1u);
   }
 }
 
@@ -236,15 +308,6 @@ __global__ void __launch_bounds__(kScanThreads)
   if (tid == kScanThreads - 1) start[nbins] = s_part[tid];
   __syncthreads();
   if (tid == 0 && n_max) *n_max = s_max;
-}
-
-__global__ void k_count_below(const uint32_t *keys, size_t n, uint32_t bound, uint32_t *count) {
-  uint32_t local = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    local += keys[i] < bound;
-  for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
 }
 
 __global__ void k_cell_keys(const uint32_t *cell, size_t n, uint32_t ncells, uint32_t *keys,
@@ -299,8 +362,12 @@ cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count, uint32_t *new_st
                              uint32_t *grp_off) {
   TileTopo T{c.tiles.ntx, c.tiles.nty, c.tiles.ntiles, c.params.periodic[0],
              c.params.periodic[1]};
-  k_tile_scan<<<1, kScanThreads, 0, c.stream>>>(T, dir_count, new_start, grp_off, c.n_max);
-  c.launches++;
+  const int nt = c.tiles.ntiles;
+  const int g = (nt + 255) / 256;
+  k_tile_newcount<<<g, 256, 0, c.stream>>>(T, dir_count, c.newcount);
+  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.newcount, nt, new_start, c.n_max);
+  k_tile_groups<<<g, 256, 0, c.stream>>>(T, dir_count, new_start, grp_off);
+  c.launches += 3;
   return cudaGetLastError();
 }
 
@@ -351,8 +418,6 @@ cudaError_t rebuild_tile_order(Ctx &c) {
   const uint32_t nt = (uint32_t)c.tiles.ntiles;
   uint32_t *start = c.tile_start[c.cur];
   cudaError_t e;
-  e = cudaMemsetAsync(c.dir_count, 0, sizeof(uint32_t) * (nt + 1), c.stream);
-  if (e != cudaSuccess) return e;
   if (n > 0) {
     k_tile_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.mk, c.tiles, c.ptc.cell, n,
                                                           c.keys[0], c.vals[0]);
@@ -363,10 +428,13 @@ cudaError_t rebuild_tile_order(Ctx &c) {
     e = cudaMemcpyAsync(c.order[c.cur], vo, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                         c.stream);
     if (e != cudaSuccess) return e;
-    k_histogram<<<grid_for(c, n, 256), 256, 0, c.stream>>>(ko, n, nt, c.dir_count);
+    k_segment_starts<<<grid_for(c, n + 1, 256), 256, 0, c.stream>>>(ko, n, nt, start);
     c.launches++;
+  } else {
+    e = cudaMemsetAsync(start, 0, sizeof(uint32_t) * (nt + 1), c.stream);
+    if (e != cudaSuccess) return e;
   }
-  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, (int)nt, start, c.n_max);
+  k_segment_max<<<1, kScanThreads, 0, c.stream>>>(start, nt, c.n_max);
   c.launches++;
   c.order_valid = true;
   return cudaGetLastError();
@@ -407,16 +475,32 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   AP_GATHER(id, uint64_t);
   AP_GATHER(flag, uint32_t);
 #undef AP_GATHER
-  // number of non-empty slots = position of the first key == ncells
-  // (upper_bound of MAX_CELL - 1, particle_base_impl.cu:454-458)
-  uint32_t *cnt = c.dir_count;
-  e = cudaMemsetAsync(cnt, 0, sizeof(uint32_t), c.stream);
-  if (e != cudaSuccess) return e;
-  k_count_below<<<g, 256, 0, c.stream>>>(ko, n, ncells, cnt);
+  // cell_start over the sorted keys; cell_start[ncells] is the number of
+  // non-empty slots (upper_bound of MAX_CELL - 1, particle_base_impl.cu:454-458)
+  if (!c.cell_start) {
+    e = cudaMalloc(&c.cell_start, sizeof(uint32_t) * ((size_t)ncells + 1));
+    if (e != cudaSuccess) return e;
+  }
+  k_segment_starts<<<grid_for(c, n + 1, 256), 256, 0, c.stream>>>(ko, n, ncells, c.cell_start);
   c.launches++;
   uint32_t live = 0;
-  e = cudaMemcpyAsync(&live, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
+  e = cudaMemcpyAsync(&live, c.cell_start + ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                      c.stream);
   if (e != cudaSuccess) return e;
+  if (c.mk.dim == 2) {
+    // the tile order of the cell-sorted particles, without another sort
+    const int nt = c.tiles.ntiles;
+    k_tile_counts_from_cells<<<(nt + 255) / 256, 256, 0, c.stream>>>(c.mk, c.tiles, c.cell_start,
+                                                                     c.dir_count);
+    c.launches++;
+    k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, nt, c.tile_start[c.cur],
+                                                    c.n_max);
+    c.launches++;
+    k_tile_fill_from_cells<<<nt < c.num_sms * 8 ? nt : c.num_sms * 8, 256, 0, c.stream>>>(
+        c.mk, c.tiles, c.cell_start, c.tile_start[c.cur], c.order[c.cur]);
+    c.launches++;
+    c.order_valid = true;
+  }
   e = cudaStreamSynchronize(c.stream);
   if (e != cudaSuccess) return e;
   *new_number = live;

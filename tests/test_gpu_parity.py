@@ -140,6 +140,27 @@ def test_sort_by_cell_bitexact():
         assert_bits(got[k], pr.p[k][:n_ref], f"sorted {k}")
 
 
+def test_tile_order_after_sort_by_cell():
+    """sort_by_cell leaves the tile order equal to a stable counting sort by
+    tile of the cell-sorted slots, and the next steps stay bit-exact."""
+    pr = _setup((64, 48), 6000, seed=17, tile=(8, 8))
+    pr.both_update_particles(0)
+    pr.data.sort_particles()
+    n_ref = oracle.sort_by_cell(pr.m, pr.p, len(pr.p["x1"]))
+    pr.p = {k: v[:n_ref].copy() for k, v in pr.p.items()}
+    assert pr.data.number == n_ref
+    keys = np.array([oracle.tile_key(pr.m, (8, 8), int(c)) for c in pr.p["cell"]], np.uint32)
+    nt = oracle.tile_key(pr.m, (8, 8), oracle.MAX_CELL)
+    order_ref = oracle.stable_counting_sort(keys, nt + 1)
+    order_ref = order_ref[keys[order_ref] < nt]
+    order_gpu, start_gpu = pr.data.tile_order()
+    assert_bits(order_gpu, order_ref, "tile order after sort_by_cell")
+    for step in range(1, 3):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL)
+
+
 def test_no_tensor_map_path_bitexact():
     """Rows packed to an odd length make the field tiles load without TMA."""
     pr = _setup((61, 45), 4000, seed=7, row_align=1)
