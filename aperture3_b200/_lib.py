@@ -121,6 +121,9 @@ SIGNATURES = {
     "ap_get_phase_times": (_i, [_vp, C.POINTER(ApPhaseTimes), _i]),
     "ap_last_error": (_i, [_vp]),
     "ap_launch_count": (C.c_uint64, [_vp]),
+    "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
+                                            C.POINTER(ApParticles), C.c_size_t,
+                                            C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),
 }
 
 

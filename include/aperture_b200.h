@@ -216,6 +216,34 @@ AP_API int ap_set_profiling(ap_ctx *ctx, int on);
  * them afterwards. */
 AP_API int ap_get_phase_times(ap_ctx *ctx, ap_phase_times *out, int reset);
 
+/* Limits of ap_update_particles_1d_noalloc. */
+#define AP_NOALLOC_MAX_CELLS 16392   /* dims[0], guard cells included */
+#define AP_NOALLOC_MAX_SPECIES 3
+
+/* No counterpart in the reference. The 1D particle update of
+ * ap_update_particles (push, deposit, periodic fold, rounding of J and Rho,
+ * wrap) for callers that cannot allocate device memory when they call it --
+ * for example a process whose device memory is fully reserved by another
+ * allocator, where a cudaMalloc would fail or fragment that pool. It needs
+ * no context and allocates nothing: the caller passes the particle and
+ * field arrays, and the library's only other device memory is a fixed
+ * file-scope array of (3 + AP_NOALLOC_MAX_SPECIES) * AP_NOALLOC_MAX_CELLS
+ * 64-bit words (about 770 KB), which every GPU that loads the library holds
+ * until the process exits. Grids with more than AP_NOALLOC_MAX_CELLS cells
+ * (AP_ERR_CAPACITY), more than AP_NOALLOC_MAX_SPECIES species
+ * (AP_ERR_CAPACITY), current smoothing (AP_ERR_UNSUPPORTED) or other than
+ * 1D (AP_ERR_UNSUPPORTED) are rejected. The first call on a device looks up
+ * the array's device address with cudaGetSymbolAddress, so make that first
+ * call before any stream capture. All calls share the array and clear it
+ * at their start: calls that overlap on the GPU (on different streams, or
+ * from different threads) race and must not be issued. The call enqueues
+ * its work on cuda_stream (0 = legacy default stream) and synchronises that
+ * stream before returning. */
+AP_API int ap_update_particles_1d_noalloc(const ap_mesh *mesh, const ap_params *params,
+                                          const ap_particles *ptc, size_t number,
+                                          const ap_fields *fields, double dt,
+                                          uint32_t step, void *cuda_stream);
+
 /* Status of the last failing call on this context. */
 AP_API int ap_last_error(const ap_ctx *ctx);
 
