@@ -1,0 +1,104 @@
+// sim_environment for one rank without MPI (src/sim_environment.h,
+// sim_environment_impl.hpp): the grid, the per-species charges and masses,
+// and the guard exchange, which on one periodic rank is done by device
+// kernels instead of MPI self-exchanges. Owns the library context.
+#ifndef APERTURE_DROPIN_SIM_ENVIRONMENT_H_
+#define APERTURE_DROPIN_SIM_ENVIRONMENT_H_
+
+#include <cmath>
+
+#include "multi_array.h"
+#include "sim_params.h"
+
+namespace Aperture {
+
+class Grid {
+ public:
+  const Quadmesh &mesh() const { return mesh_; }
+  Quadmesh &mesh() { return mesh_; }
+  int dim() const { return mesh_.dim(); }
+
+ private:
+  Quadmesh mesh_{};
+};
+
+class sim_environment {
+ public:
+  // The reference constructor (int*, char***) initialises MPI and parses
+  // the configuration file; this one takes the parsed parameters.
+  explicit sim_environment(const SimParams &params, int device = -1) : params_(params) {
+    if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    // Grid::init (src/core/grid.cpp:31-48)
+    Quadmesh &m = grid_.mesh();
+    for (int i = 0; i < 3; ++i) {
+      m.guard[i] = params.guard[i];
+      m.sizes[i] = params.size[i];
+      m.lower[i] = params.lower[i];
+      m.dims[i] = params.N[i] + 2 * params.guard[i];
+      m.delta[i] = params.size[i] / params.N[i];
+      m.inv_delta[i] = (float)(1.0 / m.delta[i]);
+    }
+    m.dimension = m.dim();
+    // setup_env (sim_environment_impl.hpp:90-101)
+    for (int i = 0; i < AP_MAX_SPECIES; ++i) {
+      charges_[i] = params.q_e;
+      masses_[i] = params.q_e;
+    }
+    charges_[0] *= -1.0f;           // electron
+    masses_[2] *= params.ion_mass;  // ion
+    ap_params p{};
+    p.num_species = params.num_species;
+    p.data_interval = (int)params.data_interval;
+    p.current_smoothing = params.current_smoothing;
+    for (int i = 0; i < 3; ++i) p.periodic[i] = params.periodic_boundary[i] ? 1 : 0;
+    for (int i = 0; i < AP_MAX_SPECIES; ++i) {
+      p.charges[i] = charges_[i];
+      p.masses[i] = masses_[i];
+    }
+    p.tile[0] = p.tile[1] = 0;
+    p.chunk = 0;
+    ap_params_ = p;
+    ap_check(ap_ctx_create(&m, &p, &ctx_), "ap_ctx_create");
+  }
+  ~sim_environment() {
+    if (ctx_) ap_ctx_destroy(ctx_);
+  }
+  sim_environment(const sim_environment &) = delete;
+  sim_environment &operator=(const sim_environment &) = delete;
+
+  SimParams &params() { return params_; }
+  const SimParams &params() const { return params_; }
+  const Grid &local_grid() const { return grid_; }
+  const Grid &grid() const { return grid_; }
+  const Quadmesh &mesh() const { return grid_.mesh(); }
+  const float *charges() const { return charges_; }
+  const float *masses() const { return masses_; }
+  ap_ctx *ctx() const { return ctx_; }
+
+  void send_array_guard_cells(multi_array<Scalar> &a) {
+    ap_check(ap_send_guard_cells(ctx_, a.view()), "send_guard_cells");
+  }
+  void send_add_array_guard_cells(multi_array<Scalar> &a) {
+    ap_check(ap_send_add_guard_cells(ctx_, a.view()), "send_add_guard_cells");
+  }
+  void send_guard_cells(vector_field<Scalar> &f) {
+    for (int i = 0; i < 3; ++i) send_array_guard_cells(f.data(i));
+  }
+  void send_guard_cells(scalar_field<Scalar> &f) { send_array_guard_cells(f.data()); }
+  void send_add_guard_cells(vector_field<Scalar> &f) {
+    for (int i = 0; i < 3; ++i) send_add_array_guard_cells(f.data(i));
+  }
+  void send_add_guard_cells(scalar_field<Scalar> &f) { send_add_array_guard_cells(f.data()); }
+
+ private:
+  SimParams params_;
+  Grid grid_;
+  float charges_[AP_MAX_SPECIES];
+  float masses_[AP_MAX_SPECIES];
+  ap_params ap_params_{};
+  ap_ctx *ctx_ = nullptr;
+};
+
+}  // namespace Aperture
+
+#endif

@@ -1,0 +1,35 @@
+// SimParams: the fields of src/sim_params.h:17-123 the particle update and
+// the field solver read, with the reference's names and defaults. Labs fill
+// it directly (the reference parses a TOML file with cpptoml).
+#ifndef APERTURE_DROPIN_SIM_PARAMS_H_
+#define APERTURE_DROPIN_SIM_PARAMS_H_
+
+#include <cstddef>
+#include <cstdint>
+
+#include "ap_common.h"
+
+namespace Aperture {
+
+struct SimParams {
+  Scalar delta_t = 0.01;
+  Scalar q_e = 1.0;
+  Scalar ion_mass = 1.0;
+  int num_species = 3;
+  bool periodic_boundary[3] = {false, false, false};
+  int current_smoothing = 0;
+  size_t data_interval = 100;
+  int sort_interval = 20;
+  uint32_t max_steps = 10000;
+  uint64_t max_ptc_number = 100;
+  Scalar B0 = 1.0;
+  int N[3] = {1, 1, 1};
+  int guard[3] = {0, 0, 0};
+  float lower[3] = {0.0, 0.0, 0.0};
+  float size[3] = {1.0, 1.0, 1.0};
+  int tile_size[3] = {1, 1, 1};
+};
+
+}  // namespace Aperture
+
+#endif
