@@ -6,11 +6,11 @@ Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 
 Two libraries are wrapped:
 
-* ``liboracle.so`` (``ap_oracle.c``): a plain-C restatement of the
-  reference algorithm (``src/cuda/algorithms/ptc_updater.cu``,
-  ``field_solver.cu``, ``sim_environment_impl.hpp``,
-  ``core/particle_base_impl.hpp``), FP32 literal, built with
-  ``-ffp-contract=off``.
+* ``liboracle.so`` (``ap_oracle.c``, ``ap_logsph.c``): a plain-C
+  restatement of the reference algorithm (``src/cuda/algorithms/
+  ptc_updater.cu``, ``field_solver.cu``, ``sim_environment_impl.hpp``,
+  ``core/particle_base_impl.hpp``; the log-spherical files are wrapped in
+  ``oracle.logsph``), FP32 literal, built with ``-ffp-contract=off``.
 * ``_ref/libapref.so`` (built by ``ref_build/Makefile`` when the reference
   tree is present): the reference's own kernel bodies compiled as host code.
   It pins the restatement; it is optional at run time.
@@ -108,8 +108,10 @@ def _build(target_dir, target):
 
 def _load_oracle():
     path = os.path.join(_HERE, "liboracle.so")
-    src = os.path.join(_HERE, "ap_oracle.c")
-    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, n) for n in ("ap_oracle.c", "ap_oracle.h", "ap_logsph.c",
+                                              "ap_logsph.h")]
+    if not os.path.exists(path) or any(os.path.getmtime(path) < os.path.getmtime(s)
+                                       for s in srcs):
         _build(_HERE, "liboracle.so")
     return C.CDLL(path)
 

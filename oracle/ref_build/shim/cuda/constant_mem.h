@@ -5,10 +5,21 @@
 #include "cuda_builtins_host.h"
 #include "core/quadmesh.h"
 namespace Aperture {
-struct ap_ref_params { int data_interval; };
+/* The SimParams members the kernels read (src/sim_params.h:17-73). */
+struct ap_ref_params {
+  int data_interval;
+  int num_species;
+  float compactness, omega, gravity, rad_cooling_coef, B0, damping_coef;
+  bool rad_cooling_on;
+  int damping_length;
+  float q_e, r_cutoff, track_percent;
+  bool inject_ions;
+};
 extern Quadmesh dev_mesh;
 extern ap_ref_params dev_params;
 extern float dev_charges[8];
 extern float dev_masses[8];
+extern int dev_rank;
+extern unsigned long long dev_ptc_id;
 }  // namespace Aperture
 #endif

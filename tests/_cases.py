@@ -71,3 +71,59 @@ def mesh_2d(N0, N1, guard=2, size=(1.0, 1.0)):
 
 CHARGES = [-1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
 MASSES = [1.0] * 8
+
+
+# ---------------------------------------------------------------------------
+# Log-spherical (ln r, theta) cases: r in [1, rmax], theta in [0, pi].
+
+def mesh_logsph(N0, N1, guard=2, rmax=50.0):
+    return oracle.make_mesh((N0, N1, 1), (guard, guard, 0),
+                            size=(float(np.log(rmax)), float(np.pi), 1.0))
+
+
+def _node_pos(m, dim, n, stagger):
+    """Quadmesh::pos(dim, n, stagger) in float64 for the initial fields."""
+    x = 1.0 if stagger else 0.5
+    return m.lower[dim] + m.delta[dim] * (n - m.guard[dim] + x)
+
+
+def logsph_fields(m, rng, omega=0.1, B0=1.0, noise=0.02, num_species=3):
+    """Dipole background B_r = 2 B0 cos(theta) / r^3, B_theta = B0 sin(theta) / r^3
+    and the corotation field E = -(Omega x r) x B of a rotating conductor,
+    each sampled at its Yee stagger, plus seeded noise in E and B."""
+    f = oracle.new_fields(m, num_species)
+    i = np.arange(m.dims[0])[None, :]
+    j = np.arange(m.dims[1])[:, None]
+    for comp, (sx, sy) in enumerate(STAG[3:]):
+        r = np.exp(_node_pos(m, 0, i, sx))
+        th = _node_pos(m, 1, j, sy)
+        br = 2 * B0 * np.cos(th) / r ** 3
+        bt = B0 * np.sin(th) / r ** 3
+        val = [br, bt, np.zeros_like(br)][comp]
+        f["Bbg"][comp][:] = val.astype(np.float32)
+    for comp, (sx, sy) in enumerate(STAG[:3]):
+        r = np.exp(_node_pos(m, 0, i, sx))
+        th = _node_pos(m, 1, j, sy)
+        br = 2 * B0 * np.cos(th) / r ** 3
+        bt = B0 * np.sin(th) / r ** 3
+        v = omega * r * np.sin(th)
+        val = [v * bt, -v * br, np.zeros_like(br)][comp]
+        f["Ebg"][comp][:] = val.astype(np.float32)
+    for c in range(3):
+        f["E"][c][:] = f["Ebg"][c] + (noise * rng.standard_normal(f["E"][c].shape)).astype(np.float32)
+        f["B"][c][:] = f["Bbg"][c] + (noise * rng.standard_normal(f["B"][c].shape)).astype(np.float32)
+    return f
+
+
+def logsph_particles(m, n, rng, gamma_max=1e3, species=(0, 1, 2)):
+    p = random_particles(m, n, rng, gamma_max=gamma_max, species=species)
+    p["x3"][:] = (np.pi * (2 * rng.random(n) - 1)).astype(np.float32)
+    return p
+
+
+def logsph_dt(m, frac=0.4):
+    return np.float32(frac * min(m.delta[0], m.delta[1]))
+
+
+LS_CHARGES = [-1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+LS_MASSES = [1.0, 1.0, 10.0, 1.0, 1.0, 1.0, 1.0, 1.0]

@@ -1,6 +1,8 @@
 """Generates the golden fixtures in this directory from the reference's own
 kernels (src/cuda/algorithms/ptc_updater.cu push/deposit and
-field_solver.cu e/b/divs), run on the host by oracle/ref_build.
+field_solver.cu e/b/divs; for logsph_*.npz the log-spherical
+ptc_updater_logsph.cu / field_solver_logsph.cu kernels and
+grid_log_sph.cpp coefficients), run on the host by oracle/ref_build.
 
 Needs the reference tree (to build oracle/_ref/libapref.so). Run from the
 repository root:  python tests/golden/make_golden.py
@@ -19,7 +21,10 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 import oracle  # noqa: E402
-from _cases import CHARGES, MASSES, mesh_1d, mesh_2d, random_fields, random_particles  # noqa: E402
+from oracle import logsph as ls  # noqa: E402
+from _cases import (CHARGES, LS_CHARGES, LS_MASSES, MASSES, logsph_dt,  # noqa: E402
+                    logsph_fields, logsph_particles, mesh_1d, mesh_2d, mesh_logsph,
+                    random_fields, random_particles)
 
 CASES = [
     # name, kind, N, seed, particles, step, data_interval
@@ -81,6 +86,66 @@ def main():
         np.savez_compressed(path, **out)
         print(path, os.path.getsize(path))
 
+    main_logsph()
+
+
+LS_CASES = [
+    # name, N, seed, particles, params
+    ("logsph_a", (64, 32), 31, 600, {}),
+    ("logsph_b", (64, 32), 32, 600, {"gravity": 0.3, "rad_cooling_on": True,
+                                     "rad_cooling_coef": 0.05, "compactness": 0.4}),
+]
+
+
+def main_logsph():
+    """One push + deposit (step 0, data_interval 1) and one field update of
+    the reference's log-spherical code on seeded dipole-field inputs."""
+    if ls.load_ref(build=True) is None:
+        raise SystemExit("reference pin library unavailable (needs the reference tree)")
+    for name, N, seed, n, opts in LS_CASES:
+        rng = np.random.default_rng(seed)
+        m = mesh_logsph(*N)
+        f = logsph_fields(m, rng)
+        p = logsph_particles(m, n, rng, gamma_max=1e6)
+        lp = ls.ls_params(**opts)
+        dt = logsph_dt(m)
+        out = {}
+        for k, v in oracle.mesh_dict(m).items():
+            out["mesh_" + k] = np.asarray(v)
+        out["lp"] = np.array([lp.compactness, lp.omega, lp.gravity, lp.rad_cooling_coef,
+                              lp.B0, lp.damping_coef, lp.rad_cooling_on, lp.damping_length],
+                             np.float64)
+        out["dt"] = np.float32(dt)
+        c = ls.ref_coef(m)
+        for k, cn in enumerate(ls.COEF_NAMES):
+            out["coef_" + cn] = c[k]
+        for k in p:
+            out["in_p_" + k] = p[k].copy()
+        for key in ("E", "B", "Ebg", "Bbg"):
+            for k in range(3):
+                out[f"in_{key}{k}"] = f[key][k].copy()
+        ls.ref_push(m, lp, p, n, dt, f["E"] + f["B"], LS_CHARGES, LS_MASSES)
+        J = [np.zeros_like(f["E"][0]) for _ in range(3)]
+        R = [np.zeros_like(f["E"][0]) for _ in range(3)]
+        ls.ref_deposit(m, lp, p, n, dt, 0, 1, J, R, c, LS_CHARGES)
+        for k in p:
+            out["out_p_" + k] = p[k]
+        for k in range(3):
+            out[f"out_J{k}"] = J[k]
+            out[f"out_Rho{k}"] = R[k]
+        f["J"] = J
+        f["Rho"] = R
+        ls.ref_update_fields(m, lp, f, c, dt)
+        for key in ("E", "B"):
+            for k in range(3):
+                out[f"out_{key}{k}"] = f[key][k]
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path))
+
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "logsph":
+        main_logsph()
+    else:
+        main()

@@ -115,7 +115,7 @@ def test_filter_matches_reference_kernel(kind, N, seed, bnd):
 
 
 def _golden_files():
-    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
 
 
 def test_golden_fixtures_present():
