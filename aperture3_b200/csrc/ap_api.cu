@@ -24,6 +24,7 @@ MeshK make_meshk(const ap_mesh &m) {
     k.red[i] = m.dims[i] - 2 * m.guard[i];
     k.delta[i] = m.delta[i];
     k.inv_delta[i] = m.inv_delta[i];
+    k.lower[i] = m.lower[i];
   }
   k.div0 = (m.dims[0] > 1) ? (~0ull / (unsigned long long)m.dims[0]) + 1ull : 0ull;
   if (m.dims[1] <= 1 && m.dims[2] <= 1)
@@ -297,6 +298,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->gather_tmp);
   cudaFree(c->cell_start);
   cudaFree(c->tmp_j);
+  cudaFree(c->coef);
   cudaFree(c->acc);
   cudaFree(c->fx_used);
   cudaFree(c->n_max);
@@ -420,6 +422,10 @@ static int smooth_current_async(ap_ctx *c, uint32_t step) {
 
 AP_API int ap_smooth_current(ap_ctx *c, uint32_t step) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
+  if (c->coord == 1) {
+    AP_TRY(launch_ls_smooth(*c, ((step + 1) % (uint32_t)c->params.data_interval) == 0));
+    return finish(c);
+  }
   AP_TRY_ST(smooth_current_async(c, step));
   return finish(c);
 }
@@ -432,11 +438,12 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   // the FP64 accumulators start at zero; J (and Rho on output steps) are
   // overwritten by the finalize pass, Rho is zeroed on other steps.
   const int ncomp = 3 + (do_rho ? pr.num_species : 0);
+  const bool ls = c->coord == 1;
   int ph = phase_begin(c, kPhFinalize);
   AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
                          c->stream));
   if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
-  if (!do_rho)
+  if (!do_rho && !ls)
     for (int s = 0; s < pr.num_species; ++s) AP_TRY(launch_zero(*c, c->fields.Rho[s]));
   AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
   phase_end(c, ph);
@@ -477,6 +484,22 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
     for (int d = 0; d < 3; ++d) P.periodic[d] = pr.periodic[d];
     P.status = c->status;
     P.number = c->number;
+    if (ls) {
+      // user_push_2d_logsph / deposit_and_move_2d_log_sph parameters; the
+      // J3 contributions are divided by the cell volume, which widens the
+      // fixed-point range by ls_kfac
+      P.ls_compactness = c->lsp.compactness;
+      P.ls_omega = c->lsp.omega;
+      P.ls_gravity = c->lsp.gravity;
+      P.ls_rad_coef = c->lsp.rad_cooling_coef;
+      P.ls_B0 = c->lsp.B0;
+      P.ls_rad_on = c->lsp.rad_cooling_on;
+      P.ls_outflow_c1 = c->mesh.dims[0] - c->lsp.damping_length + 2;
+      for (int s = 0; s < AP_MAX_SPECIES; ++s) P.mass[s] = pr.masses[s];
+      const ap_array dv = coef_array(*c, AP_COEF_DV);
+      P.dV = FieldArr{dv.ptr, (int)(dv.pitch / 4)};
+      P.qmax *= c->ls_kfac;
+    }
     if (c->mk.dim == 1) {
       ph = phase_begin(c, kPhPushDeposit);
       AP_TRY(launch_push_deposit_1d(*c, P));
@@ -514,35 +537,54 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   // send_add_guard_cells(J), and Rho on output steps (ptc_updater.cu:800-805),
   // fused with the FP64 -> FP32 rounding
   ph = phase_begin(c, kPhFinalize);
-  AP_TRY(launch_finalize_current(*c, ncomp));
-  phase_end(c, ph);
-  AP_TRY_ST(smooth_current_async(c, step));
+  if (ls) {
+    // process_j, then (ptc_updater_logsph::apply_boundary) axis_rho after
+    // the smoothing; particles that left the bulk were dropped by the move
+    // and ptc_outflow was applied there too
+    AP_TRY(launch_ls_finalize(*c, (float)dt, do_rho, pr.current_smoothing == 0));
+    if (pr.current_smoothing > 0) AP_TRY(launch_ls_smooth(*c, do_rho));
+    phase_end(c, ph);
+  } else {
+    AP_TRY(launch_finalize_current(*c, ncomp));
+    phase_end(c, ph);
+    AP_TRY_ST(smooth_current_async(c, step));
+  }
   if (!c->sync) return AP_OK;
   return check_status(c);
 }
 
 AP_API int ap_update_e_field(ap_ctx *c, double dt) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
-  AP_TRY(launch_update_e(*c, (float)dt));
+  AP_TRY(c->coord == 1 ? launch_ls_update_e(*c, (float)dt) : launch_update_e(*c, (float)dt));
   return finish(c);
 }
 
 AP_API int ap_update_b_field(ap_ctx *c, double dt) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
-  AP_TRY(launch_update_b(*c, (float)dt));
+  AP_TRY(c->coord == 1 ? launch_ls_update_b(*c, (float)dt) : launch_update_b(*c, (float)dt));
   return finish(c);
 }
 
 AP_API int ap_compute_divs(ap_ctx *c) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
-  AP_TRY(launch_divs(*c));
+  AP_TRY(c->coord == 1 ? launch_ls_divs(*c) : launch_divs(*c));
   return finish(c);
 }
 
 AP_API int ap_update_fields(ap_ctx *c, double dt, uint32_t step) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
-  // field_solver::update_fields (field_solver.cu:334-358)
   const int ph = phase_begin(c, kPhFields);
+  if (c->coord == 1) {
+    // field_solver_logsph::update_fields (field_solver_logsph.cu:354-398):
+    // B, then E, then the divergences; no guard exchange on a
+    // non-periodic grid (EdotB is not computed)
+    AP_TRY(launch_ls_update_b(*c, (float)dt));
+    AP_TRY(launch_ls_update_e(*c, (float)dt));
+    AP_TRY(launch_ls_divs(*c));
+    phase_end(c, ph);
+    return finish(c);
+  }
+  // field_solver::update_fields (field_solver.cu:334-358)
   if (step == 0) AP_TRY(launch_update_e(*c, (float)(0.5 * dt)));
   AP_TRY(launch_update_b(*c, (float)dt));
   AP_TRY(launch_update_e(*c, (float)dt));
@@ -650,6 +692,40 @@ AP_API int ap_get_phase_times(ap_ctx *c, ap_phase_times *out, int reset) {
     c->pd_launches = 0;
   }
   return AP_OK;
+}
+
+AP_API int ap_ctx_create_logsph(const ap_mesh *mesh, const ap_params *params,
+                                const ap_logsph_params *lsp, ap_ctx **out) {
+  if (!mesh || !params || !lsp || !out) return AP_ERR_INVALID;
+  *out = nullptr;
+  const MeshK mk = make_meshk(*mesh);
+  if (mk.dim != 2) return AP_ERR_UNSUPPORTED;
+  if (params->periodic[0] || params->periodic[1]) return AP_ERR_UNSUPPORTED;
+  if (lsp->damping_length < 0 || lsp->damping_length > mesh->dims[0]) return AP_ERR_INVALID;
+  ap_ctx *c = nullptr;
+  int st = ap_ctx_create(mesh, params, &c);
+  if (st != AP_OK) return st;
+  c->coord = 1;
+  c->lsp = *lsp;
+  st = logsph_setup(*c);
+  if (st != AP_OK) {
+    ap_ctx_destroy(c);
+    return st;
+  }
+  *out = c;
+  return AP_OK;
+}
+
+AP_API int ap_logsph_coef(ap_ctx *c, int which, ap_array *out) {
+  if (!c || !out || c->coord != 1 || which < 0 || which >= AP_NUM_COEF) return AP_ERR_INVALID;
+  *out = coef_array(*c, which);
+  return AP_OK;
+}
+
+AP_API int ap_logsph_field_boundary(ap_ctx *c, double omega) {
+  if (!c || !c->fields_bound || c->coord != 1) return AP_ERR_INVALID;
+  AP_TRY(launch_ls_field_boundary(*c, (float)omega));
+  return finish(c);
 }
 
 AP_API int ap_last_error(const ap_ctx *c) { return c ? c->last_error : AP_ERR_INVALID; }

@@ -95,6 +95,60 @@ __host__ __device__ constexpr int stag_y(int k) {
   return (k == 0) ? 1 : (k == 1) ? 0 : (k == 2) ? 1 : (k == 3) ? 0 : (k == 4) ? 1 : 0;
 }
 
+// ---------------------------------------------------------------------------
+// Log-spherical helpers. The reference's device code calls the float
+// functions expf, sinf, cosf, acosf, logf, atan2f (unqualified calls on
+// float arguments); these are the same functions, with their CUDA
+// accuracy, so only the transcendentals differ from an FP32 CPU run.
+
+// Quadmesh::pos(i, n, pos_in_cell) (quadmesh.h:144-150).
+__device__ __forceinline__ float mesh_pos(float lower, float delta, int n, int guard, float x) {
+  return lower + delta * ((float)(n - guard) + x);
+}
+
+// beta_phi (field_solver_logsph.cu:16-20).
+__device__ __forceinline__ float beta_phi(float compactness, float omega, float r, float theta) {
+  return -0.4f * compactness * omega * sinf(theta) / (r * r);
+}
+
+// logsph2cart / cart2logsph (ptc_updater_logsph.cu:26-44).
+__device__ __forceinline__ void logsph2cart(float &v1, float &v2, float &v3, float x2, float x3) {
+  const float v1n = v1, v2n = v2, v3n = v3;
+  const float c2 = cosf(x2), s2 = sinf(x2), c3 = cosf(x3), s3 = sinf(x3);
+  v1 = v1n * s2 * c3 + v2n * c2 * c3 - v3n * s3;
+  v2 = v1n * s2 * s3 + v2n * c2 * s3 + v3n * c3;
+  v3 = v1n * c2 - v2n * s2;
+}
+__device__ __forceinline__ void cart2logsph(float &v1, float &v2, float &v3, float x2, float x3) {
+  const float v1n = v1, v2n = v2, v3n = v3;
+  const float c2 = cosf(x2), s2 = sinf(x2), c3 = cosf(x3), s3 = sinf(x3);
+  v1 = v1n * s2 * c3 + v2n * s2 * s3 + v3n * c2;
+  v2 = v1n * c2 * c3 + v2n * c2 * s3 - v3n * s2;
+  v3 = -v1n * s3 + v2n * c3;
+}
+
+// sync_kill_perp (sync_cooling.cuh:59-86); B1..B3 are the pusher's scaled
+// fields, divided back by q_over_m here as the reference does.
+__device__ __forceinline__ void sync_kill_perp(float &p1, float &p2, float &p3, float &gamma,
+                                               float B1, float B2, float B3, float q_over_m,
+                                               float coef, float B0) {
+  B1 /= q_over_m;
+  B2 /= q_over_m;
+  B3 /= q_over_m;
+  float p = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+  const float B_sqr = B1 * B1 + B2 * B2 + B3 * B3;
+  const float pdotB = (p1 * B1 + p2 * B2 + p3 * B3);
+  const float delta_p1 = -coef * (p1 - B1 * pdotB / B_sqr);
+  const float delta_p2 = -coef * (p2 - B2 * pdotB / B_sqr);
+  const float delta_p3 = -coef * (p3 - B3 * pdotB / B_sqr);
+  const float f = sqrtf(B_sqr) / B0;
+  p1 += delta_p1 * f;
+  p2 += delta_p2 * f;
+  p3 += delta_p3 * f;
+  p = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+  gamma = sqrtf(1.0f + p * p);
+}
+
 // Zone-based wrap of one coordinate after a move of at most one cell
 // (find_zone, quadmesh.h:264-273; cell shift of copy_component_to_buffer,
 // kernels.cu:134-142). Returns false when the particle leaves through a

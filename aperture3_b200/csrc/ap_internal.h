@@ -28,6 +28,7 @@ struct MeshK {
   int red[3];
   float delta[3];
   float inv_delta[3];
+  float lower[3];
   int dim;
   unsigned long long div0;  // floor(2^64 / dims[0]) + 1: c / dims[0] = umul64hi(c, div0)
 };
@@ -95,6 +96,12 @@ struct PushDepositParams {
   uint32_t *queue;
   DevStatus *status;
   size_t number;         // 1D: particle slots
+  // log-spherical push / move (ap_logsph_params)
+  float ls_compactness, ls_omega, ls_gravity, ls_rad_coef, ls_B0;
+  int ls_rad_on;
+  int ls_outflow_c1;     // dims[0] - damping_length + 2
+  float mass[AP_MAX_SPECIES];
+  FieldArr dV;           // cell volumes (J3 and Rho are divided by them)
 };
 
 // Per-context state.
@@ -154,6 +161,13 @@ struct Ctx {
   float *tmp_j = nullptr;
   int tmp_pitch = 0;
 
+  // log-spherical grid (ap_ctx_create_logsph)
+  int coord = 0;                // 0 Cartesian, 1 log-spherical
+  ap_logsph_params lsp{};
+  float *coef = nullptr;        // AP_NUM_COEF arrays of dims[0] x dims[1]
+  size_t coef_pitch = 0;        // bytes per row
+  float ls_kfac = 1.0f;         // bound of |J3 contribution| / (|q| w)
+
   // per-phase event timing (ap_set_profiling)
   bool profiling = false;
   struct EventPair {
@@ -191,6 +205,16 @@ cudaError_t launch_zero(Ctx &c, ap_array a);
 cudaError_t launch_finalize_current(Ctx &c, int ncomp);
 cudaError_t launch_fixed_scale(Ctx &c);
 cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
+
+// log-spherical (k_logsph.cu)
+int logsph_setup(Ctx &c);  // coefficients on the host, upload, J3 bound
+ap_array coef_array(const Ctx &c, int which);
+cudaError_t launch_ls_finalize(Ctx &c, float dt, bool do_rho, bool zero_axis);
+cudaError_t launch_ls_smooth(Ctx &c, bool do_rho);
+cudaError_t launch_ls_update_b(Ctx &c, float dt);
+cudaError_t launch_ls_update_e(Ctx &c, float dt);
+cudaError_t launch_ls_divs(Ctx &c);
+cudaError_t launch_ls_field_boundary(Ctx &c, float omega);
 
 MeshK make_meshk(const ap_mesh &m);
 int ensure_scratch(Ctx &c, size_t n);

@@ -137,8 +137,8 @@ struct TileGeom {
   static constexpr int SP = CH + CH / 64;  // staged chunk, one pad word per 64
   static constexpr int HDR = 128;     // mbarrier, tile id, abort flag, counters
   static constexpr size_t stage_bytes() { return 10 * 4 * SP + 2 * SP; }
-  static size_t smem_bytes(int nrho) {
-    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + stage_bytes();
+  static size_t smem_bytes(int nrho, bool ls = false) {
+    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + stage_bytes() + (ls ? 4 * JSZ : 0);
   }
 };
 
@@ -147,8 +147,9 @@ __device__ __forceinline__ int spos(int e) { return e + (e >> 6); }
 // Write-back modes of a staged particle.
 constexpr uint8_t kWritePos = 1;  // x1, x2, x3, cell
 constexpr uint8_t kWriteMom = 2;  // p1, p2, p3, E
+constexpr uint8_t kWriteFlag = 4; // flag (log-spherical outflow)
 
-template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho>
+template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho, bool kLS>
 __global__ void __launch_bounds__(kThreads2D, MINB)
     k_push_deposit_2d(const __grid_constant__ PushDepositParams P,
                       const __grid_constant__ FieldMaps maps) {
@@ -173,6 +174,9 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
   uint32_t *s_idx = reinterpret_cast<uint32_t *>(st + 9 * SP);
   uint8_t *s_dir = reinterpret_cast<uint8_t *>(st + 10 * SP);
   uint8_t *s_mode = s_dir + SP;
+  // log-spherical: cell volumes over the J tile window
+  float *s_dv = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(st) +
+                                          G::stage_bytes());
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -225,6 +229,12 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
     for (int i = tid; i < nacc; i += kThreads2D) {
       sJhi[i] = 0;
       sJlo[i] = 0u;
+    }
+    if constexpr (kLS) {
+      for (int i = tid; i < G::JSZ; i += kThreads2D) {
+        const int gx = jx0 + i % G::JX, gy = jy0 + i / G::JX;
+        s_dv[i] = (gx < dims0 && gy < dims1) ? P.dV.ptr[(size_t)gy * P.dV.pitch + gx] : 1.0f;
+      }
     }
     if (kTMA) {
       if (!mbar_wait(mbar, phase)) atomicExch(s_abort, 1);
@@ -291,6 +301,9 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
           const int sp = ptc_type(flag);
           float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
           const bool em = !(flag & kFlagIgnoreEM);
+          // log-spherical: r at the particle (user_push_2d_logsph.cuh:36)
+          float r_push = 0.0f;
+          if constexpr (kLS) r_push = expf(mesh_pos(P.m.lower[0], P.m.delta[0], c1, g0, x1));
           if (em) {
             const float qm = P.qm[sp];
             const Weights1D Wx = weights_1d(x1, c1);
@@ -315,18 +328,77 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
               fe[q] = acc * qm;
             }
             vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
+            if constexpr (kLS) {
+              // gravity (gravity.cuh:12-26), applied with strength
+              // dev_params.gravity on every push, then sync_kill_perp
+              // when radiative cooling is on and the particle is no ion.
+              p1 -= P.dt * P.ls_gravity * P.mass[sp] / (r_push * r_push * fabsf(P.charge[sp]));
+              gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
+              if (gamma != gamma) atomicAdd(&P.status->nan_momenta, 1ull);
+              if (P.ls_rad_on && sp != 2)
+                sync_kill_perp(p1, p2, p3, gamma, fe[3], fe[4], fe[5], qm, P.ls_rad_coef,
+                               P.ls_B0);
+            }
           } else {
             gamma = P.p.E[s_idx[s]];  // the deposit reads the stored gamma
           }
-          // deposit_current_cart_2d (ptc_updater.cu:295-386)
-          const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
-          float nx1 = x1 + (v1 * P.dt) * P.m.inv_delta[0];
-          float nx2 = x2 + (v2 * P.dt) * P.m.inv_delta[1];
-          const int dc1 = (int)floorf(nx1);
-          const int dc2 = (int)floorf(nx2);
-          nx1 -= (float)dc1;
-          nx2 -= (float)dc2;
-          const float nx3 = x3 + v3 * P.dt;
+          float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
+          float nx1, nx2, nx3;
+          int dc1, dc2;
+          if constexpr (!kLS) {
+            // deposit_current_cart_2d (ptc_updater.cu:295-386)
+            nx1 = x1 + (v1 * P.dt) * P.m.inv_delta[0];
+            nx2 = x2 + (v2 * P.dt) * P.m.inv_delta[1];
+            dc1 = (int)floorf(nx1);
+            dc2 = (int)floorf(nx2);
+            nx1 -= (float)dc1;
+            nx2 -= (float)dc2;
+            nx3 = x3 + v3 * P.dt;
+          } else {
+            // deposit_and_move_2d_log_sph (ptc_updater_logsph.cu:163-233):
+            // move in Cartesian space, return to (ln r, theta, phi), rotate
+            // the velocity into the new local basis, reflect at the axis.
+            const float r1 = mesh_pos(P.m.lower[0], P.m.delta[0], c1, g0, x1);
+            const float exp_r1 = expf(r1);
+            const float r2 = mesh_pos(P.m.lower[1], P.m.delta[1], c2, g1, x2);
+            v3 = v3 - beta_phi(P.ls_compactness, P.ls_omega, exp_r1, r2);
+            float x = exp_r1 * sinf(r2) * cosf(x3);
+            float y = exp_r1 * sinf(r2) * sinf(x3);
+            float z = exp_r1 * cosf(r2);
+            logsph2cart(v1, v2, v3, r2, x3);
+            x += 1.0f * v1 * P.dt;  // alpha_gr(r) = 1
+            y += 1.0f * v2 * P.dt;
+            z += 1.0f * v3 * P.dt;
+            float r1p = sqrtf(x * x + y * y + z * z);
+            const float r2p = acosf(z / r1p);
+            const float exp_r1p = r1p;
+            r1p = logf(r1p);
+            const float r3p = atan2f(y, x);
+            cart2logsph(v1, v2, v3, r2p, r3p);
+            p1 = v1 * gamma;
+            p2 = v2 * gamma;
+            p3 = (v3 + beta_phi(P.ls_compactness, P.ls_omega, exp_r1p, r2p)) * gamma;
+            nx1 = x1 + (r1p - r1) / P.m.delta[0];
+            nx2 = x2 + (r2p - r2) / P.m.delta[1];
+            dc1 = (int)floorf(nx1);
+            dc2 = (int)floorf(nx2);
+            nx1 -= (float)dc1;
+            nx2 -= (float)dc2;
+            if (mesh_pos(P.m.lower[1], P.m.delta[1], c2 + dc2, g1, nx2) < 0.0f) {
+              dc2 += 1;
+              nx2 = 1.0f - nx2;
+              p2 = -p2;
+              p3 = -p3;
+            }
+            if ((double)mesh_pos(P.m.lower[1], P.m.delta[1], c2 + dc2, g1, nx2) >=
+                3.14159265358979323846) {
+              dc2 -= 1;
+              nx2 = 1.0f - nx2;
+              p2 = -p2;
+              p3 = -p3;
+            }
+            nx3 = r3p;
+          }
           const bool far = dc1 > 1 || dc1 < -1 || dc2 > 1 || dc2 < -1;
 
           if (!far && !(flag & kFlagIgnoreCurrent)) {
@@ -372,7 +444,10 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
                   djy[a] += movement2d(sx0[a], sx1[a], sy0, sy1);
                   if (b < 2) add_fixed(J2, o + G::JX, weight * djy[a], fscale, fx.L);
                   const float val2 = center2d(sx0[a], sx1[a], sy0, sy1);
-                  add_fixed(J3, o, -weight * v3 * val2, fscale, fx.L);
+                  if constexpr (kLS)
+                    add_fixed(J3, o, -weight * v3 * val2 / s_dv[o], fscale, fx.L);
+                  else
+                    add_fixed(J3, o, -weight * v3 * val2, fscale, fx.L);
                   if (rho) {
                     const float s1 = sx1[a] * sy1;
                     add_fixed(R, o, -weight * s1, fscale, fx.L);
@@ -396,6 +471,13 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
             if (dty > 1) dty = -1;
             if (dty < -1) dty = 1;
             dir = (uint32_t)((dty + 1) * 3 + (dtx + 1));
+            if constexpr (kLS) {
+              // ptc_outflow (ptc_updater_logsph.cu:440-455)
+              if (!(flag & kFlagIgnoreEM) && c1n > P.ls_outflow_c1) {
+                s_flag[s] = flag | kFlagIgnoreEM;
+                mode |= kWriteFlag;
+              }
+            }
           } else {
             dir = kDirGone;
             if (far)
@@ -407,8 +489,8 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
           s_x2[s] = nx2;
           s_x3[s] = nx3;
           s_cell[s] = ncell;
-          mode = kWritePos;
-          if (em) {
+          mode |= kWritePos;
+          if (em || kLS) {
             s_p1[s] = p1;
             s_p2[s] = p2;
             s_p3[s] = p3;
@@ -442,6 +524,7 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
             P.p.p3[idx] = s_p3[s];
             P.p.E[idx] = s_w[s];
           }
+          if (kLS && (mode & kWriteFlag)) P.p.flag[idx] = s_flag[s];
           P.dir[base + c0 + e] = s_dir[s];
         }
       }
@@ -644,11 +727,11 @@ __global__ void __launch_bounds__(kThreads1D)
   }
 }
 
-template <int TX, int TY, int CH, int MINB>
+template <int TX, int TY, int CH, int MINB, bool kLS = false>
 cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
   using G = TileGeom<TX, TY, CH>;
   const int nrho = P.do_rho ? P.num_species : 0;
-  const size_t smem = G::smem_bytes(nrho);
+  const size_t smem = G::smem_bytes(nrho, kLS);
   cudaError_t e = cudaMemsetAsync(P.queue, 0, sizeof(uint32_t), c.stream);
   if (e != cudaSuccess) return e;
   auto run = [&](auto kern) -> cudaError_t {
@@ -667,17 +750,20 @@ cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
     return cudaGetLastError();
   };
   if (c.use_tma) {
-    return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, true, true>)
-                    : run(k_push_deposit_2d<TX, TY, CH, MINB, true, false>);
+    return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, true, true, kLS>)
+                    : run(k_push_deposit_2d<TX, TY, CH, MINB, true, false, kLS>);
   }
-  return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, false, true>)
-                  : run(k_push_deposit_2d<TX, TY, CH, MINB, false, false>);
+  return P.do_rho ? run(k_push_deposit_2d<TX, TY, CH, MINB, false, true, kLS>)
+                  : run(k_push_deposit_2d<TX, TY, CH, MINB, false, false, kLS>);
 }
 
 // Staged chunk of 1024 particles with three CTAs per SM (default), or 2048
 // with two.
 template <int TX, int TY>
 cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
+  // log-spherical: chunk 1024, two CTAs per SM (more registers per thread
+  // for the transcendental move)
+  if (c.coord == 1) return launch_2d_tiles<TX, TY, 1024, 2, true>(c, P);
   if (c.params.chunk == 2048) return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
   return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
 }

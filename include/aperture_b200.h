@@ -198,6 +198,53 @@ AP_API int ap_get_stats(ap_ctx *ctx, ap_step_stats *stats);
  * computes per-particle gamma, cuda/core/particles.cu:10-22). */
 AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
 
+/* ---------------------------------------------------------------------
+ * Log-spherical (ln r, theta) grids: ptc_updater_logsph and
+ * field_solver_logsph (src/algorithms/ptc_updater_logsph.h:13-28,
+ * field_solver_logsph.h:10-20). Dimension 0 is ln r, dimension 1 is
+ * theta in [lower, lower + size]; both dims non-periodic.
+ *
+ * The dev_params members these kernels read (src/sim_params.h:31-48):
+ * user_push_2d_logsph.cuh:14-114 (gravity, rad_cooling_*, B0),
+ * field_solver_logsph.cu:16-26 (compactness, omega in beta_phi),
+ * ptc_updater_logsph.cu:440-455 and field_solver_logsph.cu:322-345
+ * (damping_length, damping_coef). */
+typedef struct {
+  float compactness;
+  float omega;
+  float gravity;          /* applied every push, as the reference does */
+  float rad_cooling_coef;
+  float B0;
+  float damping_coef;
+  int rad_cooling_on;
+  int damping_length;
+} ap_logsph_params;
+
+/* Coefficient arrays of Grid_LogSph (grid_log_sph.h:45-47). */
+enum {
+  AP_COEF_L1E = 0, AP_COEF_L2E, AP_COEF_L3E, AP_COEF_L1B, AP_COEF_L2B,
+  AP_COEF_L3B, AP_COEF_A1E, AP_COEF_A2E, AP_COEF_A3E, AP_COEF_A1B,
+  AP_COEF_A2B, AP_COEF_A3B, AP_COEF_DV, AP_NUM_COEF
+};
+
+/* Creates a log-spherical context: ap_ctx_create plus Grid_LogSph::
+ * compute_coef (grid_log_sph.cpp:11-126), evaluated on the host in the
+ * reference's float / double arithmetic and kept on the device. With such
+ * a context ap_update_particles runs ptc_updater_logsph::update_particles
+ * followed by its apply_boundary (ptc_updater_logsph.cu:681-836),
+ * ap_update_fields runs field_solver_logsph::update_fields
+ * (field_solver_logsph.cu:354-398; its step argument is unused) and
+ * ap_compute_divs runs compute_divs_logsph. */
+AP_API int ap_ctx_create_logsph(const ap_mesh *mesh, const ap_params *params,
+                                const ap_logsph_params *lsp, ap_ctx **out);
+/* Device view of one coefficient array (mesh_ptrs_log_sph,
+ * cuda/grids/grid_log_sph_ptrs.h:8-17); which is an AP_COEF_* value. */
+AP_API int ap_logsph_coef(ap_ctx *ctx, int which, ap_array *out);
+/* field_solver_logsph::apply_boundary(data, omega, time)
+ * (field_solver_logsph.cu:403-428) on one rank: stellar surface, outflow
+ * damping, and both axes. */
+AP_API int ap_logsph_field_boundary(ap_ctx *ctx, double omega);
+
 /* Device time per phase of the update, from CUDA events recorded on the
  * context's stream around each phase while profiling is on. */
 typedef struct {
