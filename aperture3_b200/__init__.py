@@ -10,11 +10,13 @@ loads the library and fails if it is missing.
 """
 from . import _lib  # noqa: F401
 from .sim import (FLAG_IGNORE_CURRENT, FLAG_IGNORE_EM, ELECTRON, ION, POSITRON, FieldSolver,
-                  PtcUpdater, SimData, SimEnvironment, SimParams, field_solver, ptc_updater,
+                  FieldSolverLogsph, PtcUpdater, PtcUpdaterLogsph, SimData, SimEnvironment,
+                  SimParams, field_solver, field_solver_logsph, ptc_updater, ptc_updater_logsph,
                   species_flag)
 
 __all__ = [
     "SimParams", "SimEnvironment", "SimData", "ptc_updater", "field_solver", "PtcUpdater",
-    "FieldSolver", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
+    "FieldSolver", "ptc_updater_logsph", "field_solver_logsph", "PtcUpdaterLogsph",
+    "FieldSolverLogsph", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
     "FLAG_IGNORE_CURRENT",
 ]

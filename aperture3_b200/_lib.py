@@ -88,6 +88,17 @@ class ApPhaseTimes(C.Structure):
                 ("push_deposit_launches", C.c_uint64)]
 
 
+class ApLogsphParams(C.Structure):
+    """ap_logsph_params: the dev_params members of the log-spherical kernels."""
+    _fields_ = [("compactness", C.c_float), ("omega", C.c_float), ("gravity", C.c_float),
+                ("rad_cooling_coef", C.c_float), ("B0", C.c_float),
+                ("damping_coef", C.c_float), ("rad_cooling_on", C.c_int),
+                ("damping_length", C.c_int)]
+
+
+COEF_NAMES = ("l1_e", "l2_e", "l3_e", "l1_b", "l2_b", "l3_b",
+              "A1_e", "A2_e", "A3_e", "A1_b", "A2_b", "A3_b", "dV")
+
 _vp = C.c_void_p
 _i = C.c_int
 # name -> (restype, argtypes); every function declared in aperture_b200.h
@@ -121,6 +132,10 @@ SIGNATURES = {
     "ap_get_phase_times": (_i, [_vp, C.POINTER(ApPhaseTimes), _i]),
     "ap_last_error": (_i, [_vp]),
     "ap_launch_count": (C.c_uint64, [_vp]),
+    "ap_ctx_create_logsph": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
+                                  C.POINTER(ApLogsphParams), C.POINTER(_vp)]),
+    "ap_logsph_coef": (_i, [_vp, _i, C.POINTER(ApArray)]),
+    "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),
     "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                             C.POINTER(ApParticles), C.c_size_t,
                                             C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),

@@ -16,8 +16,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (AP_MAX_CELL, AP_MAX_SPECIES, ApArray, ApDiag, ApFields, ApMesh, ApParams,
-                   ApParticles, ApStepStats, check)
+from ._lib import (AP_MAX_CELL, AP_MAX_SPECIES, ApArray, ApDiag, ApFields, ApLogsphParams,
+                   ApMesh, ApParams, ApParticles, ApStepStats, check)
 
 PTC_FIELDS = (
     ("x1", torch.float32), ("x2", torch.float32), ("x3", torch.float32),
@@ -58,6 +58,15 @@ class SimParams:
     max_steps: int = 0
     tile_size: Sequence[int] = (0, 0, 0)
     chunk: int = 0
+    # log-spherical grids (coord_system "LogSpherical"; src/sim_params.h:31-48)
+    coord_system: str = "Cartesian"
+    compactness: float = 0.5
+    omega: float = 0.2
+    gravity: float = 0.0
+    rad_cooling_on: bool = False
+    rad_cooling_coef: float = 1.0
+    damping_length: int = 30
+    damping_coef: float = 0.002
 
     @classmethod
     def from_toml(cls, path: str) -> "SimParams":
@@ -111,8 +120,18 @@ class SimEnvironment:
         self.ap_params = ap
         self._lib = _lib.lib()
         ctx = C.c_void_p()
-        check(self._lib.ap_ctx_create(C.byref(self.mesh), C.byref(ap), C.byref(ctx)),
-              "ap_ctx_create")
+        self.logsph = str(params.coord_system).lower() in ("logspherical", "logsph", "log_sph")
+        if self.logsph:
+            lp = ApLogsphParams(float(params.compactness), float(params.omega),
+                                float(params.gravity), float(params.rad_cooling_coef),
+                                float(params.B0), float(params.damping_coef),
+                                int(bool(params.rad_cooling_on)), int(params.damping_length))
+            self.ls_params = lp
+            check(self._lib.ap_ctx_create_logsph(C.byref(self.mesh), C.byref(ap), C.byref(lp),
+                                                 C.byref(ctx)), "ap_ctx_create_logsph")
+        else:
+            check(self._lib.ap_ctx_create(C.byref(self.mesh), C.byref(ap), C.byref(ctx)),
+                  "ap_ctx_create")
         self.ctx = ctx
 
     @staticmethod
@@ -164,6 +183,15 @@ class SimEnvironment:
         for a in (field if isinstance(field, (list, tuple)) else [field]):
             check(self._lib.ap_send_add_guard_cells(self.ctx, array_view(a)),
                   "ap_send_add_guard_cells")
+
+    def logsph_coef(self, which: int) -> np.ndarray:
+        """Host copy of one Grid_LogSph coefficient array (grid_log_sph.h:45-47),
+        shape (dims[1], dims[0])."""
+        a = ApArray()
+        check(self._lib.ap_logsph_coef(self.ctx, int(which), C.byref(a)), "ap_logsph_coef")
+        d0, d1 = self.mesh.dims[0], self.mesh.dims[1]
+        rows = device_to_host(a.ptr, a.pitch * d1).view(np.float32).reshape(d1, -1)
+        return rows[:, :d0].copy()
 
     def launch_count(self) -> int:
         return int(self._lib.ap_launch_count(self.ctx))
@@ -401,6 +429,45 @@ class field_solver:
         check(self.env._lib.ap_update_b_field(self.env.ctx, float(dt)), "ap_update_b_field")
 
 
+class ptc_updater_logsph:
+    """ptc_updater_logsph (src/algorithms/ptc_updater_logsph.h:13-28)."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.logsph:
+            raise ValueError("ptc_updater_logsph needs coord_system = 'LogSpherical'")
+        self.env = env
+
+    def update_particles(self, data: SimData, dt: float, step: int = 0):
+        """update_particles then apply_boundary (ptc_updater_logsph.cu:681-836)."""
+        check(self.env._lib.ap_update_particles(self.env.ctx, float(dt), int(step)),
+              "ap_update_particles")
+
+    def apply_boundary(self, data: SimData, dt: float, step: int = 0):
+        """Run by update_particles already (axis current, outflow flags, and
+        dropping particles that left the grid)."""
+
+
+class field_solver_logsph:
+    """field_solver_logsph (src/algorithms/field_solver_logsph.h:10-20)."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.logsph:
+            raise ValueError("field_solver_logsph needs coord_system = 'LogSpherical'")
+        self.env = env
+
+    def update_fields(self, data: SimData, dt: float, time: float = 0.0):
+        check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), 0), "ap_update_fields")
+
+    def apply_boundary(self, data: SimData, omega: float, time: float = 0.0):
+        check(self.env._lib.ap_logsph_field_boundary(self.env.ctx, float(omega)),
+              "ap_logsph_field_boundary")
+
+    def compute_divs(self, data: SimData):
+        check(self.env._lib.ap_compute_divs(self.env.ctx), "ap_compute_divs")
+
+
 # Python-style aliases
 PtcUpdater = ptc_updater
 FieldSolver = field_solver
+PtcUpdaterLogsph = ptc_updater_logsph
+FieldSolverLogsph = field_solver_logsph
