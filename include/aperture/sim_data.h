@@ -75,6 +75,26 @@ struct sim_data {
     bind();
   }
 
+  // sim_data::init_bg_B_field / init_bg_E_field (src/sim_data.h:23-37):
+  // the background and the field itself start from f, guards refreshed.
+  template <class Func>
+  void init_bg_B_field(int component, const Func &f) {
+    Bbg.initialize(component, f);
+    B.initialize(component, f);
+    env.send_array_guard_cells(Bbg.data(component));
+    env.send_array_guard_cells(B.data(component));
+  }
+  template <class Func>
+  void init_bg_E_field(int component, const Func &f) {
+    Ebg.initialize(component, f);
+    E.initialize(component, f);
+    env.send_array_guard_cells(Ebg.data(component));
+    env.send_array_guard_cells(E.data(component));
+  }
+  // The device keeps the background fields in Ebg / Bbg, which the kernels
+  // read directly; nothing to upload (cuda/sim_data.cu:224-228).
+  void init_bg_fields() {}
+
   // Tells the library that particle slots changed outside its calls (after
   // filling or editing them on the host or with other kernels).
   void particles_modified() {

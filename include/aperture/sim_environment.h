@@ -6,6 +6,7 @@
 #define APERTURE_DROPIN_SIM_ENVIRONMENT_H_
 
 #include <cmath>
+#include <cstring>
 
 #include "multi_array.h"
 #include "sim_params.h"
@@ -58,7 +59,22 @@ class sim_environment {
     p.tile[0] = p.tile[1] = 0;
     p.chunk = 0;
     ap_params_ = p;
-    ap_check(ap_ctx_create(&m, &p, &ctx_), "ap_ctx_create");
+    if (std::strcmp(params.coord_system, "LogSpherical") == 0) {
+      // Grid_LogSph (src/grids/grid_log_sph.cpp:11-126): the library
+      // computes the coefficient arrays when the context is created
+      ap_logsph_params lp{};
+      lp.compactness = params.compactness;
+      lp.omega = params.omega;
+      lp.gravity = params.gravity;
+      lp.rad_cooling_coef = params.rad_cooling_coef;
+      lp.B0 = params.B0;
+      lp.damping_coef = params.damping_coef;
+      lp.rad_cooling_on = params.rad_cooling_on ? 1 : 0;
+      lp.damping_length = params.damping_length;
+      ap_check(ap_ctx_create_logsph(&m, &p, &lp, &ctx_), "ap_ctx_create_logsph");
+    } else {
+      ap_check(ap_ctx_create(&m, &p, &ctx_), "ap_ctx_create");
+    }
   }
   ~sim_environment() {
     if (ctx_) ap_ctx_destroy(ctx_);

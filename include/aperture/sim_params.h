@@ -28,6 +28,15 @@ struct SimParams {
   float lower[3] = {0.0, 0.0, 0.0};
   float size[3] = {1.0, 1.0, 1.0};
   int tile_size[3] = {1, 1, 1};
+  // log-spherical grids (src/sim_params.h:31-48, 110)
+  const char *coord_system = "Cartesian";
+  Scalar compactness = 0.5;
+  float omega = 0.2;
+  Scalar gravity = 0.0;
+  bool rad_cooling_on = false;
+  Scalar rad_cooling_coef = 1.0;
+  int damping_length = 30;
+  float damping_coef = 0.002;
 };
 
 }  // namespace Aperture

@@ -9,11 +9,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = "/usr/local/cuda"
 
 
-def _build(tmp_path):
-    exe = str(tmp_path / "box_lab")
+def _build(tmp_path, lab="box_lab"):
+    exe = str(tmp_path / lab)
     libdir = os.path.join(ROOT, "aperture3_b200")
     cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
-           "-I", f"{CUDA}/include", os.path.join(ROOT, "tests", "cpp", "box_lab.cpp"),
+           "-I", f"{CUDA}/include", os.path.join(ROOT, "tests", "cpp", lab + ".cpp"),
            "-o", exe, "-L", libdir, "-laperture_b200", f"-Wl,-rpath,{libdir}",
            "-L", f"{CUDA}/lib64", "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -23,6 +23,7 @@ def _build(tmp_path):
 
 def test_dropin_headers_compile(tmp_path):
     _build(tmp_path)
+    _build(tmp_path, "pulsar_lab")
 
 
 @pytest.mark.gpu
@@ -30,3 +31,10 @@ def test_dropin_box_lab_runs(tmp_path):
     exe = _build(tmp_path)
     r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "box_lab ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_dropin_pulsar_lab_runs(tmp_path):
+    exe = _build(tmp_path, "pulsar_lab")
+    r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "pulsar_lab ok" in r.stdout, r.stdout + r.stderr
