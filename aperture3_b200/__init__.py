@@ -9,13 +9,13 @@ sim_data) over that ABI. There is no CPU fallback: importing the classes
 loads the library and fails if it is missing.
 """
 from . import _lib  # noqa: F401
-from .sim import (FLAG_IGNORE_CURRENT, FLAG_IGNORE_EM, ELECTRON, ION, POSITRON, FieldSolver,
+from .sim import (Batch, FLAG_IGNORE_CURRENT, FLAG_IGNORE_EM, ELECTRON, ION, POSITRON, FieldSolver,
                   FieldSolverLogsph, PtcUpdater, PtcUpdaterLogsph, SimData, SimEnvironment,
                   SimParams, field_solver, field_solver_logsph, ptc_updater, ptc_updater_logsph,
                   species_flag)
 
 __all__ = [
-    "SimParams", "SimEnvironment", "SimData", "ptc_updater", "field_solver", "PtcUpdater",
+    "Batch", "SimParams", "SimEnvironment", "SimData", "ptc_updater", "field_solver", "PtcUpdater",
     "FieldSolver", "ptc_updater_logsph", "field_solver_logsph", "PtcUpdaterLogsph",
     "FieldSolverLogsph", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
     "FLAG_IGNORE_CURRENT",

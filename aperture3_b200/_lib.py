@@ -136,6 +136,16 @@ SIGNATURES = {
                                   C.POINTER(ApLogsphParams), C.POINTER(_vp)]),
     "ap_logsph_coef": (_i, [_vp, _i, C.POINTER(ApArray)]),
     "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),
+    "ap_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
+    "ap_batch_destroy": (_i, [_vp]),
+    "ap_batch_set_stream": (_i, [_vp, _vp]),
+    "ap_batch_update_particles": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32]),
+    "ap_batch_update_fields": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32]),
+    "ap_batch_sort_by_cell": (_i, [_vp]),
+    "ap_batch_sync": (_i, [_vp, C.POINTER(_i)]),
+    "ap_batch_autotune": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32, C.POINTER(_i)]),
+    "ap_set_tile_shape": (_i, [_vp, _i, _i]),
+    "ap_get_tile_shape": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
     "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                             C.POINTER(ApParticles), C.c_size_t,
                                             C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),

@@ -404,7 +404,7 @@ AP_API int ap_smooth_array(ap_ctx *c, ap_array a) {
   return finish(c);
 }
 
-static int smooth_current_async(ap_ctx *c, uint32_t step) {
+static int smooth_current_async(Ctx *c, uint32_t step) {
   int bnd[4] = {!c->params.periodic[0], !c->params.periodic[0], !c->params.periodic[1],
                 !c->params.periodic[1]};
   const bool out = ((step + 1) % (uint32_t)c->params.data_interval) == 0;
@@ -430,8 +430,14 @@ AP_API int ap_smooth_current(ap_ctx *c, uint32_t step) {
   return finish(c);
 }
 
-AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
-  if (!c || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+}  // extern "C"
+
+namespace apb {
+
+// First part of an update: zero the accumulators, refresh the weight bound
+// and the tile order if needed, and fill the kernel parameters. Returns
+// AP_OK; *has_work is false when there are no particles.
+int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work) {
   const ap_params &pr = c->params;
   const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
   // data.J.initialize(); data.Rho[i].initialize() (ptc_updater.cu:752-755):
@@ -448,9 +454,9 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
   phase_end(c, ph);
 
+  std::memset(&P, 0, sizeof(P));
+  *has_work = c->number > 0;
   if (c->number > 0) {
-    PushDepositParams P;
-    std::memset(&P, 0, sizeof(P));
     P.m = c->mk;
     P.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
                c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
@@ -500,12 +506,7 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
       P.dV = FieldArr{dv.ptr, (int)(dv.pitch / 4)};
       P.qmax *= c->ls_kfac;
     }
-    if (c->mk.dim == 1) {
-      ph = phase_begin(c, kPhPushDeposit);
-      AP_TRY(launch_push_deposit_1d(*c, P));
-      phase_end(c, ph);
-      c->pd_launches++;
-    } else {
+    if (c->mk.dim == 2) {
       if (!c->order_valid) {
         ph = phase_begin(c, kPhRebuild);
         AP_TRY(rebuild_tile_order(*c));
@@ -517,25 +518,32 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
       P.dir = c->dir;
       P.dir_count = c->dir_count;
       P.queue = c->queue;
-      ph = phase_begin(c, kPhPushDeposit);
-      AP_TRY(launch_push_deposit_2d(*c, P));
-      phase_end(c, ph);
-      c->pd_launches++;
-      if (incremental_order(*c)) {
-        const int nxt = c->cur ^ 1;
-        ph = phase_begin(c, kPhOrder);
-        AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
-        AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur], c->order[c->cur], c->dir,
-                                    c->grp_off, c->order[nxt]));
-        phase_end(c, ph);
-        c->cur = nxt;
-      } else {
-        c->order_valid = false;
-      }
     }
   }
-  // send_add_guard_cells(J), and Rho on output steps (ptc_updater.cu:800-805),
-  // fused with the FP64 -> FP32 rounding
+  return AP_OK;
+}
+
+// Last part: the tile-order update from the directions the kernel wrote,
+// then rounding (and folding / process_j) of the current and smoothing.
+int update_complete(Ctx *c, double dt, uint32_t step, bool had_work) {
+  const ap_params &pr = c->params;
+  const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
+  const int ncomp = 3 + (do_rho ? pr.num_species : 0);
+  const bool ls = c->coord == 1;
+  int ph;
+  if (had_work && c->mk.dim == 2) {
+    if (incremental_order(*c)) {
+      const int nxt = c->cur ^ 1;
+      ph = phase_begin(c, kPhOrder);
+      AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
+      AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur], c->order[c->cur], c->dir,
+                                  c->grp_off, c->order[nxt]));
+      phase_end(c, ph);
+      c->cur = nxt;
+    } else {
+      c->order_valid = false;
+    }
+  }
   ph = phase_begin(c, kPhFinalize);
   if (ls) {
     // process_j, then (ptc_updater_logsph::apply_boundary) axis_rho after
@@ -545,10 +553,33 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
     if (pr.current_smoothing > 0) AP_TRY(launch_ls_smooth(*c, do_rho));
     phase_end(c, ph);
   } else {
+    // send_add_guard_cells(J), and Rho on output steps (ptc_updater.cu:800-805),
+    // fused with the rounding of the exact sums
     AP_TRY(launch_finalize_current(*c, ncomp));
     phase_end(c, ph);
     AP_TRY_ST(smooth_current_async(c, step));
   }
+  return AP_OK;
+}
+
+int ctx_check_status(Ctx *c) { return check_status(c); }
+
+}  // namespace apb
+
+extern "C" {
+
+AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
+  if (!c || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  PushDepositParams P;
+  bool has_work = false;
+  AP_TRY_ST(update_prepare(c, dt, step, P, &has_work));
+  if (has_work) {
+    const int ph = phase_begin(c, kPhPushDeposit);
+    AP_TRY(c->mk.dim == 1 ? launch_push_deposit_1d(*c, P) : launch_push_deposit_2d(*c, P));
+    phase_end(c, ph);
+    c->pd_launches++;
+  }
+  AP_TRY_ST(update_complete(c, dt, step, has_work));
   if (!c->sync) return AP_OK;
   return check_status(c);
 }
@@ -726,6 +757,36 @@ AP_API int ap_logsph_field_boundary(ap_ctx *c, double omega) {
   if (!c || !c->fields_bound || c->coord != 1) return AP_ERR_INVALID;
   AP_TRY(launch_ls_field_boundary(*c, (float)omega));
   return finish(c);
+}
+
+AP_API int ap_set_tile_shape(ap_ctx *c, int tx, int ty) {
+  if (!c || c->mk.dim != 2 || !is_supported_tile(tx, ty)) return AP_ERR_INVALID;
+  if (c->stream) AP_TRY(cudaStreamSynchronize(c->stream));
+  c->params.tile[0] = tx;
+  c->params.tile[1] = ty;
+  choose_tiles(*c);
+  const size_t nt = (size_t)c->tiles.ntiles;
+  cudaFree(c->dir_count);
+  cudaFree(c->grp_off);
+  cudaFree(c->newcount);
+  cudaFree(c->tile_start[0]);
+  cudaFree(c->tile_start[1]);
+  c->dir_count = c->grp_off = c->newcount = c->tile_start[0] = c->tile_start[1] = nullptr;
+  AP_TRY(cudaMalloc(&c->dir_count, sizeof(uint32_t) * (nt * 10 + 16)));
+  AP_TRY(cudaMalloc(&c->grp_off, sizeof(uint32_t) * (nt * 9 + 16)));
+  AP_TRY(cudaMalloc(&c->newcount, sizeof(uint32_t) * (nt + 16)));
+  AP_TRY(cudaMalloc(&c->tile_start[0], sizeof(uint32_t) * (nt + 1)));
+  AP_TRY(cudaMalloc(&c->tile_start[1], sizeof(uint32_t) * (nt + 1)));
+  if (c->fields_bound) c->use_tma = setup_tensor_maps(*c);
+  c->order_valid = false;
+  return AP_OK;
+}
+
+AP_API int ap_get_tile_shape(const ap_ctx *c, int *tx, int *ty) {
+  if (!c || !tx || !ty) return AP_ERR_INVALID;
+  *tx = c->tiles.tx;
+  *ty = c->tiles.ty;
+  return AP_OK;
 }
 
 AP_API int ap_last_error(const ap_ctx *c) { return c ? c->last_error : AP_ERR_INVALID; }

@@ -1,0 +1,365 @@
+// Batched mode: many independent 2D Cartesian runs advanced together.
+//
+// Each run is an ordinary context. A step of the batch enqueues, on one
+// stream and without host synchronisation: each run's zeroing (and tile
+// order rebuild when needed), ONE persistent push / deposit launch per
+// group of runs that share a tile shape, chunk and field-load path (CTAs
+// draw (run, tile) items from one queue over all the group's tiles, so
+// small runs fill the GPU together), then each run's order update and
+// current finalize. The per-run kernel parameters and tensor maps go to
+// the device as an array of RunDesc through a double-buffered pinned
+// staging area.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "ap_internal.h"
+
+using namespace apb;
+
+struct ap_ctx : public apb::Ctx {};
+
+namespace {
+
+struct Group {
+  int tx, ty, chunk;
+  bool tma;
+  std::vector<int> members;  // indices into the batch's runs
+};
+
+}  // namespace
+
+struct ap_batch {
+  std::vector<Ctx *> runs;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  // staging: RunDesc[nruns] then base[nruns + 2 * groups] per slot
+  unsigned char *h_stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  int slot = 0;
+  unsigned char *d_stage = nullptr;
+  size_t stage_bytes = 0;
+  uint32_t *queue = nullptr;
+  // autotuning: time the push / deposit per class when set
+  bool tuning = false;
+  std::vector<int> tune_class;   // class of each run
+  std::vector<float> tune_ms;    // per class, last step
+  std::vector<cudaEvent_t> tune_ev;
+};
+
+namespace {
+
+int stage_layout(const ap_batch *b, size_t *desc_bytes) {
+  *desc_bytes = sizeof(RunDesc) * b->runs.size();
+  return AP_OK;
+}
+
+void release(ap_batch *b) {
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int i = 0; i < 2; ++i) {
+    if (b->h_stage[i]) cudaFreeHost(b->h_stage[i]);
+    if (b->stage_ev[i]) cudaEventDestroy(b->stage_ev[i]);
+  }
+  cudaFree(b->d_stage);
+  cudaFree(b->queue);
+  for (cudaEvent_t e : b->tune_ev) cudaEventDestroy(e);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+}
+
+std::vector<Group> make_groups(const ap_batch *b, const std::vector<bool> &active,
+                               const std::vector<int> *only_class, int cls) {
+  std::map<std::tuple<int, int, int, bool>, int> idx;
+  std::vector<Group> gs;
+  for (int r = 0; r < (int)b->runs.size(); ++r) {
+    if (!active[r]) continue;
+    if (only_class && (*only_class)[r] != cls) continue;
+    const Ctx *c = b->runs[r];
+    const int chunk = c->params.chunk == 2048 ? 2048 : 1024;
+    auto key = std::make_tuple(c->tiles.tx, c->tiles.ty, chunk, c->use_tma);
+    auto it = idx.find(key);
+    if (it == idx.end()) {
+      idx[key] = (int)gs.size();
+      gs.push_back(Group{c->tiles.tx, c->tiles.ty, chunk, c->use_tma, {}});
+      it = idx.find(key);
+    }
+    gs[it->second].members.push_back(r);
+  }
+  return gs;
+}
+
+int fail_cuda(cudaError_t e) {
+  return e == cudaErrorMemoryAllocation ? AP_ERR_NOMEM : AP_ERR_CUDA;
+}
+
+#define B_TRY(expr)                                 \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) return fail_cuda(_e);    \
+  } while (0)
+
+#define B_TRY_ST(expr)               \
+  do {                               \
+    int _s = (expr);                 \
+    if (_s != AP_OK) return _s;      \
+  } while (0)
+
+// Launches the push / deposit of the given groups from staged descriptors.
+int launch_groups(ap_batch *b, const std::vector<Group> &gs,
+                  const std::vector<PushDepositParams> &P, bool do_rho) {
+  if (gs.empty()) return AP_OK;
+  const int s = b->slot;
+  b->slot ^= 1;
+  B_TRY(cudaEventSynchronize(b->stage_ev[s]));  // the copy that last used this slot is done
+  RunDesc *hd = reinterpret_cast<RunDesc *>(b->h_stage[s]);
+  const size_t nr = b->runs.size();
+  uint32_t *hbase = reinterpret_cast<uint32_t *>(b->h_stage[s] + sizeof(RunDesc) * nr);
+  size_t k = 0, kb = 0;
+  std::vector<size_t> desc_off, base_off;
+  std::vector<uint32_t> totals;
+  std::vector<int> max_sp;
+  for (const Group &g : gs) {
+    desc_off.push_back(k);
+    base_off.push_back(kb);
+    uint32_t total = 0;
+    int msp = 1;
+    for (int r : g.members) {
+      hbase[kb++] = total;
+      std::memcpy(&hd[k].maps, &b->runs[r]->maps, sizeof(FieldMaps));
+      hd[k].P = P[r];
+      total += (uint32_t)b->runs[r]->tiles.ntiles;
+      msp = std::max(msp, b->runs[r]->params.num_species);
+      ++k;
+    }
+    hbase[kb++] = total;
+    totals.push_back(total);
+    max_sp.push_back(msp);
+  }
+  const size_t bytes = sizeof(RunDesc) * nr + sizeof(uint32_t) * kb;
+  B_TRY(cudaMemcpyAsync(b->d_stage, b->h_stage[s], bytes, cudaMemcpyHostToDevice, b->stream));
+  B_TRY(cudaEventRecord(b->stage_ev[s], b->stream));
+  const RunDesc *dd = reinterpret_cast<const RunDesc *>(b->d_stage);
+  const uint32_t *db = reinterpret_cast<const uint32_t *>(b->d_stage + sizeof(RunDesc) * nr);
+  for (size_t gi = 0; gi < gs.size(); ++gi) {
+    const Group &g = gs[gi];
+    B_TRY(launch_push_deposit_2d_batch(b->stream, b->num_sms, g.tx, g.ty, g.chunk, g.tma, do_rho,
+                                       max_sp[gi], dd + desc_off[gi], db + base_off[gi],
+                                       (int)g.members.size(), totals[gi], b->queue));
+    for (int r : g.members) {
+      b->runs[r]->launches++;
+      b->runs[r]->pd_launches++;
+    }
+  }
+  return AP_OK;
+}
+
+int batch_update(ap_batch *b, const double *dt, uint32_t step) {
+  const size_t n = b->runs.size();
+  std::vector<PushDepositParams> P(n);
+  std::vector<bool> work(n, false);
+  bool do_rho = false;
+  for (size_t r = 0; r < n; ++r) {
+    Ctx *c = b->runs[r];
+    bool w = false;
+    B_TRY_ST(update_prepare(c, dt[r], step, P[r], &w));
+    work[r] = w;
+    do_rho = ((step + 1) % (uint32_t)c->params.data_interval) == 0;
+  }
+  if (!b->tuning) {
+    B_TRY_ST(launch_groups(b, make_groups(b, work, nullptr, 0), P, do_rho));
+  } else {
+    const int ncls = (int)b->tune_ms.size();
+    for (int cl = 0; cl < ncls; ++cl) {
+      auto gs = make_groups(b, work, &b->tune_class, cl);
+      B_TRY(cudaEventRecord(b->tune_ev[2 * cl], b->stream));
+      B_TRY_ST(launch_groups(b, gs, P, do_rho));
+      B_TRY(cudaEventRecord(b->tune_ev[2 * cl + 1], b->stream));
+    }
+    B_TRY(cudaStreamSynchronize(b->stream));
+    for (int cl = 0; cl < ncls; ++cl) {
+      float ms = 0.0f;
+      B_TRY(cudaEventElapsedTime(&ms, b->tune_ev[2 * cl], b->tune_ev[2 * cl + 1]));
+      b->tune_ms[cl] = ms;
+    }
+  }
+  for (size_t r = 0; r < n; ++r) B_TRY_ST(update_complete(b->runs[r], dt[r], step, work[r]));
+  return AP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+AP_API int ap_batch_create(ap_ctx *const *runs, int nruns, ap_batch **out) {
+  if (!runs || nruns < 1 || !out) return AP_ERR_INVALID;
+  *out = nullptr;
+  for (int r = 0; r < nruns; ++r) {
+    const Ctx *c = runs[r];
+    if (!c || c->mk.dim != 2 || c->coord != 0 || !c->fields_bound || !c->ptc_bound)
+      return AP_ERR_INVALID;
+    for (int q = 0; q < r; ++q)
+      if (runs[q] == runs[r]) return AP_ERR_INVALID;
+    // one charge-deposition schedule for the whole batch
+    if (c->params.data_interval != runs[0]->params.data_interval) return AP_ERR_INVALID;
+  }
+  ap_batch *b = new (std::nothrow) ap_batch();
+  if (!b) return AP_ERR_NOMEM;
+  for (int r = 0; r < nruns; ++r) b->runs.push_back(runs[r]);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  size_t desc_bytes = 0;
+  stage_layout(b, &desc_bytes);
+  b->stage_bytes = desc_bytes + sizeof(uint32_t) * (2 * (size_t)nruns + 2);
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
+  b->own_stream = ok;
+  for (int i = 0; i < 2 && ok; ++i) {
+    ok = cudaMallocHost(reinterpret_cast<void **>(&b->h_stage[i]), b->stage_bytes) ==
+             cudaSuccess &&
+         cudaEventCreateWithFlags(&b->stage_ev[i], cudaEventDisableTiming) == cudaSuccess;
+    if (ok) ok = cudaEventRecord(b->stage_ev[i], b->stream) == cudaSuccess;
+  }
+  ok = ok && cudaMalloc(reinterpret_cast<void **>(&b->d_stage), b->stage_bytes) == cudaSuccess &&
+       cudaMalloc(reinterpret_cast<void **>(&b->queue), 16) == cudaSuccess;
+  if (!ok) {
+    release(b);
+    delete b;
+    return AP_ERR_NOMEM;
+  }
+  for (Ctx *c : b->runs) {
+    ap_set_stream(static_cast<ap_ctx *>(c), b->stream);
+    c->sync = false;
+  }
+  *out = b;
+  return AP_OK;
+}
+
+AP_API int ap_batch_destroy(ap_batch *b) {
+  if (!b) return AP_ERR_INVALID;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  // the runs go back to synchronous calls on the default stream
+  for (Ctx *c : b->runs) {
+    ap_set_stream(static_cast<ap_ctx *>(c), nullptr);
+    c->sync = true;
+  }
+  release(b);
+  delete b;
+  return AP_OK;
+}
+
+AP_API int ap_batch_set_stream(ap_batch *b, void *stream) {
+  if (!b) return AP_ERR_INVALID;
+  B_TRY(cudaStreamSynchronize(b->stream));
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  b->own_stream = false;
+  b->stream = static_cast<cudaStream_t>(stream);
+  for (Ctx *c : b->runs) ap_set_stream(static_cast<ap_ctx *>(c), b->stream);
+  for (int i = 0; i < 2; ++i) B_TRY(cudaEventRecord(b->stage_ev[i], b->stream));
+  return AP_OK;
+}
+
+AP_API int ap_batch_update_particles(ap_batch *b, const double *dt, uint32_t step) {
+  if (!b || !dt) return AP_ERR_INVALID;
+  return batch_update(b, dt, step);
+}
+
+AP_API int ap_batch_update_fields(ap_batch *b, const double *dt, uint32_t step) {
+  if (!b || !dt) return AP_ERR_INVALID;
+  for (size_t r = 0; r < b->runs.size(); ++r) {
+    int st = ap_update_fields(static_cast<ap_ctx *>(b->runs[r]), dt[r], step);
+    if (st != AP_OK) return st;
+  }
+  return AP_OK;
+}
+
+AP_API int ap_batch_sort_by_cell(ap_batch *b) {
+  if (!b) return AP_ERR_INVALID;
+  for (Ctx *c : b->runs) {
+    int st = ap_sort_by_cell(static_cast<ap_ctx *>(c));
+    if (st != AP_OK) return st;
+  }
+  return AP_OK;
+}
+
+AP_API int ap_batch_sync(ap_batch *b, int *failed_run) {
+  if (!b) return AP_ERR_INVALID;
+  if (failed_run) *failed_run = -1;
+  B_TRY(cudaStreamSynchronize(b->stream));
+  for (size_t r = 0; r < b->runs.size(); ++r) {
+    int st = ctx_check_status(b->runs[r]);
+    if (st != AP_OK) {
+      if (failed_run) *failed_run = (int)r;
+      return st;
+    }
+  }
+  return AP_OK;
+}
+
+AP_API int ap_batch_autotune(ap_batch *b, const double *dt, uint32_t step, int *steps_used) {
+  if (!b || !dt) return AP_ERR_INVALID;
+  // classes: runs with the same grid size
+  std::map<std::pair<int, int>, int> cls;
+  b->tune_class.assign(b->runs.size(), 0);
+  for (size_t r = 0; r < b->runs.size(); ++r) {
+    auto key = std::make_pair(b->runs[r]->mesh.dims[0], b->runs[r]->mesh.dims[1]);
+    auto it = cls.find(key);
+    if (it == cls.end()) it = cls.emplace(key, (int)cls.size()).first;
+    b->tune_class[r] = it->second;
+  }
+  const int ncls = (int)cls.size();
+  for (cudaEvent_t e : b->tune_ev) cudaEventDestroy(e);
+  b->tune_ev.assign(2 * ncls, nullptr);
+  for (auto &e : b->tune_ev) B_TRY(cudaEventCreate(&e));
+  b->tune_ms.assign(ncls, 0.0f);
+  const int cand[4][2] = {{16, 16}, {32, 16}, {16, 8}, {8, 8}};
+  std::vector<float> best(ncls, 1e30f);
+  std::vector<int> best_k(ncls, 0);
+  int used = 0;
+  b->tuning = true;
+  int st = AP_OK;
+  for (int k = 0; k < 4 && st == AP_OK; ++k) {
+    // a candidate needs three tiles per dim for the per-step order update
+    std::vector<bool> ok(ncls, false);
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+      const Ctx *c = b->runs[r];
+      const bool fits = (c->mk.red[0] + cand[k][0] - 1) / cand[k][0] >= 3 &&
+                        (c->mk.red[1] + cand[k][1] - 1) / cand[k][1] >= 3;
+      if (fits) {
+        ok[b->tune_class[r]] = true;
+        st = ap_set_tile_shape(static_cast<ap_ctx *>(b->runs[r]), cand[k][0], cand[k][1]);
+        if (st != AP_OK) break;
+      }
+    }
+    // the first step after a shape change includes the order rebuild: time
+    // the second
+    for (int rep = 0; rep < 2 && st == AP_OK; ++rep) {
+      st = batch_update(b, dt, step + (uint32_t)used);
+      if (st == AP_OK) st = ap_batch_update_fields(b, dt, step + (uint32_t)used);
+      ++used;
+    }
+    if (st != AP_OK) break;
+    for (int cl = 0; cl < ncls; ++cl)
+      if (ok[cl] && b->tune_ms[cl] < best[cl]) {
+        best[cl] = b->tune_ms[cl];
+        best_k[cl] = k;
+      }
+  }
+  b->tuning = false;
+  if (st == AP_OK)
+    for (size_t r = 0; r < b->runs.size() && st == AP_OK; ++r) {
+      const int k = best_k[b->tune_class[r]];
+      int tx = 0, ty = 0;
+      ap_get_tile_shape(static_cast<ap_ctx *>(b->runs[r]), &tx, &ty);
+      if (tx != cand[k][0] || ty != cand[k][1])
+        st = ap_set_tile_shape(static_cast<ap_ctx *>(b->runs[r]), cand[k][0], cand[k][1]);
+    }
+  if (steps_used) *steps_used = used;
+  return st;
+}
+
+}  // extern "C"

@@ -104,6 +104,13 @@ struct PushDepositParams {
   FieldArr dV;           // cell volumes (J3 and Rho are divided by them)
 };
 
+// One run of a batched launch: its tensor maps and its parameters, in
+// device memory (the maps must be 64-byte aligned).
+struct alignas(64) RunDesc {
+  FieldMaps maps;
+  PushDepositParams P;
+};
+
 // Per-context state.
 struct Ctx {
   int device = 0;
@@ -217,6 +224,22 @@ cudaError_t launch_ls_divs(Ctx &c);
 cudaError_t launch_ls_field_boundary(Ctx &c, float omega);
 
 MeshK make_meshk(const ap_mesh &m);
+
+// The update of one context in three parts (ap_api.cu): prepare (zeroing,
+// tile-order rebuild, kernel parameters), the push / deposit launch, and
+// complete (order update, finalize, smoothing). ctx_check_status reads the
+// device status word back (waits for the stream).
+int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work);
+int update_complete(Ctx *c, double dt, uint32_t step, bool had_work);
+int ctx_check_status(Ctx *c);
+
+// One persistent push / deposit launch over the tiles of several 2D
+// Cartesian runs with the same tile shape, chunk and field-load path.
+// runs / base are device arrays (base has nruns + 1 entries).
+cudaError_t launch_push_deposit_2d_batch(cudaStream_t stream, int num_sms, int tx, int ty,
+                                         int chunk, bool tma, bool do_rho, int max_species,
+                                         const RunDesc *runs, const uint32_t *base, int nruns,
+                                         uint32_t total_tiles, uint32_t *queue);
 int ensure_scratch(Ctx &c, size_t n);
 
 }  // namespace apb

@@ -149,10 +149,30 @@ constexpr uint8_t kWritePos = 1;  // x1, x2, x3, cell
 constexpr uint8_t kWriteMom = 2;  // p1, p2, p3, E
 constexpr uint8_t kWriteFlag = 4; // flag (log-spherical outflow)
 
-template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho, bool kLS>
-__global__ void __launch_bounds__(kThreads2D, MINB)
-    k_push_deposit_2d(const __grid_constant__ PushDepositParams P,
-                      const __grid_constant__ FieldMaps maps) {
+// Shared-memory copy of one run's parameters (batched launches only).
+template <bool kMulti>
+__device__ __forceinline__ uint32_t *param_smem() {
+  if constexpr (kMulti) {
+    __shared__ __align__(16) uint32_t buf[sizeof(PushDepositParams) / 4];
+    return buf;
+  } else {
+    return nullptr;
+  }
+}
+
+// The fused push + deposit over the tiles of one run (kMulti false: the
+// parameters P0 and tensor maps maps0 live in the kernel's parameter
+// space) or of a batch of runs (kMulti true: runs[r] in global memory,
+// run r owning tiles [base[r], base[r + 1]) of one queue; each CTA copies
+// the parameters of the run whose tile it takes into shared memory, so
+// the per-particle code reads them from there and not through global
+// loads that the particle stores could alias).
+template <int TX, int TY, int CH, bool kTMA, bool kRho, bool kLS, bool kMulti>
+__device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
+                                                   const CUtensorMap *maps0,
+                                                   const RunDesc *__restrict__ runs,
+                                                   const uint32_t *__restrict__ base, int nruns,
+                                                   uint32_t *queue) {
   using G = TileGeom<TX, TY, CH>;
   constexpr int SP = G::SP;
   constexpr int PER_THREAD = CH / kThreads2D;
@@ -162,33 +182,8 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
   int *s_abort = reinterpret_cast<int *>(smem + 12);
   uint32_t *s_cnt = reinterpret_cast<uint32_t *>(smem + 16);
   float *sF = reinterpret_cast<float *>(smem + G::HDR);
-  const int ncomp = 3 + (kRho ? P.num_species : 0);
-  int *sJhi = reinterpret_cast<int *>(sF + 6 * G::FSZ);
-  unsigned *sJlo = reinterpret_cast<unsigned *>(sJhi + ncomp * G::JSZ);
-  float *st = reinterpret_cast<float *>(sJlo + ncomp * G::JSZ);
-  float *s_x1 = st, *s_x2 = st + SP, *s_x3 = st + 2 * SP;
-  float *s_p1 = st + 3 * SP, *s_p2 = st + 4 * SP, *s_p3 = st + 5 * SP;
-  float *s_w = st + 6 * SP;  // weight in, gamma out
-  uint32_t *s_cell = reinterpret_cast<uint32_t *>(st + 7 * SP);
-  uint32_t *s_flag = reinterpret_cast<uint32_t *>(st + 8 * SP);
-  uint32_t *s_idx = reinterpret_cast<uint32_t *>(st + 9 * SP);
-  uint8_t *s_dir = reinterpret_cast<uint8_t *>(st + 10 * SP);
-  uint8_t *s_mode = s_dir + SP;
-  // log-spherical: cell volumes over the J tile window
-  float *s_dv = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(st) +
-                                          G::stage_bytes());
-
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
-  const int g0 = P.m.guard[0], g1 = P.m.guard[1];
-  const int nacc = ncomp * G::JSZ;
-
-  // fixed-point format of this update, from the largest tile population
-  const int lg = max(4, bits_of(*P.n_max));
-  const FixedFmt fx = fixed_format(lg, 63 - 2 * lg, P.qmax * *P.wmax);
-  const float fscale = ldexpf(1.0f, fx.S);
-  if (blockIdx.x == 0 && tid == 0) *P.fx_used = fx;
 
   if (tid == 0) {
     if (kTMA) mbar_init(mbar, 1);
@@ -196,13 +191,62 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
   }
   __syncthreads();
 
+  uint32_t *s_pbuf = param_smem<kMulti>();
   uint32_t phase = 0;
   for (;;) {
-    if (tid == 0) *s_tile = (int)atomicAdd(P.queue, 1u);
+    if (tid == 0) *s_tile = (int)atomicAdd(queue, 1u);
     if (tid < 10) s_cnt[tid] = 0;
     __syncthreads();
-    const int t = *s_tile;
-    if (t >= P.t.ntiles) break;
+    const int g = *s_tile;
+    const CUtensorMap *mp = maps0;
+    int t = g;
+    if constexpr (kMulti) {
+      if ((uint32_t)g >= base[nruns]) break;
+      int lo = 0, hi = nruns - 1;  // largest r with base[r] <= g
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= (uint32_t)g) lo = mid;
+        else hi = mid - 1;
+      }
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&runs[lo].P);
+      for (int i = tid; i < (int)(sizeof(PushDepositParams) / 4); i += kThreads2D)
+        s_pbuf[i] = src[i];
+      __syncthreads();
+      mp = runs[lo].maps.m;
+      t = g - (int)base[lo];
+    } else {
+      if (g >= P0.t.ntiles) break;
+    }
+    const PushDepositParams &P =
+        kMulti ? *reinterpret_cast<const PushDepositParams *>(s_pbuf) : P0;
+
+    // shared-memory layout of this run (the charge tile depends on its
+    // number of species)
+    const int ncomp = 3 + (kRho ? P.num_species : 0);
+    int *sJhi = reinterpret_cast<int *>(sF + 6 * G::FSZ);
+    unsigned *sJlo = reinterpret_cast<unsigned *>(sJhi + ncomp * G::JSZ);
+    float *st = reinterpret_cast<float *>(sJlo + ncomp * G::JSZ);
+    float *s_x1 = st, *s_x2 = st + SP, *s_x3 = st + 2 * SP;
+    float *s_p1 = st + 3 * SP, *s_p2 = st + 4 * SP, *s_p3 = st + 5 * SP;
+    float *s_w = st + 6 * SP;  // weight in, gamma out
+    uint32_t *s_cell = reinterpret_cast<uint32_t *>(st + 7 * SP);
+    uint32_t *s_flag = reinterpret_cast<uint32_t *>(st + 8 * SP);
+    uint32_t *s_idx = reinterpret_cast<uint32_t *>(st + 9 * SP);
+    uint8_t *s_dir = reinterpret_cast<uint8_t *>(st + 10 * SP);
+    uint8_t *s_mode = s_dir + SP;
+    // log-spherical: cell volumes over the J tile window
+    float *s_dv = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(st) +
+                                            G::stage_bytes());
+    const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
+    const int g0 = P.m.guard[0], g1 = P.m.guard[1];
+    const int nacc = ncomp * G::JSZ;
+
+    // fixed-point format of this update, from the largest tile population
+    const int lg = max(4, bits_of(*P.n_max));
+    const FixedFmt fx = fixed_format(lg, 63 - 2 * lg, P.qmax * *P.wmax);
+    const float fscale = ldexpf(1.0f, fx.S);
+    if (t == 0 && tid == 0) *P.fx_used = fx;
+
     const int tix = t % P.t.ntx, tiy = t / P.t.ntx;
     const int x0 = g0 + tix * TX, y0 = g1 + tiy * TY;
     const int xs = (x0 - 1) & ~3, ys = y0 - 1;
@@ -214,7 +258,7 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
         fence_proxy_async_smem();
         mbar_expect_tx(mbar, 6u * G::BX * G::BY * 4u);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) tma_load_2d(sF + k * G::FSZ, &maps.m[k], xs, ys, mbar);
+        for (int k = 0; k < 6; ++k) tma_load_2d(sF + k * G::FSZ, mp + k, xs, ys, mbar);
       }
     } else {
       for (int i = tid; i < 6 * G::BX * G::BY; i += kThreads2D) {
@@ -546,6 +590,23 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
   }
 }
 
+template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho, bool kLS>
+__global__ void __launch_bounds__(kThreads2D, MINB)
+    k_push_deposit_2d(const __grid_constant__ PushDepositParams P,
+                      const __grid_constant__ FieldMaps maps) {
+  push_deposit_tiles<TX, TY, CH, kTMA, kRho, kLS, false>(P, maps.m, nullptr, nullptr, 0, P.queue);
+}
+
+// Many independent Cartesian runs in one persistent launch: CTAs take
+// (run, tile) work items from one queue over all runs' tiles.
+template <int TX, int TY, int CH, int MINB, bool kTMA, bool kRho>
+__global__ void __launch_bounds__(kThreads2D, MINB)
+    k_push_deposit_2d_batch(const RunDesc *__restrict__ runs, const uint32_t *__restrict__ base,
+                            int nruns, uint32_t *queue) {
+  push_deposit_tiles<TX, TY, CH, kTMA, kRho, false, true>(runs[0].P, nullptr, runs, base, nruns,
+                                                           queue);
+}
+
 // ---------------------------------------------------------------------------
 // 1D: the whole line is small, so each CTA takes a contiguous chunk of
 // particle slots, finds the cell range it touches, and deposits into a
@@ -803,6 +864,69 @@ cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P) {
   if (tx == 8 && ty == 8) return launch_2d_chunk<8, 8>(c, P);
   if (tx == 16 && ty == 8) return launch_2d_chunk<16, 8>(c, P);
   if (tx == 4 && ty == 4) return launch_2d_chunk<4, 4>(c, P);
+  return cudaErrorInvalidValue;
+}
+
+namespace {
+
+template <int TX, int TY, int CH, int MINB>
+cudaError_t launch_batch_tiles(cudaStream_t stream, int num_sms, bool tma, bool do_rho,
+                               int max_species, const RunDesc *runs, const uint32_t *base,
+                               int nruns, uint32_t total, uint32_t *queue) {
+  using G = TileGeom<TX, TY, CH>;
+  const size_t smem = G::smem_bytes(do_rho ? max_species : 0);
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  auto run = [&](auto kern) -> cudaError_t {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads2D, smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint32_t grid = (uint32_t)num_sms * per_sm;
+    if (grid > total) grid = total;
+    if (grid < 1) grid = 1;
+    kern<<<grid, kThreads2D, smem, stream>>>(runs, base, nruns, queue);
+    return cudaGetLastError();
+  };
+  if (tma)
+    return do_rho ? run(k_push_deposit_2d_batch<TX, TY, CH, MINB, true, true>)
+                  : run(k_push_deposit_2d_batch<TX, TY, CH, MINB, true, false>);
+  return do_rho ? run(k_push_deposit_2d_batch<TX, TY, CH, MINB, false, true>)
+                : run(k_push_deposit_2d_batch<TX, TY, CH, MINB, false, false>);
+}
+
+template <int TX, int TY>
+cudaError_t launch_batch_chunk(cudaStream_t stream, int num_sms, int chunk, bool tma,
+                               bool do_rho, int max_species, const RunDesc *runs,
+                               const uint32_t *base, int nruns, uint32_t total,
+                               uint32_t *queue) {
+  if (chunk == 2048)
+    return launch_batch_tiles<TX, TY, 2048, 2>(stream, num_sms, tma, do_rho, max_species, runs,
+                                               base, nruns, total, queue);
+  return launch_batch_tiles<TX, TY, 1024, 3>(stream, num_sms, tma, do_rho, max_species, runs,
+                                             base, nruns, total, queue);
+}
+
+}  // namespace
+
+cudaError_t launch_push_deposit_2d_batch(cudaStream_t stream, int num_sms, int tx, int ty,
+                                         int chunk, bool tma, bool do_rho, int max_species,
+                                         const RunDesc *runs, const uint32_t *base, int nruns,
+                                         uint32_t total, uint32_t *queue) {
+  if (total == 0) return cudaSuccess;
+#define AP_BATCH_SHAPE(X, Y)                                                                 \
+  if (tx == X && ty == Y)                                                                    \
+    return launch_batch_chunk<X, Y>(stream, num_sms, chunk, tma, do_rho, max_species, runs, \
+                                    base, nruns, total, queue);
+  AP_BATCH_SHAPE(16, 16)
+  AP_BATCH_SHAPE(32, 16)
+  AP_BATCH_SHAPE(8, 8)
+  AP_BATCH_SHAPE(16, 8)
+  AP_BATCH_SHAPE(4, 4)
+#undef AP_BATCH_SHAPE
   return cudaErrorInvalidValue;
 }
 

@@ -429,6 +429,82 @@ class field_solver:
         check(self.env._lib.ap_update_b_field(self.env.ctx, float(dt)), "ap_update_b_field")
 
 
+class Batch:
+    """Batched mode (ap_batch_*): many independent 2D Cartesian runs, each a
+    SimData of its own SimEnvironment, advanced with one persistent
+    push / deposit launch per tile shape and no host synchronisation between
+    steps. Each run's particles equal those of the same run advanced alone."""
+
+    def __init__(self, runs: Sequence["SimData"]):
+        self.runs = list(runs)
+        self._lib = _lib.lib()
+        arr = (C.c_void_p * len(self.runs))(*[d.env.ctx.value for d in self.runs])
+        b = C.c_void_p()
+        check(self._lib.ap_batch_create(arr, len(self.runs), C.byref(b)), "ap_batch_create")
+        self.handle = b
+        # each run's own time step (SimParams.delta_t) unless one is given
+        self.dt = [float(d.env.params.delta_t) for d in self.runs]
+
+    def _dts(self, dt):
+        vals = self.dt if dt is None else (
+            [float(dt)] * len(self.runs) if np.isscalar(dt) else [float(x) for x in dt])
+        return (C.c_double * len(self.runs))(*vals)
+
+    def set_stream(self, stream: torch.cuda.Stream):
+        check(self._lib.ap_batch_set_stream(self.handle, C.c_void_p(stream.cuda_stream)),
+              "ap_batch_set_stream")
+
+    def update_particles(self, step: int, dt=None):
+        """One particle update of every run (dt: None for each run's own
+        delta_t, a scalar, or one value per run)."""
+        check(self._lib.ap_batch_update_particles(self.handle, self._dts(dt), int(step)),
+              "ap_batch_update_particles")
+
+    def update_fields(self, step: int, dt=None):
+        check(self._lib.ap_batch_update_fields(self.handle, self._dts(dt), int(step)),
+              "ap_batch_update_fields")
+
+    def sort_particles(self):
+        check(self._lib.ap_batch_sort_by_cell(self.handle), "ap_batch_sort_by_cell")
+        for d in self.runs:
+            n = C.c_size_t()
+            check(self._lib.ap_get_number(d.env.ctx, C.byref(n)), "ap_get_number")
+            d.number = int(n.value)
+
+    def sync(self):
+        bad = C.c_int(-1)
+        st = self._lib.ap_batch_sync(self.handle, C.byref(bad))
+        check(st, f"ap_batch_sync (run {bad.value})")
+
+    def autotune(self, step: int, dt=None) -> int:
+        """Runs the tile-shape autotuner; returns the number of complete
+        steps (particles, then fields) it advanced every run by."""
+        used = C.c_int(0)
+        check(self._lib.ap_batch_autotune(self.handle, self._dts(dt), int(step), C.byref(used)),
+              "ap_batch_autotune")
+        return int(used.value)
+
+    def tile_shapes(self):
+        out = []
+        for d in self.runs:
+            tx, ty = C.c_int(), C.c_int()
+            check(self._lib.ap_get_tile_shape(d.env.ctx, C.byref(tx), C.byref(ty)),
+                  "ap_get_tile_shape")
+            out.append((tx.value, ty.value))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.ap_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ptc_updater_logsph:
     """ptc_updater_logsph (src/algorithms/ptc_updater_logsph.h:13-28)."""
 

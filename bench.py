@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
+    ap.add_argument("--workload", default="box", choices=["box", "batched"],
+                    help="box: the 2D box (headline line); batched: many uneven boxes "
+                         "through ap_batch_* against the same runs one at a time")
+    ap.add_argument("--runs", type=int, default=24, help="batched: number of runs")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="seconds for the whole --impl reference run")
     return ap.parse_args()
@@ -402,6 +406,110 @@ def run_ours(args, rank, world, local_rank):
     env.close()
 
 
+AUTOTUNE_STEPS = 8  # 4 candidate tile shapes x 2 steps (ap_batch_autotune)
+
+
+def run_batched(args):
+    """Batched uneven boxes: `runs` independent periodic boxes, side uniform
+    in {128, 192, 256, 384, 512}, 16-128 particles per cell (even), the
+    box2d field setup, each with its own dt. Two legs from the same seeded
+    initial states, timing the same steps: one at a time through the plain
+    path (each run created, advanced with the lab loop -- synchronous
+    update_particles, update_fields, sort every sort_interval steps -- and
+    freed before the next), then all runs together through one batch, whose
+    first AUTOTUNE_STEPS steps are the autotuner's (the single runs take
+    the same steps untimed). Wall clock between device synchronisations;
+    aggregate particle-steps/s."""
+    import numpy as np
+    import torch
+    from aperture3_b200 import Batch, SimData, SimEnvironment, field_solver, ic, ptc_updater
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(4)
+    specs = [(int(rng.choice([128, 192, 256, 384, 512])), 2 * int(rng.integers(8, 65)))
+             for _ in range(args.runs)]
+
+    def make(r):
+        side, ppc = specs[r]
+        params, fields, ptc = ic.box2d(seed=5000 + r, N=side, ppc=ppc, device=dev)
+        n = ptc["x1"].numel()
+        env = SimEnvironment(params)
+        data = SimData(env, capacity=n)
+        data.set_fields_device(fields)
+        data.set_particles_device(ptc)
+        return env, data, n
+
+    s_first = AUTOTUNE_STEPS + args.warmup
+    steps = range(s_first, s_first + args.steps)
+
+    # one at a time through the plain path
+    t_alone, total = 0.0, 0
+    for r in range(len(specs)):
+        env, data, n = make(r)
+        total += n
+        pusher, solver = ptc_updater(env), field_solver(env)
+        dt = env.params.delta_t
+
+        def step(s):
+            pusher.update_particles(data, dt, s)
+            solver.update_fields(data, dt, s)
+            if s % args.sort_interval == 0 and s != 0:
+                data.sort_particles()
+        for s in range(s_first):
+            step(s)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in steps:
+            step(s)
+        torch.cuda.synchronize()
+        t_alone += time.perf_counter() - t0
+        env.close()
+        del data
+        torch.cuda.empty_cache()
+    alone = total * args.steps / t_alone
+
+    # the same runs in one batch
+    runs = [make(r) for r in range(len(specs))]
+    torch.cuda.synchronize()
+    batch = Batch([d for _, d, _ in runs])
+
+    def bstep(s):
+        batch.update_particles(s)
+        batch.update_fields(s)
+        if s % args.sort_interval == 0 and s != 0:
+            batch.sort_particles()
+    used = batch.autotune(0)
+    assert used == AUTOTUNE_STEPS, used
+    for s in range(used, s_first):
+        bstep(s)
+    batch.sync()
+    t0 = time.perf_counter()
+    for s in steps:
+        bstep(s)
+    batch.sync()
+    t_batch = time.perf_counter() - t0
+    batched = total * args.steps / t_batch
+    shapes = {}
+    for (side, ppc), shape in zip(specs, batch.tile_shapes()):
+        shapes[str(side)] = f"{shape[0]}x{shape[1]}"
+    batch.close()
+    line = {
+        "metric": "aggregate particle-steps/s (batched uneven boxes)", "value": batched,
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded, aperture3_b200.ic.box2d per run)",
+        "config": {"workload": f"{args.runs} periodic boxes, side in {{128,192,256,384,512}}, "
+                               "16-128 ppc, random-mode fields, own dt each",
+                   "runs": args.runs, "particles": total, "timed_steps": [steps[0], steps[-1]],
+                   "sides": [sp[0] for sp in specs], "ppc": [sp[1] for sp in specs]},
+        "one_at_a_time": alone, "speedup_vs_one_at_a_time": batched / alone,
+        "autotune_steps": used, "tile_shapes": shapes,
+    }
+    print(json.dumps(line), flush=True)
+    for env, _, _ in runs:
+        env.close()
+
+
 def run_e2e(args, env, data, pusher, solver, dt, stream, n):
     import torch
     from aperture3_b200._lib import ApDiag, check
@@ -474,6 +582,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
+        if args.workload == "batched":
+            if rank == 0:
+                run_batched(args)
+            return
         run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

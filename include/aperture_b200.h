@@ -245,6 +245,47 @@ AP_API int ap_logsph_coef(ap_ctx *ctx, int which, ap_array *out);
  * damping, and both axes. */
 AP_API int ap_logsph_field_boundary(ap_ctx *ctx, double omega);
 
+/* ---------------------------------------------------------------------
+ * Batched mode (new; the reference runs one simulation per process).
+ * A batch advances many independent 2D Cartesian runs, each an ordinary
+ * context with bound fields and particles, with ONE persistent
+ * push / deposit launch per tile shape over all runs' tiles, the small
+ * per-run kernels enqueued on one stream, and no host synchronisation
+ * between steps. Every run gives the same particles, bit for bit, as when
+ * it is advanced alone through ap_update_particles. All runs share one
+ * data_interval. The batch takes over the runs' streams and sets them
+ * asynchronous (ap_set_sync 0). */
+typedef struct ap_batch ap_batch;
+
+AP_API int ap_batch_create(ap_ctx *const *runs, int nruns, ap_batch **out);
+/* Destroy a batch before its runs; the runs go back to synchronous calls
+ * on the default stream. */
+AP_API int ap_batch_destroy(ap_batch *batch);
+/* Stream of the batch (default: a private non-blocking stream). */
+AP_API int ap_batch_set_stream(ap_batch *batch, void *cuda_stream);
+/* ap_update_particles for every run; dt[r] is the time step of run r (the
+ * runs advance in lockstep, each with its own dt). */
+AP_API int ap_batch_update_particles(ap_batch *batch, const double *dt, uint32_t step);
+/* ap_update_fields for every run, dt as above. */
+AP_API int ap_batch_update_fields(ap_batch *batch, const double *dt, uint32_t step);
+/* ap_sort_by_cell for every run. */
+AP_API int ap_batch_sort_by_cell(ap_batch *batch);
+/* Waits for the batch and returns the first non-OK device status of a run
+ * (run index in *failed_run, -1 if none; may be NULL). */
+AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
+/* Project autotuner: advances the batch by *steps_used complete steps
+ * (particle update, then field update) starting at `step`, timing the
+ * push / deposit of each class of runs (same grid size) with every
+ * candidate tile shape, and keeps the fastest shape per class. Particle
+ * results do not depend on the tile shape; J can differ in the last bits
+ * (the fixed-point scale follows the largest tile population). */
+AP_API int ap_batch_autotune(ap_batch *batch, const double *dt, uint32_t step,
+                             int *steps_used);
+/* Tile shape of one run (16x16, 32x16, 16x8, 8x8 or 4x4); rebuilds its
+ * tile order at the next update. */
+AP_API int ap_set_tile_shape(ap_ctx *ctx, int tx, int ty);
+AP_API int ap_get_tile_shape(const ap_ctx *ctx, int *tx, int *ty);
+
 /* Device time per phase of the update, from CUDA events recorded on the
  * context's stream around each phase while profiling is on. */
 typedef struct {

@@ -1,0 +1,119 @@
+"""Batched mode: many uneven periodic boxes, each with its own time step,
+advanced by one persistent push / deposit launch per tile shape
+(ap_batch_*). Each run in the batch must give the same particles, bit for
+bit, as the same run advanced alone through the plain path, and the same
+fields (bit for bit with the same tile shape; within 1e-6 of the maximum
+after the autotuner changed the shape, which moves the fixed-point scale of
+the current)."""
+import numpy as np
+import pytest
+
+import oracle
+from _cases import mesh_2d, random_fields, random_particles
+from _gpu_helpers import assert_bits, make_params
+from aperture3_b200 import Batch, SimData, SimEnvironment, field_solver, ptc_updater
+
+pytestmark = pytest.mark.gpu
+
+
+def _specs(seed, nruns):
+    rng = np.random.default_rng(seed)
+    return [(int(rng.choice([32, 48, 64, 96])), int(rng.choice([32, 48, 64])),
+             int(rng.integers(2, 9)), seed * 1000 + r) for r in range(nruns)]
+
+
+def _make(spec, data_interval=2):
+    N0, N1, ppc, s = spec
+    n = N0 * N1 * ppc
+    params = make_params((N0, N1), periodic=(True, True), capacity=n,
+                         data_interval=data_interval)
+    params.delta_t = float(np.float32(0.45 / max(N0, N1)))
+    rng = np.random.default_rng(s)
+    m = mesh_2d(N0, N1)
+    f = random_fields(m, rng, amp=0.3)
+    for key in ("E", "B", "Ebg", "Bbg"):
+        for c in range(3):
+            oracle.send_guard_cells(m, f[key][c], (1, 1, 0))
+    p = random_particles(m, n, rng, gamma_max=100.0)
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=n)
+    data.set_fields(f)
+    data.set_particles(p)
+    return env, data
+
+
+def _step_alone(runs, step):
+    for env, data in runs:
+        ptc_updater(env).update_particles(data, env.params.delta_t, step)
+        field_solver(env).update_fields(data, env.params.delta_t, step)
+
+
+def _compare(alone, batched, tol=0.0):
+    for r, ((_, da), (_, db)) in enumerate(zip(alone, batched)):
+        pa, pb = da.particles_host(), db.particles_host()
+        for k in ("x1", "x2", "x3", "p1", "p2", "p3", "E", "cell", "flag", "weight", "id"):
+            assert_bits(pb[k], pa[k], f"run {r}: particles.{k}")
+        fa, fb = da.fields_host(), db.fields_host()
+        for key in ("J", "E", "B"):
+            for c in range(3):
+                if tol == 0.0:
+                    assert_bits(fb[key][c], fa[key][c], f"run {r}: {key}{c + 1}")
+                else:
+                    scale = max(np.abs(fa[key][c]).max(), 1e-30)
+                    err = np.abs(fb[key][c].astype(np.float64) - fa[key][c]).max() / scale
+                    assert err <= tol, f"run {r}: {key}{c + 1} {err:.3g}"
+
+
+def _close(batch, *groups):
+    batch.close()
+    for g in groups:
+        for env, _ in g:
+            env.close()
+
+
+def test_batch_equals_alone():
+    specs = _specs(1, 12)
+    alone = [_make(s) for s in specs]
+    batched = [_make(s) for s in specs]
+    batch = Batch([d for _, d in batched])
+    assert len(set(batch.dt)) > 1  # uneven boxes, each with its own dt
+    for step in range(7):
+        _step_alone(alone, step)
+        batch.update_particles(step)
+        batch.update_fields(step)
+        if step == 3:
+            for _, data in alone:
+                data.sort_particles()
+            batch.sort_particles()
+    batch.sync()
+    _compare(alone, batched)
+    _close(batch, alone, batched)
+
+
+def test_batch_autotune_then_steps():
+    specs = _specs(2, 8)
+    alone = [_make(s) for s in specs]
+    batched = [_make(s) for s in specs]
+    batch = Batch([d for _, d in batched])
+    used = batch.autotune(0)
+    assert used >= 2
+    for step in range(used):
+        _step_alone(alone, step)
+    for step in range(used, used + 4):
+        _step_alone(alone, step)
+        batch.update_particles(step)
+        batch.update_fields(step)
+    batch.sync()
+    shapes = batch.tile_shapes()
+    assert all(s in ((16, 16), (32, 16), (16, 8), (8, 8)) for s in shapes)
+    _compare(alone, batched, tol=1e-6)
+    _close(batch, alone, batched)
+
+
+def test_batch_rejects_mixed_data_interval():
+    a = _make((32, 32, 2, 5), data_interval=2)
+    b = _make((32, 32, 2, 6), data_interval=3)
+    with pytest.raises(Exception):
+        Batch([a[1], b[1]])
+    a[0].close()
+    b[0].close()
