@@ -96,6 +96,13 @@ class ApLogsphParams(C.Structure):
                 ("damping_length", C.c_int)]
 
 
+class ApPairParams(C.Structure):
+    """ap_pair_params: pair injection of the served 1D gap runs."""
+    _fields_ = [("gamma_thr", C.c_float), ("free_path", C.c_float),
+                ("pair_energy", C.c_float), ("enabled", C.c_int), ("seed", C.c_uint64),
+                ("first_id", C.c_uint64)]
+
+
 COEF_NAMES = ("l1_e", "l2_e", "l3_e", "l1_b", "l2_b", "l3_b",
               "A1_e", "A2_e", "A3_e", "A1_b", "A2_b", "A3_b", "dV")
 
@@ -138,14 +145,24 @@ SIGNATURES = {
     "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),
     "ap_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "ap_batch_destroy": (_i, [_vp]),
+    "ap_batch_add": (_i, [_vp, _vp]),
+    "ap_batch_remove": (_i, [_vp, _vp]),
+    "ap_batch_size": (_i, [_vp, C.POINTER(_i)]),
     "ap_batch_set_stream": (_i, [_vp, _vp]),
-    "ap_batch_update_particles": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32]),
-    "ap_batch_update_fields": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32]),
+    "ap_batch_update_particles": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
+    "ap_batch_update_fields": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "ap_batch_sort_by_cell": (_i, [_vp]),
     "ap_batch_sync": (_i, [_vp, C.POINTER(_i)]),
-    "ap_batch_autotune": (_i, [_vp, C.POINTER(C.c_double), C.c_uint32, C.POINTER(_i)]),
+    "ap_batch_autotune": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                               C.POINTER(_i)]),
     "ap_set_tile_shape": (_i, [_vp, _i, _i]),
     "ap_get_tile_shape": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
+    "ap_set_pair_params": (_i, [_vp, C.POINTER(ApPairParams)]),
+    "ap_get_pair_stats": (_i, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                               C.POINTER(C.c_uint64)]),
+    "ap_inject_pairs": (_i, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64),
+                             C.POINTER(C.c_uint64)]),
+    "ap_batch_inject_pairs": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                             C.POINTER(ApParticles), C.c_size_t,
                                             C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),

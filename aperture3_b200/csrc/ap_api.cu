@@ -146,6 +146,7 @@ int finish(Ctx *c) {
 }
 
 int check_status(Ctx *c) {
+  if (refresh_number(c) != AP_OK) return fail(c, AP_ERR_CUDA);
   cudaError_t e = cudaMemcpyAsync(c->status_host, c->status, sizeof(DevStatus),
                                   cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e);
@@ -299,6 +300,9 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->cell_start);
   cudaFree(c->tmp_j);
   cudaFree(c->coef);
+  cudaFree(c->pair_chunks);
+  cudaFree(c->pstate);
+  if (c->pstate_host) cudaFreeHost(c->pstate_host);
   cudaFree(c->acc);
   cudaFree(c->fx_used);
   cudaFree(c->n_max);
@@ -350,6 +354,7 @@ AP_API int ap_bind_fields(ap_ctx *c, const ap_fields *f) {
     if (!valid_array(f->Rho[s], m)) return fail(c, AP_ERR_INVALID);
   c->fields = *f;
   c->fields_bound = true;
+  c->rho_is_zero = false;
   c->use_tma = setup_tensor_maps(*c);
   if (!c->acc) {
     c->acc_comp = (size_t)m.dims[0] * m.dims[1] * m.dims[2];
@@ -378,6 +383,7 @@ AP_API int ap_bind_particles(ap_ctx *c, const ap_particles *p, size_t number, si
   c->order_valid = false;
   c->scale_valid = false;
   AP_TRY_ST(alloc_particle_state(c, capacity));
+  AP_TRY_ST(push_number(c));
   return AP_OK;
 }
 
@@ -387,11 +393,13 @@ AP_API int ap_particles_modified(ap_ctx *c, size_t number) {
   c->number = number;
   c->order_valid = false;
   c->scale_valid = false;
+  AP_TRY_ST(push_number(c));
   return AP_OK;
 }
 
 AP_API int ap_get_number(const ap_ctx *c, size_t *n) {
   if (!c || !n) return AP_ERR_INVALID;
+  if (refresh_number(const_cast<ap_ctx *>(c)) != AP_OK) return AP_ERR_CUDA;
   *n = c->number;
   return AP_OK;
 }
@@ -449,14 +457,21 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
   AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
                          c->stream));
   if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
-  if (!do_rho && !ls)
+  // Rho keeps the zeros of the last step without charge deposition
+  if (!do_rho && !ls && !c->rho_is_zero) {
     for (int s = 0; s < pr.num_species; ++s) AP_TRY(launch_zero(*c, c->fields.Rho[s]));
+    c->rho_is_zero = true;
+  }
   AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
   phase_end(c, ph);
 
   std::memset(&P, 0, sizeof(P));
-  *has_work = c->number > 0;
-  if (c->number > 0) {
+  // with a device-side count, 1D kernels work over the capacity and read
+  // the live count on the device; 2D needs the host count for the order
+  const bool device_count = c->pstate && c->mk.dim == 1;
+  if (c->pstate && !device_count) AP_TRY_ST(refresh_number(c));
+  *has_work = device_count ? c->capacity > 0 : c->number > 0;
+  if (*has_work) {
     P.m = c->mk;
     P.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
                c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
@@ -489,7 +504,8 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
     P.do_rho = do_rho ? 1 : 0;
     for (int d = 0; d < 3; ++d) P.periodic[d] = pr.periodic[d];
     P.status = c->status;
-    P.number = c->number;
+    P.number = device_count ? c->capacity : c->number;
+    P.d_number = device_count ? &c->pstate->number : nullptr;
     if (ls) {
       // user_push_2d_logsph / deposit_and_move_2d_log_sph parameters; the
       // J3 contributions are divided by the cell volume, which widens the
@@ -530,6 +546,7 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work) {
   const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
   const int ncomp = 3 + (do_rho ? pr.num_species : 0);
   const bool ls = c->coord == 1;
+  if (do_rho || ls) c->rho_is_zero = false;  // the finalize writes Rho
   int ph;
   if (had_work && c->mk.dim == 2) {
     if (incremental_order(*c)) {
@@ -639,11 +656,18 @@ AP_API int ap_send_add_guard_cells(ap_ctx *c, ap_array a) {
 AP_API int ap_sort_by_cell(ap_ctx *c) {
   if (!c || !c->ptc_bound) return AP_ERR_INVALID;
   size_t n = 0;
+  // a 1D context with a device-side count sorts over its capacity and keeps
+  // the count on the device (no host synchronisation)
+  const bool device_count = c->pstate && c->mk.dim == 1;
+  if (!device_count) AP_TRY_ST(refresh_number(c));
   const int ph = phase_begin(c, kPhSort);
   c->order_valid = false;  // sort_by_cell rebuilds the 2D tile order
   AP_TRY(sort_by_cell(*c, &n));
   phase_end(c, ph);
-  c->number = n;
+  if (!device_count) {
+    c->number = n;
+    AP_TRY_ST(push_number(c));
+  }
   return AP_OK;
 }
 
@@ -664,6 +688,7 @@ AP_API int ap_get_tile_order(ap_ctx *c, const uint32_t **order, const uint32_t *
 
 AP_API int ap_get_stats(ap_ctx *c, ap_step_stats *s) {
   if (!c || !s) return AP_ERR_INVALID;
+  AP_TRY_ST(refresh_number(c));
   AP_TRY(cudaMemcpyAsync(c->status_host, c->status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                          c->stream));
   AP_TRY(cudaStreamSynchronize(c->stream));
@@ -683,6 +708,7 @@ AP_API int ap_get_stats(ap_ctx *c, ap_step_stats *s) {
 
 AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
   if (!c || !out || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  AP_TRY_ST(refresh_number(c));
   AP_TRY(launch_diagnostics(*c, c->diag_dev));
   AP_TRY(cudaMemcpyAsync(c->diag_host, c->diag_dev, sizeof(double) * 6, cudaMemcpyDeviceToHost,
                          c->stream));
@@ -757,6 +783,57 @@ AP_API int ap_logsph_field_boundary(ap_ctx *c, double omega) {
   if (!c || !c->fields_bound || c->coord != 1) return AP_ERR_INVALID;
   AP_TRY(launch_ls_field_boundary(*c, (float)omega));
   return finish(c);
+}
+
+AP_API int ap_set_pair_params(ap_ctx *c, const ap_pair_params *pp) {
+  if (!c || !pp) return AP_ERR_INVALID;
+  if (pp->enabled && (!(pp->free_path > 0.0f) || !(pp->pair_energy >= 0.0f) ||
+                      !(pp->gamma_thr > pp->pair_energy + 1.0f)))
+    return fail(c, AP_ERR_INVALID);
+  AP_TRY_ST(refresh_number(c));
+  if (!c->pstate) {
+    AP_TRY(cudaMalloc(&c->pstate, sizeof(PairState)));
+    AP_TRY(cudaMallocHost(reinterpret_cast<void **>(&c->pstate_host), sizeof(PairState)));
+  }
+  c->pair = *pp;
+  // the device state starts from the host count and the given first id
+  PairState s{};
+  s.number = (uint32_t)c->number;
+  s.next_id = pp->first_id;
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  AP_TRY(cudaMemcpy(c->pstate, &s, sizeof(s), cudaMemcpyHostToDevice));
+  c->number_stale = false;
+  return AP_OK;
+}
+
+AP_API int ap_get_pair_stats(ap_ctx *c, uint64_t *particle_steps, uint64_t *emitted_total,
+                             uint64_t *dropped_total) {
+  if (!c) return AP_ERR_INVALID;
+  if (!c->pstate) {
+    if (particle_steps) *particle_steps = 0;
+    if (emitted_total) *emitted_total = 0;
+    if (dropped_total) *dropped_total = 0;
+    return AP_OK;
+  }
+  c->number_stale = true;
+  AP_TRY_ST(refresh_number(c));
+  if (particle_steps) *particle_steps = c->pstate_host->particle_steps;
+  if (emitted_total) *emitted_total = c->pstate_host->emitted_total;
+  if (dropped_total) *dropped_total = c->pstate_host->dropped_total;
+  return AP_OK;
+}
+
+AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitted,
+                           uint64_t *dropped) {
+  if (!c || !c->ptc_bound) return AP_ERR_INVALID;
+  if (emitted) *emitted = 0;
+  if (dropped) *dropped = 0;
+  if (!c->pair.enabled) return AP_OK;
+  AP_TRY_ST(enqueue_pairs(*c, (float)dt, step));
+  AP_TRY_ST(refresh_number(c));
+  if (emitted) *emitted = c->pstate_host->emitted;
+  if (dropped) *dropped = c->pstate_host->dropped;
+  return AP_OK;
 }
 
 AP_API int ap_set_tile_shape(ap_ctx *c, int tx, int ty) {

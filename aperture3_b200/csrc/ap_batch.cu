@@ -27,10 +27,22 @@ struct ap_ctx : public apb::Ctx {};
 namespace {
 
 struct Group {
+  int dim;
   int tx, ty, chunk;
   bool tma;
   std::vector<int> members;  // indices into the batch's runs
 };
+
+// Work items of a run in a batched launch: tiles (2D) or chunks of
+// particle slots (1D).
+uint32_t work_items(const Ctx *c) {
+  if (c->mk.dim == 1) {
+    // with a device-side count the kernel covers the capacity
+    const size_t n = c->pstate ? c->capacity : c->number;
+    return (uint32_t)((n + kChunk1DSlots - 1) / kChunk1DSlots);
+  }
+  return (uint32_t)c->tiles.ntiles;
+}
 
 }  // namespace
 
@@ -45,6 +57,7 @@ struct ap_batch {
   int slot = 0;
   unsigned char *d_stage = nullptr;
   size_t stage_bytes = 0;
+  size_t cap_runs = 0;  // runs the staging buffers hold
   uint32_t *queue = nullptr;
   // autotuning: time the push / deposit per class when set
   bool tuning = false;
@@ -54,11 +67,6 @@ struct ap_batch {
 };
 
 namespace {
-
-int stage_layout(const ap_batch *b, size_t *desc_bytes) {
-  *desc_bytes = sizeof(RunDesc) * b->runs.size();
-  return AP_OK;
-}
 
 void release(ap_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
@@ -74,18 +82,21 @@ void release(ap_batch *b) {
 
 std::vector<Group> make_groups(const ap_batch *b, const std::vector<bool> &active,
                                const std::vector<int> *only_class, int cls) {
-  std::map<std::tuple<int, int, int, bool>, int> idx;
+  std::map<std::tuple<int, int, int, int, bool>, int> idx;
   std::vector<Group> gs;
   for (int r = 0; r < (int)b->runs.size(); ++r) {
     if (!active[r]) continue;
     if (only_class && (*only_class)[r] != cls) continue;
     const Ctx *c = b->runs[r];
-    const int chunk = c->params.chunk == 2048 ? 2048 : 1024;
-    auto key = std::make_tuple(c->tiles.tx, c->tiles.ty, chunk, c->use_tma);
+    const int dim = c->mk.dim;
+    const int chunk = dim == 1 ? kChunk1DSlots : (c->params.chunk == 2048 ? 2048 : 1024);
+    const int tx = dim == 1 ? 0 : c->tiles.tx, ty = dim == 1 ? 0 : c->tiles.ty;
+    const bool tma = dim == 1 ? false : c->use_tma;
+    auto key = std::make_tuple(dim, tx, ty, chunk, tma);
     auto it = idx.find(key);
     if (it == idx.end()) {
       idx[key] = (int)gs.size();
-      gs.push_back(Group{c->tiles.tx, c->tiles.ty, chunk, c->use_tma, {}});
+      gs.push_back(Group{dim, tx, ty, chunk, tma, {}});
       it = idx.find(key);
     }
     gs[it->second].members.push_back(r);
@@ -117,7 +128,7 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
   b->slot ^= 1;
   B_TRY(cudaEventSynchronize(b->stage_ev[s]));  // the copy that last used this slot is done
   RunDesc *hd = reinterpret_cast<RunDesc *>(b->h_stage[s]);
-  const size_t nr = b->runs.size();
+  const size_t nr = b->cap_runs;
   uint32_t *hbase = reinterpret_cast<uint32_t *>(b->h_stage[s] + sizeof(RunDesc) * nr);
   size_t k = 0, kb = 0;
   std::vector<size_t> desc_off, base_off;
@@ -132,7 +143,7 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
       hbase[kb++] = total;
       std::memcpy(&hd[k].maps, &b->runs[r]->maps, sizeof(FieldMaps));
       hd[k].P = P[r];
-      total += (uint32_t)b->runs[r]->tiles.ntiles;
+      total += work_items(b->runs[r]);
       msp = std::max(msp, b->runs[r]->params.num_species);
       ++k;
     }
@@ -140,16 +151,23 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
     totals.push_back(total);
     max_sp.push_back(msp);
   }
-  const size_t bytes = sizeof(RunDesc) * nr + sizeof(uint32_t) * kb;
-  B_TRY(cudaMemcpyAsync(b->d_stage, b->h_stage[s], bytes, cudaMemcpyHostToDevice, b->stream));
+  B_TRY(cudaMemcpyAsync(b->d_stage, b->h_stage[s], sizeof(RunDesc) * k, cudaMemcpyHostToDevice,
+                        b->stream));
+  B_TRY(cudaMemcpyAsync(b->d_stage + sizeof(RunDesc) * nr, b->h_stage[s] + sizeof(RunDesc) * nr,
+                        sizeof(uint32_t) * kb, cudaMemcpyHostToDevice, b->stream));
   B_TRY(cudaEventRecord(b->stage_ev[s], b->stream));
   const RunDesc *dd = reinterpret_cast<const RunDesc *>(b->d_stage);
   const uint32_t *db = reinterpret_cast<const uint32_t *>(b->d_stage + sizeof(RunDesc) * nr);
   for (size_t gi = 0; gi < gs.size(); ++gi) {
     const Group &g = gs[gi];
-    B_TRY(launch_push_deposit_2d_batch(b->stream, b->num_sms, g.tx, g.ty, g.chunk, g.tma, do_rho,
-                                       max_sp[gi], dd + desc_off[gi], db + base_off[gi],
-                                       (int)g.members.size(), totals[gi], b->queue));
+    if (g.dim == 1)
+      B_TRY(launch_push_deposit_1d_batch(b->stream, b->num_sms, do_rho, dd + desc_off[gi],
+                                         db + base_off[gi], (int)g.members.size(), totals[gi]));
+    else
+      B_TRY(launch_push_deposit_2d_batch(b->stream, b->num_sms, g.tx, g.ty, g.chunk, g.tma,
+                                         do_rho, max_sp[gi], dd + desc_off[gi],
+                                         db + base_off[gi], (int)g.members.size(), totals[gi],
+                                         b->queue));
     for (int r : g.members) {
       b->runs[r]->launches++;
       b->runs[r]->pd_launches++;
@@ -158,7 +176,7 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
   return AP_OK;
 }
 
-int batch_update(ap_batch *b, const double *dt, uint32_t step) {
+int batch_update(ap_batch *b, const double *dt, const uint32_t *steps) {
   const size_t n = b->runs.size();
   std::vector<PushDepositParams> P(n);
   std::vector<bool> work(n, false);
@@ -166,9 +184,11 @@ int batch_update(ap_batch *b, const double *dt, uint32_t step) {
   for (size_t r = 0; r < n; ++r) {
     Ctx *c = b->runs[r];
     bool w = false;
-    B_TRY_ST(update_prepare(c, dt[r], step, P[r], &w));
+    B_TRY_ST(update_prepare(c, dt[r], steps[r], P[r], &w));
     work[r] = w;
-    do_rho = ((step + 1) % (uint32_t)c->params.data_interval) == 0;
+    // one kernel variant for all: charge deposition when any run needs it
+    // (runs without it skip the charge terms through P.do_rho)
+    do_rho = do_rho || ((steps[r] + 1) % (uint32_t)c->params.data_interval) == 0;
   }
   if (!b->tuning) {
     B_TRY_ST(launch_groups(b, make_groups(b, work, nullptr, 0), P, do_rho));
@@ -187,8 +207,40 @@ int batch_update(ap_batch *b, const double *dt, uint32_t step) {
       b->tune_ms[cl] = ms;
     }
   }
-  for (size_t r = 0; r < n; ++r) B_TRY_ST(update_complete(b->runs[r], dt[r], step, work[r]));
+  for (size_t r = 0; r < n; ++r)
+    B_TRY_ST(update_complete(b->runs[r], dt[r], steps[r], work[r]));
   return AP_OK;
+}
+
+bool run_ok(const ap_ctx *c) {
+  return c && c->mk.dim <= 2 && c->coord == 0 && c->fields_bound && c->ptc_bound;
+}
+
+// Staging for up to n runs (descriptors and work-item offsets), grown
+// geometrically; waits for the stream before replacing buffers.
+int ensure_stage(ap_batch *b, size_t n) {
+  if (n <= b->cap_runs) return AP_OK;
+  size_t cap = b->cap_runs ? b->cap_runs : 8;
+  while (cap < n) cap *= 2;
+  if (b->stream) B_TRY(cudaStreamSynchronize(b->stream));
+  const size_t bytes = sizeof(RunDesc) * cap + sizeof(uint32_t) * (2 * cap + 2);
+  for (int i = 0; i < 2; ++i) {
+    if (b->h_stage[i]) cudaFreeHost(b->h_stage[i]);
+    b->h_stage[i] = nullptr;
+    B_TRY(cudaMallocHost(reinterpret_cast<void **>(&b->h_stage[i]), bytes));
+  }
+  cudaFree(b->d_stage);
+  b->d_stage = nullptr;
+  B_TRY(cudaMalloc(reinterpret_cast<void **>(&b->d_stage), bytes));
+  b->stage_bytes = bytes;
+  b->cap_runs = cap;
+  return AP_OK;
+}
+
+void adopt(ap_batch *b, ap_ctx *c) {
+  b->runs.push_back(c);
+  ap_set_stream(c, b->stream);
+  c->sync = false;
 }
 
 }  // namespace
@@ -196,46 +248,59 @@ int batch_update(ap_batch *b, const double *dt, uint32_t step) {
 extern "C" {
 
 AP_API int ap_batch_create(ap_ctx *const *runs, int nruns, ap_batch **out) {
-  if (!runs || nruns < 1 || !out) return AP_ERR_INVALID;
+  if ((nruns > 0 && !runs) || nruns < 0 || !out) return AP_ERR_INVALID;
   *out = nullptr;
   for (int r = 0; r < nruns; ++r) {
-    const Ctx *c = runs[r];
-    if (!c || c->mk.dim != 2 || c->coord != 0 || !c->fields_bound || !c->ptc_bound)
-      return AP_ERR_INVALID;
+    if (!run_ok(runs[r])) return AP_ERR_INVALID;
     for (int q = 0; q < r; ++q)
       if (runs[q] == runs[r]) return AP_ERR_INVALID;
-    // one charge-deposition schedule for the whole batch
-    if (c->params.data_interval != runs[0]->params.data_interval) return AP_ERR_INVALID;
   }
   ap_batch *b = new (std::nothrow) ap_batch();
   if (!b) return AP_ERR_NOMEM;
-  for (int r = 0; r < nruns; ++r) b->runs.push_back(runs[r]);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
-  size_t desc_bytes = 0;
-  stage_layout(b, &desc_bytes);
-  b->stage_bytes = desc_bytes + sizeof(uint32_t) * (2 * (size_t)nruns + 2);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
   b->own_stream = ok;
-  for (int i = 0; i < 2 && ok; ++i) {
-    ok = cudaMallocHost(reinterpret_cast<void **>(&b->h_stage[i]), b->stage_bytes) ==
-             cudaSuccess &&
-         cudaEventCreateWithFlags(&b->stage_ev[i], cudaEventDisableTiming) == cudaSuccess;
-    if (ok) ok = cudaEventRecord(b->stage_ev[i], b->stream) == cudaSuccess;
-  }
-  ok = ok && cudaMalloc(reinterpret_cast<void **>(&b->d_stage), b->stage_bytes) == cudaSuccess &&
-       cudaMalloc(reinterpret_cast<void **>(&b->queue), 16) == cudaSuccess;
+  for (int i = 0; i < 2 && ok; ++i)
+    ok = cudaEventCreateWithFlags(&b->stage_ev[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventRecord(b->stage_ev[i], b->stream) == cudaSuccess;
+  ok = ok && cudaMalloc(reinterpret_cast<void **>(&b->queue), 16) == cudaSuccess &&
+       ensure_stage(b, nruns > 8 ? nruns : 8) == AP_OK;
   if (!ok) {
     release(b);
     delete b;
     return AP_ERR_NOMEM;
   }
-  for (Ctx *c : b->runs) {
-    ap_set_stream(static_cast<ap_ctx *>(c), b->stream);
-    c->sync = false;
-  }
+  for (int r = 0; r < nruns; ++r) adopt(b, runs[r]);
   *out = b;
+  return AP_OK;
+}
+
+AP_API int ap_batch_add(ap_batch *b, ap_ctx *c) {
+  if (!b || !run_ok(c)) return AP_ERR_INVALID;
+  if (std::find(b->runs.begin(), b->runs.end(), static_cast<Ctx *>(c)) != b->runs.end())
+    return AP_ERR_INVALID;
+  B_TRY_ST(ensure_stage(b, b->runs.size() + 1));
+  adopt(b, c);
+  return AP_OK;
+}
+
+AP_API int ap_batch_remove(ap_batch *b, ap_ctx *c) {
+  if (!b || !c) return AP_ERR_INVALID;
+  auto it = std::find(b->runs.begin(), b->runs.end(), static_cast<Ctx *>(c));
+  if (it == b->runs.end()) return AP_ERR_INVALID;
+  B_TRY(cudaStreamSynchronize(b->stream));
+  b->runs.erase(it);
+  // the run goes back to synchronous calls on the default stream
+  ap_set_stream(c, nullptr);
+  c->sync = true;
+  return AP_OK;
+}
+
+AP_API int ap_batch_size(const ap_batch *b, int *nruns) {
+  if (!b || !nruns) return AP_ERR_INVALID;
+  *nruns = (int)b->runs.size();
   return AP_OK;
 }
 
@@ -263,15 +328,15 @@ AP_API int ap_batch_set_stream(ap_batch *b, void *stream) {
   return AP_OK;
 }
 
-AP_API int ap_batch_update_particles(ap_batch *b, const double *dt, uint32_t step) {
-  if (!b || !dt) return AP_ERR_INVALID;
-  return batch_update(b, dt, step);
+AP_API int ap_batch_update_particles(ap_batch *b, const double *dt, const uint32_t *steps) {
+  if (!b || !dt || !steps) return AP_ERR_INVALID;
+  return batch_update(b, dt, steps);
 }
 
-AP_API int ap_batch_update_fields(ap_batch *b, const double *dt, uint32_t step) {
-  if (!b || !dt) return AP_ERR_INVALID;
+AP_API int ap_batch_update_fields(ap_batch *b, const double *dt, const uint32_t *steps) {
+  if (!b || !dt || !steps) return AP_ERR_INVALID;
   for (size_t r = 0; r < b->runs.size(); ++r) {
-    int st = ap_update_fields(static_cast<ap_ctx *>(b->runs[r]), dt[r], step);
+    int st = ap_update_fields(static_cast<ap_ctx *>(b->runs[r]), dt[r], steps[r]);
     if (st != AP_OK) return st;
   }
   return AP_OK;
@@ -282,6 +347,16 @@ AP_API int ap_batch_sort_by_cell(ap_batch *b) {
   for (Ctx *c : b->runs) {
     int st = ap_sort_by_cell(static_cast<ap_ctx *>(c));
     if (st != AP_OK) return st;
+  }
+  return AP_OK;
+}
+
+AP_API int ap_batch_inject_pairs(ap_batch *b, const double *dt, const uint32_t *steps) {
+  if (!b || !dt || !steps) return AP_ERR_INVALID;
+  for (size_t r = 0; r < b->runs.size(); ++r) {
+    Ctx *c = b->runs[r];
+    if (!c->pair.enabled) continue;
+    B_TRY_ST(enqueue_pairs(*c, (float)dt[r], steps[r]));
   }
   return AP_OK;
 }
@@ -300,8 +375,10 @@ AP_API int ap_batch_sync(ap_batch *b, int *failed_run) {
   return AP_OK;
 }
 
-AP_API int ap_batch_autotune(ap_batch *b, const double *dt, uint32_t step, int *steps_used) {
-  if (!b || !dt) return AP_ERR_INVALID;
+AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *steps,
+                             int *steps_used) {
+  if (!b || !dt || !steps) return AP_ERR_INVALID;
+  std::vector<uint32_t> cur(steps, steps + b->runs.size());
   // classes: runs with the same grid size
   std::map<std::pair<int, int>, int> cls;
   b->tune_class.assign(b->runs.size(), 0);
@@ -327,6 +404,7 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, uint32_t step, int *
     std::vector<bool> ok(ncls, false);
     for (size_t r = 0; r < b->runs.size(); ++r) {
       const Ctx *c = b->runs[r];
+      if (c->mk.dim != 2) continue;  // 1D runs have no tiles
       const bool fits = (c->mk.red[0] + cand[k][0] - 1) / cand[k][0] >= 3 &&
                         (c->mk.red[1] + cand[k][1] - 1) / cand[k][1] >= 3;
       if (fits) {
@@ -338,8 +416,9 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, uint32_t step, int *
     // the first step after a shape change includes the order rebuild: time
     // the second
     for (int rep = 0; rep < 2 && st == AP_OK; ++rep) {
-      st = batch_update(b, dt, step + (uint32_t)used);
-      if (st == AP_OK) st = ap_batch_update_fields(b, dt, step + (uint32_t)used);
+      st = batch_update(b, dt, cur.data());
+      if (st == AP_OK) st = ap_batch_update_fields(b, dt, cur.data());
+      for (uint32_t &x : cur) ++x;
       ++used;
     }
     if (st != AP_OK) break;
@@ -352,6 +431,7 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, uint32_t step, int *
   b->tuning = false;
   if (st == AP_OK)
     for (size_t r = 0; r < b->runs.size() && st == AP_OK; ++r) {
+      if (b->runs[r]->mk.dim != 2) continue;
       const int k = best_k[b->tune_class[r]];
       int tx = 0, ty = 0;
       ap_get_tile_shape(static_cast<ap_ctx *>(b->runs[r]), &tx, &ty);

@@ -149,6 +149,41 @@ __device__ __forceinline__ void sync_kill_perp(float &p1, float &p2, float &p3, 
   gamma = sqrtf(1.0f + p * p);
 }
 
+// ---------------------------------------------------------------------------
+// Philox4x32-10 counter-based generator (J. K. Salmon, M. A. Moraes,
+// R. O. Dror, D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC 2011): ten rounds of two 32x32 -> 64-bit products with the published
+// multipliers and Weyl key increments. Host and device give the same bits.
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ void philox4x32_10(const uint32_t ctr_in[4],
+                                                      const uint32_t key_in[2],
+                                                      uint32_t out[4]) {
+  uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+  uint32_t k0 = key_in[0], k1 = key_in[1];
+  for (int round = 0; round < 10; ++round) {
+    const uint32_t hi0 = mulhi32(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    const uint32_t hi1 = mulhi32(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0;
+    c1 = n1;
+    c2 = n2;
+    c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
 // Zone-based wrap of one coordinate after a move of at most one cell
 // (find_zone, quadmesh.h:264-273; cell shift of copy_component_to_buffer,
 // kernels.cu:134-142). Returns false when the particle leaves through a

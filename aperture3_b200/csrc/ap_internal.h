@@ -95,13 +95,29 @@ struct PushDepositParams {
   uint32_t *dir_count;   // ntiles * 10
   uint32_t *queue;
   DevStatus *status;
-  size_t number;         // 1D: particle slots
+  size_t number;         // 1D: particle slots (an upper bound when d_number is set)
+  const uint32_t *d_number;  // 1D: live slots kept on the device, or null
   // log-spherical push / move (ap_logsph_params)
   float ls_compactness, ls_omega, ls_gravity, ls_rad_coef, ls_B0;
   int ls_rad_on;
   int ls_outflow_c1;     // dims[0] - damping_length + 2
   float mass[AP_MAX_SPECIES];
   FieldArr dV;           // cell volumes (J3 and Rho are divided by them)
+};
+
+// Device-side particle bookkeeping of a context with pair injection: the
+// live slot count (updated by injection and sort on the device, so that the
+// step loop needs no host round trip), counters of the last injection and
+// running totals. The host copy Ctx::number is refreshed at sync points.
+struct PairState {
+  uint32_t number;
+  uint32_t emitted;        // last injection
+  uint32_t dropped;        // last injection, over capacity
+  uint32_t old_number;     // last injection: live slots before it
+  unsigned long long next_id;
+  unsigned long long particle_steps;  // sum of live slots over injections
+  unsigned long long emitted_total;
+  unsigned long long dropped_total;
 };
 
 // One run of a batched launch: its tensor maps and its parameters, in
@@ -168,6 +184,15 @@ struct Ctx {
   float *tmp_j = nullptr;
   int tmp_pitch = 0;
 
+  // pair injection (ap_set_pair_params)
+  ap_pair_params pair{};
+  uint32_t *pair_chunks = nullptr;  // per-chunk counts then offsets, then totals
+  size_t pair_cap_chunks = 0;
+  PairState *pstate = nullptr;      // device (allocated with the pair parameters)
+  PairState *pstate_host = nullptr; // pinned mirror
+  bool number_stale = false;        // the device count moved since the last read
+  bool rho_is_zero = false;         // Rho arrays hold zeros (skip re-zeroing)
+
   // log-spherical grid (ap_ctx_create_logsph)
   int coord = 0;                // 0 Cartesian, 1 log-spherical
   ap_logsph_params lsp{};
@@ -213,6 +238,14 @@ cudaError_t launch_finalize_current(Ctx &c, int ncomp);
 cudaError_t launch_fixed_scale(Ctx &c);
 cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
 
+// pair injection (k_pairs.cu): enqueue mark / scan / append on the device
+// count (no host synchronisation); refresh_number reads the device state
+// back when it moved (waits for the stream); push_number writes the host
+// count to the device.
+int enqueue_pairs(Ctx &c, float dt, uint32_t step);
+int refresh_number(Ctx *c);
+int push_number(Ctx *c);
+
 // log-spherical (k_logsph.cu)
 int logsph_setup(Ctx &c);  // coefficients on the host, upload, J3 bound
 ap_array coef_array(const Ctx &c, int which);
@@ -240,6 +273,12 @@ cudaError_t launch_push_deposit_2d_batch(cudaStream_t stream, int num_sms, int t
                                          int chunk, bool tma, bool do_rho, int max_species,
                                          const RunDesc *runs, const uint32_t *base, int nruns,
                                          uint32_t total_tiles, uint32_t *queue);
+// The same for 1D runs: work items are chunks of 2048 particle slots
+// (base[r] = first chunk of run r).
+cudaError_t launch_push_deposit_1d_batch(cudaStream_t stream, int num_sms, bool do_rho,
+                                         const RunDesc *runs, const uint32_t *base, int nruns,
+                                         uint32_t total_chunks);
+constexpr int kChunk1DSlots = 2048;
 int ensure_scratch(Ctx &c, size_t n);
 
 }  // namespace apb

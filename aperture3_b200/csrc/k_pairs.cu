@@ -1,0 +1,247 @@
+// Pair injection for the served 1D gap runs (semantics in aperture_b200.h,
+// ap_pair_params). Three launches, in slot order so that the result does
+// not depend on scheduling:
+//   1. mark:   per particle, emit or not (Philox draw); per-chunk counts,
+//   2. scan:   one CTA turns the chunk counts into offsets and clamps the
+//              total to the free capacity,
+//   3. append: per chunk, a block scan ranks the emitters; rank k writes
+//              its pair to slots number + 2k, number + 2k + 1 and loses
+//              the photon energy.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "ap_device.cuh"
+#include "ap_internal.h"
+
+namespace apb {
+
+namespace {
+
+constexpr int kPairThreads = 256;
+constexpr int kPairPerThread = 4;
+constexpr int kPairChunk = kPairThreads * kPairPerThread;  // 1024 slots
+constexpr uint32_t kFlagSecondary = 1u << 7;  // ParticleFlag::secondary
+
+struct PairK {
+  float gamma_thr, free_path, pair_energy, dt;
+  uint32_t key[2];
+};
+
+__device__ __forceinline__ double uniform_of(uint32_t step, uint64_t id, const uint32_t key[2]) {
+  const uint32_t ctr[4] = {step, (uint32_t)id, (uint32_t)(id >> 32), 0u};
+  uint32_t out[4];
+  philox4x32_10(ctr, key, out);
+  return ((double)(out[0] >> 8) + 0.5) * (1.0 / 16777216.0);
+}
+
+// The emission test of one live particle (no writes).
+__device__ __forceinline__ bool emit_test(const PairK &K, const PtcK &p, const uint64_t *ids,
+                                          size_t idx, uint32_t step) {
+  if (p.cell[idx] == AP_MAX_CELL) return false;
+  const float gamma = p.E[idx];
+  if (!(gamma > K.gamma_thr)) return false;
+  const float p1 = p.p1[idx], p2 = p.p2[idx], p3 = p.p3[idx];
+  const float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+  const float ds = (pm / gamma) * K.dt;
+  const double prob = 1.0 - exp(-(double)ds / (double)K.free_path);
+  return uniform_of(step, ids[idx], K.key) < prob;
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair_mark(PairK K, PtcK p, const uint64_t *ids, const PairState *st, uint32_t step,
+                uint8_t *emit, uint32_t *chunk_count, uint32_t nchunks) {
+  const size_t number = st->number;
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kPairPerThread; ++k) {
+      const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
+      const bool e = idx < number && emit_test(K, p, ids, idx, step);
+      if (idx < number) emit[idx] = e ? 1 : 0;
+      cnt += __syncthreads_count(e);
+    }
+    if (threadIdx.x == 0) chunk_count[ch] = (uint32_t)cnt;
+  }
+}
+
+// One CTA: exclusive scan of the chunk counts into offs; the total is
+// clamped to the free capacity, and the device state moves on: the old
+// count and next id go to tot[] for the append pass.
+__global__ void __launch_bounds__(1024)
+    k_pair_scan(const uint32_t *chunk_count, uint32_t nchunks, uint32_t *offs, size_t capacity,
+                PairState *st, uint32_t *tot) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t b0 = 0; b0 < nchunks; b0 += blockDim.x) {
+    const uint32_t i = b0 + threadIdx.x;
+    const uint32_t v = i < nchunks ? chunk_count[i] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0u;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp ? s_warp[warp - 1] : 0u) + s_carry;
+    if (i < nchunks) offs[i] = before + x - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) s_carry = before + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const uint32_t total = s_carry;
+    const uint32_t old = st->number;
+    const size_t free_slots = capacity > old ? capacity - old : 0;
+    const uint32_t room = (uint32_t)(free_slots / 2 > 0xffffffffu ? 0xffffffffu : free_slots / 2);
+    const uint32_t em = total < room ? total : room;
+    const unsigned long long id0 = st->next_id;
+    tot[0] = em;
+    tot[1] = old;
+    tot[2] = (uint32_t)id0;
+    tot[3] = (uint32_t)(id0 >> 32);
+    st->old_number = old;
+    st->emitted = em;
+    st->dropped = total - em;
+    st->number = old + 2 * em;
+    st->next_id = id0 + 2ull * em;
+    st->particle_steps += old;
+    st->emitted_total += em;
+    st->dropped_total += total - em;
+  }
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair_append(PairK K, PtcK p, uint64_t *ids, const uint8_t *emit, const uint32_t *offs,
+                  const uint32_t *tot, uint32_t nchunks) {
+  __shared__ uint32_t s_warp[kPairThreads / 32];
+  const uint32_t emitted = tot[0];
+  const size_t number = tot[1];
+  const uint64_t id_base = (uint64_t)tot[2] | ((uint64_t)tot[3] << 32);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float Eph = K.pair_energy;
+  float q = sqrtf(0.25f * Eph * Eph - 1.0f);
+  if (q != q) q = 0.0f;
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    // thread t ranks slots ch * kPairChunk + t * kPairPerThread + [0, 4)
+    const size_t first = (size_t)ch * kPairChunk + (size_t)threadIdx.x * kPairPerThread;
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < kPairPerThread; ++k)
+      if (first + k < number) mine += emit[first + k];
+    uint32_t x = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += s_warp[w];
+    uint32_t rank = offs[ch] + before + x - mine;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kPairPerThread; ++k) {
+      const size_t idx = first + k;
+      if (idx >= number || !emit[idx]) continue;
+      const uint32_t r = rank++;
+      if (r >= emitted) continue;  // over capacity: this parent keeps its energy
+      const float gamma = p.E[idx];
+      const float p1 = p.p1[idx], p2 = p.p2[idx], p3 = p.p3[idx];
+      const float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+      const float gn = gamma - Eph;
+      const float scale = sqrtf(gn * gn - 1.0f) / pm;
+      p.p1[idx] = p1 * scale;
+      p.p2[idx] = p2 * scale;
+      p.p3[idx] = p3 * scale;
+      p.E[idx] = gn;
+      const float pp = p1 > 0.0f ? q : (p1 < 0.0f ? -q : 0.0f);  // sgn(p1) * q
+      const float ep = sqrtf(1.0f + pp * pp);
+      const size_t d = number + 2 * (size_t)r;
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        p.x1[d + m] = p.x1[idx];
+        p.x2[d + m] = p.x2[idx];
+        p.x3[d + m] = p.x3[idx];
+        p.p1[d + m] = pp;
+        p.p2[d + m] = 0.0f;
+        p.p3[d + m] = 0.0f;
+        p.E[d + m] = ep;
+        p.w[d + m] = p.w[idx];
+        p.cell[d + m] = p.cell[idx];
+        p.flag[d + m] = kFlagSecondary | ((uint32_t)m << 29);  // electron, then positron
+        ids[d + m] = id_base + 2 * (uint64_t)r + (uint64_t)m;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int enqueue_pairs(Ctx &c, float dt, uint32_t step) {
+  if (!c.pstate || c.capacity == 0) return AP_OK;
+  // work over the capacity: the live count is only known on the device
+  const uint32_t nchunks = (uint32_t)((c.capacity + kPairChunk - 1) / kPairChunk);
+  if (nchunks + 4 > c.pair_cap_chunks) {
+    cudaFree(c.pair_chunks);
+    c.pair_chunks = nullptr;
+    const size_t cap = (size_t)nchunks + 64;
+    if (cudaMalloc(&c.pair_chunks, sizeof(uint32_t) * (2 * cap + 8)) != cudaSuccess)
+      return AP_ERR_NOMEM;
+    c.pair_cap_chunks = cap;
+  }
+  uint32_t *counts = c.pair_chunks, *offs = c.pair_chunks + c.pair_cap_chunks;
+  uint32_t *tot = offs + c.pair_cap_chunks;
+  PairK K;
+  K.gamma_thr = c.pair.gamma_thr;
+  K.free_path = c.pair.free_path;
+  K.pair_energy = c.pair.pair_energy;
+  K.dt = dt;
+  K.key[0] = (uint32_t)c.pair.seed;
+  K.key[1] = (uint32_t)(c.pair.seed >> 32);
+  PtcK p{c.ptc.x1, c.ptc.x2, c.ptc.x3, c.ptc.p1, c.ptc.p2,
+         c.ptc.p3, c.ptc.E,  c.ptc.weight, c.ptc.cell, c.ptc.flag};
+  const uint32_t grid = nchunks < (uint32_t)c.num_sms * 8 ? nchunks : (uint32_t)c.num_sms * 8;
+  k_pair_mark<<<grid, kPairThreads, 0, c.stream>>>(K, p, c.ptc.id, c.pstate, step, c.dir,
+                                                   counts, nchunks);
+  k_pair_scan<<<1, 1024, 0, c.stream>>>(counts, nchunks, offs, c.capacity, c.pstate, tot);
+  k_pair_append<<<grid, kPairThreads, 0, c.stream>>>(K, p, c.ptc.id, c.dir, offs, tot, nchunks);
+  c.launches += 3;
+  c.number_stale = true;
+  if (c.mk.dim == 2) c.order_valid = false;  // appended slots are in no tile list
+  return cudaGetLastError() == cudaSuccess ? AP_OK : AP_ERR_CUDA;
+}
+
+int refresh_number(Ctx *c) {
+  if (!c->pstate || !c->number_stale) return AP_OK;
+  cudaError_t e = cudaMemcpyAsync(c->pstate_host, c->pstate, sizeof(PairState),
+                                  cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return AP_ERR_CUDA;
+  c->number = c->pstate_host->number;
+  c->number_stale = false;
+  return AP_OK;
+}
+
+int push_number(Ctx *c) {
+  if (!c->pstate) return AP_OK;
+  const uint32_t n = (uint32_t)c->number;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&c->pstate->number, &n, sizeof(n), cudaMemcpyHostToDevice);
+  c->number_stale = false;
+  return e == cudaSuccess ? AP_OK : AP_ERR_CUDA;
+}
+
+}  // namespace apb

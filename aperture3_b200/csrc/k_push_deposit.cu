@@ -470,7 +470,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
             const Acc32 J1{sJhi, sJlo}, J2{sJhi + G::JSZ, sJlo + G::JSZ},
                 J3{sJhi + 2 * G::JSZ, sJlo + 2 * G::JSZ};
             const Acc32 R{sJhi + (3 + sp) * G::JSZ, sJlo + (3 + sp) * G::JSZ};
-            const bool rho = kRho && sp < P.num_species;
+            const bool rho = kRho && P.do_rho && sp < P.num_species;
             const int obase = (c2 + jb - jy0) * G::JX + (c1 + ib - jx0);
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
@@ -630,161 +630,199 @@ __device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weigh
   return acc;
 }
 
+// One chunk of kChunk1D particle slots of a 1D run: push, deposit into a
+// shared-memory window over the cells the chunk touches (or straight into
+// the global accumulators when the window would not fit), move.
+template <bool kRho>
+__device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P, size_t ch,
+                                                      int *sWhi, unsigned *sWlo, int &s_lo,
+                                                      int &s_hi) {
+  const int tid = threadIdx.x;
+  const int n0 = P.m.dims[0], g0 = P.m.guard[0];
+  const int ncomp = 3 + (kRho ? P.num_species : 0);
+  const int win_comp = kWin1D / ncomp;
+  // A window sums at most kChunk1D contributions per cell; the global
+  // accumulators at most `number`.
+  const int lgw = bits_of(kChunk1D);
+  const size_t number = P.d_number ? (size_t)*P.d_number : P.number;
+  const int lgn = bits_of((uint32_t)min(number, (size_t)0x7fffffff));
+  const FixedFmt fx = fixed_format(lgw, min(63 - 2 * lgw, 62 - lgn), P.qmax * *P.wmax);
+  const float fscale = ldexpf(1.0f, fx.S);
+  if (ch == 0 && tid == 0) *P.fx_used = fx;
+  const size_t first = ch * kChunk1D;
+  if (tid == 0) {
+    s_lo = INT_MAX;
+    s_hi = INT_MIN;
+  }
+  __syncthreads();
+  uint32_t cells[kItems1D];
+  int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+  for (int k = 0; k < kItems1D; ++k) {
+    const size_t idx = first + (size_t)k * kThreads1D + tid;
+    cells[k] = idx < number ? P.p.cell[idx] : AP_MAX_CELL;
+    if (cells[k] != AP_MAX_CELL) {
+      lo = min(lo, (int)cells[k]);
+      hi = max(hi, (int)cells[k]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((tid & 31) == 0 && lo <= hi) {
+    atomicMin(&s_lo, lo);
+    atomicMax(&s_hi, hi);
+  }
+  __syncthreads();
+  const int wlo = s_lo - 2;
+  const int wlen = s_hi - s_lo + 5;
+  const bool use_smem = (s_lo <= s_hi) && wlen <= win_comp;
+  if (use_smem)
+    for (int i = tid; i < ncomp * win_comp; i += kThreads1D) {
+      sWhi[i] = 0;
+      sWlo[i] = 0u;
+    }
+  __syncthreads();
+
+#pragma unroll 1
+  for (int k = 0; k < kItems1D; ++k) {
+    const size_t idx = first + (size_t)k * kThreads1D + tid;
+    uint32_t c = cells[k];
+    if (c == AP_MAX_CELL) continue;
+    if ((int)c < g0 || (int)c >= n0 - g0) {  // ptc_updater.cu:30-33
+      P.p.cell[idx] = AP_MAX_CELL;
+      continue;
+    }
+    const uint32_t flag = P.p.flag[idx];
+    float x1 = P.p.x1[idx];
+    float p1 = P.p.p1[idx], p2 = P.p.p2[idx], p3 = P.p.p3[idx];
+    if (p1 != p1 || p2 != p2 || p3 != p3) {
+      atomicAdd(&P.status->nan_momenta, 1ull);
+      continue;
+    }
+    const int sp = ptc_type(flag);
+    const int c1 = (int)c;
+    float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
+    const bool em = !(flag & kFlagIgnoreEM);
+    if (em) {
+      // ptc_push_cart_1d (ptc_updater.cu:21-76): only the x stagger bit
+      // matters in 1D.
+      const float qm = P.qm[sp];
+      const Weights1D W = weights_1d(x1, c1);
+      float fe[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) fe[q] = interp_1d_global(P.F[q], W, c1, stag_x(q)) * qm;
+      vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
+      P.p.p1[idx] = p1;
+      P.p.p2[idx] = p2;
+      P.p.p3[idx] = p3;
+      P.p.E[idx] = gamma;
+    } else {
+      gamma = P.p.E[idx];
+    }
+    // deposit_current_cart_1d (ptc_updater.cu:220-293)
+    const float w = P.p.w[idx];
+    const float x2 = P.p.x2[idx], x3 = P.p.x3[idx];
+    const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
+    float nx1 = x1 + (v1 * P.dt) / P.m.delta[0];
+    const int dc1 = (int)floorf(nx1);
+    nx1 -= (float)dc1;
+    const bool far = dc1 > 1 || dc1 < -1;
+    P.p.x1[idx] = nx1;
+    P.p.x2[idx] = x2 + v2 * P.dt;
+    P.p.x3[idx] = x3 + v3 * P.dt;
+    if (!far && !(flag & kFlagIgnoreCurrent)) {
+      const float weight = P.charge[sp] * w;
+      const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
+      float djx = 0.0f;
+#pragma unroll
+      for (int i = -2; i <= 1; ++i) {
+        if (i < i0 || i > i1) continue;
+        const float sx0 = cic(-x1 + i + 1);
+        const float sx1 = cic(-nx1 + (i + 1 - dc1));
+        const int off = i + c1;
+        djx += sx1 - sx0;
+        const float a1 = -weight * djx;
+        const float val1 = 0.5f * (sx0 + sx1);
+        const float a2 = weight * v2 * val1;
+        const float a3 = weight * v3 * val1;
+        if (use_smem) {
+          const Acc32 W{sWhi, sWlo};
+          add_fixed(W, off + 1 - wlo, a1, fscale, fx.L);
+          add_fixed(W, win_comp + off - wlo, a2, fscale, fx.L);
+          add_fixed(W, 2 * win_comp + off - wlo, a3, fscale, fx.L);
+          if (kRho && P.do_rho && sp < P.num_species)
+            add_fixed(W, (3 + sp) * win_comp + off - wlo, weight * sx1, fscale, fx.L);
+        } else {
+          auto gadd = [&](int k2, int x, float v) {
+            atomicAdd(P.acc + k2 * P.acc_comp + x,
+                      (unsigned long long)__float2ll_rn(v * fscale));
+          };
+          gadd(0, off + 1, a1);
+          gadd(1, off, a2);
+          gadd(2, off, a3);
+          if (kRho && P.do_rho && sp < P.num_species) gadd(3 + sp, off, weight * sx1);
+        }
+      }
+    }
+    int cn = c1 + dc1;
+    bool keep = !far && wrap_coord(cn, g0, n0, P.m.red[0], P.periodic[0]);
+    if (!keep) atomicAdd(far ? &P.status->moved_far : &P.status->lost, 1ull);
+    P.p.cell[idx] = keep ? (uint32_t)cn : AP_MAX_CELL;
+  }
+  __syncthreads();
+  if (use_smem) {
+    for (int i = tid; i < ncomp * wlen; i += kThreads1D) {
+      const int comp = i / wlen, o = i % wlen;
+      const int si = comp * win_comp + o;
+      const long long v = (long long)sWhi[si] * (1ll << fx.L) + (long long)sWlo[si];
+      if (v == 0) continue;
+      const int gx = wlo + o;
+      if (gx < 0 || gx >= n0) continue;
+      atomicAdd(P.acc + comp * P.acc_comp + gx, (unsigned long long)v);
+    }
+  }
+  __syncthreads();
+}
+
 template <bool kRho>
 __global__ void __launch_bounds__(kThreads1D)
     k_push_deposit_1d(const __grid_constant__ PushDepositParams P) {
   __shared__ int sWhi[kWin1D];
   __shared__ unsigned sWlo[kWin1D];
   __shared__ int s_lo, s_hi;
-  const int tid = threadIdx.x;
-  const int n0 = P.m.dims[0], g0 = P.m.guard[0];
-  const int ncomp = 3 + (kRho ? P.num_species : 0);
-  const int win_comp = kWin1D / ncomp;
   const size_t nchunks = (P.number + kChunk1D - 1) / kChunk1D;
-  // A window sums at most kChunk1D contributions per cell; the global
-  // accumulators at most `number`.
-  const int lgw = bits_of(kChunk1D);
-  const int lgn = bits_of((uint32_t)min(P.number, (size_t)0x7fffffff));
-  const FixedFmt fx = fixed_format(lgw, min(63 - 2 * lgw, 62 - lgn), P.qmax * *P.wmax);
-  const float fscale = ldexpf(1.0f, fx.S);
-  if (blockIdx.x == 0 && tid == 0) *P.fx_used = fx;
+  for (size_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+    push_deposit_1d_chunk<kRho>(P, ch, sWhi, sWlo, s_lo, s_hi);
+}
 
-  for (size_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const size_t first = ch * kChunk1D;
-    if (tid == 0) {
-      s_lo = INT_MAX;
-      s_hi = INT_MIN;
+// Many independent 1D runs in one launch: work item g is chunk
+// g - base[r] of run r; the CTA copies that run's parameters into shared
+// memory before the chunk.
+template <bool kRho>
+__global__ void __launch_bounds__(kThreads1D)
+    k_push_deposit_1d_batch(const RunDesc *__restrict__ runs, const uint32_t *__restrict__ base,
+                            int nruns) {
+  __shared__ int sWhi[kWin1D];
+  __shared__ unsigned sWlo[kWin1D];
+  __shared__ int s_lo, s_hi;
+  __shared__ __align__(16) uint32_t s_pbuf[sizeof(PushDepositParams) / 4];
+  const uint32_t total = base[nruns];
+  const PushDepositParams &P = *reinterpret_cast<const PushDepositParams *>(s_pbuf);
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    int lo = 0, hi = nruns - 1;  // largest r with base[r] <= g
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (base[mid] <= g) lo = mid;
+      else hi = mid - 1;
     }
+    __syncthreads();  // the previous chunk is done with s_pbuf
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&runs[lo].P);
+    for (int i = threadIdx.x; i < (int)(sizeof(PushDepositParams) / 4); i += kThreads1D)
+      s_pbuf[i] = src[i];
     __syncthreads();
-    uint32_t cells[kItems1D];
-    int lo = INT_MAX, hi = INT_MIN;
-#pragma unroll
-    for (int k = 0; k < kItems1D; ++k) {
-      const size_t idx = first + (size_t)k * kThreads1D + tid;
-      cells[k] = idx < P.number ? P.p.cell[idx] : AP_MAX_CELL;
-      if (cells[k] != AP_MAX_CELL) {
-        lo = min(lo, (int)cells[k]);
-        hi = max(hi, (int)cells[k]);
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    if ((tid & 31) == 0 && lo <= hi) {
-      atomicMin(&s_lo, lo);
-      atomicMax(&s_hi, hi);
-    }
-    __syncthreads();
-    const int wlo = s_lo - 2;
-    const int wlen = s_hi - s_lo + 5;
-    const bool use_smem = (s_lo <= s_hi) && wlen <= win_comp;
-    if (use_smem)
-      for (int i = tid; i < ncomp * win_comp; i += kThreads1D) {
-        sWhi[i] = 0;
-        sWlo[i] = 0u;
-      }
-    __syncthreads();
-
-#pragma unroll 1
-    for (int k = 0; k < kItems1D; ++k) {
-      const size_t idx = first + (size_t)k * kThreads1D + tid;
-      uint32_t c = cells[k];
-      if (c == AP_MAX_CELL) continue;
-      if ((int)c < g0 || (int)c >= n0 - g0) {  // ptc_updater.cu:30-33
-        P.p.cell[idx] = AP_MAX_CELL;
-        continue;
-      }
-      const uint32_t flag = P.p.flag[idx];
-      float x1 = P.p.x1[idx];
-      float p1 = P.p.p1[idx], p2 = P.p.p2[idx], p3 = P.p.p3[idx];
-      if (p1 != p1 || p2 != p2 || p3 != p3) {
-        atomicAdd(&P.status->nan_momenta, 1ull);
-        continue;
-      }
-      const int sp = ptc_type(flag);
-      const int c1 = (int)c;
-      float gamma = sqrtf(1.0f + p1 * p1 + p2 * p2 + p3 * p3);
-      const bool em = !(flag & kFlagIgnoreEM);
-      if (em) {
-        // ptc_push_cart_1d (ptc_updater.cu:21-76): only the x stagger bit
-        // matters in 1D.
-        const float qm = P.qm[sp];
-        const Weights1D W = weights_1d(x1, c1);
-        float fe[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) fe[q] = interp_1d_global(P.F[q], W, c1, stag_x(q)) * qm;
-        vay_push(p1, p2, p3, gamma, fe[0], fe[1], fe[2], fe[3], fe[4], fe[5]);
-        P.p.p1[idx] = p1;
-        P.p.p2[idx] = p2;
-        P.p.p3[idx] = p3;
-        P.p.E[idx] = gamma;
-      } else {
-        gamma = P.p.E[idx];
-      }
-      // deposit_current_cart_1d (ptc_updater.cu:220-293)
-      const float w = P.p.w[idx];
-      const float x2 = P.p.x2[idx], x3 = P.p.x3[idx];
-      const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
-      float nx1 = x1 + (v1 * P.dt) / P.m.delta[0];
-      const int dc1 = (int)floorf(nx1);
-      nx1 -= (float)dc1;
-      const bool far = dc1 > 1 || dc1 < -1;
-      P.p.x1[idx] = nx1;
-      P.p.x2[idx] = x2 + v2 * P.dt;
-      P.p.x3[idx] = x3 + v3 * P.dt;
-      if (!far && !(flag & kFlagIgnoreCurrent)) {
-        const float weight = P.charge[sp] * w;
-        const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
-        float djx = 0.0f;
-#pragma unroll
-        for (int i = -2; i <= 1; ++i) {
-          if (i < i0 || i > i1) continue;
-          const float sx0 = cic(-x1 + i + 1);
-          const float sx1 = cic(-nx1 + (i + 1 - dc1));
-          const int off = i + c1;
-          djx += sx1 - sx0;
-          const float a1 = -weight * djx;
-          const float val1 = 0.5f * (sx0 + sx1);
-          const float a2 = weight * v2 * val1;
-          const float a3 = weight * v3 * val1;
-          if (use_smem) {
-            const Acc32 W{sWhi, sWlo};
-            add_fixed(W, off + 1 - wlo, a1, fscale, fx.L);
-            add_fixed(W, win_comp + off - wlo, a2, fscale, fx.L);
-            add_fixed(W, 2 * win_comp + off - wlo, a3, fscale, fx.L);
-            if (kRho && sp < P.num_species)
-              add_fixed(W, (3 + sp) * win_comp + off - wlo, weight * sx1, fscale, fx.L);
-          } else {
-            auto gadd = [&](int k2, int x, float v) {
-              atomicAdd(P.acc + k2 * P.acc_comp + x,
-                        (unsigned long long)__float2ll_rn(v * fscale));
-            };
-            gadd(0, off + 1, a1);
-            gadd(1, off, a2);
-            gadd(2, off, a3);
-            if (kRho && sp < P.num_species) gadd(3 + sp, off, weight * sx1);
-          }
-        }
-      }
-      int cn = c1 + dc1;
-      bool keep = !far && wrap_coord(cn, g0, n0, P.m.red[0], P.periodic[0]);
-      if (!keep) atomicAdd(far ? &P.status->moved_far : &P.status->lost, 1ull);
-      P.p.cell[idx] = keep ? (uint32_t)cn : AP_MAX_CELL;
-    }
-    __syncthreads();
-    if (use_smem) {
-      for (int i = tid; i < ncomp * wlen; i += kThreads1D) {
-        const int comp = i / wlen, o = i % wlen;
-        const int si = comp * win_comp + o;
-        const long long v = (long long)sWhi[si] * (1ll << fx.L) + (long long)sWlo[si];
-        if (v == 0) continue;
-        const int gx = wlo + o;
-        if (gx < 0 || gx >= n0) continue;
-        atomicAdd(P.acc + comp * P.acc_comp + gx, (unsigned long long)v);
-      }
-    }
-    __syncthreads();
+    push_deposit_1d_chunk<kRho>(P, g - base[lo], sWhi, sWlo, s_lo, s_hi);
   }
 }
 
@@ -928,6 +966,18 @@ cudaError_t launch_push_deposit_2d_batch(cudaStream_t stream, int num_sms, int t
   AP_BATCH_SHAPE(4, 4)
 #undef AP_BATCH_SHAPE
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_push_deposit_1d_batch(cudaStream_t stream, int num_sms, bool do_rho,
+                                         const RunDesc *runs, const uint32_t *base, int nruns,
+                                         uint32_t total_chunks) {
+  if (total_chunks == 0) return cudaSuccess;
+  const uint32_t grid = total_chunks < (uint32_t)num_sms * 8 ? total_chunks : (uint32_t)num_sms * 8;
+  if (do_rho)
+    k_push_deposit_1d_batch<true><<<grid, kThreads1D, 0, stream>>>(runs, base, nruns);
+  else
+    k_push_deposit_1d_batch<false><<<grid, kThreads1D, 0, stream>>>(runs, base, nruns);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_push_deposit_1d(Ctx &c, const PushDepositParams &P) {

@@ -311,10 +311,12 @@ __global__ void __launch_bounds__(kScanThreads)
 }
 
 __global__ void k_cell_keys(const uint32_t *cell, size_t n, uint32_t ncells, uint32_t *keys,
-                            uint32_t *vals) {
+                            uint32_t *vals, const uint32_t *d_number) {
+  // slots at or beyond a device-side live count are empty
+  const size_t live = d_number ? (size_t)*d_number : n;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t c = cell[i];
+    uint32_t c = i < live ? cell[i] : AP_MAX_CELL;
     keys[i] = (c == AP_MAX_CELL) ? ncells : c;
     vals[i] = (uint32_t)i;
   }
@@ -441,13 +443,16 @@ cudaError_t rebuild_tile_order(Ctx &c) {
 }
 
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
-  const size_t n = c.number;
+  // a 1D context with a device-side count (pair injection) sorts over its
+  // capacity and writes the new count on the device
+  const bool device_count = c.pstate && c.mk.dim == 1;
+  const size_t n = device_count ? c.capacity : c.number;
   *new_number = 0;
   if (n == 0) return cudaSuccess;
   const uint32_t ncells =
       (uint32_t)c.mesh.dims[0] * (uint32_t)c.mesh.dims[1] * (uint32_t)c.mesh.dims[2];
-  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.ptc.cell, n, ncells, c.keys[0],
-                                                        c.vals[0]);
+  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(
+      c.ptc.cell, n, ncells, c.keys[0], c.vals[0], device_count ? &c.pstate->number : nullptr);
   c.launches++;
   uint32_t *ko, *vo;
   cudaError_t e = radix_pairs(c, n, bits_for(ncells), &ko, &vo);
@@ -483,6 +488,11 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   }
   k_segment_starts<<<grid_for(c, n + 1, 256), 256, 0, c.stream>>>(ko, n, ncells, c.cell_start);
   c.launches++;
+  if (device_count) {
+    c.number_stale = true;
+    return cudaMemcpyAsync(&c.pstate->number, c.cell_start + ncells, sizeof(uint32_t),
+                           cudaMemcpyDeviceToDevice, c.stream);
+  }
   uint32_t live = 0;
   e = cudaMemcpyAsync(&live, c.cell_start + ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                       c.stream);

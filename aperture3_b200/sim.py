@@ -184,6 +184,14 @@ class SimEnvironment:
             check(self._lib.ap_send_add_guard_cells(self.ctx, array_view(a)),
                   "ap_send_add_guard_cells")
 
+    def set_pair_params(self, gamma_thr: float = 1e6, free_path: float = 0.05,
+                        pair_energy: float = 50.0, seed: int = 0, first_id: int = 1 << 40,
+                        enabled: bool = True):
+        """Pair injection of this run (ap_pair_params)."""
+        pp = _lib.ApPairParams(float(gamma_thr), float(free_path), float(pair_energy),
+                               int(bool(enabled)), int(seed), int(first_id))
+        check(self._lib.ap_set_pair_params(self.ctx, C.byref(pp)), "ap_set_pair_params")
+
     def logsph_coef(self, which: int) -> np.ndarray:
         """Host copy of one Grid_LogSph coefficient array (grid_log_sph.h:45-47),
         shape (dims[1], dims[0])."""
@@ -310,6 +318,7 @@ class SimData:
               "ap_particles_modified")
 
     def particles_host(self) -> Dict[str, np.ndarray]:
+        self.refresh_number()
         torch.cuda.synchronize()
         out = {}
         for name, _ in PTC_FIELDS:
@@ -321,9 +330,34 @@ class SimData:
         """sim_data::sort_particles (sim_data_impl.hpp:78-89)."""
         lib = self.env._lib
         check(lib.ap_sort_by_cell(self.env.ctx), "ap_sort_by_cell")
+        self.refresh_number()
+
+    def refresh_number(self):
         n = C.c_size_t()
-        check(lib.ap_get_number(self.env.ctx, C.byref(n)), "ap_get_number")
+        check(self.env._lib.ap_get_number(self.env.ctx, C.byref(n)), "ap_get_number")
         self.number = int(n.value)
+
+    def pair_stats(self):
+        """(particle_steps, pairs created, pairs dropped) since pair injection
+        was enabled."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(self.env._lib.ap_get_pair_stats(self.env.ctx, C.byref(a), C.byref(b), C.byref(c)),
+              "ap_get_pair_stats")
+        return int(a.value), int(b.value), int(c.value)
+
+    def sort_particles_async(self):
+        """sort_by_cell without reading the new count back (1D runs with pair
+        injection keep it on the device)."""
+        check(self.env._lib.ap_sort_by_cell(self.env.ctx), "ap_sort_by_cell")
+
+    def inject_pairs(self, dt: float, step: int):
+        """Pair injection after the particle update of `step` (see
+        SimEnvironment.set_pair_params); returns (emitted, dropped)."""
+        em, dr = C.c_uint64(), C.c_uint64()
+        check(self.env._lib.ap_inject_pairs(self.env.ctx, float(dt), int(step), C.byref(em),
+                                            C.byref(dr)), "ap_inject_pairs")
+        self.refresh_number()
+        return int(em.value), int(dr.value)
 
     def tile_order(self):
         """(order, tile_start) of the per-step tile counting sort, as host arrays."""
@@ -435,52 +469,76 @@ class Batch:
     push / deposit launch per tile shape and no host synchronisation between
     steps. Each run's particles equal those of the same run advanced alone."""
 
-    def __init__(self, runs: Sequence["SimData"]):
+    def __init__(self, runs: Sequence["SimData"] = ()):
         self.runs = list(runs)
         self._lib = _lib.lib()
-        arr = (C.c_void_p * len(self.runs))(*[d.env.ctx.value for d in self.runs])
+        arr = (C.c_void_p * max(len(self.runs), 1))(*[d.env.ctx.value for d in self.runs])
         b = C.c_void_p()
         check(self._lib.ap_batch_create(arr, len(self.runs), C.byref(b)), "ap_batch_create")
         self.handle = b
-        # each run's own time step (SimParams.delta_t) unless one is given
-        self.dt = [float(d.env.params.delta_t) for d in self.runs]
+
+    @property
+    def dt(self):
+        """Each run's own time step (SimParams.delta_t)."""
+        return [float(d.env.params.delta_t) for d in self.runs]
+
+    def add(self, data: "SimData"):
+        check(self._lib.ap_batch_add(self.handle, data.env.ctx), "ap_batch_add")
+        self.runs.append(data)
+
+    def remove(self, data: "SimData"):
+        check(self._lib.ap_batch_remove(self.handle, data.env.ctx), "ap_batch_remove")
+        self.runs.remove(data)
 
     def _dts(self, dt):
         vals = self.dt if dt is None else (
             [float(dt)] * len(self.runs) if np.isscalar(dt) else [float(x) for x in dt])
         return (C.c_double * len(self.runs))(*vals)
 
+    def _steps(self, steps):
+        vals = [int(steps)] * len(self.runs) if np.isscalar(steps) else [int(x) for x in steps]
+        return (C.c_uint32 * len(self.runs))(*vals)
+
     def set_stream(self, stream: torch.cuda.Stream):
         check(self._lib.ap_batch_set_stream(self.handle, C.c_void_p(stream.cuda_stream)),
               "ap_batch_set_stream")
 
-    def update_particles(self, step: int, dt=None):
-        """One particle update of every run (dt: None for each run's own
-        delta_t, a scalar, or one value per run)."""
-        check(self._lib.ap_batch_update_particles(self.handle, self._dts(dt), int(step)),
+    def update_particles(self, steps, dt=None):
+        """One particle update of every run. steps: the step number of all
+        runs or one per run; dt: None for each run's own delta_t, a scalar,
+        or one value per run."""
+        check(self._lib.ap_batch_update_particles(self.handle, self._dts(dt),
+                                                  self._steps(steps)),
               "ap_batch_update_particles")
 
-    def update_fields(self, step: int, dt=None):
-        check(self._lib.ap_batch_update_fields(self.handle, self._dts(dt), int(step)),
+    def update_fields(self, steps, dt=None):
+        check(self._lib.ap_batch_update_fields(self.handle, self._dts(dt), self._steps(steps)),
               "ap_batch_update_fields")
+
+    def inject_pairs(self, steps, dt=None):
+        """Pair injection of every run that has it enabled (one device
+        synchronisation); refreshes each run's particle number."""
+        check(self._lib.ap_batch_inject_pairs(self.handle, self._dts(dt), self._steps(steps)),
+              "ap_batch_inject_pairs")
+        for d in self.runs:
+            d.refresh_number()
 
     def sort_particles(self):
         check(self._lib.ap_batch_sort_by_cell(self.handle), "ap_batch_sort_by_cell")
         for d in self.runs:
-            n = C.c_size_t()
-            check(self._lib.ap_get_number(d.env.ctx, C.byref(n)), "ap_get_number")
-            d.number = int(n.value)
+            d.refresh_number()
 
     def sync(self):
         bad = C.c_int(-1)
         st = self._lib.ap_batch_sync(self.handle, C.byref(bad))
         check(st, f"ap_batch_sync (run {bad.value})")
 
-    def autotune(self, step: int, dt=None) -> int:
+    def autotune(self, steps, dt=None) -> int:
         """Runs the tile-shape autotuner; returns the number of complete
         steps (particles, then fields) it advanced every run by."""
         used = C.c_int(0)
-        check(self._lib.ap_batch_autotune(self.handle, self._dts(dt), int(step), C.byref(used)),
+        check(self._lib.ap_batch_autotune(self.handle, self._dts(dt), self._steps(steps),
+                                          C.byref(used)),
               "ap_batch_autotune")
         return int(used.value)
 

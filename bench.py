@@ -54,9 +54,15 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
-    ap.add_argument("--workload", default="box", choices=["box", "batched"],
+    ap.add_argument("--workload", default="box", choices=["box", "batched", "served"],
                     help="box: the 2D box (headline line); batched: many uneven boxes "
-                         "through ap_batch_* against the same runs one at a time")
+                         "through ap_batch_* against the same runs one at a time; served: "
+                         "a Poisson stream of 1D gap runs, continuous batching against "
+                         "first-come-first-served one at a time")
+    ap.add_argument("--steps-scale", type=float, default=0.05,
+                    help="served: run lengths are 200-5000 steps times this factor")
+    ap.add_argument("--hbm-budget", type=float, default=60.0,
+                    help="served: GB of device memory the resident runs may occupy")
     ap.add_argument("--runs", type=int, default=24, help="batched: number of runs")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="seconds for the whole --impl reference run")
@@ -510,6 +516,40 @@ def run_batched(args):
         env.close()
 
 
+def run_served(args):
+    """Served stream of 1D gap runs: `runs` requests with Poisson arrivals
+    (50/s), 512-16384 cells, 32-256 particles per cell, 200-5000 steps
+    scaled by --steps-scale, E_parallel ramp amplitude in [0.1, 10], pair
+    injection above gamma 1e6 (exponential free path, mean 0.05, Philox).
+    Leg 1: continuous batching under the HBM budget; leg 2: the same
+    requests first come, first served, one at a time through the plain
+    path. Wall clock; aggregate particle-steps/s and completion latency
+    (finish - arrival) percentiles."""
+    import torch
+    from aperture3_b200 import serve
+
+    lo, hi = max(1, int(200 * args.steps_scale)), max(2, int(5000 * args.steps_scale))
+    reqs = serve.request_stream(args.runs, seed=5, rate=50.0, steps=(lo, hi))
+    dev = torch.device("cuda", 0)
+    # warm the code paths (module loads, kernel first launches)
+    serve.run_alone(serve.GapRequest(rid=-1, cells=512, ppc=32, steps=3, ramp=1.0, seed=9),
+                    dev, keep_result=False)
+    server = serve.GapServer(dev, hbm_budget=args.hbm_budget * 1e9, round_steps=16)
+    st_b = server.serve(reqs, realtime=True)
+    st_a = serve.serve_one_at_a_time(reqs, dev, realtime=True)
+    line = {
+        "metric": "aggregate particle-steps/s (served 1D gap runs)", "value": st_b["throughput"],
+        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded request stream, aperture3_b200.serve)",
+        "config": {"workload": f"{args.runs} requests, Poisson 50/s, 512-16384 cells, "
+                               f"32-256 ppc, {lo}-{hi} steps, pair injection",
+                   "hbm_budget_gb": args.hbm_budget},
+        "served": st_b, "one_at_a_time": st_a,
+        "speedup_vs_one_at_a_time": st_b["throughput"] / st_a["throughput"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_e2e(args, env, data, pusher, solver, dt, stream, n):
     import torch
     from aperture3_b200._lib import ApDiag, check
@@ -582,9 +622,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.workload == "batched":
+        if args.workload in ("batched", "served"):
             if rank == 0:
-                run_batched(args)
+                (run_batched if args.workload == "batched" else run_served)(args)
             return
         run_ours(args, rank, world, local_rank)
     finally:

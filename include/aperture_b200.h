@@ -252,39 +252,90 @@ AP_API int ap_logsph_field_boundary(ap_ctx *ctx, double omega);
  * push / deposit launch per tile shape over all runs' tiles, the small
  * per-run kernels enqueued on one stream, and no host synchronisation
  * between steps. Every run gives the same particles, bit for bit, as when
- * it is advanced alone through ap_update_particles. All runs share one
- * data_interval. The batch takes over the runs' streams and sets them
- * asynchronous (ap_set_sync 0). */
+ * it is advanced alone through ap_update_particles. Runs may be 1D or 2D
+ * Cartesian and each has its own time step and step counter. The batch
+ * takes over the runs' streams and sets them asynchronous (ap_set_sync 0). */
 typedef struct ap_batch ap_batch;
 
 AP_API int ap_batch_create(ap_ctx *const *runs, int nruns, ap_batch **out);
 /* Destroy a batch before its runs; the runs go back to synchronous calls
  * on the default stream. */
 AP_API int ap_batch_destroy(ap_batch *batch);
+/* Adds a run to / removes a run from a batch (continuous batching: runs join
+ * and leave between steps); a removed run goes back to synchronous calls on
+ * the default stream. ap_batch_create accepts nruns == 0. */
+AP_API int ap_batch_add(ap_batch *batch, ap_ctx *run);
+AP_API int ap_batch_remove(ap_batch *batch, ap_ctx *run);
+AP_API int ap_batch_size(const ap_batch *batch, int *nruns);
 /* Stream of the batch (default: a private non-blocking stream). */
 AP_API int ap_batch_set_stream(ap_batch *batch, void *cuda_stream);
-/* ap_update_particles for every run; dt[r] is the time step of run r (the
- * runs advance in lockstep, each with its own dt). */
-AP_API int ap_batch_update_particles(ap_batch *batch, const double *dt, uint32_t step);
-/* ap_update_fields for every run, dt as above. */
-AP_API int ap_batch_update_fields(ap_batch *batch, const double *dt, uint32_t step);
+/* ap_update_particles for every run: dt[r] and steps[r] are the time step
+ * and step number of run r. */
+AP_API int ap_batch_update_particles(ap_batch *batch, const double *dt,
+                                     const uint32_t *steps);
+/* ap_update_fields for every run, dt and steps as above. */
+AP_API int ap_batch_update_fields(ap_batch *batch, const double *dt, const uint32_t *steps);
 /* ap_sort_by_cell for every run. */
 AP_API int ap_batch_sort_by_cell(ap_batch *batch);
 /* Waits for the batch and returns the first non-OK device status of a run
  * (run index in *failed_run, -1 if none; may be NULL). */
 AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
 /* Project autotuner: advances the batch by *steps_used complete steps
- * (particle update, then field update) starting at `step`, timing the
+ * (particle update, then field update) starting at steps[r], timing the
  * push / deposit of each class of runs (same grid size) with every
  * candidate tile shape, and keeps the fastest shape per class. Particle
  * results do not depend on the tile shape; J can differ in the last bits
  * (the fixed-point scale follows the largest tile population). */
-AP_API int ap_batch_autotune(ap_batch *batch, const double *dt, uint32_t step,
+AP_API int ap_batch_autotune(ap_batch *batch, const double *dt, const uint32_t *steps,
                              int *steps_used);
 /* Tile shape of one run (16x16, 32x16, 16x8, 8x8 or 4x4); rebuilds its
  * tile order at the next update. */
 AP_API int ap_set_tile_shape(ap_ctx *ctx, int tx, int ty);
 AP_API int ap_get_tile_shape(const ap_ctx *ctx, int *tx, int *ty);
+
+/* ---------------------------------------------------------------------
+ * Pair injection (the served 1D gap runs; the reference's analogue is
+ * radiative_transfer::produce_pairs, src/cuda/radiation/
+ * radiative_transfer.cu:99-177, 252-301, and the 1D gap lab's
+ * produce_pair, labs/1dgap/src/cuda/radiation/user_radiative_functions.cuh:
+ * 80-131). A live particle with gamma > gamma_thr travels ds = |v| dt per
+ * step and emits with probability 1 - exp(-ds / free_path), the uniform
+ * number drawn from Philox4x32-10 keyed on (seed) with counter (step,
+ * particle id); the photon energy pair_energy leaves the parent (its
+ * momentum is rescaled to gamma - pair_energy) and becomes an e-/e+ pair at
+ * the parent's position, each member with p1 = sgn(p1_parent) *
+ * sqrt(pair_energy^2 / 4 - 1), the parent's weight and the secondary flag.
+ * New particles are appended after the live slots in slot order of their
+ * parents; ids are first_id, first_id + 1, ... in that order. Emissions
+ * beyond the particle capacity are dropped (counted). */
+typedef struct {
+  float gamma_thr;     /* 1e6 in the served workload                      */
+  float free_path;     /* mean free path, in the units of x (0.05)        */
+  float pair_energy;   /* photon energy converted into one pair           */
+  int enabled;
+  uint64_t seed;       /* per-run key of the random stream                */
+  uint64_t first_id;   /* id given to the next created particle           */
+} ap_pair_params;
+
+/* Enables (or changes) pair injection. From then on the context keeps its
+ * live particle count on the device: the 1D update, the injection and the
+ * 1D sort read and write it there without host synchronisation, and calls
+ * that report the count (ap_get_number, ap_sync, ...) read it back. */
+AP_API int ap_set_pair_params(ap_ctx *ctx, const ap_pair_params *params);
+/* Running totals since ap_set_pair_params: particle-steps (live slots summed
+ * over injection passes), pairs created, pairs dropped over capacity
+ * (waits for the stream). */
+AP_API int ap_get_pair_stats(ap_ctx *ctx, uint64_t *particle_steps, uint64_t *emitted_total,
+                             uint64_t *dropped_total);
+/* One injection pass over the live particles (after the particle update of
+ * `step`, with that step's dt); waits for the stream. *emitted (may be
+ * NULL) receives the number of pairs created; *dropped (may be NULL) those
+ * over capacity. */
+AP_API int ap_inject_pairs(ap_ctx *ctx, double dt, uint32_t step, uint64_t *emitted,
+                           uint64_t *dropped);
+/* The same for every run of a batch that has pair injection enabled (dt[r]
+ * and steps[r] per run), with one synchronisation for the whole batch. */
+AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32_t *steps);
 
 /* Device time per phase of the update, from CUDA events recorded on the
  * context's stream around each phase while profiling is on. */

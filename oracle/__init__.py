@@ -147,6 +147,9 @@ for _name, _res, _args in [
     ("or_sort_by_cell", _sz, [_vp, _vp, _sz]),
     ("or_tile_key", C.c_uint32, [_vp, _vp, C.c_uint32]),
     ("or_tile_order", _sz, [_vp, _vp, _vp, _vp, _sz, _vp, _vp]),
+    ("or_philox4x32_10", None, [_vp, _vp, _vp]),
+    ("or_inject_pairs", _sz, [_vp, _sz, _sz, C.c_float, C.c_uint32, C.c_float, C.c_float,
+                              C.c_float, C.c_uint64, C.c_uint64, _vp, _vp]),
 ]:
     _f = getattr(lib, _name)
     _f.restype = _res
@@ -318,6 +321,23 @@ def tile_order(m, tile, cell, order_in):
     n = lib.or_tile_order(C.byref(m), _fa(tile, C.c_int, 2), _p(cell), _p(order_in),
                           len(order_in), _p(out), _p(ts))
     return out[:n], ts
+
+
+def philox4x32_10(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    out = (C.c_uint32 * 4)()
+    lib.or_philox4x32_10(c, k, out)
+    return list(out)
+
+
+def inject_pairs(p, num, cap, dt, step, gamma_thr, free_path, pair_energy, seed, first_id):
+    """Pair injection in slot order. Returns (new_num, emitted, dropped)."""
+    s = ptc_struct(p)
+    em, dr = C.c_uint64(), C.c_uint64()
+    n = lib.or_inject_pairs(C.byref(s), num, cap, dt, step, gamma_thr, free_path, pair_energy,
+                            seed, first_id, C.byref(em), C.byref(dr))
+    return int(n), int(em.value), int(dr.value)
 
 
 # ---------------------------------------------------------------------------

@@ -892,3 +892,84 @@ size_t or_tile_order(const or_mesh *m, const int tile[2], const uint32_t *cell,
   free(perm);
   return live;
 }
+
+/* ------------------------------------------------------------------ */
+/* Philox4x32-10 and pair injection (see ap_oracle.h).                 */
+
+static inline uint32_t or_mulhi(uint32_t a, uint32_t b) {
+  return (uint32_t)(((uint64_t)a * (uint64_t)b) >> 32);
+}
+
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int round = 0; round < 10; round++) {
+    uint32_t hi0 = or_mulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = or_mulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+size_t or_inject_pairs(or_ptc *p, size_t num, size_t cap, float dt, uint32_t step,
+                       float gamma_thr, float free_path, float pair_energy,
+                       uint64_t seed, uint64_t first_id, uint64_t *emitted,
+                       uint64_t *dropped) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const size_t room = cap > num ? (cap - num) / 2 : 0;
+  float q = sqrtf(0.25f * pair_energy * pair_energy - 1.0f);
+  if (q != q) q = 0.0f;
+  size_t k = 0, want = 0;
+  for (size_t idx = 0; idx < num; idx++) {
+    if (p->cell[idx] == OR_MAX_CELL) continue;
+    float gamma = p->E[idx];
+    if (!(gamma > gamma_thr)) continue;
+    float p1 = p->p1[idx], p2 = p->p2[idx], p3 = p->p3[idx];
+    float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+    float ds = (pm / gamma) * dt;
+    double prob = 1.0 - exp(-(double)ds / (double)free_path);
+    uint64_t id = p->id[idx];
+    const uint32_t ctr[4] = {step, (uint32_t)id, (uint32_t)(id >> 32), 0u};
+    uint32_t out[4];
+    or_philox4x32_10(ctr, key, out);
+    double u = ((double)(out[0] >> 8) + 0.5) * (1.0 / 16777216.0);
+    if (!(u < prob)) continue;
+    want++;
+    if (k >= room) continue;
+    float gn = gamma - pair_energy;
+    float scale = sqrtf(gn * gn - 1.0f) / pm;
+    p->p1[idx] = p1 * scale;
+    p->p2[idx] = p2 * scale;
+    p->p3[idx] = p3 * scale;
+    p->E[idx] = gn;
+    float pp = p1 > 0.0f ? q : (p1 < 0.0f ? -q : 0.0f);
+    float ep = sqrtf(1.0f + pp * pp);
+    for (int m = 0; m < 2; m++) {
+      size_t d = num + 2 * k + (size_t)m;
+      p->x1[d] = p->x1[idx];
+      p->x2[d] = p->x2[idx];
+      p->x3[d] = p->x3[idx];
+      p->p1[d] = pp;
+      p->p2[d] = 0.0f;
+      p->p3[d] = 0.0f;
+      p->E[d] = ep;
+      p->weight[d] = p->weight[idx];
+      p->cell[d] = p->cell[idx];
+      p->flag[d] = (1u << 7) | ((uint32_t)m << 29);
+      p->id[d] = first_id + 2 * (uint64_t)k + (uint64_t)m;
+    }
+    k++;
+  }
+  if (emitted) *emitted = k;
+  if (dropped) *dropped = want - k;
+  return num + 2 * k;
+}

@@ -159,6 +159,24 @@ size_t or_tile_order(const or_mesh *m, const int tile[2], const uint32_t *cell,
                      const uint32_t *order_in, size_t n, uint32_t *order_out,
                      uint32_t *tile_start);
 
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011). */
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Pair injection of the served 1D gap runs (the library's build semantics;
+ * the reference analogue is radiative_transfer::produce_pairs and the 1D
+ * gap lab's produce_pair, user_radiative_functions.cuh:80-131): in slot
+ * order, a live particle with E > gamma_thr emits with probability
+ * 1 - exp(-(|p| / E) dt / free_path), the uniform number being
+ * ((out0 >> 8) + 0.5) / 2^24 of Philox4x32-10 with counter (step, id_lo,
+ * id_hi, 0) and key (seed_lo, seed_hi); emitter k (k < free slots / 2)
+ * loses pair_energy and appends an e- and an e+ at slots num + 2k,
+ * num + 2k + 1 with ids first_id + 2k, + 1. Returns the new number;
+ * *emitted / *dropped get the counts. */
+size_t or_inject_pairs(or_ptc *p, size_t num, size_t cap, float dt, uint32_t step,
+                       float gamma_thr, float free_path, float pair_energy,
+                       uint64_t seed, uint64_t first_id, uint64_t *emitted,
+                       uint64_t *dropped);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,10 +110,25 @@ def test_batch_autotune_then_steps():
     _close(batch, alone, batched)
 
 
-def test_batch_rejects_mixed_data_interval():
-    a = _make((32, 32, 2, 5), data_interval=2)
-    b = _make((32, 32, 2, 6), data_interval=3)
-    with pytest.raises(Exception):
-        Batch([a[1], b[1]])
-    a[0].close()
-    b[0].close()
+def test_batch_mixed_steps_and_data_interval():
+    """Runs at different step numbers, with different charge-deposition
+    schedules, in one batch."""
+    specs = _specs(3, 5)
+    dis = [1, 2, 3, 2, 1]
+    alone = [_make(s, data_interval=d) for s, d in zip(specs, dis)]
+    batched = [_make(s, data_interval=d) for s, d in zip(specs, dis)]
+    offs = [0, 3, 1, 7, 2]
+    batch = Batch([d for _, d in batched])
+    for k in range(5):
+        for (env, data), o in zip(alone, offs):
+            ptc_updater(env).update_particles(data, env.params.delta_t, o + k)
+            field_solver(env).update_fields(data, env.params.delta_t, o + k)
+        batch.update_particles([o + k for o in offs])
+        batch.update_fields([o + k for o in offs])
+    batch.sync()
+    _compare(alone, batched)
+    for r, ((_, da), (_, db)) in enumerate(zip(alone, batched)):
+        fa, fb = da.fields_host(), db.fields_host()
+        for s_ in range(len(fa["Rho"])):
+            assert_bits(fb["Rho"][s_], fa["Rho"][s_], f"run {r}: Rho{s_}")
+    _close(batch, alone, batched)
