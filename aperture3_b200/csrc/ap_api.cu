@@ -445,7 +445,8 @@ namespace apb {
 // First part of an update: zero the accumulators, refresh the weight bound
 // and the tile order if needed, and fill the kernel parameters. Returns
 // AP_OK; *has_work is false when there are no particles.
-int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work) {
+int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work,
+                   bool batched) {
   const ap_params &pr = c->params;
   const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
   // data.J.initialize(); data.Rho[i].initialize() (ptc_updater.cu:752-755):
@@ -454,15 +455,16 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
   const int ncomp = 3 + (do_rho ? pr.num_species : 0);
   const bool ls = c->coord == 1;
   int ph = phase_begin(c, kPhFinalize);
-  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
-                         c->stream));
+  if (!batched)
+    AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
+                           c->stream));
   if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
   // Rho keeps the zeros of the last step without charge deposition
   if (!do_rho && !ls && !c->rho_is_zero) {
     for (int s = 0; s < pr.num_species; ++s) AP_TRY(launch_zero(*c, c->fields.Rho[s]));
     c->rho_is_zero = true;
   }
-  AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  if (!batched) AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
   phase_end(c, ph);
 
   std::memset(&P, 0, sizeof(P));
@@ -541,7 +543,7 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
 
 // Last part: the tile-order update from the directions the kernel wrote,
 // then rounding (and folding / process_j) of the current and smoothing.
-int update_complete(Ctx *c, double dt, uint32_t step, bool had_work) {
+int update_complete(Ctx *c, double dt, uint32_t step, bool had_work, bool batched) {
   const ap_params &pr = c->params;
   const bool do_rho = ((step + 1) % (uint32_t)pr.data_interval) == 0;
   const int ncomp = 3 + (do_rho ? pr.num_species : 0);
@@ -561,6 +563,7 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work) {
       c->order_valid = false;
     }
   }
+  if (batched && c->mk.dim == 1 && !ls) return AP_OK;  // batched finalize and smoothing
   ph = phase_begin(c, kPhFinalize);
   if (ls) {
     // process_j, then (ptc_updater_logsph::apply_boundary) axis_rho after
@@ -580,6 +583,59 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work) {
 }
 
 int ctx_check_status(Ctx *c) { return check_status(c); }
+
+int update_smooth(Ctx *c, uint32_t step) { return smooth_current_async(c, step); }
+
+int fill_run1d(Ctx *c, double dt, uint32_t step, Run1D &d) {
+  std::memset(&d, 0, sizeof(d));
+  const ap_mesh &m = c->mesh;
+  const ap_fields &f = c->fields;
+  auto fa = [](const ap_array &a) { return FieldArr{a.ptr, (int)(a.pitch / sizeof(float))}; };
+  d.n0 = m.dims[0];
+  d.g0 = m.guard[0];
+  d.r0 = m.dims[0] - 2 * m.guard[0];
+  d.per0 = c->params.periodic[0];
+  d.id0 = m.inv_delta[0];
+  for (int k = 0; k < 3; ++k) {
+    d.E[k] = fa(f.E[k]);
+    d.B[k] = fa(f.B[k]);
+    d.Eb[k] = fa(f.Ebg[k]);
+    d.Bb[k] = fa(f.Bbg[k]);
+    d.J[k] = fa(f.J[k]);
+  }
+  for (int s = 0; s < c->params.num_species; ++s) d.Rho[s] = fa(f.Rho[s]);
+  d.divE = fa(f.divE);
+  d.divB = fa(f.divB);
+  d.has_divs = f.divE.ptr && f.divB.ptr;
+  d.acc = c->acc;
+  d.acc_comp = c->acc_comp;
+  d.fx = c->fx_used;
+  const bool do_rho = ((step + 1) % (uint32_t)c->params.data_interval) == 0;
+  d.ncomp = 3 + (do_rho ? c->params.num_species : 0);
+  d.zero_comps = d.ncomp;
+  d.dt = (float)dt;
+  d.dt_half = step == 0 ? (float)(0.5 * dt) : 0.0f;
+  d.step = step;
+  if (c->pstate && c->pair.enabled) {
+    if (ensure_pair_scratch(*c) != AP_OK) return AP_ERR_NOMEM;
+    d.counts = c->pair_chunks;
+    d.offs = c->pair_chunks + c->pair_cap_chunks;
+    d.tot = d.offs + c->pair_cap_chunks;
+    d.gamma_thr = c->pair.gamma_thr;
+    d.free_path = c->pair.free_path;
+    d.pair_energy = c->pair.pair_energy;
+    d.pair_dt = (float)dt;
+    d.key[0] = (uint32_t)c->pair.seed;
+    d.key[1] = (uint32_t)(c->pair.seed >> 32);
+    d.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
+               c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
+    d.ids = c->ptc.id;
+    d.pst = c->pstate;
+    d.emit = c->dir;
+    d.capacity = c->capacity;
+  }
+  return AP_OK;
+}
 
 }  // namespace apb
 

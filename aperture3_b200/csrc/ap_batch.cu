@@ -59,6 +59,14 @@ struct ap_batch {
   size_t stage_bytes = 0;
   size_t cap_runs = 0;  // runs the staging buffers hold
   uint32_t *queue = nullptr;
+  // staging ring for the descriptors of the batched 1D launches
+  struct Slot {
+    unsigned char *h = nullptr, *d = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+  };
+  Slot ring[8];
+  int ring_next = 0;
   // autotuning: time the push / deposit per class when set
   bool tuning = false;
   std::vector<int> tune_class;   // class of each run
@@ -77,6 +85,11 @@ void release(ap_batch *b) {
   cudaFree(b->d_stage);
   cudaFree(b->queue);
   for (cudaEvent_t e : b->tune_ev) cudaEventDestroy(e);
+  for (auto &s : b->ring) {
+    if (s.h) cudaFreeHost(s.h);
+    cudaFree(s.d);
+    if (s.ev) cudaEventDestroy(s.ev);
+  }
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -119,6 +132,55 @@ int fail_cuda(cudaError_t e) {
     int _s = (expr);                 \
     if (_s != AP_OK) return _s;      \
   } while (0)
+
+// Copies `bytes` from src to a device staging slot, in stream order; the
+// slot's host buffer is reused only after its previous copy completed.
+int stage(ap_batch *b, const void *src, size_t bytes, const unsigned char **dptr) {
+  auto &s = b->ring[b->ring_next];
+  b->ring_next = (b->ring_next + 1) % 8;
+  if (!s.ev) B_TRY(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+  else B_TRY(cudaEventSynchronize(s.ev));
+  if (bytes > s.cap) {
+    B_TRY(cudaStreamSynchronize(b->stream));
+    if (s.h) cudaFreeHost(s.h);
+    cudaFree(s.d);
+    s.h = s.d = nullptr;
+    s.cap = 0;
+    const size_t cap = bytes * 2 > 4096 ? bytes * 2 : 4096;
+    B_TRY(cudaMallocHost(reinterpret_cast<void **>(&s.h), cap));
+    B_TRY(cudaMalloc(reinterpret_cast<void **>(&s.d), cap));
+    s.cap = cap;
+  }
+  std::memcpy(s.h, src, bytes);
+  B_TRY(cudaMemcpyAsync(s.d, s.h, bytes, cudaMemcpyHostToDevice, b->stream));
+  B_TRY(cudaEventRecord(s.ev, b->stream));
+  *dptr = s.d;
+  return AP_OK;
+}
+
+// Stages 1D run descriptors followed by their work-item offsets (items[r]
+// per run) and returns the device addresses and the total.
+int stage_run1d(ap_batch *b, const std::vector<Run1D> &d, const std::vector<uint32_t> &items,
+                const Run1D **dd, const uint32_t **db, uint32_t *total) {
+  const size_t n = d.size();
+  std::vector<unsigned char> buf(sizeof(Run1D) * n + sizeof(uint32_t) * (n + 1));
+  std::memcpy(buf.data(), d.data(), sizeof(Run1D) * n);
+  uint32_t *base = reinterpret_cast<uint32_t *>(buf.data() + sizeof(Run1D) * n);
+  uint32_t t = 0;
+  for (size_t r = 0; r < n; ++r) {
+    base[r] = t;
+    t += items[r];
+  }
+  base[n] = t;
+  const unsigned char *dp = nullptr;
+  B_TRY_ST(stage(b, buf.data(), buf.size(), &dp));
+  *dd = reinterpret_cast<const Run1D *>(dp);
+  *db = reinterpret_cast<const uint32_t *>(dp + sizeof(Run1D) * n);
+  *total = t;
+  return AP_OK;
+}
+
+bool is_1d(const Ctx *c) { return c->mk.dim == 1 && c->coord == 0; }
 
 // Launches the push / deposit of the given groups from staged descriptors.
 int launch_groups(ap_batch *b, const std::vector<Group> &gs,
@@ -181,14 +243,35 @@ int batch_update(ap_batch *b, const double *dt, const uint32_t *steps) {
   std::vector<PushDepositParams> P(n);
   std::vector<bool> work(n, false);
   bool do_rho = false;
+  // 1D runs: accumulator clearing and finalize are batched launches
+  std::vector<Run1D> d1;
+  std::vector<uint32_t> zero_items, fin_items;
+  std::vector<int> idx1;
   for (size_t r = 0; r < n; ++r) {
     Ctx *c = b->runs[r];
     bool w = false;
-    B_TRY_ST(update_prepare(c, dt[r], steps[r], P[r], &w));
+    const bool one = is_1d(c);
+    B_TRY_ST(update_prepare(c, dt[r], steps[r], P[r], &w, one));
+    if (one) {
+      Run1D d;
+      B_TRY_ST(fill_run1d(c, dt[r], steps[r], d));
+      d1.push_back(d);
+      zero_items.push_back(
+          (uint32_t)(((size_t)d.zero_comps * d.acc_comp + 255) / 256));
+      fin_items.push_back((uint32_t)((d.n0 + 255) / 256));
+      idx1.push_back((int)r);
+    }
     work[r] = w;
     // one kernel variant for all: charge deposition when any run needs it
     // (runs without it skip the charge terms through P.do_rho)
     do_rho = do_rho || ((steps[r] + 1) % (uint32_t)c->params.data_interval) == 0;
+  }
+  const Run1D *dd = nullptr;
+  const uint32_t *db = nullptr;
+  uint32_t tot = 0;
+  if (!d1.empty()) {
+    B_TRY_ST(stage_run1d(b, d1, zero_items, &dd, &db, &tot));
+    B_TRY(launch_b1_zero(b->stream, b->num_sms, dd, db, (int)d1.size(), tot));
   }
   if (!b->tuning) {
     B_TRY_ST(launch_groups(b, make_groups(b, work, nullptr, 0), P, do_rho));
@@ -208,7 +291,16 @@ int batch_update(ap_batch *b, const double *dt, const uint32_t *steps) {
     }
   }
   for (size_t r = 0; r < n; ++r)
-    B_TRY_ST(update_complete(b->runs[r], dt[r], steps[r], work[r]));
+    B_TRY_ST(update_complete(b->runs[r], dt[r], steps[r], work[r], is_1d(b->runs[r])));
+  if (!d1.empty()) {
+    B_TRY_ST(stage_run1d(b, d1, fin_items, &dd, &db, &tot));
+    B_TRY(launch_b1_finalize(b->stream, b->num_sms, dd, db, (int)d1.size(), tot));
+    for (size_t k = 0; k < idx1.size(); ++k) {
+      Ctx *c = b->runs[idx1[k]];
+      if (c->params.current_smoothing > 0) B_TRY_ST(update_smooth(c, steps[idx1[k]]));
+      c->launches += 2;
+    }
+  }
   return AP_OK;
 }
 
@@ -335,10 +427,35 @@ AP_API int ap_batch_update_particles(ap_batch *b, const double *dt, const uint32
 
 AP_API int ap_batch_update_fields(ap_batch *b, const double *dt, const uint32_t *steps) {
   if (!b || !dt || !steps) return AP_ERR_INVALID;
+  // 1D runs: four batched launches (initial E half step where a run is at
+  // step 0, B, E, divergences); 2D runs one by one
+  std::vector<Run1D> d1;
+  std::vector<uint32_t> items;
+  bool any_half = false;
   for (size_t r = 0; r < b->runs.size(); ++r) {
-    int st = ap_update_fields(static_cast<ap_ctx *>(b->runs[r]), dt[r], steps[r]);
-    if (st != AP_OK) return st;
+    Ctx *c = b->runs[r];
+    if (!is_1d(c)) {
+      int st = ap_update_fields(static_cast<ap_ctx *>(c), dt[r], steps[r]);
+      if (st != AP_OK) return st;
+      continue;
+    }
+    Run1D d;
+    B_TRY_ST(fill_run1d(c, dt[r], steps[r], d));
+    any_half = any_half || d.dt_half > 0.0f;
+    d1.push_back(d);
+    items.push_back((uint32_t)((d.r0 + 255) / 256));
+    c->launches += 3;
   }
+  if (d1.empty()) return AP_OK;
+  const Run1D *dd = nullptr;
+  const uint32_t *db = nullptr;
+  uint32_t tot = 0;
+  B_TRY_ST(stage_run1d(b, d1, items, &dd, &db, &tot));
+  const int nr = (int)d1.size();
+  if (any_half) B_TRY(launch_b1_fields(b->stream, b->num_sms, dd, db, nr, tot, 0));
+  B_TRY(launch_b1_fields(b->stream, b->num_sms, dd, db, nr, tot, 1));
+  B_TRY(launch_b1_fields(b->stream, b->num_sms, dd, db, nr, tot, 2));
+  B_TRY(launch_b1_fields(b->stream, b->num_sms, dd, db, nr, tot, 3));
   return AP_OK;
 }
 
@@ -353,11 +470,29 @@ AP_API int ap_batch_sort_by_cell(ap_batch *b) {
 
 AP_API int ap_batch_inject_pairs(ap_batch *b, const double *dt, const uint32_t *steps) {
   if (!b || !dt || !steps) return AP_ERR_INVALID;
+  // 1D runs: three batched launches over all their chunks; 2D runs one by one
+  std::vector<Run1D> d1;
+  std::vector<uint32_t> items;
   for (size_t r = 0; r < b->runs.size(); ++r) {
     Ctx *c = b->runs[r];
-    if (!c->pair.enabled) continue;
-    B_TRY_ST(enqueue_pairs(*c, (float)dt[r], steps[r]));
+    if (!c->pair.enabled || !c->pstate) continue;
+    if (!is_1d(c)) {
+      B_TRY_ST(enqueue_pairs(*c, (float)dt[r], steps[r]));
+      continue;
+    }
+    Run1D d;
+    B_TRY_ST(fill_run1d(c, dt[r], steps[r], d));
+    d1.push_back(d);
+    items.push_back(pair_chunks_of(*c));
+    c->number_stale = true;
+    c->launches += 3;
   }
+  if (d1.empty()) return AP_OK;
+  const Run1D *dd = nullptr;
+  const uint32_t *db = nullptr;
+  uint32_t tot = 0;
+  B_TRY_ST(stage_run1d(b, d1, items, &dd, &db, &tot));
+  B_TRY(launch_b1_pairs(b->stream, b->num_sms, dd, db, (int)d1.size(), tot));
   return AP_OK;
 }
 
@@ -365,14 +500,18 @@ AP_API int ap_batch_sync(ap_batch *b, int *failed_run) {
   if (!b) return AP_ERR_INVALID;
   if (failed_run) *failed_run = -1;
   B_TRY(cudaStreamSynchronize(b->stream));
+  // the status words of batched runs accumulate between syncs: read, then
+  // clear them
+  int first = AP_OK;
   for (size_t r = 0; r < b->runs.size(); ++r) {
     int st = ctx_check_status(b->runs[r]);
-    if (st != AP_OK) {
+    B_TRY(cudaMemsetAsync(b->runs[r]->status, 0, sizeof(DevStatus), b->stream));
+    if (st != AP_OK && first == AP_OK) {
       if (failed_run) *failed_run = (int)r;
-      return st;
+      first = st;
     }
   }
-  return AP_OK;
+  return first;
 }
 
 AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *steps,

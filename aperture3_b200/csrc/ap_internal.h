@@ -120,6 +120,47 @@ struct PairState {
   unsigned long long dropped_total;
 };
 
+// A 1D run in the batched per-step launches other than the push / deposit
+// (accumulator clearing, current finalize, field update, pair injection):
+// everything a kernel needs, so that one launch serves all 1D runs.
+struct Run1D {
+  int n0, g0, r0, per0;
+  float id0;
+  FieldArr E[3], B[3], Eb[3], Bb[3], J[3], Rho[AP_MAX_SPECIES], divE, divB;
+  unsigned long long *acc;
+  size_t acc_comp;
+  const FixedFmt *fx;
+  int zero_comps;  // accumulator components to clear before the push
+  int ncomp;       // components the finalize rounds (3 + species on charge steps)
+  float dt;        // field update
+  float dt_half;   // the initial E half step (step 0), else 0
+  int has_divs;
+  // pair injection
+  float gamma_thr, free_path, pair_energy, pair_dt;
+  uint32_t key[2];
+  uint32_t step;
+  PtcK p;
+  uint64_t *ids;
+  PairState *pst;
+  uint8_t *emit;
+  uint32_t *counts, *offs, *tot;
+  size_t capacity;
+};
+
+// Batched 1D launches (k_fields.cu, k_pairs.cu). base has nruns + 1
+// entries: run r owns work items [base[r], base[r + 1]). Items are blocks
+// of 256 accumulator words (zero), 256 cells (finalize), 256 bulk cells
+// (fields), 1024 particle slots (pairs).
+cudaError_t launch_b1_zero(cudaStream_t s, int num_sms, const Run1D *runs, const uint32_t *base,
+                           int nruns, uint32_t total);
+cudaError_t launch_b1_finalize(cudaStream_t s, int num_sms, const Run1D *runs,
+                               const uint32_t *base, int nruns, uint32_t total);
+// which: 0 initial E half step, 1 B, 2 E, 3 divergences
+cudaError_t launch_b1_fields(cudaStream_t s, int num_sms, const Run1D *runs, const uint32_t *base,
+                             int nruns, uint32_t total, int which);
+cudaError_t launch_b1_pairs(cudaStream_t s, int num_sms, const Run1D *runs,
+                            const uint32_t *base, int nruns, uint32_t total);
+
 // One run of a batched launch: its tensor maps and its parameters, in
 // device memory (the maps must be 64-byte aligned).
 struct alignas(64) RunDesc {
@@ -243,6 +284,8 @@ cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
 // back when it moved (waits for the stream); push_number writes the host
 // count to the device.
 int enqueue_pairs(Ctx &c, float dt, uint32_t step);
+int ensure_pair_scratch(Ctx &c);
+uint32_t pair_chunks_of(const Ctx &c);
 int refresh_number(Ctx *c);
 int push_number(Ctx *c);
 
@@ -262,8 +305,18 @@ MeshK make_meshk(const ap_mesh &m);
 // tile-order rebuild, kernel parameters), the push / deposit launch, and
 // complete (order update, finalize, smoothing). ctx_check_status reads the
 // device status word back (waits for the stream).
-int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work);
-int update_complete(Ctx *c, double dt, uint32_t step, bool had_work);
+// batched: the caller clears the accumulators (and, for 1D runs, runs the
+// finalize) in batched launches; the device status word is not cleared, so
+// it accumulates until the batch reads it.
+int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool *has_work,
+                   bool batched = false);
+int update_complete(Ctx *c, double dt, uint32_t step, bool had_work, bool batched = false);
+// Smoothing after a finalize done elsewhere (batched 1D runs).
+int update_smooth(Ctx *c, uint32_t step);
+// Fills the 1D batch descriptor of a context (fields, accumulators, pair
+// scratch) for the given step and dt.
+int fill_run1d(Ctx *c, double dt, uint32_t step, Run1D &d);
+
 int ctx_check_status(Ctx *c);
 
 // One persistent push / deposit launch over the tiles of several 2D

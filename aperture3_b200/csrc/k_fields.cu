@@ -50,14 +50,14 @@ __device__ __forceinline__ void store_with_images(const Arr &a, const Geo &G, in
       if (a2 || b) a(ix[a2], jx[b]) = v;
 }
 
-// compute_e_update2d (field_solver.cu:45-84) / compute_e_update1d (:14-43).
-__global__ void k_update_e(Geo G, Arr e1, Arr e2, Arr e3, Arr b1, Arr b2, Arr b3, Arr b01,
-                           Arr b02, Arr b03, Arr j1, Arr j2, Arr j3, float dt) {
-  const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int n2 = (G.dim > 1 ? G.g1 : 0) + blockIdx.y * blockDim.y + threadIdx.y;
-  if (n1 >= G.n0 - G.g0) return;
+// compute_e_update2d (field_solver.cu:45-84) / compute_e_update1d (:14-43)
+// for bulk cell (n1, n2).
+__device__ __forceinline__ void e_update_cell(const Geo &G, const Arr &e1, const Arr &e2,
+                                              const Arr &e3, const Arr &b1, const Arr &b2,
+                                              const Arr &b3, const Arr &b01, const Arr &b02,
+                                              const Arr &b03, const Arr &j1, const Arr &j2,
+                                              const Arr &j3, float dt, int n1, int n2) {
   if (G.dim > 1) {
-    if (n2 >= G.n1 - G.g1) return;
     const float v1 = e1(n1, n2) + dt * ((b3(n1, n2 + 1) - b3(n1, n2) - b03(n1, n2 + 1) +
                                          b03(n1, n2)) * G.id1 - j1(n1, n2));
     const float v2 = e2(n1, n2) + dt * ((b3(n1, n2) - b3(n1 + 1, n2) - b03(n1, n2) +
@@ -82,14 +82,22 @@ __global__ void k_update_e(Geo G, Arr e1, Arr e2, Arr e3, Arr b1, Arr b2, Arr b3
   }
 }
 
-// compute_b_update2d (field_solver.cu:160-193) / compute_b_update1d (:133-158).
-__global__ void k_update_b(Geo G, Arr e1, Arr e2, Arr e3, Arr e01, Arr e02, Arr e03, Arr b1,
-                           Arr b2, Arr b3, float dt) {
+__global__ void k_update_e(Geo G, Arr e1, Arr e2, Arr e3, Arr b1, Arr b2, Arr b3, Arr b01,
+                           Arr b02, Arr b03, Arr j1, Arr j2, Arr j3, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = (G.dim > 1 ? G.g1 : 0) + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0) return;
+  if (G.dim > 1 && n2 >= G.n1 - G.g1) return;
+  e_update_cell(G, e1, e2, e3, b1, b2, b3, b01, b02, b03, j1, j2, j3, dt, n1, n2);
+}
+
+// compute_b_update2d (field_solver.cu:160-193) / compute_b_update1d (:133-158)
+// for bulk cell (n1, n2).
+__device__ __forceinline__ void b_update_cell(const Geo &G, const Arr &e1, const Arr &e2,
+                                              const Arr &e3, const Arr &e01, const Arr &e02,
+                                              const Arr &e03, const Arr &b1, const Arr &b2,
+                                              const Arr &b3, float dt, int n1, int n2) {
   if (G.dim > 1) {
-    if (n2 >= G.n1 - G.g1) return;
     const float v1 = b1(n1, n2) - dt * (e3(n1, n2) - e3(n1, n2 - 1) - e03(n1, n2) +
                                         e03(n1, n2 - 1)) * G.id1;
     const float v2 = b2(n1, n2) - dt * (e3(n1 - 1, n2) - e3(n1, n2) - e03(n1 - 1, n2) +
@@ -115,14 +123,22 @@ __global__ void k_update_b(Geo G, Arr e1, Arr e2, Arr e3, Arr e01, Arr e02, Arr 
   }
 }
 
-// compute_divs_2d (field_solver.cu:261-288) / compute_divs_1d (:237-259).
-__global__ void k_divs(Geo G, Arr e1, Arr e2, Arr b1, Arr b2, Arr e01, Arr e02, Arr b01,
-                       Arr b02, Arr divE, Arr divB) {
+__global__ void k_update_b(Geo G, Arr e1, Arr e2, Arr e3, Arr e01, Arr e02, Arr e03, Arr b1,
+                           Arr b2, Arr b3, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = (G.dim > 1 ? G.g1 : 0) + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0) return;
+  if (G.dim > 1 && n2 >= G.n1 - G.g1) return;
+  b_update_cell(G, e1, e2, e3, e01, e02, e03, b1, b2, b3, dt, n1, n2);
+}
+
+// compute_divs_2d (field_solver.cu:261-288) / compute_divs_1d (:237-259) for
+// bulk cell (n1, n2).
+__device__ __forceinline__ void divs_cell(const Geo &G, const Arr &e1, const Arr &e2,
+                                          const Arr &b1, const Arr &b2, const Arr &e01,
+                                          const Arr &e02, const Arr &b01, const Arr &b02,
+                                          const Arr &divE, const Arr &divB, int n1, int n2) {
   if (G.dim > 1) {
-    if (n2 >= G.n1 - G.g1) return;
     divE(n1, n2) = (e1(n1 + 1, n2) - e01(n1 + 1, n2) - e1(n1, n2) + e01(n1, n2)) * G.id0 +
                    (e2(n1, n2 + 1) - e02(n1, n2 + 1) - e2(n1, n2) + e02(n1, n2)) * G.id1;
     divB(n1, n2) = (b1(n1, n2) - b01(n1, n2) - b1(n1 - 1, n2) + b01(n1 - 1, n2)) * G.id0 +
@@ -131,6 +147,15 @@ __global__ void k_divs(Geo G, Arr e1, Arr e2, Arr b1, Arr b2, Arr e01, Arr e02, 
     divE(n1, 0) = (e1(n1 + 1, 0) - e01(n1 + 1, 0) - e1(n1, 0) + e01(n1, 0)) * G.id0;
     divB(n1, 0) = (b1(n1, 0) - b01(n1, 0) - b1(n1 - 1, 0) + b01(n1 - 1, 0)) * G.id0;
   }
+}
+
+__global__ void k_divs(Geo G, Arr e1, Arr e2, Arr b1, Arr b2, Arr e01, Arr e02, Arr b01,
+                       Arr b02, Arr divE, Arr divB) {
+  const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int n2 = (G.dim > 1 ? G.g1 : 0) + blockIdx.y * blockDim.y + threadIdx.y;
+  if (n1 >= G.n0 - G.g0) return;
+  if (G.dim > 1 && n2 >= G.n1 - G.g1) return;
+  divs_cell(G, e1, e2, b1, b2, e01, e02, b01, b02, divE, divB, n1, n2);
 }
 
 // Guard strips of one dim: mode 0 copies interior strips into the opposite
@@ -209,6 +234,27 @@ __global__ void k_copy_bulk(Geo G, Arr src, Arr dst) {
 // exact, so the order of the adds does not matter; the only rounding is the
 // final conversion (int64 -> double is exact below 2^53, then one rounding
 // to FP32).
+__device__ __forceinline__ void finalize_cell(const Geo &G, const unsigned long long *a,
+                                              int acc_pitch, double inv, const Arr &out, int x,
+                                              int y) {
+  int xi = -1, yi = -1;
+  if (G.per0) {
+    if (x >= G.g0 && x < 2 * G.g0) xi = x + G.r0;
+    else if (x >= G.n0 - 2 * G.g0 && x < G.n0 - G.g0) xi = x - G.r0;
+  }
+  if (G.dim > 1 && G.per1) {
+    if (y >= G.g1 && y < 2 * G.g1) yi = y + G.r1;
+    else if (y >= G.n1 - 2 * G.g1 && y < G.n1 - G.g1) yi = y - G.r1;
+  }
+  unsigned long long v = a[(size_t)y * acc_pitch + x];
+  if (xi >= 0) v += a[(size_t)y * acc_pitch + xi];
+  if (yi >= 0) {
+    v += a[(size_t)yi * acc_pitch + x];
+    if (xi >= 0) v += a[(size_t)yi * acc_pitch + xi];
+  }
+  out(x, y) = (float)((double)(long long)v * inv);
+}
+
 __global__ void k_finalize(Geo G, const unsigned long long *__restrict__ acc, int acc_pitch,
                            size_t acc_comp, const FixedFmt *fmt, int ncomp, Arr o0, Arr o1,
                            Arr o2, Arr o3, Arr o4, Arr o5, Arr o6, Arr o7, Arr o8, Arr o9,
@@ -222,25 +268,8 @@ __global__ void k_finalize(Geo G, const unsigned long long *__restrict__ acc, in
   const unsigned long long *a = acc + comp * acc_comp;
   const double inv = ldexp(1.0, -fmt->S);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
-       t += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(t % G.n0), y = (int)(t / G.n0);
-    int xi = -1, yi = -1;
-    if (G.per0) {
-      if (x >= G.g0 && x < 2 * G.g0) xi = x + G.r0;
-      else if (x >= G.n0 - 2 * G.g0 && x < G.n0 - G.g0) xi = x - G.r0;
-    }
-    if (G.dim > 1 && G.per1) {
-      if (y >= G.g1 && y < 2 * G.g1) yi = y + G.r1;
-      else if (y >= G.n1 - 2 * G.g1 && y < G.n1 - G.g1) yi = y - G.r1;
-    }
-    unsigned long long v = a[(size_t)y * acc_pitch + x];
-    if (xi >= 0) v += a[(size_t)y * acc_pitch + xi];
-    if (yi >= 0) {
-      v += a[(size_t)yi * acc_pitch + x];
-      if (xi >= 0) v += a[(size_t)yi * acc_pitch + xi];
-    }
-    out(x, y) = (float)((double)(long long)v * inv);
-  }
+       t += (size_t)gridDim.x * blockDim.x)
+    finalize_cell(G, a, acc_pitch, inv, out, (int)(t % G.n0), (int)(t / G.n0));
 }
 
 Geo make_geo(const Ctx &c) {
@@ -271,6 +300,121 @@ void bulk_launch_shape(const Geo &G, dim3 &grid, dim3 &block) {
 }
 
 }  // namespace
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Batched 1D launches: work item g belongs to run r with base[r] <= g <
+// base[r + 1]; the per-cell arithmetic is the single-run kernels'.
+
+__device__ __forceinline__ int run_of(const uint32_t *base, int nruns, uint32_t g) {
+  int lo = 0, hi = nruns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ Arr farr(const FieldArr &a) { return Arr{a.ptr, a.pitch}; }
+
+__device__ __forceinline__ Geo geo1(const Run1D &R) {
+  Geo G;
+  G.n0 = R.n0;
+  G.n1 = 1;
+  G.g0 = R.g0;
+  G.g1 = 0;
+  G.r0 = R.r0;
+  G.r1 = 0;
+  G.per0 = R.per0;
+  G.per1 = 0;
+  G.dim = 1;
+  G.id0 = R.id0;
+  G.id1 = 0.0f;
+  return G;
+}
+
+__global__ void k_b1_zero(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base,
+                          int nruns) {
+  const uint32_t total = base[nruns];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const int r = run_of(base, nruns, g);
+    const Run1D &R = runs[r];
+    const size_t w = (size_t)(g - base[r]) * 256 + threadIdx.x;
+    if (w < (size_t)R.zero_comps * R.acc_comp) R.acc[w] = 0ull;
+  }
+}
+
+__global__ void k_b1_finalize(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base,
+                              int nruns) {
+  const uint32_t total = base[nruns];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const int r = run_of(base, nruns, g);
+    const Run1D &R = runs[r];
+    const int x = (int)(g - base[r]) * 256 + threadIdx.x;
+    if (x >= R.n0) continue;
+    const Geo G = geo1(R);
+    const double inv = ldexp(1.0, -R.fx->S);
+    for (int comp = 0; comp < R.ncomp; ++comp) {
+      const Arr out = farr(comp < 3 ? R.J[comp] : R.Rho[comp - 3]);
+      finalize_cell(G, R.acc + comp * R.acc_comp, R.n0, inv, out, x, 0);
+    }
+  }
+}
+
+__global__ void k_b1_fields(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base,
+                            int nruns, int which) {
+  const uint32_t total = base[nruns];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const int r = run_of(base, nruns, g);
+    const Run1D &R = runs[r];
+    const int n1 = R.g0 + (int)(g - base[r]) * 256 + threadIdx.x;
+    if (n1 >= R.n0 - R.g0) continue;
+    const Geo G = geo1(R);
+    if (which == 0 || which == 2) {
+      const float dt = which == 0 ? R.dt_half : R.dt;
+      if (which == 0 && !(dt > 0.0f)) continue;
+      e_update_cell(G, farr(R.E[0]), farr(R.E[1]), farr(R.E[2]), farr(R.B[0]), farr(R.B[1]),
+                    farr(R.B[2]), farr(R.Bb[0]), farr(R.Bb[1]), farr(R.Bb[2]), farr(R.J[0]),
+                    farr(R.J[1]), farr(R.J[2]), dt, n1, 0);
+    } else if (which == 1) {
+      b_update_cell(G, farr(R.E[0]), farr(R.E[1]), farr(R.E[2]), farr(R.Eb[0]), farr(R.Eb[1]),
+                    farr(R.Eb[2]), farr(R.B[0]), farr(R.B[1]), farr(R.B[2]), R.dt, n1, 0);
+    } else if (R.has_divs) {
+      divs_cell(G, farr(R.E[0]), farr(R.E[1]), farr(R.B[0]), farr(R.B[1]), farr(R.Eb[0]),
+                farr(R.Eb[1]), farr(R.Bb[0]), farr(R.Bb[1]), farr(R.divE), farr(R.divB), n1, 0);
+    }
+  }
+}
+
+uint32_t grid_of(uint32_t total, int num_sms) {
+  const uint32_t cap = (uint32_t)num_sms * 16;
+  return total < cap ? total : cap;
+}
+
+}  // namespace
+
+cudaError_t launch_b1_zero(cudaStream_t s, int num_sms, const Run1D *runs, const uint32_t *base,
+                           int nruns, uint32_t total) {
+  if (total == 0) return cudaSuccess;
+  k_b1_zero<<<grid_of(total, num_sms), 256, 0, s>>>(runs, base, nruns);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_b1_finalize(cudaStream_t s, int num_sms, const Run1D *runs,
+                               const uint32_t *base, int nruns, uint32_t total) {
+  if (total == 0) return cudaSuccess;
+  k_b1_finalize<<<grid_of(total, num_sms), 256, 0, s>>>(runs, base, nruns);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_b1_fields(cudaStream_t s, int num_sms, const Run1D *runs, const uint32_t *base,
+                             int nruns, uint32_t total, int which) {
+  if (total == 0) return cudaSuccess;
+  k_b1_fields<<<grid_of(total, num_sms), 256, 0, s>>>(runs, base, nruns, which);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_update_e(Ctx &c, float dt) {
   const ap_fields &f = c.fields;

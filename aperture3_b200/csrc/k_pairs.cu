@@ -48,29 +48,27 @@ __device__ __forceinline__ bool emit_test(const PairK &K, const PtcK &p, const u
   return uniform_of(step, ids[idx], K.key) < prob;
 }
 
-__global__ void __launch_bounds__(kPairThreads)
-    k_pair_mark(PairK K, PtcK p, const uint64_t *ids, const PairState *st, uint32_t step,
-                uint8_t *emit, uint32_t *chunk_count, uint32_t nchunks) {
-  const size_t number = st->number;
-  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    int cnt = 0;
+// Marks the emitters of chunk ch and stores the chunk's count.
+__device__ __forceinline__ void mark_chunk(const PairK &K, const PtcK &p, const uint64_t *ids,
+                                           size_t number, uint32_t step, uint8_t *emit,
+                                           uint32_t *chunk_count, uint32_t ch) {
+  int cnt = 0;
 #pragma unroll
-    for (int k = 0; k < kPairPerThread; ++k) {
-      const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
-      const bool e = idx < number && emit_test(K, p, ids, idx, step);
-      if (idx < number) emit[idx] = e ? 1 : 0;
-      cnt += __syncthreads_count(e);
-    }
-    if (threadIdx.x == 0) chunk_count[ch] = (uint32_t)cnt;
+  for (int k = 0; k < kPairPerThread; ++k) {
+    const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
+    const bool e = idx < number && emit_test(K, p, ids, idx, step);
+    if (idx < number) emit[idx] = e ? 1 : 0;
+    cnt += __syncthreads_count(e);
   }
+  if (threadIdx.x == 0) chunk_count[ch] = (uint32_t)cnt;
 }
 
-// One CTA: exclusive scan of the chunk counts into offs; the total is
-// clamped to the free capacity, and the device state moves on: the old
-// count and next id go to tot[] for the append pass.
-__global__ void __launch_bounds__(1024)
-    k_pair_scan(const uint32_t *chunk_count, uint32_t nchunks, uint32_t *offs, size_t capacity,
-                PairState *st, uint32_t *tot) {
+// One CTA of 1024 threads: exclusive scan of the chunk counts into offs; the
+// total is clamped to the free capacity and the device state moves on; the
+// old count and next id go to tot[] for the append pass.
+__device__ __forceinline__ void scan_chunks(const uint32_t *chunk_count, uint32_t nchunks,
+                                            uint32_t *offs, size_t capacity, PairState *st,
+                                            uint32_t *tot) {
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
   if (threadIdx.x == 0) s_carry = 0;
@@ -123,9 +121,10 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
-__global__ void __launch_bounds__(kPairThreads)
-    k_pair_append(PairK K, PtcK p, uint64_t *ids, const uint8_t *emit, const uint32_t *offs,
-                  const uint32_t *tot, uint32_t nchunks) {
+// Appends the pairs of the emitters of chunk ch (ranked in slot order).
+__device__ __forceinline__ void append_chunk(const PairK &K, const PtcK &p, uint64_t *ids,
+                                             const uint8_t *emit, const uint32_t *offs,
+                                             const uint32_t *tot, uint32_t ch) {
   __shared__ uint32_t s_warp[kPairThreads / 32];
   const uint32_t emitted = tot[0];
   const size_t number = tot[1];
@@ -134,57 +133,129 @@ __global__ void __launch_bounds__(kPairThreads)
   const float Eph = K.pair_energy;
   float q = sqrtf(0.25f * Eph * Eph - 1.0f);
   if (q != q) q = 0.0f;
-  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    // thread t ranks slots ch * kPairChunk + t * kPairPerThread + [0, 4)
-    const size_t first = (size_t)ch * kPairChunk + (size_t)threadIdx.x * kPairPerThread;
-    uint32_t mine = 0;
+  // thread t ranks slots ch * kPairChunk + t * kPairPerThread + [0, 4)
+  const size_t first = (size_t)ch * kPairChunk + (size_t)threadIdx.x * kPairPerThread;
+  uint32_t mine = 0;
 #pragma unroll
-    for (int k = 0; k < kPairPerThread; ++k)
-      if (first + k < number) mine += emit[first + k];
-    uint32_t x = mine;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+  for (int k = 0; k < kPairPerThread; ++k)
+    if (first + k < number) mine += emit[first + k];
+  uint32_t x = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += s_warp[w];
+  uint32_t rank = offs[ch] + before + x - mine;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kPairPerThread; ++k) {
+    const size_t idx = first + k;
+    if (idx >= number || !emit[idx]) continue;
+    const uint32_t r = rank++;
+    if (r >= emitted) continue;  // over capacity: this parent keeps its energy
+    const float gamma = p.E[idx];
+    const float p1 = p.p1[idx], p2 = p.p2[idx], p3 = p.p3[idx];
+    const float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
+    const float gn = gamma - Eph;
+    const float scale = sqrtf(gn * gn - 1.0f) / pm;
+    p.p1[idx] = p1 * scale;
+    p.p2[idx] = p2 * scale;
+    p.p3[idx] = p3 * scale;
+    p.E[idx] = gn;
+    const float pp = p1 > 0.0f ? q : (p1 < 0.0f ? -q : 0.0f);  // sgn(p1) * q
+    const float ep = sqrtf(1.0f + pp * pp);
+    const size_t d = number + 2 * (size_t)r;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      p.x1[d + m] = p.x1[idx];
+      p.x2[d + m] = p.x2[idx];
+      p.x3[d + m] = p.x3[idx];
+      p.p1[d + m] = pp;
+      p.p2[d + m] = 0.0f;
+      p.p3[d + m] = 0.0f;
+      p.E[d + m] = ep;
+      p.w[d + m] = p.w[idx];
+      p.cell[d + m] = p.cell[idx];
+      p.flag[d + m] = kFlagSecondary | ((uint32_t)m << 29);  // electron, then positron
+      ids[d + m] = id_base + 2 * (uint64_t)r + (uint64_t)m;
     }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    uint32_t before = 0;
-    for (int w = 0; w < warp; ++w) before += s_warp[w];
-    uint32_t rank = offs[ch] + before + x - mine;
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kPairPerThread; ++k) {
-      const size_t idx = first + k;
-      if (idx >= number || !emit[idx]) continue;
-      const uint32_t r = rank++;
-      if (r >= emitted) continue;  // over capacity: this parent keeps its energy
-      const float gamma = p.E[idx];
-      const float p1 = p.p1[idx], p2 = p.p2[idx], p3 = p.p3[idx];
-      const float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
-      const float gn = gamma - Eph;
-      const float scale = sqrtf(gn * gn - 1.0f) / pm;
-      p.p1[idx] = p1 * scale;
-      p.p2[idx] = p2 * scale;
-      p.p3[idx] = p3 * scale;
-      p.E[idx] = gn;
-      const float pp = p1 > 0.0f ? q : (p1 < 0.0f ? -q : 0.0f);  // sgn(p1) * q
-      const float ep = sqrtf(1.0f + pp * pp);
-      const size_t d = number + 2 * (size_t)r;
-#pragma unroll
-      for (int m = 0; m < 2; ++m) {
-        p.x1[d + m] = p.x1[idx];
-        p.x2[d + m] = p.x2[idx];
-        p.x3[d + m] = p.x3[idx];
-        p.p1[d + m] = pp;
-        p.p2[d + m] = 0.0f;
-        p.p3[d + m] = 0.0f;
-        p.E[d + m] = ep;
-        p.w[d + m] = p.w[idx];
-        p.cell[d + m] = p.cell[idx];
-        p.flag[d + m] = kFlagSecondary | ((uint32_t)m << 29);  // electron, then positron
-        ids[d + m] = id_base + 2 * (uint64_t)r + (uint64_t)m;
-      }
-    }
+  }
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair_mark(PairK K, PtcK p, const uint64_t *ids, const PairState *st, uint32_t step,
+                uint8_t *emit, uint32_t *chunk_count, uint32_t nchunks) {
+  const size_t number = st->number;
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+    mark_chunk(K, p, ids, number, step, emit, chunk_count, ch);
+}
+
+__global__ void __launch_bounds__(1024)
+    k_pair_scan(const uint32_t *chunk_count, uint32_t nchunks, uint32_t *offs, size_t capacity,
+                PairState *st, uint32_t *tot) {
+  scan_chunks(chunk_count, nchunks, offs, capacity, st, tot);
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair_append(PairK K, PtcK p, uint64_t *ids, const uint8_t *emit, const uint32_t *offs,
+                  const uint32_t *tot, uint32_t nchunks) {
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+    append_chunk(K, p, ids, emit, offs, tot, ch);
+}
+
+// Batched over 1D runs: work item g is chunk g - base[r] of run r.
+__device__ __forceinline__ int run_of(const uint32_t *base, int nruns, uint32_t g) {
+  int lo = 0, hi = nruns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ PairK pairk_of(const Run1D &R) {
+  PairK K;
+  K.gamma_thr = R.gamma_thr;
+  K.free_path = R.free_path;
+  K.pair_energy = R.pair_energy;
+  K.dt = R.pair_dt;
+  K.key[0] = R.key[0];
+  K.key[1] = R.key[1];
+  return K;
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_b1_pair_mark(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base, int nruns) {
+  const uint32_t total = base[nruns];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const int r = run_of(base, nruns, g);
+    const Run1D &R = runs[r];
+    mark_chunk(pairk_of(R), R.p, R.ids, R.pst->number, R.step, R.emit, R.counts,
+               g - base[r]);
+  }
+}
+
+__global__ void __launch_bounds__(1024)
+    k_b1_pair_scan(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base) {
+  const int r = blockIdx.x;
+  const Run1D &R = runs[r];
+  const uint32_t n = base[r + 1] - base[r];
+  if (n == 0) return;
+  scan_chunks(R.counts, n, R.offs, R.capacity, R.pst, R.tot);
+}
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_b1_pair_append(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base,
+                     int nruns) {
+  const uint32_t total = base[nruns];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const int r = run_of(base, nruns, g);
+    const Run1D &R = runs[r];
+    append_chunk(pairk_of(R), R.p, R.ids, R.emit, R.offs, R.tot, g - base[r]);
   }
 }
 
@@ -193,15 +264,8 @@ __global__ void __launch_bounds__(kPairThreads)
 int enqueue_pairs(Ctx &c, float dt, uint32_t step) {
   if (!c.pstate || c.capacity == 0) return AP_OK;
   // work over the capacity: the live count is only known on the device
-  const uint32_t nchunks = (uint32_t)((c.capacity + kPairChunk - 1) / kPairChunk);
-  if (nchunks + 4 > c.pair_cap_chunks) {
-    cudaFree(c.pair_chunks);
-    c.pair_chunks = nullptr;
-    const size_t cap = (size_t)nchunks + 64;
-    if (cudaMalloc(&c.pair_chunks, sizeof(uint32_t) * (2 * cap + 8)) != cudaSuccess)
-      return AP_ERR_NOMEM;
-    c.pair_cap_chunks = cap;
-  }
+  const uint32_t nchunks = pair_chunks_of(c);
+  if (ensure_pair_scratch(c) != AP_OK) return AP_ERR_NOMEM;
   uint32_t *counts = c.pair_chunks, *offs = c.pair_chunks + c.pair_cap_chunks;
   uint32_t *tot = offs + c.pair_cap_chunks;
   PairK K;
@@ -222,6 +286,35 @@ int enqueue_pairs(Ctx &c, float dt, uint32_t step) {
   c.number_stale = true;
   if (c.mk.dim == 2) c.order_valid = false;  // appended slots are in no tile list
   return cudaGetLastError() == cudaSuccess ? AP_OK : AP_ERR_CUDA;
+}
+
+cudaError_t launch_b1_pairs(cudaStream_t s, int num_sms, const Run1D *runs,
+                            const uint32_t *base, int nruns, uint32_t total) {
+  if (total == 0) return cudaSuccess;
+  const uint32_t cap = (uint32_t)num_sms * 8;
+  const uint32_t grid = total < cap ? total : cap;
+  k_b1_pair_mark<<<grid, kPairThreads, 0, s>>>(runs, base, nruns);
+  k_b1_pair_scan<<<nruns, 1024, 0, s>>>(runs, base);
+  k_b1_pair_append<<<grid, kPairThreads, 0, s>>>(runs, base, nruns);
+  return cudaGetLastError();
+}
+
+// Pair scratch of a context (chunk counts, offsets, totals) for its
+// capacity; also used by the batched injection.
+int ensure_pair_scratch(Ctx &c) {
+  const uint32_t nchunks = (uint32_t)((c.capacity + kPairChunk - 1) / kPairChunk);
+  if (nchunks + 4 <= c.pair_cap_chunks) return AP_OK;
+  cudaFree(c.pair_chunks);
+  c.pair_chunks = nullptr;
+  const size_t cap = (size_t)nchunks + 64;
+  if (cudaMalloc(&c.pair_chunks, sizeof(uint32_t) * (2 * cap + 8)) != cudaSuccess)
+    return AP_ERR_NOMEM;
+  c.pair_cap_chunks = cap;
+  return AP_OK;
+}
+
+uint32_t pair_chunks_of(const Ctx &c) {
+  return (uint32_t)((c.capacity + kPairChunk - 1) / kPairChunk);
 }
 
 int refresh_number(Ctx *c) {

@@ -59,7 +59,7 @@ def parse():
                          "through ap_batch_* against the same runs one at a time; served: "
                          "a Poisson stream of 1D gap runs, continuous batching against "
                          "first-come-first-served one at a time")
-    ap.add_argument("--steps-scale", type=float, default=0.05,
+    ap.add_argument("--steps-scale", type=float, default=1.0,
                     help="served: run lengths are 200-5000 steps times this factor")
     ap.add_argument("--hbm-budget", type=float, default=60.0,
                     help="served: GB of device memory the resident runs may occupy")
