@@ -156,6 +156,7 @@ SIGNATURES = {
     "ap_batch_autotune": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
                                C.POINTER(_i)]),
     "ap_set_tile_shape": (_i, [_vp, _i, _i]),
+    "ap_set_compaction": (_i, [_vp, _i]),
     "ap_get_tile_shape": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
     "ap_set_pair_params": (_i, [_vp, C.POINTER(ApPairParams)]),
     "ap_get_pair_stats": (_i, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),

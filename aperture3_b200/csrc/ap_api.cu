@@ -300,6 +300,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->cell_start);
   cudaFree(c->tmp_j);
   cudaFree(c->coef);
+  cudaFree(c->compact_buf);
   cudaFree(c->pair_chunks);
   cudaFree(c->pstate);
   if (c->pstate_host) cudaFreeHost(c->pstate_host);
@@ -529,6 +530,17 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
         ph = phase_begin(c, kPhRebuild);
         AP_TRY(rebuild_tile_order(*c));
         phase_end(c, ph);
+        c->since_compact = 0;
+      }
+      c->compact_now = false;
+      if (c->compact_interval > 0 && incremental_order(*c) &&
+          ++c->since_compact >= c->compact_interval) {
+        // this update writes the store in tile order (into the scratch
+        // store, copied back after the order update)
+        AP_TRY(compact_store(*c, &P.cout, &P.cout_id));
+        P.id = c->ptc.id;
+        c->compact_now = true;
+        c->since_compact = 0;
       }
       P.t = c->tiles;
       P.order = c->order[c->cur];
@@ -555,9 +567,17 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work, bool batche
       const int nxt = c->cur ^ 1;
       ph = phase_begin(c, kPhOrder);
       AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
-      AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur], c->order[c->cur], c->dir,
+      // after a compacting push the particle at list position q sits in slot q
+      AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur],
+                                  c->compact_now ? nullptr : c->order[c->cur], c->dir,
                                   c->grp_off, c->order[nxt]));
       phase_end(c, ph);
+      if (c->compact_now) {
+        ph = phase_begin(c, kPhSort);
+        AP_TRY(compact_copy_back(*c, c->tile_start[c->cur] + c->tiles.ntiles));
+        phase_end(c, ph);
+        c->compact_now = false;
+      }
       c->cur = nxt;
     } else {
       c->order_valid = false;
@@ -889,6 +909,13 @@ AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitte
   AP_TRY_ST(refresh_number(c));
   if (emitted) *emitted = c->pstate_host->emitted;
   if (dropped) *dropped = c->pstate_host->dropped;
+  return AP_OK;
+}
+
+AP_API int ap_set_compaction(ap_ctx *c, int interval) {
+  if (!c || interval < 0) return AP_ERR_INVALID;
+  c->compact_interval = interval;
+  c->since_compact = 0;
   return AP_OK;
 }
 

@@ -97,6 +97,11 @@ struct PushDepositParams {
   DevStatus *status;
   size_t number;         // 1D: particle slots (an upper bound when d_number is set)
   const uint32_t *d_number;  // 1D: live slots kept on the device, or null
+  // 2D compaction step: every member of the particle at tile-list position
+  // q is written to slot q of this scratch store (null pointers otherwise)
+  PtcK cout;
+  uint64_t *cout_id;
+  const uint64_t *id;
   // log-spherical push / move (ap_logsph_params)
   float ls_compactness, ls_omega, ls_gravity, ls_rad_coef, ls_B0;
   int ls_rad_on;
@@ -233,6 +238,11 @@ struct Ctx {
   PairState *pstate_host = nullptr; // pinned mirror
   bool number_stale = false;        // the device count moved since the last read
   bool rho_is_zero = false;         // Rho arrays hold zeros (skip re-zeroing)
+  int compact_interval = 0;         // 2D: rewrite the store in tile order every n updates
+  int since_compact = 0;
+  void *compact_buf = nullptr;      // scratch copy of the store (48 B per slot)
+  size_t compact_cap = 0;
+  bool compact_now = false;         // this update writes the store in tile order
 
   // log-spherical grid (ap_ctx_create_logsph)
   int coord = 0;                // 0 Cartesian, 1 log-spherical
@@ -267,6 +277,11 @@ cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start,
                                  const uint32_t *grp_off, uint32_t *new_order);
 cudaError_t rebuild_tile_order(Ctx &c);
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number);
+// Compaction: the scratch store the push / deposit writes into (allocated on
+// first use), and the copy back into the caller's arrays; `live` is the
+// device-side count of written slots, the slots after it become empty.
+cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id);
+cudaError_t compact_copy_back(Ctx &c, const uint32_t *live);
 
 cudaError_t launch_fold_guards(Ctx &c, ap_array a);
 cudaError_t launch_copy_guards(Ctx &c, ap_array a);

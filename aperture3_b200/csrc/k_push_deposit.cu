@@ -100,6 +100,16 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Waits until at most N of this thread's committed groups are in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Bits needed to represent n (ceil(log2(n + 1))).
 __device__ __forceinline__ int bits_of(uint32_t n) { return 32 - __clz(n); }
 
@@ -126,6 +136,13 @@ __device__ __forceinline__ void add_fixed(const Acc32 &a, int o, float v, float 
   atomicAdd(a.lo + o, (unsigned)X & ((1u << L) - 1u));
 }
 
+// Chunks of at most 512 particles are double-buffered: the loads of the
+// next chunk run while the current one is pushed and deposited.
+template <int CH>
+constexpr bool pipelined() {
+  return CH <= 512;
+}
+
 template <int TX, int TY, int CH>
 struct TileGeom {
   static constexpr int BX = TX + 8;   // field box width: x start rounded down to 4 floats
@@ -137,8 +154,9 @@ struct TileGeom {
   static constexpr int SP = CH + CH / 64;  // staged chunk, one pad word per 64
   static constexpr int HDR = 128;     // mbarrier, tile id, abort flag, counters
   static constexpr size_t stage_bytes() { return 10 * 4 * SP + 2 * SP; }
+  static constexpr int NBUF = pipelined<CH>() ? 2 : 1;
   static size_t smem_bytes(int nrho, bool ls = false) {
-    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + stage_bytes() + (ls ? 4 * JSZ : 0);
+    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + NBUF * stage_bytes() + (ls ? 4 * JSZ : 0);
   }
 };
 
@@ -226,17 +244,9 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     int *sJhi = reinterpret_cast<int *>(sF + 6 * G::FSZ);
     unsigned *sJlo = reinterpret_cast<unsigned *>(sJhi + ncomp * G::JSZ);
     float *st = reinterpret_cast<float *>(sJlo + ncomp * G::JSZ);
-    float *s_x1 = st, *s_x2 = st + SP, *s_x3 = st + 2 * SP;
-    float *s_p1 = st + 3 * SP, *s_p2 = st + 4 * SP, *s_p3 = st + 5 * SP;
-    float *s_w = st + 6 * SP;  // weight in, gamma out
-    uint32_t *s_cell = reinterpret_cast<uint32_t *>(st + 7 * SP);
-    uint32_t *s_flag = reinterpret_cast<uint32_t *>(st + 8 * SP);
-    uint32_t *s_idx = reinterpret_cast<uint32_t *>(st + 9 * SP);
-    uint8_t *s_dir = reinterpret_cast<uint8_t *>(st + 10 * SP);
-    uint8_t *s_mode = s_dir + SP;
     // log-spherical: cell volumes over the J tile window
     float *s_dv = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(st) +
-                                            G::stage_bytes());
+                                            G::NBUF * G::stage_bytes());
     const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
     const int g0 = P.m.guard[0], g1 = P.m.guard[1];
     const int nacc = ncomp * G::JSZ;
@@ -295,29 +305,56 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     // 3. particles of this tile, CH at a time
     const uint32_t base = P.tile_start[t];
     const int n_t = (int)(P.tile_start[t + 1] - base);
-    for (int c0 = 0; c0 < n_t; c0 += CH) {
+    constexpr int kStageFloats = (int)(G::stage_bytes() / 4);
+    // 3a. coalesced asynchronous load of the chunk at c0 into buffer b
+    auto issue = [&](int c0, int b) {
+      float *sb = st + b * kStageFloats;
       const int nch = min(CH, n_t - c0);
-      // 3a. coalesced asynchronous load of the chunk
 #pragma unroll
       for (int k = 0; k < PER_THREAD; ++k) {
         const int e = tid + k * kThreads2D;
         if (e < nch) {
           const int s = spos(e);
           const uint32_t idx = P.order[base + c0 + e];
-          s_idx[s] = idx;
-          cp_async4(s_cell + s, P.p.cell + idx);
-          cp_async4(s_flag + s, P.p.flag + idx);
-          cp_async4(s_x1 + s, P.p.x1 + idx);
-          cp_async4(s_x2 + s, P.p.x2 + idx);
-          cp_async4(s_x3 + s, P.p.x3 + idx);
-          cp_async4(s_p1 + s, P.p.p1 + idx);
-          cp_async4(s_p2 + s, P.p.p2 + idx);
-          cp_async4(s_p3 + s, P.p.p3 + idx);
-          cp_async4(s_w + s, P.p.w + idx);
+          reinterpret_cast<uint32_t *>(sb + 9 * SP)[s] = idx;
+          cp_async4(sb + 7 * SP + s, P.p.cell + idx);
+          cp_async4(sb + 8 * SP + s, P.p.flag + idx);
+          cp_async4(sb + s, P.p.x1 + idx);
+          cp_async4(sb + SP + s, P.p.x2 + idx);
+          cp_async4(sb + 2 * SP + s, P.p.x3 + idx);
+          cp_async4(sb + 3 * SP + s, P.p.p1 + idx);
+          cp_async4(sb + 4 * SP + s, P.p.p2 + idx);
+          cp_async4(sb + 5 * SP + s, P.p.p3 + idx);
+          cp_async4(sb + 6 * SP + s, P.p.w + idx);
         }
       }
-      cp_async_wait_all();
+      cp_async_commit();
+    };
+    int buf = 0;
+    if (G::NBUF == 2 && n_t > 0) issue(0, 0);
+    for (int c0 = 0; c0 < n_t; c0 += CH) {
+      const int nch = min(CH, n_t - c0);
+      if (G::NBUF == 2) {
+        if (c0 + CH < n_t) {
+          issue(c0 + CH, buf ^ 1);
+          cp_async_wait_group<1>();
+        } else {
+          cp_async_wait_group<0>();
+        }
+      } else {
+        issue(c0, 0);
+        cp_async_wait_group<0>();
+      }
       __syncthreads();
+      float *stc = st + buf * kStageFloats;
+      float *s_x1 = stc, *s_x2 = stc + SP, *s_x3 = stc + 2 * SP;
+      float *s_p1 = stc + 3 * SP, *s_p2 = stc + 4 * SP, *s_p3 = stc + 5 * SP;
+      float *s_w = stc + 6 * SP;  // weight in, gamma out
+      uint32_t *s_cell = reinterpret_cast<uint32_t *>(stc + 7 * SP);
+      uint32_t *s_flag = reinterpret_cast<uint32_t *>(stc + 8 * SP);
+      uint32_t *s_idx = reinterpret_cast<uint32_t *>(stc + 9 * SP);
+      uint8_t *s_dir = reinterpret_cast<uint8_t *>(stc + 10 * SP);
+      uint8_t *s_mode = s_dir + SP;
       // 3b. push + deposit: lane l of warp w takes element l*CH/32 + w*PER_THREAD + k
       for (int k = 0; k < PER_THREAD; ++k) {
         const int e = lane * (CH / 32) + warp * PER_THREAD + k;
@@ -556,6 +593,23 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
           const int s = spos(e);
           const uint8_t mode = s_mode[s];
           const uint32_t idx = s_idx[s];
+          if (P.cout.x1) {
+            // compaction: every member to its tile-list position
+            const size_t q = base + c0 + e;
+            P.cout.x1[q] = s_x1[s];
+            P.cout.x2[q] = s_x2[s];
+            P.cout.x3[q] = s_x3[s];
+            P.cout.p1[q] = s_p1[s];
+            P.cout.p2[q] = s_p2[s];
+            P.cout.p3[q] = s_p3[s];
+            P.cout.E[q] = (mode & kWriteMom) ? s_w[s] : P.p.E[idx];
+            P.cout.w[q] = P.p.w[idx];
+            P.cout.cell[q] = s_cell[s];
+            P.cout.flag[q] = s_flag[s];
+            P.cout_id[q] = P.id[idx];
+            P.dir[base + c0 + e] = s_dir[s];
+            continue;
+          }
           if (mode & kWritePos) {
             P.p.x1[idx] = s_x1[s];
             P.p.x2[idx] = s_x2[s];
@@ -573,6 +627,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
         }
       }
       __syncthreads();
+      if (G::NBUF == 2) buf ^= 1;
     }
 
     // 4. flush the current (and charge) tile once
@@ -864,6 +919,7 @@ cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
   // for the transcendental move)
   if (c.coord == 1) return launch_2d_tiles<TX, TY, 1024, 2, true>(c, P);
   if (c.params.chunk == 2048) return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
+  if (c.params.chunk == 512) return launch_2d_tiles<TX, TY, 512, 3>(c, P);
   return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
 }
 

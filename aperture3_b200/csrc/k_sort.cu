@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kScatterThreads)
       }
       if (dst != 0xffffffffu) {
         if (dst < capacity)
-          new_order[dst] = old_order[p];
+          new_order[dst] = old_order ? old_order[p] : p;  // no old order: slot = position
         else
           atomicAdd(&status->tile_faults, 1ull);
       }
@@ -411,6 +411,71 @@ int ensure_scratch(Ctx &c, size_t n) {
   if (cudaMalloc(&c.gather_tmp, cap * sizeof(uint64_t)) != cudaSuccess) return AP_ERR_NOMEM;
   c.scratch_cap = cap;
   return AP_OK;
+}
+
+// After a compaction: the slots after the live ones are empty.
+__global__ void k_compact_tail(const uint32_t *live, uint32_t *cell, size_t n) {
+  const uint32_t m = *live;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (i >= m) cell[i] = AP_MAX_CELL;
+}
+
+namespace {
+
+ap_particles store_layout(void *buf, size_t cap) {
+  unsigned char *b = static_cast<unsigned char *>(buf);
+  ap_particles s;
+  s.id = reinterpret_cast<uint64_t *>(b);
+  s.x1 = reinterpret_cast<float *>(b + 8 * cap);
+  s.x2 = s.x1 + cap;
+  s.x3 = s.x2 + cap;
+  s.p1 = s.x3 + cap;
+  s.p2 = s.p1 + cap;
+  s.p3 = s.p2 + cap;
+  s.E = s.p3 + cap;
+  s.weight = s.E + cap;
+  s.cell = reinterpret_cast<uint32_t *>(s.weight + cap);
+  s.flag = s.cell + cap;
+  return s;
+}
+
+}  // namespace
+
+cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id) {
+  const size_t n = c.capacity > c.number ? c.capacity : c.number;
+  if (!c.compact_buf || c.compact_cap < n) {
+    cudaFree(c.compact_buf);
+    c.compact_buf = nullptr;
+    cudaError_t e = cudaMalloc(&c.compact_buf, n * 48);
+    if (e != cudaSuccess) return e;
+    c.compact_cap = n;
+  }
+  const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
+  *out = PtcK{s.x1, s.x2, s.x3, s.p1, s.p2, s.p3, s.E, s.weight, s.cell, s.flag};
+  *out_id = s.id;
+  return cudaSuccess;
+}
+
+cudaError_t compact_copy_back(Ctx &c, const uint32_t *live) {
+  const size_t n = c.number;
+  if (n == 0) return cudaSuccess;
+  const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
+  const struct {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  } back[11] = {{c.ptc.x1, s.x1, 4}, {c.ptc.x2, s.x2, 4},         {c.ptc.x3, s.x3, 4},
+                {c.ptc.p1, s.p1, 4}, {c.ptc.p2, s.p2, 4},         {c.ptc.p3, s.p3, 4},
+                {c.ptc.E, s.E, 4},   {c.ptc.weight, s.weight, 4}, {c.ptc.cell, s.cell, 4},
+                {c.ptc.id, s.id, 8}, {c.ptc.flag, s.flag, 4}};
+  for (const auto &m : back) {
+    cudaError_t e = cudaMemcpyAsync(m.dst, m.src, n * m.bytes, cudaMemcpyDeviceToDevice, c.stream);
+    if (e != cudaSuccess) return e;
+  }
+  k_compact_tail<<<grid_for(c, n, 256), 256, 0, c.stream>>>(live, c.ptc.cell, n);
+  c.launches++;
+  return cudaGetLastError();
 }
 
 // Builds the tile order from scratch: stable sort of slots [0, number) by

@@ -151,6 +151,78 @@ def box2d(seed: int = 0, N: int = 1024, ppc: int = 64, gamma_max: float = 1e3,
     return params, fields, ptc
 
 
+def logsph(seed: int = 0, N: int = 1024, ppc: int = 32, rmax: float = 50.0,
+           scale_height: float = 0.5, gamma_max: float = 1e6, omega: float = 0.1,
+           B0: float = 1.0, device="cpu"):
+    """Config: 2D log-spherical grid, x1 = ln r in [0, ln rmax], x2 = theta in
+    [0, pi], N x N cells, guard 2. Dipole background B_r = 2 B0 cos(theta) /
+    r^3, B_theta = B0 sin(theta) / r^3 (labs/pulsar/src/main.cpp:49-58) and
+    the corotation field E = -(Omega x r) x B, each on its Yee stagger; B and
+    E start equal to their backgrounds. Pairs per cell drawn from a Poisson
+    law of mean ppc / 2 * exp(-(r - 1) / scale_height) at the cell centre;
+    momenta along the local B direction (random sign) with gamma
+    log-uniform in [1, gamma_max]; dt = 0.4 * min(delta). Returns (params,
+    fields, particles); params.coord_system is "LogSpherical"."""
+    from .sim import SimParams
+    guard = 2
+    d0 = float(np.float32(np.float32(math.log(rmax)) / np.float32(N)))
+    d1 = float(np.float32(np.float32(math.pi) / np.float32(N)))
+    params = SimParams(N=(N, N, 1), guard=(guard, guard, 0), lower=(0.0, 0.0, 0.0),
+                       size=(float(np.float32(math.log(rmax))), float(np.float32(math.pi)), 1.0),
+                       delta_t=float(np.float32(0.4 * min(d0, d1))), q_e=1.0, num_species=2,
+                       periodic_boundary=(False, False, False), data_interval=100, B0=B0,
+                       coord_system="LogSpherical", compactness=0.0, omega=omega,
+                       damping_length=32)
+    g = _gen(seed, device)
+    dims = N + 2 * guard
+    n_idx = torch.arange(dims, device=device)
+    stag = [(0, 1), (1, 0), (1, 1), (1, 0), (0, 1), (0, 0)]  # E1..E3, B1..B3 (x, y)
+
+    def pos(d, n, s, delta):
+        return delta * (n.double() - guard + (1.0 if s else 0.5))
+    comps = []
+    for k in range(6):
+        r = torch.exp(pos(0, n_idx, stag[k][0], d0))[None, :]
+        th = pos(1, n_idx, stag[k][1], d1)[:, None]
+        br = 2.0 * B0 * torch.cos(th) / r ** 3
+        bt = B0 * torch.sin(th) / r ** 3
+        if k >= 3:
+            val = [br, bt, torch.zeros_like(br)][k - 3]
+        else:
+            v = omega * r * torch.sin(th)
+            val = [v * bt, -v * br, torch.zeros_like(br)][k]
+        comps.append(val.float().contiguous())
+    # particles
+    rc = torch.exp(pos(0, n_idx[guard:guard + N], 0, d0))
+    lam = (ppc / 2.0) * torch.exp(-(rc - 1.0) / scale_height)
+    lam2 = lam[None, :].expand(N, N).contiguous()
+    npc = torch.poisson(lam2.double(), generator=g).long().reshape(-1)
+    cx = torch.arange(N, device=device) + guard
+    cells = (cx[None, :] + cx[:, None] * dims).reshape(-1).repeat_interleave(npc)
+    c1 = cells % dims
+    c2 = cells // dims
+    th = pos(1, c2, 0, d1)
+    rr = torch.exp(pos(0, c1, 0, d0))
+    br = 2.0 * torch.cos(th) / rr ** 3
+    bt = torch.sin(th) / rr ** 3
+    bn = torch.sqrt(br * br + bt * bt)
+
+    def sampler(n):
+        u = torch.rand(n // 2, generator=g, device=device, dtype=torch.float64)
+        gam = torch.exp(u * math.log(gamma_max))
+        pm = torch.sqrt(torch.clamp(gam * gam - 1.0, min=0.0))
+        sgn = torch.where(torch.rand(n // 2, generator=g, device=device) < 0.5, -1.0, 1.0)
+        pm = (pm * sgn).repeat_interleave(2)
+        return torch.stack([pm * br.repeat_interleave(2) / bn.repeat_interleave(2),
+                            pm * bt.repeat_interleave(2) / bn.repeat_interleave(2),
+                            torch.zeros_like(pm)])
+    ptc = _pairs(cells, g, device, sampler)
+    params.max_ptc_number = int(ptc["x1"].numel())
+    fields = {"E": comps[:3], "B": comps[3:], "Ebg": [c.clone() for c in comps[:3]],
+              "Bbg": [c.clone() for c in comps[3:]]}
+    return params, fields, ptc
+
+
 def to_numpy_ptc(ptc: Dict[str, torch.Tensor]) -> Dict[str, np.ndarray]:
     out = {}
     for k, v in ptc.items():

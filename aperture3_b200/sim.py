@@ -192,6 +192,11 @@ class SimEnvironment:
                                int(bool(enabled)), int(seed), int(first_id))
         check(self._lib.ap_set_pair_params(self.ctx, C.byref(pp)), "ap_set_pair_params")
 
+    def set_compaction(self, interval: int):
+        """Rewrite the 2D particle store in tile order every `interval`
+        updates (0: never). Particles change slots, not values."""
+        check(self._lib.ap_set_compaction(self.ctx, int(interval)), "ap_set_compaction")
+
     def logsph_coef(self, which: int) -> np.ndarray:
         """Host copy of one Grid_LogSph coefficient array (grid_log_sph.h:45-47),
         shape (dims[1], dims[0])."""

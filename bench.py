@@ -50,15 +50,20 @@ def parse():
     ap.add_argument("--tile", type=int, nargs=2, default=(16, 16))
     ap.add_argument("--sort-interval", type=int, default=20)
     ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--compact", type=int, default=4,
+                    help="rewrite the particle store in tile order every n steps (0: never); "
+                         "particles keep their values, only their slots change")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
-    ap.add_argument("--workload", default="box", choices=["box", "batched", "served"],
+    ap.add_argument("--workload", default="box",
+                    choices=["box", "batched", "served", "logsph"],
                     help="box: the 2D box (headline line); batched: many uneven boxes "
                          "through ap_batch_* against the same runs one at a time; served: "
                          "a Poisson stream of 1D gap runs, continuous batching against "
-                         "first-come-first-served one at a time")
+                         "first-come-first-served one at a time; logsph: the log-spherical "
+                         "1024x1024 grid (ptc_updater_logsph + field_solver_logsph)")
     ap.add_argument("--steps-scale", type=float, default=1.0,
                     help="served: run lengths are 200-5000 steps times this factor")
     ap.add_argument("--hbm-budget", type=float, default=60.0,
@@ -79,6 +84,7 @@ def workload_config(args, tile):
                      f"{args.sort_interval} steps"),
         "grid": [args.N, args.N], "ppc": args.ppc, "particles": n,
         "tile": list(tile), "sort_interval": args.sort_interval,
+        "compaction_interval": args.compact,
         "l2": "inputs larger than L2 (particle SoA 48 B x N_p)",
     }
 
@@ -309,6 +315,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream()
     env.set_stream(stream)
     env.set_sync(False)
+    env.set_compaction(args.compact)
     pusher, solver = ptc_updater(env), field_solver(env)
     dt = params.delta_t
     lib = env._lib
@@ -516,6 +523,81 @@ def run_batched(args):
         env.close()
 
 
+def run_logsph(args):
+    """Log-spherical grid 1024 x 1024, r in [1, 50], dipole B with corotation
+    E, 32 particles per cell scaled by exp(-(r - 1) / 0.5), gamma up to 1e6
+    along B (aperture3_b200.ic.logsph). A step is the pulsar lab's loop body:
+    ptc_updater_logsph::update_particles, field_solver_logsph::update_fields
+    and apply_boundary, sort every sort_interval steps. Device time (CUDA
+    events) over `steps` steps after `warmup`."""
+    import torch
+    from aperture3_b200 import (SimData, SimEnvironment, field_solver_logsph, ic,
+                                ptc_updater_logsph)
+    from aperture3_b200._lib import ApPhaseTimes, check
+
+    dev = torch.device("cuda", 0)
+    params, fields, ptc = ic.logsph(seed=11, N=args.N, ppc=32, device=dev)
+    n = ptc["x1"].numel()
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=n)
+    data.set_fields_device(fields)
+    data.set_particles_device(ptc)
+    del ptc
+    stream = torch.cuda.Stream()
+    env.set_stream(stream)
+    env.set_sync(False)
+    pusher, solver = ptc_updater_logsph(env), field_solver_logsph(env)
+    dt = params.delta_t
+    lib = env._lib
+
+    def one_step(s):
+        pusher.update_particles(data, dt, s)
+        solver.update_fields(data, dt, s * dt)
+        solver.apply_boundary(data, params.omega, s * dt)
+        if s % args.sort_interval == 0 and s != 0:
+            data.sort_particles()
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for s in range(args.warmup):
+            one_step(s)
+        env.sync()
+        check(lib.ap_set_profiling(env.ctx, 1), "profiling")
+        check(lib.ap_get_phase_times(env.ctx, ApPhaseTimes(), 1), "reset")
+        n0 = data.number
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(args.warmup, args.warmup + args.steps):
+            one_step(s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        env.sync()
+    ms = e0.elapsed_time(e1)
+    pt = ApPhaseTimes()
+    check(lib.ap_get_phase_times(env.ctx, pt, 1), "phase times")
+    data.refresh_number()
+    live = (n0 + data.number) / 2
+    line = {
+        "metric": "particle-steps/s (log-spherical push+move+deposit)",
+        "value": live * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded, aperture3_b200.ic.logsph)",
+        "config": {"workload": f"log-spherical {args.N}x{args.N}, r in [1,50], dipole B, "
+                               "32 ppc x exp(-(r-1)/0.5), gamma up to 1e6 along B",
+                   "particles_start": n0, "particles_end": data.number},
+        "phases_ms_per_step": {"push_deposit": pt.push_deposit_ms / args.steps,
+                               "tile_sort": pt.order_ms / args.steps,
+                               "rebuild": pt.rebuild_ms / args.steps,
+                               "finalize": pt.finalize_ms / args.steps,
+                               "fields": pt.fields_ms / args.steps,
+                               "sort_by_cell": pt.sort_ms / args.steps},
+    }
+    print(json.dumps(line), flush=True)
+    env.close()
+
+
 def run_served(args):
     """Served stream of 1D gap runs: `runs` requests with Poisson arrivals
     (50/s), 512-16384 cells, 32-256 particles per cell, 200-5000 steps
@@ -622,9 +704,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.workload in ("batched", "served"):
+        if args.workload in ("batched", "served", "logsph"):
             if rank == 0:
-                (run_batched if args.workload == "batched" else run_served)(args)
+                {"batched": run_batched, "served": run_served,
+                 "logsph": run_logsph}[args.workload](args)
             return
         run_ours(args, rank, world, local_rank)
     finally:

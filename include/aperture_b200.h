@@ -74,7 +74,7 @@ typedef struct {
   float masses[AP_MAX_SPECIES];
   int tile[2];               /* sort tile in cells; 0 picks a default       */
   int chunk;                 /* particles staged per pass in the 2D kernel:
-                                1024 or 2048; 0 picks a default             */
+                                512, 1024 or 2048; 0 picks a default        */
 } ap_params;
 
 typedef struct {
@@ -178,6 +178,15 @@ AP_API int ap_compute_divs(ap_ctx *ctx);
  * 9-127): periodic copy / fold of the guard strips. */
 AP_API int ap_send_guard_cells(ap_ctx *ctx, ap_array a);
 AP_API int ap_send_add_guard_cells(ap_ctx *ctx, ap_array a);
+
+/* 2D: every `interval` updates (0 = never, the default), rewrite the
+ * particle arrays in tile order before the push, so that each tile's
+ * particles sit in consecutive slots again (new; between sorts the
+ * reference keeps every particle in its slot). Particles change slots, not
+ * values; slots after the live ones become empty (cell == AP_MAX_CELL).
+ * This bounds the scatter of the particle accesses that grows as particles
+ * cross tiles. */
+AP_API int ap_set_compaction(ap_ctx *ctx, int interval);
 
 /* sim_data::sort_particles -> particle_base::sort_by_cell
  * (sim_data_impl.hpp:78-89, cuda/core/particle_base_impl.cu:435-487):
