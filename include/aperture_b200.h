@@ -74,7 +74,7 @@ typedef struct {
   float masses[AP_MAX_SPECIES];
   int tile[2];               /* sort tile in cells; 0 picks a default       */
   int chunk;                 /* particles staged per pass in the 2D kernel:
-                                512, 1024 or 2048; 0 picks a default        */
+                                256, 512, 1024 or 2048; 0 picks a default   */
 } ap_params;
 
 typedef struct {

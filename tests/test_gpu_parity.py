@@ -46,7 +46,7 @@ def test_2d_push_deposit_bitexact(tile):
         pr.check_current(J_TOL, rho=True)
 
 
-@pytest.mark.parametrize("chunk", [512, 2048])
+@pytest.mark.parametrize("chunk", [256, 1024, 2048])
 def test_2d_push_deposit_bitexact_chunks(chunk):
     """The staged-chunk variants (512 double-buffered, 2048) give the same
     bits; tiles of 16 x 16 with 64 particles per cell need several chunks."""
