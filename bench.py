@@ -185,9 +185,11 @@ def cpu_threads():
 
 
 class CpuBox:
-    """The same step on the host: the reference's own push/deposit/FDTD
-    kernels compiled for the host (oracle/_ref) when present, else the C
-    restatement (oracle/liboracle.so), with all host threads."""
+    """The same step on the host, on all host threads: the reference's own
+    push and deposit kernels compiled for the host (oracle/_ref/
+    libapref_mt.so, kind "reference") when that library was built, else
+    the C restatement (oracle/liboracle.so, kind "port"); the guard fold,
+    wrap, FDTD and sort are the restatement's in both cases."""
 
     def __init__(self, params, fields_np, ptc_np, threads):
         import numpy as np
@@ -207,12 +209,24 @@ class CpuBox:
         self.charges = [-q] + [q] * 7
         self.masses = [q] * 8
         self.periodic = [1, 1, 0]
-        self.kind = "port"
+        self.ref = oracle.load_ref_mt(build=False) is not None
+        self.kind = "reference" if self.ref else "port"
+
+    def describe(self):
+        if self.ref:
+            return ("the reference's push and deposit kernels compiled for the host "
+                    "(oracle/_ref), restated guard fold, wrap, FDTD and sort")
+        return "C restatement of the reference (oracle/liboracle.so)"
 
     def step(self, step):
-        self.o.update_particles(self.m, self.p, self.n, self.f, self.params.delta_t, step,
-                                self.params.data_interval, 2, 0, self.charges, self.masses,
-                                self.periodic, self.threads)
+        if self.ref:
+            self.o.ref_update_particles_mt(self.m, self.p, self.n, self.f, self.params.delta_t,
+                                           step, self.params.data_interval, 2, self.charges,
+                                           self.masses, self.periodic, self.threads)
+        else:
+            self.o.update_particles(self.m, self.p, self.n, self.f, self.params.delta_t, step,
+                                    self.params.data_interval, 2, 0, self.charges, self.masses,
+                                    self.periodic, self.threads)
         self.o.update_fields(self.m, self.f, self.params.delta_t, step, self.periodic)
         if step % 20 == 0 and step != 0:
             self.n = self.o.sort_by_cell(self.m, self.p, self.n)
@@ -250,7 +264,7 @@ def time_cpu(args, budget_s, min_steps=1, max_steps=None):
     el = time.perf_counter() - t
     rate = box.n * nsteps / el
     desc = (f"{args.N}x{args.N} grid, {ppc} ppc ({box.n} particles), {nsteps} step(s) after "
-            f"1 warm-up, {threads} threads ({box.kind})")
+            f"1 warm-up, {threads} threads, {box.describe()}")
     return rate, threads, desc, box.kind
 
 
@@ -277,7 +291,7 @@ def run_reference(args, rank):
     el = time.perf_counter() - t
     value = box.n * args.steps / el
     sample = (f"{args.N}x{args.N} grid, {ppc} ppc ({box.n} particles) of the {args.ppc}-ppc "
-              f"workload, {args.steps} timed steps")
+              f"workload, {args.steps} timed steps, {box.describe()}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,

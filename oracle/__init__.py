@@ -402,3 +402,61 @@ def ref_compute_divs(m, f):
 
 def ref_filter(m, j, tmp, bnd):
     load_ref().ref_filter(C.byref(m), _p(j), _p(tmp), _fa(bnd, C.c_int, 4))
+
+
+# ---------------------------------------------------------------------------
+# The reference's own push / deposit kernels on all host threads (timing
+# build, oracle/_ref/libapref_mt.so): the CPU baseline of the benchmark.
+
+_REF_MT_PATH = os.path.join(_HERE, "_ref", "libapref_mt.so")
+ref_mt = None
+
+
+def load_ref_mt(build=True):
+    """Load (building if the reference tree is present) the threaded
+    reference library, or None when it is not available."""
+    global ref_mt
+    if ref_mt is not None:
+        return ref_mt
+    if not os.path.exists(_REF_MT_PATH) and build and os.path.isdir("/root/reference/src"):
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_mt.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_MT_PATH):
+        return None
+    r = C.CDLL(_REF_MT_PATH)
+    r.ref_push_mt.restype = None
+    r.ref_push_mt.argtypes = [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, C.c_int]
+    r.ref_deposit_mt.restype = None
+    r.ref_deposit_mt.argtypes = [_vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int, _vp, _vp,
+                                 C.c_int, _vp, C.c_int]
+    ref_mt = r
+    return ref_mt
+
+
+def ref_update_particles_mt(m, p, num, f, dt, step, data_interval, num_species, charges,
+                            masses, periodic, nthreads):
+    """ptc_updater::update_particles (ptc_updater.cu:748-841) with the
+    reference's push and deposit kernels (ptc_updater.cu:78-141, 295-386)
+    on nthreads host threads, then the guard fold and in-place wrap of this
+    module (sim_environment_impl.hpp:274-448)."""
+    r = load_ref_mt()
+    for c in range(3):
+        f["J"][c][:] = 0
+    for s in range(num_species):
+        f["Rho"][s][:] = 0
+    if num:
+        s = ptc_struct(p)
+        F = [f["E"][0], f["E"][1], f["E"][2], f["B"][0], f["B"][1], f["B"][2]]
+        r.ref_push_mt(C.byref(m), C.byref(s), num, np.float32(dt), _arr(F, 6), _fa(charges),
+                      _fa(masses), nthreads)
+        r.ref_deposit_mt(C.byref(m), C.byref(s), num, np.float32(dt), step, data_interval,
+                         _arr(f["J"], 3), _arr(f["Rho"][:num_species], 8), num_species,
+                         _fa(charges), nthreads)
+    for c in range(3):
+        send_add_guard_cells(m, f["J"][c], periodic)
+    if (step + 1) % data_interval == 0:
+        for s in range(num_species):
+            send_add_guard_cells(m, f["Rho"][s], periodic)
+    return wrap_particles(m, p, num, periodic)

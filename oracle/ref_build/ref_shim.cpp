@@ -21,7 +21,13 @@
 #include "cuda/algorithms/ptc_updater_helper.cuh"
 #include "cuda/algorithms/vay_push.cuh"
 
+#ifdef AP_REF_MT
+#include <omp.h>
+#include <stdlib.h>
+thread_local ap_ref_dim3 blockIdx, blockDim, threadIdx, gridDim;
+#else
 ap_ref_dim3 blockIdx, blockDim, threadIdx, gridDim;
+#endif
 
 namespace Aperture {
 Quadmesh dev_mesh;
@@ -212,5 +218,83 @@ void ref_filter(const ref_mesh *m, float *j, float *tmp, const int bnd[4]) {
   size_t n = (size_t)m->dims[0] * m->dims[1] * m->dims[2];
   for (size_t i = 0; i < n; i++) j[i] = tmp[i];
 }
+
+#ifdef AP_REF_MT
+/* Timing build (libapref_mt.so): the same kernels on all host threads.
+ * Each thread runs the push and the deposit as a one-thread launch over a
+ * contiguous slice of the particles; the deposit of each thread goes to a
+ * private current / charge buffer (the kernels' atomicAdd is a plain add)
+ * and the buffers are summed in thread order afterwards. */
+static ref_ptc slice(const ref_ptc *p, size_t lo) {
+  ref_ptc s = *p;
+  s.x1 += lo; s.x2 += lo; s.x3 += lo;
+  s.p1 += lo; s.p2 += lo; s.p3 += lo;
+  s.E += lo; s.weight += lo; s.cell += lo; s.id += lo; s.flag += lo;
+  return s;
+}
+
+void ref_push_mt(const ref_mesh *m, const ref_ptc *p, size_t num, float dt,
+                 float *const F[6], const float charges[8], const float masses[8],
+                 int nthreads) {
+  /* the mesh and charges are process globals, set before the threads start */
+  set_mesh(m);
+  for (int i = 0; i < 8; i++) { dev_charges[i] = charges[i]; dev_masses[i] = masses[i]; }
+#pragma omp parallel num_threads(nthreads)
+  {
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+    const size_t lo = num * (size_t)t / nt, hi = num * (size_t)(t + 1) / nt;
+    const ref_ptc s = slice(p, lo);
+    data_ptrs d;
+    d.E1 = pp(F[0], m); d.E2 = pp(F[1], m); d.E3 = pp(F[2], m);
+    d.B1 = pp(F[3], m); d.B2 = pp(F[4], m); d.B3 = pp(F[5], m);
+    d.particles = to_pd(&s);
+    one_thread();
+    if (dev_mesh.dim() == 1)
+      Kernels::ptc_push_cart_1d(d, hi - lo, dt);
+    else
+      Kernels::ptc_push_cart_2d(d, hi - lo, dt);
+  }
+}
+
+void ref_deposit_mt(const ref_mesh *m, const ref_ptc *p, size_t num, float dt,
+                    uint32_t step, int data_interval, float *const J[3],
+                    float *const Rho[8], int num_species, const float charges[8],
+                    int nthreads) {
+  set_mesh(m);
+  dev_params.data_interval = data_interval;
+  for (int i = 0; i < 8; i++) dev_charges[i] = charges[i];
+  const size_t ncell = (size_t)m->dims[0] * m->dims[1] * m->dims[2];
+  const int ncomp = 3 + num_species;
+  float *priv = (float *)calloc((size_t)nthreads * ncomp * ncell, sizeof(float));
+  if (!priv) return;
+#pragma omp parallel num_threads(nthreads)
+  {
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+    const size_t lo = num * (size_t)t / nt, hi = num * (size_t)(t + 1) / nt;
+    const ref_ptc s = slice(p, lo);
+    float *base = priv + (size_t)t * ncomp * ncell;
+    data_ptrs d;
+    d.J1 = pp(base, m); d.J2 = pp(base + ncell, m); d.J3 = pp(base + 2 * ncell, m);
+    pitchptr<Scalar> rho[8];
+    for (int sp = 0; sp < num_species; sp++) rho[sp] = pp(base + (3 + sp) * ncell, m);
+    d.Rho = rho;
+    d.particles = to_pd(&s);
+    one_thread();
+    if (dev_mesh.dim() == 1)
+      Kernels::deposit_current_cart_1d(d, hi - lo, dt, step);
+    else
+      Kernels::deposit_current_cart_2d(d, hi - lo, dt, step);
+  }
+  for (int t = 0; t < nthreads; t++) {
+    const float *base = priv + (size_t)t * ncomp * ncell;
+#pragma omp parallel for num_threads(nthreads)
+    for (size_t i = 0; i < ncell; i++) {
+      for (int c = 0; c < 3; c++) J[c][i] += base[c * ncell + i];
+      for (int sp = 0; sp < num_species; sp++) Rho[sp][i] += base[(3 + sp) * ncell + i];
+    }
+  }
+  free(priv);
+}
+#endif
 
 }  // extern "C"

@@ -13,7 +13,12 @@ using std::max;
 using std::min;
 
 struct ap_ref_dim3 { unsigned x, y, z; };
+#ifdef AP_REF_MT
+/* multi-threaded timing build: every host thread emulates its own launch */
+extern thread_local ap_ref_dim3 blockIdx, blockDim, threadIdx, gridDim;
+#else
 extern ap_ref_dim3 blockIdx, blockDim, threadIdx, gridDim;
+#endif
 
 #define __global__
 #define __device__

@@ -160,3 +160,30 @@ def test_oracle_matches_golden(path):
         _same(f["B"][k], z[f"fs_B{k}"], f"B{k + 1}")
     _same(f["divE"], z["fs_divE"], "divE")
     _same(f["divB"], z["fs_divB"], "divB")
+
+
+REF_MT = oracle.load_ref_mt(build=True)
+
+
+@pytest.mark.skipif(REF_MT is None, reason="threaded reference library not built")
+@pytest.mark.parametrize("nthreads", [1, 3])
+def test_threaded_reference_update_matches_oracle(nthreads):
+    """The CPU baseline (the reference's kernels on several host threads)
+    computes what the oracle computes with the same particle split: the
+    same particles bit for bit, and the same current (both sum per-thread
+    buffers in thread order)."""
+    m, f, p = _case("2d", (64, 32), 5, n=6000)
+    f["Rho"] = [np.zeros_like(f["J"][0]) for _ in range(2)]
+    fo, fr = oracle.copy_fields(f), oracle.copy_fields(f)
+    po, pr = oracle.copy_ptc(p), oracle.copy_ptc(p)
+    dt = np.float32(0.5 * m.delta[0])
+    n = len(p["x1"])
+    oracle.update_particles(m, po, n, fo, dt, 3, 1, 2, 0, CHARGES, MASSES, [1, 1, 0], nthreads)
+    oracle.ref_update_particles_mt(m, pr, n, fr, dt, 3, 1, 2, CHARGES, MASSES, [1, 1, 0],
+                                   nthreads)
+    for k in po:
+        _same(pr[k], po[k], f"particles.{k}")
+    for c in range(3):
+        _same(fr["J"][c], fo["J"][c], f"J{c + 1}")
+    for s in range(2):
+        _same(fr["Rho"][s], fo["Rho"][s], f"Rho{s}")
