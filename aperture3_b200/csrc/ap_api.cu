@@ -379,6 +379,7 @@ AP_API int ap_bind_particles(ap_ctx *c, const ap_particles *p, size_t number, si
     return fail(c, AP_ERR_INVALID);
   c->ptc = *p;
   c->number = number;
+  c->store_base = 0;
   c->capacity = capacity;
   c->ptc_bound = true;
   c->order_valid = false;
@@ -392,6 +393,7 @@ AP_API int ap_particles_modified(ap_ctx *c, size_t number) {
   if (!c || !c->ptc_bound) return AP_ERR_INVALID;
   if (number > c->capacity) return fail(c, AP_ERR_CAPACITY);
   c->number = number;
+  c->store_base = 0;
   c->order_valid = false;
   c->scale_valid = false;
   AP_TRY_ST(push_number(c));
@@ -402,6 +404,14 @@ AP_API int ap_get_number(const ap_ctx *c, size_t *n) {
   if (!c || !n) return AP_ERR_INVALID;
   if (refresh_number(const_cast<ap_ctx *>(c)) != AP_OK) return AP_ERR_CUDA;
   *n = c->number;
+  return AP_OK;
+}
+
+AP_API int ap_get_slot_range(const ap_ctx *c, size_t *first, size_t *end) {
+  if (!c || !first || !end) return AP_ERR_INVALID;
+  if (refresh_number(const_cast<ap_ctx *>(c)) != AP_OK) return AP_ERR_CUDA;
+  *first = c->store_base;
+  *end = c->number;
   return AP_OK;
 }
 
@@ -567,16 +577,18 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work, bool batche
       const int nxt = c->cur ^ 1;
       ph = phase_begin(c, kPhOrder);
       AP_TRY(launch_tile_scan(*c, c->dir_count, c->tile_start[nxt], c->grp_off));
-      // after a compacting push the particle at list position q sits in slot q
+      // after a compacting push the particle at list position q sits in
+      // slot compact_dst + q
       AP_TRY(launch_order_scatter(*c, c->tile_start[c->cur],
                                   c->compact_now ? nullptr : c->order[c->cur], c->dir,
-                                  c->grp_off, c->order[nxt]));
+                                  c->grp_off, c->order[nxt], (uint32_t)c->compact_dst));
       phase_end(c, ph);
       if (c->compact_now) {
         ph = phase_begin(c, kPhSort);
-        AP_TRY(compact_copy_back(*c, c->tile_start[c->cur] + c->tiles.ntiles));
+        AP_TRY(compact_finish(*c, c->tile_start[c->cur] + c->tiles.ntiles));
         phase_end(c, ph);
         c->compact_now = false;
+        c->compact_dst = 0;
       }
       c->cur = nxt;
     } else {
@@ -742,6 +754,7 @@ AP_API int ap_sort_by_cell(ap_ctx *c) {
   phase_end(c, ph);
   if (!device_count) {
     c->number = n;
+    c->store_base = 0;
     AP_TRY_ST(push_number(c));
   }
   return AP_OK;

@@ -243,6 +243,9 @@ struct Ctx {
   void *compact_buf = nullptr;      // scratch copy of the store (48 B per slot)
   size_t compact_cap = 0;
   bool compact_now = false;         // this update writes the store in tile order
+  size_t store_base = 0;            // lowest slot that may hold a particle
+  size_t compact_dst = 0;           // first slot of this compaction's output
+  bool compact_direct = false;      // output in the caller's free half, no copy back
 
   // log-spherical grid (ap_ctx_create_logsph)
   int coord = 0;                // 0 Cartesian, 1 log-spherical
@@ -272,16 +275,18 @@ cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P);
 cudaError_t launch_push_deposit_1d(Ctx &c, const PushDepositParams &P);
 cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count,
                              uint32_t *new_start, uint32_t *grp_off);
+// old_order null: the particle at list position p sits in slot slot0 + p.
 cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start,
                                  const uint32_t *old_order, const uint8_t *dir,
-                                 const uint32_t *grp_off, uint32_t *new_order);
+                                 const uint32_t *grp_off, uint32_t *new_order,
+                                 uint32_t slot0 = 0);
 cudaError_t rebuild_tile_order(Ctx &c);
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number);
 // Compaction: the scratch store the push / deposit writes into (allocated on
 // first use), and the copy back into the caller's arrays; `live` is the
 // device-side count of written slots, the slots after it become empty.
 cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id);
-cudaError_t compact_copy_back(Ctx &c, const uint32_t *live);
+cudaError_t compact_finish(Ctx &c, const uint32_t *live);
 
 cudaError_t launch_fold_guards(Ctx &c, ap_array a);
 cudaError_t launch_copy_guards(Ctx &c, ap_array a);

@@ -116,16 +116,21 @@ __global__ void k_tile_groups(TileTopo T, const uint32_t *__restrict__ cnt,
 
 // One CTA per source tile: stable rank within each direction group. The
 // tile's list is cut into one contiguous segment per warp; pass 1 counts the
-// directions of each segment with warp ballots, one barrier turns the counts
-// into per-warp offsets, and pass 2 walks the segment again, ranking lanes
-// that share a direction with __match_any_sync, so every entry lands at
-// group offset + entries of that direction before it.
+// directions of each segment (each lane adds its entries into packed
+// per-direction counters, summed over the warp at the end), one barrier
+// turns the counts into per-warp offsets, and pass 2 walks the segment
+// again 32 entries at a time, ranking lanes that share a direction (a
+// ballot for the entries that stay in the tile, nearly all of them;
+// __match_any_sync for the rest), so every entry lands at group offset +
+// entries of that direction before it. Both passes issue the loads of four
+// 32-entry steps before using them.
 __global__ void __launch_bounds__(kScatterThreads)
     k_order_scatter(int ntiles, const uint32_t *__restrict__ old_start,
                     const uint32_t *__restrict__ old_order, const uint8_t *__restrict__ dir,
                     const uint32_t *__restrict__ grp_off, uint32_t *__restrict__ new_order,
-                    uint32_t capacity, DevStatus *status) {
+                    uint32_t capacity, uint32_t slot0, DevStatus *status) {
   constexpr int kWarps = kScatterThreads / 32;
+  constexpr int kU = 4;  // 32-entry steps per batch of loads
   __shared__ uint32_t s_cnt[kWarps][10];
   __shared__ uint32_t s_base[kWarps][10];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -135,17 +140,47 @@ __global__ void __launch_bounds__(kScatterThreads)
     const uint32_t n = e - b;
     const uint32_t seg = ((n + kWarps * 32 - 1) / (kWarps * 32)) * 32;
     const uint32_t w0 = b + min(n, warp * seg), w1 = b + min(n, (warp + 1) * seg);
-    // pass 1: direction counts of this warp's segment
-    uint32_t mycnt = 0;  // lane f < 10 holds the count of direction f
-    for (uint32_t p = w0 + lane; p < w1 + 31; p += 32) {
-      if (p - lane >= w1) break;
-      const uint32_t d = p < w1 ? dir[p] : 10u;
+    // pass 1: direction counts of this warp's segment; packed counters of
+    // 16 bits, directions 0-3 in c0, 4-7 in c1, 8-9 in c2, summed over the
+    // warp into lane f's mycnt every 256 batches (at most 32 x 4 x 256 =
+    // 32768 entries per counter in between)
+    unsigned long long c0 = 0, c1 = 0, c2 = 0;
+    uint32_t mycnt = 0;  // lane f < 10: count of direction f
+    auto flush = [&]() {
 #pragma unroll
-      for (uint32_t f = 0; f < 10; ++f) {
-        const uint32_t m = __ballot_sync(0xffffffffu, d == f);
-        if (lane == (int)f) mycnt += __popc(m);
+      for (int o = 16; o > 0; o >>= 1) {
+        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+      }
+      const unsigned long long w = lane < 4 ? c0 : (lane < 8 ? c1 : c2);
+      if (lane < 10) mycnt += (uint32_t)((w >> (16 * (lane & 3))) & 0xffffull);
+      c0 = c1 = c2 = 0;
+    };
+    int batches = 0;
+    for (uint32_t q = w0; q < w1; q += 32 * kU) {
+      if (++batches == 256) {
+        flush();
+        batches = 0;
+      }
+      uint32_t d[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const uint32_t p = q + 32 * k + lane;
+        d[k] = p < w1 ? dir[p] : 10u;
+      }
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const unsigned long long one = 1ull << (16 * (d[k] & 3u));
+        if (d[k] < 4u)
+          c0 += one;
+        else if (d[k] < 8u)
+          c1 += one;
+        else if (d[k] < 10u)
+          c2 += one;
       }
     }
+    flush();
     if (lane < 10) s_cnt[warp][lane] = mycnt;
     __syncthreads();
     if (lane < 9) {
@@ -154,34 +189,43 @@ __global__ void __launch_bounds__(kScatterThreads)
       s_base[warp][lane] = off;
     }
     __syncwarp();
-    // pass 2: stable placement; entries that stay in the tile (direction 4,
-    // nearly all of them) are ranked with one ballot, the rest with
-    // __match_any_sync
+    // pass 2: stable placement
     uint32_t base4 = s_base[warp][4];
-    for (uint32_t p = w0 + lane; p < w1 + 31; p += 32) {
-      if (p - lane >= w1) break;
-      const bool valid = p < w1;
-      const uint32_t d = valid ? dir[p] : 10u;
-      const uint32_t stay = __ballot_sync(0xffffffffu, d == 4u);
-      const uint32_t other = __ballot_sync(0xffffffffu, d < 9u && d != 4u);
-      uint32_t dst = 0xffffffffu;
-      if (d == 4u) dst = base4 + __popc(stay & lt);
-      base4 += __popc(stay);
-      if (other) {
-        if ((other >> lane) & 1u) {
-          const uint32_t peers = __match_any_sync(other, d);
-          const uint32_t bs = s_base[warp][d];
-          dst = bs + __popc(peers & lt);
-          __syncwarp(other);
-          if ((peers & lt) == 0u) s_base[warp][d] = bs + __popc(peers);
-        }
-        __syncwarp();
+    for (uint32_t q = w0; q < w1; q += 32 * kU) {
+      uint32_t d[kU], src[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const uint32_t p = q + 32 * k + lane;
+        d[k] = p < w1 ? dir[p] : 10u;
+        // no old order (after a compacting push): the particle at list
+        // position p sits in slot slot0 + p
+        src[k] = p < w1 ? (old_order ? old_order[p] : slot0 + p) : 0u;
       }
-      if (dst != 0xffffffffu) {
-        if (dst < capacity)
-          new_order[dst] = old_order ? old_order[p] : p;  // no old order: slot = position
-        else
-          atomicAdd(&status->tile_faults, 1ull);
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        if (q + 32 * k >= w1) break;
+        const uint32_t dk = d[k];
+        const uint32_t stay = __ballot_sync(0xffffffffu, dk == 4u);
+        const uint32_t other = __ballot_sync(0xffffffffu, dk < 9u && dk != 4u);
+        uint32_t dst = 0xffffffffu;
+        if (dk == 4u) dst = base4 + __popc(stay & lt);
+        base4 += __popc(stay);
+        if (other) {
+          if ((other >> lane) & 1u) {
+            const uint32_t peers = __match_any_sync(other, dk);
+            const uint32_t bs = s_base[warp][dk];
+            dst = bs + __popc(peers & lt);
+            __syncwarp(other);
+            if ((peers & lt) == 0u) s_base[warp][dk] = bs + __popc(peers);
+          }
+          __syncwarp();
+        }
+        if (dst != 0xffffffffu) {
+          if (dst < capacity)
+            new_order[dst] = src[k];
+          else
+            atomicAdd(&status->tile_faults, 1ull);
+        }
       }
     }
     __syncthreads();
@@ -252,8 +296,10 @@ __global__ void k_tile_fill_from_cells(MeshK m, TilesK T, const uint32_t *__rest
 // Keys for the full rebuild: tile of a bulk cell, ntiles otherwise; cells
 // outside the bulk are emptied as the reference push does (ptc_updater.cu:
 // 87-90).
-__global__ void k_tile_keys(MeshK m, TilesK T, uint32_t *cell, size_t n, uint32_t *keys,
-                            uint32_t *vals) {
+// Keys of slots base + i, i < n (vals = the slots).
+__global__ void k_tile_keys(MeshK m, TilesK T, uint32_t *cell, size_t base, size_t n,
+                            uint32_t *keys, uint32_t *vals) {
+  cell += base;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     uint32_t c = cell[i];
@@ -310,15 +356,16 @@ __global__ void __launch_bounds__(kScanThreads)
   if (tid == 0 && n_max) *n_max = s_max;
 }
 
-__global__ void k_cell_keys(const uint32_t *cell, size_t n, uint32_t ncells, uint32_t *keys,
-                            uint32_t *vals, const uint32_t *d_number) {
-  // slots at or beyond a device-side live count are empty
-  const size_t live = d_number ? (size_t)*d_number : n;
+// Keys of slots base + i, i < n (vals = the slots); slots at or beyond a
+// device-side live count are empty.
+__global__ void k_cell_keys(const uint32_t *cell, size_t base, size_t n, uint32_t ncells,
+                            uint32_t *keys, uint32_t *vals, const uint32_t *d_number) {
+  const size_t live = d_number ? (size_t)*d_number : base + n;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t c = i < live ? cell[i] : AP_MAX_CELL;
+    const uint32_t c = base + i < live ? cell[base + i] : AP_MAX_CELL;
     keys[i] = (c == AP_MAX_CELL) ? ncells : c;
-    vals[i] = (uint32_t)i;
+    vals[i] = (uint32_t)(base + i);
   }
 }
 
@@ -375,11 +422,11 @@ cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count, uint32_t *new_st
 
 cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start, const uint32_t *old_order,
                                  const uint8_t *dir, const uint32_t *grp_off,
-                                 uint32_t *new_order) {
+                                 uint32_t *new_order, uint32_t slot0) {
   int grid = c.tiles.ntiles < c.num_sms * 8 ? c.tiles.ntiles : c.num_sms * 8;
   k_order_scatter<<<grid, kScatterThreads, 0, c.stream>>>(c.tiles.ntiles, old_start, old_order,
                                                           dir, grp_off, new_order,
-                                                          (uint32_t)c.order_cap, c.status);
+                                                          (uint32_t)c.order_cap, slot0, c.status);
   c.launches++;
   return cudaGetLastError();
 }
@@ -442,7 +489,31 @@ ap_particles store_layout(void *buf, size_t cap) {
 
 }  // namespace
 
+// Output of a compaction. When the caller's capacity leaves a free region
+// as large as the occupied one ([store_base, number) holds every particle;
+// the other half of the capacity is empty), the push writes the tile-ordered
+// copy straight into it and the old region becomes empty slots; otherwise
+// into the scratch store, copied back afterwards.
 cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id) {
+  const size_t half = c.capacity / 2;
+  const size_t used = c.number - c.store_base;
+  if (c.store_base == 0 && c.number <= half) {
+    c.compact_direct = true;
+    c.compact_dst = half;
+  } else if (c.store_base >= half && used <= c.store_base) {
+    c.compact_direct = true;
+    c.compact_dst = 0;
+  } else {
+    c.compact_direct = false;
+    c.compact_dst = 0;
+  }
+  if (c.compact_direct) {
+    const size_t d = c.compact_dst;
+    *out = PtcK{c.ptc.x1 + d, c.ptc.x2 + d, c.ptc.x3 + d, c.ptc.p1 + d,  c.ptc.p2 + d,
+                c.ptc.p3 + d, c.ptc.E + d,  c.ptc.weight + d, c.ptc.cell + d, c.ptc.flag + d};
+    *out_id = c.ptc.id + d;
+    return cudaSuccess;
+  }
   const size_t n = c.capacity > c.number ? c.capacity : c.number;
   if (!c.compact_buf || c.compact_cap < n) {
     cudaFree(c.compact_buf);
@@ -457,37 +528,55 @@ cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id) {
   return cudaSuccess;
 }
 
-cudaError_t compact_copy_back(Ctx &c, const uint32_t *live) {
-  const size_t n = c.number;
+// After the order update of a compacting push: `live` (device) slots were
+// written from compact_dst on. Direct output: the old region becomes empty
+// and the new high-water mark is compact_dst + (number - store_base);
+// scratch output: copied back to slots [0, number). Either way the slots
+// between the written ones and the high-water mark become empty.
+cudaError_t compact_finish(Ctx &c, const uint32_t *live) {
+  const size_t n = c.number - c.store_base;
   if (n == 0) return cudaSuccess;
-  const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
-  const struct {
-    void *dst;
-    const void *src;
-    size_t bytes;
-  } back[11] = {{c.ptc.x1, s.x1, 4}, {c.ptc.x2, s.x2, 4},         {c.ptc.x3, s.x3, 4},
-                {c.ptc.p1, s.p1, 4}, {c.ptc.p2, s.p2, 4},         {c.ptc.p3, s.p3, 4},
-                {c.ptc.E, s.E, 4},   {c.ptc.weight, s.weight, 4}, {c.ptc.cell, s.cell, 4},
-                {c.ptc.id, s.id, 8}, {c.ptc.flag, s.flag, 4}};
-  for (const auto &m : back) {
-    cudaError_t e = cudaMemcpyAsync(m.dst, m.src, n * m.bytes, cudaMemcpyDeviceToDevice, c.stream);
+  cudaError_t e;
+  if (c.compact_direct) {
+    e = cudaMemsetAsync(c.ptc.cell + c.store_base, 0xff, n * sizeof(uint32_t), c.stream);
     if (e != cudaSuccess) return e;
+  } else {
+    const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
+    const struct {
+      void *dst;
+      const void *src;
+      size_t bytes;
+    } back[11] = {{c.ptc.x1, s.x1, 4}, {c.ptc.x2, s.x2, 4},         {c.ptc.x3, s.x3, 4},
+                  {c.ptc.p1, s.p1, 4}, {c.ptc.p2, s.p2, 4},         {c.ptc.p3, s.p3, 4},
+                  {c.ptc.E, s.E, 4},   {c.ptc.weight, s.weight, 4}, {c.ptc.cell, s.cell, 4},
+                  {c.ptc.id, s.id, 8}, {c.ptc.flag, s.flag, 4}};
+    for (const auto &m : back) {
+      e = cudaMemcpyAsync(m.dst, m.src, n * m.bytes, cudaMemcpyDeviceToDevice, c.stream);
+      if (e != cudaSuccess) return e;
+    }
+    if (c.store_base > 0) {
+      e = cudaMemsetAsync(c.ptc.cell + n, 0xff, (c.number - n) * sizeof(uint32_t), c.stream);
+      if (e != cudaSuccess) return e;
+    }
   }
-  k_compact_tail<<<grid_for(c, n, 256), 256, 0, c.stream>>>(live, c.ptc.cell, n);
+  k_compact_tail<<<grid_for(c, n, 256), 256, 0, c.stream>>>(live, c.ptc.cell + c.compact_dst, n);
   c.launches++;
+  c.number = c.compact_dst + n;
+  c.store_base = c.compact_dst;
   return cudaGetLastError();
 }
 
-// Builds the tile order from scratch: stable sort of slots [0, number) by
-// tile key, then tile offsets from a histogram.
+// Builds the tile order from scratch: stable sort of slots
+// [store_base, number) by tile key, then tile offsets from a histogram.
 cudaError_t rebuild_tile_order(Ctx &c) {
-  const size_t n = c.number;
+  const size_t n = c.number - c.store_base;
   const uint32_t nt = (uint32_t)c.tiles.ntiles;
   uint32_t *start = c.tile_start[c.cur];
   cudaError_t e;
   if (n > 0) {
-    k_tile_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.mk, c.tiles, c.ptc.cell, n,
-                                                          c.keys[0], c.vals[0]);
+    k_tile_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.mk, c.tiles, c.ptc.cell,
+                                                          c.store_base, n, c.keys[0],
+                                                          c.vals[0]);
     c.launches++;
     uint32_t *ko, *vo;
     e = radix_pairs(c, n, bits_for(nt), &ko, &vo);
@@ -509,15 +598,19 @@ cudaError_t rebuild_tile_order(Ctx &c) {
 
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   // a 1D context with a device-side count (pair injection) sorts over its
-  // capacity and writes the new count on the device
+  // capacity and writes the new count on the device; a 2D store after a
+  // compaction into the upper half sorts slots [store_base, number)
   const bool device_count = c.pstate && c.mk.dim == 1;
-  const size_t n = device_count ? c.capacity : c.number;
+  const size_t base = device_count ? 0 : c.store_base;
+  const size_t n = (device_count ? c.capacity : c.number) - base;
   *new_number = 0;
   if (n == 0) return cudaSuccess;
   const uint32_t ncells =
       (uint32_t)c.mesh.dims[0] * (uint32_t)c.mesh.dims[1] * (uint32_t)c.mesh.dims[2];
-  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(
-      c.ptc.cell, n, ncells, c.keys[0], c.vals[0], device_count ? &c.pstate->number : nullptr);
+  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.ptc.cell, base, n, ncells, c.keys[0],
+                                                        c.vals[0],
+                                                        device_count ? &c.pstate->number
+                                                                     : nullptr);
   c.launches++;
   uint32_t *ko, *vo;
   cudaError_t e = radix_pairs(c, n, bits_for(ncells), &ko, &vo);

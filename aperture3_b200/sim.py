@@ -342,6 +342,14 @@ class SimData:
         check(self.env._lib.ap_get_number(self.env.ctx, C.byref(n)), "ap_get_number")
         self.number = int(n.value)
 
+    def slot_range(self):
+        """(first, end): slots [first, end) hold every particle."""
+        a, b = C.c_size_t(), C.c_size_t()
+        check(self.env._lib.ap_get_slot_range(self.env.ctx, C.byref(a), C.byref(b)),
+              "ap_get_slot_range")
+        self.number = int(b.value)
+        return int(a.value), int(b.value)
+
     def pair_stats(self):
         """(particle_steps, pairs created, pairs dropped) since pair injection
         was enabled."""

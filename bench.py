@@ -83,6 +83,7 @@ def workload_config(args, tile):
                      "deposit + tile counting sort + Yee FDTD, sort_by_cell every "
                      f"{args.sort_interval} steps"),
         "grid": [args.N, args.N], "ppc": args.ppc, "particles": n,
+        "capacity": 2 * n if args.compact else n,
         "tile": list(tile), "sort_interval": args.sort_interval,
         "compaction_interval": args.compact,
         "l2": "inputs larger than L2 (particle SoA 48 B x N_p)",
@@ -321,7 +322,9 @@ def run_ours(args, rank, world, local_rank):
     params.chunk = args.chunk
     n = ptc["x1"].numel()
     env = SimEnvironment(params)
-    data = SimData(env, capacity=n)
+    # twice the particles: compactions write the tile-ordered store into the
+    # free half instead of copying it back
+    data = SimData(env, capacity=2 * n if args.compact else n)
     data.set_fields_device(fields)
     data.set_particles_device(ptc)
     del ptc
@@ -652,6 +655,11 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
     from aperture3_b200.sim import PTC_FIELDS
 
     names = [k for k, _ in PTC_FIELDS]
+    # the initial state of the end-to-end run: the current particles, sorted
+    # by cell into slots [0, n) (the periodic box loses none)
+    data.sort_particles()
+    if data.number != n:
+        raise RuntimeError(f"expected {n} particles after the sort, found {data.number}")
     host = {k: torch.empty_like(data.particles[k][:n], device="cpu").pin_memory() for k in names}
     fhost = {k: [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in getattr(data, k)]
              for k in ("E", "B", "J")}
@@ -686,8 +694,9 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
             if s % args.sort_interval == 0 and s != 0:
                 data.sort_particles()
             check(lib.ap_diagnostics(env.ctx, diag), "ap_diagnostics")
+        first, end = data.slot_range()  # host-side bounds, no synchronisation
         for k in names:
-            host[k].copy_(data.particles[k][:n], non_blocking=True)
+            host[k][:end - first].copy_(data.particles[k][first:end], non_blocking=True)
         for k in fhost:
             for h, a in zip(fhost[k], getattr(data, k)):
                 h.copy_(a, non_blocking=True)
@@ -695,6 +704,9 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
     torch.cuda.synchronize()
     env.sync()
     ms = e0.elapsed_time(e1)
+    live = int((host["cell"][:end - first] != -1).sum())  # int32 view of MAX_CELL
+    if live != n:
+        raise RuntimeError(f"end-to-end run returned {live} particles, expected {n}")
     return {"value": n * args.steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps,
             "d2h_bytes_per_step": d2h / args.steps + d2h_diag, "ms": ms,

@@ -152,6 +152,10 @@ AP_API int ap_bind_particles(ap_ctx *ctx, const ap_particles *ptc,
  * since the last update; the tile order is rebuilt at the next update. */
 AP_API int ap_particles_modified(ap_ctx *ctx, size_t number);
 AP_API int ap_get_number(const ap_ctx *ctx, size_t *number);
+/* Slots [*first, *end) hold every particle (holes included); first is 0
+ * unless a compaction wrote the store into the upper half of the capacity
+ * (ap_set_compaction), end is the particle number. */
+AP_API int ap_get_slot_range(const ap_ctx *ctx, size_t *first, size_t *end);
 
 /* ptc_updater::update_particles(sim_data&, double dt, uint32_t step)
  * (ptc_updater.cu:748-841): zero J (and Rho), push, deposit + move, fold

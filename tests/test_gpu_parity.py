@@ -26,15 +26,15 @@ def _fields(m, rng, amp=0.3):
 
 
 def _setup(N, nptc, seed, tile=(0, 0), periodic=(True, True), data_interval=1, row_align=4,
-           gamma_max=50.0, chunk=0):
+           gamma_max=50.0, chunk=0, capacity=None):
     params = make_params(N, periodic=periodic, data_interval=data_interval, tile=tile,
-                         capacity=nptc)
+                         capacity=capacity or nptc)
     params.chunk = chunk
     m = oracle.make_mesh(params.N, params.guard, size=params.size)
     rng = np.random.default_rng(seed)
     f = _fields(m, rng)
     p = random_particles(m, nptc, rng, gamma_max=gamma_max)
-    return Pair(params, f, p, row_align=row_align)
+    return Pair(params, f, p, capacity=capacity, row_align=row_align)
 
 
 @pytest.mark.parametrize("tile", [(4, 4), (8, 8), (16, 16), (16, 8)])
@@ -57,24 +57,51 @@ def test_2d_push_deposit_bitexact_chunks(chunk):
         pr.check_current(J_TOL, rho=True)
 
 
-@pytest.mark.parametrize("interval", [1, 3])
-def test_2d_compaction_keeps_every_particle(interval):
-    """With the store rewritten in tile order every `interval` updates the
-    particles change slots but not values: compared by id they equal the
-    oracle bit for bit, and the current is unchanged."""
-    pr = _setup((64, 48), 20000, seed=8, tile=(8, 8))
+PTC_KEYS = ("x1", "x2", "x3", "p1", "p2", "p3", "E", "cell", "flag", "weight", "id")
+
+
+def _same_by_id(got, ref, what):
+    live_g = got["cell"] != oracle.MAX_CELL
+    live_o = ref["cell"] != oracle.MAX_CELL
+    ig = np.argsort(got["id"][live_g], kind="stable")
+    io = np.argsort(ref["id"][live_o], kind="stable")
+    for k in PTC_KEYS:
+        assert_bits(got[k][live_g][ig], ref[k][live_o][io], f"{what}: {k}")
+
+
+@pytest.mark.parametrize("interval,spare", [(1, 1), (3, 1), (1, 2), (3, 2)])
+def test_2d_compaction_keeps_every_particle(interval, spare):
+    """With the store rewritten in tile order every `interval` updates (into
+    scratch and copied back when the capacity equals the particle count,
+    into the free half of a capacity of twice the count) the particles
+    change slots but not values: compared by id they equal the oracle bit
+    for bit, the current is unchanged, and a sort_by_cell afterwards gives
+    the oracle's cells and, per cell, the same particles."""
+    n = 20000
+    pr = _setup((64, 48), n, seed=8, tile=(8, 8), capacity=spare * n)
     pr.env.set_compaction(interval)
     for step in range(5):
         pr.both_update_particles(step)
         got = pr.data.particles_host()
-        live_g = got["cell"] != oracle.MAX_CELL
-        live_o = pr.p["cell"] != oracle.MAX_CELL
-        ig = np.argsort(got["id"][live_g], kind="stable")
-        io = np.argsort(pr.p["id"][live_o], kind="stable")
-        for k in ("x1", "x2", "x3", "p1", "p2", "p3", "E", "cell", "flag", "weight", "id"):
-            assert_bits(got[k][live_g][ig], pr.p[k][live_o][io], f"step {step}: {k}")
+        first, end = pr.data.slot_range()
+        assert end - first <= n and (spare == 2 or first == 0)
+        assert np.all(got["cell"][:first] == oracle.MAX_CELL)
+        _same_by_id(got, pr.p, f"step {step}")
         pr.check_current(J_TOL, rho=True)
-    assert not np.array_equal(got["id"][:len(pr.p["id"])], pr.p["id"])  # slots did move
+    # slots did move (into the upper half, or within the lower one)
+    assert first > 0 or not np.array_equal(got["id"][:len(pr.p["id"])], pr.p["id"])
+    pr.data.sort_particles()
+    n_ref = oracle.sort_by_cell(pr.m, pr.p, len(pr.p["x1"]))
+    got = pr.data.particles_host()
+    assert pr.data.number == n_ref and pr.data.slot_range() == (0, n_ref)
+    og = np.lexsort((got["id"], got["cell"]))
+    oo = np.lexsort((pr.p["id"][:n_ref], pr.p["cell"][:n_ref]))
+    assert_bits(got["cell"], pr.p["cell"][:n_ref], "cells after sort_by_cell")
+    for k in PTC_KEYS:
+        assert_bits(got[k][og], pr.p[k][:n_ref][oo], f"after sort_by_cell: {k}")
+    # and the update continues from the sorted store
+    pr.both_update_particles(5)
+    _same_by_id(pr.data.particles_host(), pr.p, "step 5")
 
 
 def test_2d_tile_order_is_stable_counting_sort():
