@@ -298,6 +298,8 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->cub_tmp);
   cudaFree(c->gather_tmp);
   cudaFree(c->cell_start);
+  cudaFree(c->cell_count);
+  cudaFree(c->sort_max);
   cudaFree(c->tmp_j);
   cudaFree(c->coef);
   cudaFree(c->compact_buf);
@@ -749,12 +751,10 @@ AP_API int ap_sort_by_cell(ap_ctx *c) {
   const bool device_count = c->pstate && c->mk.dim == 1;
   if (!device_count) AP_TRY_ST(refresh_number(c));
   const int ph = phase_begin(c, kPhSort);
-  c->order_valid = false;  // sort_by_cell rebuilds the 2D tile order
-  AP_TRY(sort_by_cell(*c, &n));
+  AP_TRY(sort_by_cell(*c, &n));  // also leaves the 2D tile order of the sorted store
   phase_end(c, ph);
   if (!device_count) {
-    c->number = n;
-    c->store_base = 0;
+    c->number = n;  // sort_by_cell set store_base
     AP_TRY_ST(push_number(c));
   }
   return AP_OK;

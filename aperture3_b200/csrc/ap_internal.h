@@ -217,6 +217,8 @@ struct Ctx {
   void *gather_tmp = nullptr;
   size_t scratch_cap = 0;
   uint32_t *cell_start = nullptr;  // ncells + 1 entries, set by sort_by_cell
+  uint32_t *cell_count = nullptr;  // ncells + 1 entries (tile-local sort)
+  uint32_t *sort_max = nullptr;    // device: largest cell population (tile-local sort)
 
   // fixed-point current / charge accumulators (3 + num_species components)
   unsigned long long *acc = nullptr;

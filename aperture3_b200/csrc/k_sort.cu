@@ -277,7 +277,7 @@ __global__ void k_tile_counts_from_cells(MeshK m, TilesK T, const uint32_t *__re
 
 __global__ void k_tile_fill_from_cells(MeshK m, TilesK T, const uint32_t *__restrict__ cs,
                                        const uint32_t *__restrict__ tile_start,
-                                       uint32_t *__restrict__ order) {
+                                       uint32_t *__restrict__ order, uint32_t slot0) {
   for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
     const int tx = t % T.ntx, ty = t / T.ntx;
     const int x0 = m.guard[0] + tx * T.tx;
@@ -287,7 +287,7 @@ __global__ void k_tile_fill_from_cells(MeshK m, TilesK T, const uint32_t *__rest
     uint32_t out = tile_start[t];
     for (int y = y0; y < y1; ++y) {
       const uint32_t a = cs[y * m.dims[0] + x0], b = cs[y * m.dims[0] + x1];
-      for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) order[out + (i - a)] = i;
+      for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) order[out + (i - a)] = slot0 + i;
       out += b - a;
     }
   }
@@ -489,6 +489,22 @@ ap_particles store_layout(void *buf, size_t cap) {
 
 }  // namespace
 
+// The scratch store (48 B per slot, allocated on first use).
+static cudaError_t compact_store_scratch(Ctx &c, PtcK *out, uint64_t **out_id) {
+  const size_t n = c.capacity > c.number ? c.capacity : c.number;
+  if (!c.compact_buf || c.compact_cap < n) {
+    cudaFree(c.compact_buf);
+    c.compact_buf = nullptr;
+    cudaError_t e = cudaMalloc(&c.compact_buf, n * 48);
+    if (e != cudaSuccess) return e;
+    c.compact_cap = n;
+  }
+  const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
+  *out = PtcK{s.x1, s.x2, s.x3, s.p1, s.p2, s.p3, s.E, s.weight, s.cell, s.flag};
+  *out_id = s.id;
+  return cudaSuccess;
+}
+
 // Output of a compaction. When the caller's capacity leaves a free region
 // as large as the occupied one ([store_base, number) holds every particle;
 // the other half of the capacity is empty), the push writes the tile-ordered
@@ -514,18 +530,7 @@ cudaError_t compact_store(Ctx &c, PtcK *out, uint64_t **out_id) {
     *out_id = c.ptc.id + d;
     return cudaSuccess;
   }
-  const size_t n = c.capacity > c.number ? c.capacity : c.number;
-  if (!c.compact_buf || c.compact_cap < n) {
-    cudaFree(c.compact_buf);
-    c.compact_buf = nullptr;
-    cudaError_t e = cudaMalloc(&c.compact_buf, n * 48);
-    if (e != cudaSuccess) return e;
-    c.compact_cap = n;
-  }
-  const ap_particles s = store_layout(c.compact_buf, c.compact_cap);
-  *out = PtcK{s.x1, s.x2, s.x3, s.p1, s.p2, s.p3, s.E, s.weight, s.cell, s.flag};
-  *out_id = s.id;
-  return cudaSuccess;
+  return compact_store_scratch(c, out, out_id);
 }
 
 // After the order update of a compacting push: `live` (device) slots were
@@ -596,15 +601,38 @@ cudaError_t rebuild_tile_order(Ctx &c) {
   return cudaGetLastError();
 }
 
+namespace {
+
+
+// Tile-order derived from the cell starts of a store sorted into slots
+// [slot0, slot0 + live).
+cudaError_t tile_order_from_cells(Ctx &c, uint32_t slot0) {
+  const int nt = c.tiles.ntiles;
+  k_tile_counts_from_cells<<<(nt + 255) / 256, 256, 0, c.stream>>>(c.mk, c.tiles, c.cell_start,
+                                                                   c.dir_count);
+  k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, nt, c.tile_start[c.cur], c.n_max);
+  k_tile_fill_from_cells<<<nt < c.num_sms * 8 ? nt : c.num_sms * 8, 256, 0, c.stream>>>(
+      c.mk, c.tiles, c.cell_start, c.tile_start[c.cur], c.order[c.cur], slot0);
+  c.launches += 3;
+  c.order_valid = true;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   // a 1D context with a device-side count (pair injection) sorts over its
   // capacity and writes the new count on the device; a 2D store after a
   // compaction into the upper half sorts slots [store_base, number)
+  c.order_valid = false;
   const bool device_count = c.pstate && c.mk.dim == 1;
   const size_t base = device_count ? 0 : c.store_base;
   const size_t n = (device_count ? c.capacity : c.number) - base;
   *new_number = 0;
-  if (n == 0) return cudaSuccess;
+  if (n == 0) {
+    c.store_base = 0;
+    return cudaSuccess;
+  }
   const uint32_t ncells =
       (uint32_t)c.mesh.dims[0] * (uint32_t)c.mesh.dims[1] * (uint32_t)c.mesh.dims[2];
   k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.ptc.cell, base, n, ncells, c.keys[0],
@@ -616,15 +644,35 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   cudaError_t e = radix_pairs(c, n, bits_for(ncells), &ko, &vo);
   if (e != cudaSuccess) return e;
   const int g = grid_for(c, n, 256);
-  // rearrange every SoA member through the gather buffer
-  // (cuda/core/particle_base_impl.cu:466-487)
-#define AP_GATHER(FIELD, T)                                                                \
-  do {                                                                                      \
-    k_gather<T><<<g, 256, 0, c.stream>>>(c.ptc.FIELD, vo, n, (T *)c.gather_tmp);           \
-    c.launches++;                                                                           \
-    e = cudaMemcpyAsync(c.ptc.FIELD, c.gather_tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, \
-                        c.stream);                                                          \
-    if (e != cudaSuccess) return e;                                                         \
+  // With compaction on and a free half of the capacity, each member is
+  // gathered straight into that half (the store then occupies
+  // [out0, out0 + live)); otherwise through the gather buffer and back to
+  // slots [0, live) (cuda/core/particle_base_impl.cu:466-487). One member at
+  // a time: the random reads of one array stay in L2, those of eleven at once
+  // do not.
+  const size_t half = c.capacity / 2;
+  size_t out0 = 0;
+  bool direct = false;
+  if (!device_count && c.compact_interval > 0) {
+    if (c.store_base == 0 && c.number <= half) {
+      direct = true;
+      out0 = half;
+    } else if (c.store_base >= half && n <= c.store_base) {
+      direct = true;
+      out0 = 0;
+    }
+  }
+#define AP_GATHER(FIELD, T)                                                                  \
+  do {                                                                                        \
+    if (direct) {                                                                             \
+      k_gather<T><<<g, 256, 0, c.stream>>>(c.ptc.FIELD, vo, n, (T *)c.ptc.FIELD + out0);      \
+    } else {                                                                                  \
+      k_gather<T><<<g, 256, 0, c.stream>>>(c.ptc.FIELD, vo, n, (T *)c.gather_tmp);           \
+      e = cudaMemcpyAsync(c.ptc.FIELD, c.gather_tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, \
+                          c.stream);                                                          \
+      if (e != cudaSuccess) return e;                                                         \
+    }                                                                                         \
+    c.launches++;                                                                             \
   } while (0)
   AP_GATHER(x1, float);
   AP_GATHER(x2, float);
@@ -638,6 +686,10 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   AP_GATHER(id, uint64_t);
   AP_GATHER(flag, uint32_t);
 #undef AP_GATHER
+  if (direct && out0 > 0) {  // the old particles sat below the new range: empty them
+    e = cudaMemsetAsync(c.ptc.cell, 0xff, c.number * sizeof(uint32_t), c.stream);
+    if (e != cudaSuccess) return e;
+  }
   // cell_start over the sorted keys; cell_start[ncells] is the number of
   // non-empty slots (upper_bound of MAX_CELL - 1, particle_base_impl.cu:454-458)
   if (!c.cell_start) {
@@ -657,21 +709,13 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   if (e != cudaSuccess) return e;
   if (c.mk.dim == 2) {
     // the tile order of the cell-sorted particles, without another sort
-    const int nt = c.tiles.ntiles;
-    k_tile_counts_from_cells<<<(nt + 255) / 256, 256, 0, c.stream>>>(c.mk, c.tiles, c.cell_start,
-                                                                     c.dir_count);
-    c.launches++;
-    k_scan_counts<<<1, kScanThreads, 0, c.stream>>>(c.dir_count, nt, c.tile_start[c.cur],
-                                                    c.n_max);
-    c.launches++;
-    k_tile_fill_from_cells<<<nt < c.num_sms * 8 ? nt : c.num_sms * 8, 256, 0, c.stream>>>(
-        c.mk, c.tiles, c.cell_start, c.tile_start[c.cur], c.order[c.cur]);
-    c.launches++;
-    c.order_valid = true;
+    e = tile_order_from_cells(c, (uint32_t)out0);
+    if (e != cudaSuccess) return e;
   }
   e = cudaStreamSynchronize(c.stream);
   if (e != cudaSuccess) return e;
-  *new_number = live;
+  c.store_base = out0;
+  *new_number = out0 + live;
   return cudaSuccess;
 }
 

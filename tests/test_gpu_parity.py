@@ -92,8 +92,10 @@ def test_2d_compaction_keeps_every_particle(interval, spare):
     assert first > 0 or not np.array_equal(got["id"][:len(pr.p["id"])], pr.p["id"])
     pr.data.sort_particles()
     n_ref = oracle.sort_by_cell(pr.m, pr.p, len(pr.p["x1"]))
-    got = pr.data.particles_host()
-    assert pr.data.number == n_ref and pr.data.slot_range() == (0, n_ref)
+    first, end = pr.data.slot_range()
+    # sorted into slots [0, live), or into the free half with compaction on
+    assert end - first == n_ref and first in (0, spare * n // 2)
+    got = {k: v[first:end] for k, v in pr.data.particles_host().items()}
     og = np.lexsort((got["id"], got["cell"]))
     oo = np.lexsort((pr.p["id"][:n_ref], pr.p["cell"][:n_ref]))
     assert_bits(got["cell"], pr.p["cell"][:n_ref], "cells after sort_by_cell")
@@ -197,6 +199,39 @@ def test_sort_by_cell_bitexact():
     got = pr.data.particles_host()
     for k, _ in oracle.PTC_FIELDS:
         assert_bits(got[k], pr.p[k][:n_ref], f"sorted {k}")
+
+
+@pytest.mark.parametrize("tile,crowd", [((8, 8), 0), ((16, 16), 0), ((16, 8), 5000)])
+def test_sort_by_cell_after_updates_bitexact(tile, crowd):
+    """sort_by_cell right after updates (the tile-local path: per-tile cell
+    histograms, ranks by slot within each cell, one gather) gives the
+    oracle's stable sort slot for slot; a cell holding more than 4096
+    particles (crowd) takes the radix path, with the same result."""
+    pr = _setup((64, 48), 12000, seed=21, tile=tile, capacity=12000 + crowd)
+    if crowd:
+        # `crowd` more particles at rest in one cell
+        rng = np.random.default_rng(3)
+        n0 = len(pr.p["x1"])
+        extra = random_particles(pr.m, crowd, rng, gamma_max=1.0)
+        c0 = pr.p["cell"][0]
+        extra["cell"][:] = c0
+        for k in ("p1", "p2", "p3"):
+            extra[k][:] = 0
+        extra["E"][:] = 1
+        extra["id"][:] = np.arange(n0, n0 + crowd, dtype=np.uint64)
+        pr.p = {k: np.concatenate([pr.p[k], extra[k]]) for k in pr.p}
+        pr.data.set_particles(pr.p)
+    for step in range(3):
+        pr.both_update_particles(step)
+    pr.data.sort_particles()
+    n_ref = oracle.sort_by_cell(pr.m, pr.p, len(pr.p["x1"]))
+    assert pr.data.number == n_ref and pr.data.slot_range() == (0, n_ref)
+    got = pr.data.particles_host()
+    for k, _ in oracle.PTC_FIELDS:
+        assert_bits(got[k], pr.p[k][:n_ref], f"sorted {k}")
+    pr.p = {k: v[:n_ref].copy() for k, v in pr.p.items()}
+    pr.both_update_particles(3)
+    pr.check_particles()
 
 
 def test_tile_order_after_sort_by_cell():
