@@ -319,7 +319,7 @@ __global__ void k_tile_keys(MeshK m, TilesK T, uint32_t *cell, size_t base, size
       }
     }
     keys[i] = key;
-    vals[i] = (uint32_t)i;
+    vals[i] = (uint32_t)(base + i);
   }
 }
 

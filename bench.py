@@ -54,6 +54,8 @@ def parse():
                     help="rewrite the particle store in tile order every n steps (0: never); "
                          "particles keep their values, only their slots change")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batched workload: keep every run's tile shape")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
@@ -436,7 +438,15 @@ def run_ours(args, rank, world, local_rank):
     env.close()
 
 
-AUTOTUNE_STEPS = 8  # 4 candidate tile shapes x 2 steps (ap_batch_autotune)
+AUTOTUNE_STEPS = 8  # 2 candidate tile shapes x 4 steps (ap_batch_autotune)
+
+
+def check_live(data, n, what):
+    """Every particle of a periodic box is still in the store."""
+    first, end = data.slot_range()
+    live = int((data.particles["cell"][first:end] != -1).sum())  # int32 view of MAX_CELL
+    if live != n:
+        raise RuntimeError(f"{what}: {live} particles in the store, expected {n}")
 
 
 def run_batched(args):
@@ -464,9 +474,10 @@ def run_batched(args):
         params, fields, ptc = ic.box2d(seed=5000 + r, N=side, ppc=ppc, device=dev)
         n = ptc["x1"].numel()
         env = SimEnvironment(params)
-        data = SimData(env, capacity=n)
+        data = SimData(env, capacity=2 * n if args.compact else n)
         data.set_fields_device(fields)
         data.set_particles_device(ptc)
+        env.set_compaction(args.compact)
         return env, data, n
 
     s_first = AUTOTUNE_STEPS + args.warmup
@@ -493,6 +504,7 @@ def run_batched(args):
             step(s)
         torch.cuda.synchronize()
         t_alone += time.perf_counter() - t0
+        check_live(data, n, f"run {r} alone")
         env.close()
         del data
         torch.cuda.empty_cache()
@@ -508,8 +520,11 @@ def run_batched(args):
         batch.update_fields(s)
         if s % args.sort_interval == 0 and s != 0:
             batch.sort_particles()
-    used = batch.autotune(0)
-    assert used == AUTOTUNE_STEPS, used
+    if args.no_autotune:
+        used = 0
+    else:
+        used = batch.autotune(0)
+        assert used == AUTOTUNE_STEPS, used
     for s in range(used, s_first):
         bstep(s)
     batch.sync()
@@ -519,6 +534,8 @@ def run_batched(args):
     batch.sync()
     t_batch = time.perf_counter() - t0
     batched = total * args.steps / t_batch
+    for r, (_, d, n) in enumerate(runs):
+        check_live(d, n, f"run {r} in the batch")
     shapes = {}
     for (side, ppc), shape in zip(specs, batch.tile_shapes()):
         shapes[str(side)] = f"{shape[0]}x{shape[1]}"
@@ -531,6 +548,7 @@ def run_batched(args):
         "config": {"workload": f"{args.runs} periodic boxes, side in {{128,192,256,384,512}}, "
                                "16-128 ppc, random-mode fields, own dt each",
                    "runs": args.runs, "particles": total, "timed_steps": [steps[0], steps[-1]],
+                   "compaction_interval": args.compact,
                    "sides": [sp[0] for sp in specs], "ppc": [sp[1] for sp in specs]},
         "one_at_a_time": alone, "speedup_vs_one_at_a_time": batched / alone,
         "autotune_steps": used, "tile_shapes": shapes,

@@ -295,8 +295,9 @@ AP_API int ap_batch_sort_by_cell(ap_batch *batch);
 AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
 /* Project autotuner: advances the batch by *steps_used complete steps
  * (particle update, then field update) starting at steps[r], timing the
- * push / deposit of each class of runs (same grid size) with every
- * candidate tile shape, and keeps the fastest shape per class. Particle
+ * push / deposit of each class of runs (same grid size) over three steps
+ * with each candidate tile shape (16x16, 32x16), and keeps the fastest
+ * shape per class. Particle
  * results do not depend on the tile shape; J can differ in the last bits
  * (the fixed-point scale follows the largest tile population). */
 AP_API int ap_batch_autotune(ap_batch *batch, const double *dt, const uint32_t *steps,

@@ -69,6 +69,25 @@ def _same_by_id(got, ref, what):
         assert_bits(got[k][live_g][ig], ref[k][live_o][io], f"{what}: {k}")
 
 
+def test_2d_upper_half_store_with_rebuilt_order():
+    """A grid of 2 x 2 tiles has no incremental tile order (rebuilt from the
+    slots every step); with compaction on, a sort moves the store into the
+    upper half of a doubled capacity and the rebuilt order must follow it."""
+    n = 4096
+    pr = _setup((32, 32), n, seed=12, tile=(16, 16), capacity=2 * n)
+    pr.env.set_compaction(3)
+    for step in range(2):
+        pr.both_update_particles(step)
+    pr.data.sort_particles()
+    n_ref = oracle.sort_by_cell(pr.m, pr.p, len(pr.p["x1"]))
+    assert pr.data.slot_range() == (n, n + n_ref)
+    for step in range(2, 5):
+        pr.both_update_particles(step)
+        got = pr.data.particles_host()
+        _same_by_id(got, pr.p, f"step {step}")
+        pr.check_current(J_TOL, rho=True)
+
+
 @pytest.mark.parametrize("interval,spare", [(1, 1), (3, 1), (1, 2), (3, 2)])
 def test_2d_compaction_keeps_every_particle(interval, spare):
     """With the store rewritten in tile order every `interval` updates (into
