@@ -404,6 +404,9 @@ def run_ours(args, rank, world, local_rank):
                     "fields": pt.fields_ms / args.steps,
                     "sort_by_cell": pt.sort_ms / args.steps}}
 
+    env.sync()
+    check_live(data, n, "box")  # the periodic box keeps every particle
+
     # e2e through the C ABI with host buffers: upload the run's initial state
     # from pinned host memory, run the steps, read the FP64 diagnostics back
     # every step, download the final particles and fields.
