@@ -150,6 +150,12 @@ for _name, _res, _args in [
     ("or_philox4x32_10", None, [_vp, _vp, _vp]),
     ("or_inject_pairs", _sz, [_vp, _sz, _sz, C.c_float, C.c_uint32, C.c_float, C.c_float,
                               C.c_float, C.c_uint64, C.c_uint64, _vp, _vp]),
+    ("or_update_ptc_1dgap", _u64, [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, _vp, _vp]),
+    ("or_update_ptc_1dgap_f64", _u64, [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, _vp, _vp]),
+    ("or_filter_gap", None, [_vp, _vp, _vp, _vp]),
+    ("or_update_particles_1dgap", _u64, [_vp, _vp, _sz, _vp, C.c_float, C.c_int, C.c_int,
+                                         _vp, _vp, _vp]),
+    ("or_update_fields_1dgap", None, [_vp, _vp, _vp, C.c_float, C.c_float]),
 ]:
     _f = getattr(lib, _name)
     _f.restype = _res
@@ -460,3 +466,61 @@ def ref_update_particles_mt(m, p, num, f, dt, step, data_interval, num_species, 
         for s in range(num_species):
             send_add_guard_cells(m, f["Rho"][s], periodic)
     return wrap_particles(m, p, num, periodic)
+
+
+
+# ---------------------------------------------------------------------------
+# 1D gap lab (ptc_updater_1dgap.cu, field_solver_1dgap.cu).
+
+def update_ptc_1dgap(m, p, num, dt, E3, J1, Rho, charges, masses, f64=False):
+    """update_ptc_1dgap on slots [0, num): float adds into J1 / Rho, or
+    double adds of the same float contributions (f64). Returns the count of
+    moves of more than one cell."""
+    s = ptc_struct(p)
+    fn = lib.or_update_ptc_1dgap_f64 if f64 else lib.or_update_ptc_1dgap
+    return fn(C.byref(m), C.byref(s), num, np.float32(dt), _p(E3), _p(J1), _arr(Rho, 8),
+              _fa(charges), _fa(masses))
+
+
+def filter_gap(m, j, tmp, bnd):
+    lib.or_filter_gap(C.byref(m), _p(j), _p(tmp), _fa(bnd, C.c_int, 2))
+
+
+def update_particles_1dgap(m, p, num, f, dt, smoothing, num_species, charges, masses, bnd):
+    s = ptc_struct(p)
+    fs = fields_struct(f)
+    return lib.or_update_particles_1dgap(C.byref(m), C.byref(s), num, C.byref(fs),
+                                         np.float32(dt), smoothing, num_species, _fa(charges),
+                                         _fa(masses), _fa(bnd, C.c_int, 2))
+
+
+def update_fields_1dgap(m, E1, J1, B0, dt):
+    lib.or_update_fields_1dgap(C.byref(m), _p(E1), _p(J1), np.float32(B0), np.float32(dt))
+
+
+_REF_GAP_PATH = os.path.join(_HERE, "_ref", "libapref_gap.so")
+ref_gap = None
+
+
+def load_ref_gap(build=True):
+    """The 1D gap lab's own kernels on the host (pin library), or None."""
+    global ref_gap
+    if ref_gap is not None:
+        return ref_gap
+    if not os.path.exists(_REF_GAP_PATH) and build and os.path.isdir("/root/reference/src"):
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_gap.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_GAP_PATH):
+        return None
+    r = C.CDLL(_REF_GAP_PATH)
+    r.ref_gap_push_deposit.restype = None
+    r.ref_gap_push_deposit.argtypes = [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, C.c_int, _vp,
+                                       _vp]
+    r.ref_gap_filter.restype = None
+    r.ref_gap_filter.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int]
+    r.ref_gap_update_e.restype = None
+    r.ref_gap_update_e.argtypes = [_vp, _vp, _vp, C.c_float, C.c_float]
+    ref_gap = r
+    return ref_gap

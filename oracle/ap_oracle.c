@@ -973,3 +973,131 @@ size_t or_inject_pairs(or_ptc *p, size_t num, size_t cap, float dt, uint32_t ste
   if (dropped) *dropped = want - k;
   return num + 2 * k;
 }
+
+/* ------------------------------------------------------------------------
+ * 1D gap lab (ptc_updater_1dgap.cu, field_solver_1dgap.cu). */
+
+/* Quadmesh::pos(i, n, pos_in_cell) (quadmesh.h:144-150) in dimension 0. */
+static inline float gap_pos(const or_mesh *m, int n, float x) {
+  return m->lower[0] + m->delta[0] * ((float)(n - m->guard[0]) + x);
+}
+
+/* update_ptc_1dgap (ptc_updater_1dgap.cu:75-161); J1 / Rho adds through
+ * the two accumulator types of the f32 and f64 entry points. */
+#define GAP_BODY(ACC_T)                                                          \
+  uint64_t far = 0;                                                              \
+  const int g = m->guard[0], n0 = m->dims[0];                                    \
+  for (size_t idx = 0; idx < num; idx++) {                                       \
+    uint32_t c = p->cell[idx];                                                   \
+    if (c == OR_MAX_CELL) continue;                                                 \
+    if ((int)c < g || (int)c >= n0 - g) { /* is_in_bulk */                       \
+      p->cell[idx] = OR_MAX_CELL;                                                   \
+      continue;                                                                  \
+    }                                                                            \
+    float p1 = p->p1[idx];                                                       \
+    const float x1 = p->x1[idx];                                                 \
+    float gamma = p->E[idx];                                                     \
+    const uint32_t flag = p->flag[idx];                                          \
+    const int sp = ptc_type(flag);                                               \
+    float beta = gap_pos(m, (int)c, x1); /* beta_phi(x) = x */                   \
+    const float Dr = (x1 < 0.5f ? E3[c] * (0.5f + x1) + E3[c - 1] * (0.5f - x1)  \
+                                : E3[c] * (1.5f - x1) + E3[c + 1] * (x1 - 0.5f)); \
+    const float E_term = Dr * charges[sp] / masses[sp] * dt;                     \
+    p1 += E_term;                                                                \
+    const double sgn = beta < 0.0 ? -1.0 : 1.0;                                  \
+    const double f = ((double)gamma - sgn * (double)p1) /                        \
+                     (1.0 + (double)(beta * beta));                              \
+    p1 = (float)((double)p1 + (double)(beta / gamma) * f * f * (double)dt);      \
+    p->p1[idx] = p1;                                                             \
+    gamma = sqrtf(1.0f + p1 * p1 + beta * beta);                                 \
+    float vr = (float)((sgn * (double)p1 / (double)gamma + (double)(beta * beta)) / \
+                       (1.0 + (double)(beta * beta)));                           \
+    if (beta < 0.0f) vr *= -1.0f;                                                \
+    float new_x1 = x1 + vr * dt * m->inv_delta[0];                               \
+    const int dc1 = (int)floorf(new_x1);                                         \
+    if (dc1 > 1 || dc1 < -1) far++;                                              \
+    new_x1 -= (float)dc1;                                                        \
+    p->cell[idx] = (uint32_t)((int)c + dc1);                                     \
+    p->x1[idx] = new_x1;                                                         \
+    beta = gap_pos(m, (int)c + dc1, new_x1);                                     \
+    gamma = sqrtf(1.0f + p1 * p1 + beta * beta);                                 \
+    p->E[idx] = gamma;                                                           \
+    if (!(flag & FLAG_IGNORE_CURRENT)) {                                         \
+      const float weight = -charges[sp] * p->weight[idx];                        \
+      const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);             \
+      float djx = 0.0f;                                                          \
+      for (int i = i0; i <= i1; i++) {                                           \
+        const float sx0 = cic(-x1 + i + 1);                                      \
+        const float sx1 = cic(-new_x1 + (i + 1 - dc1));                          \
+        djx += sx1 - sx0;                                                        \
+        J1[i + (int)c + 1] += (ACC_T)(weight * djx * m->delta[0] / dt);          \
+        Rho[sp][i + (int)c] += (ACC_T)(-weight * sx1);                           \
+      }                                                                          \
+    }                                                                            \
+  }                                                                              \
+  return far;
+
+uint64_t or_update_ptc_1dgap(const or_mesh *m, or_ptc *p, size_t num, float dt,
+                             const float *E3, float *J1, float *const Rho[8],
+                             const float charges[8], const float masses[8]) {
+  GAP_BODY(float)
+}
+
+uint64_t or_update_ptc_1dgap_f64(const or_mesh *m, or_ptc *p, size_t num, float dt,
+                                 const float *E3, double *J1, double *const Rho[8],
+                                 const float charges[8], const float masses[8]) {
+  GAP_BODY(double)
+}
+#undef GAP_BODY
+
+/* filter_current1d (ptc_updater_1dgap.cu:196-213). */
+void or_filter_gap(const or_mesh *m, const float *j, float *tmp, const int bnd[2]) {
+  const int g = m->guard[0], n = m->dims[0];
+  for (int i = 0; i < n; i++) {
+    const int dp = (bnd[1] && i == n - g - 1) ? 0 : 1;
+    const int dm = (bnd[0] && i == g) ? 0 : 1;
+    const float jp = (i + dp < n) ? j[i + dp] : 0.0f;
+    const float jm = (i - dm >= 0) ? j[i - dm] : 0.0f;
+    float t = 0.5f * j[i];
+    t += 0.25f * jp;
+    t += 0.25f * jm;
+    tmp[i] = t;
+  }
+}
+
+uint64_t or_update_particles_1dgap(const or_mesh *m, or_ptc *p, size_t num, or_fields *f,
+                                   float dt, int smoothing, int num_species,
+                                   const float charges[8], const float masses[8],
+                                   const int bnd[2]) {
+  const size_t n = (size_t)m->dims[0];
+  if (num == 0) return 0;
+  for (int c = 0; c < 3; c++) zero_field(m, f->J[c]);
+  for (int s = 0; s < num_species; s++) zero_field(m, f->Rho[s]);
+  /* E3 = E1, smoothed through E2 (ptc_updater_1dgap.cu:232-240) */
+  memcpy(f->E[2], f->E[0], n * sizeof(float));
+  for (int it = 0; it < smoothing; it++) {
+    or_filter_gap(m, f->E[2], f->E[1], bnd);
+    memcpy(f->E[2], f->E[1], n * sizeof(float));
+  }
+  const uint64_t far = or_update_ptc_1dgap(m, p, num, dt, f->E[2], f->J[0], f->Rho, charges,
+                                           masses);
+  float *tmp = (float *)calloc(n, sizeof(float));
+  for (int it = 0; it < smoothing; it++) {
+    or_filter_gap(m, f->J[0], tmp, bnd);
+    memcpy(f->J[0], tmp, n * sizeof(float));
+    for (int s = 0; s < num_species; s++) {
+      or_filter_gap(m, f->Rho[s], tmp, bnd);
+      memcpy(f->Rho[s], tmp, n * sizeof(float));
+    }
+  }
+  free(tmp);
+  return far;
+}
+
+/* update_e_1dgap (field_solver_1dgap.cu:14-24) with j0 = B0 * 1.6
+ * (field_solver_1dgap.cu:33). */
+void or_update_fields_1dgap(const or_mesh *m, float *E1, const float *J1, float B0, float dt) {
+  const float j0 = (float)(B0 * 1.6);
+  for (int i = m->guard[0] + 1; i < m->dims[0] - m->guard[0] - 1; i++)
+    E1[i] += (j0 - J1[i]) * dt;
+}

@@ -177,6 +177,37 @@ size_t or_inject_pairs(or_ptc *p, size_t num, size_t cap, float dt, uint32_t ste
                        uint64_t seed, uint64_t first_id, uint64_t *emitted,
                        uint64_t *dropped);
 
+/* 1D gap pusher (ptc_updater_1dgap.cu:75-161, the 1dgap lab's
+ * update_particles): per live particle in slot order, the E_parallel
+ * interpolation from E3 (the smoothed copy of E1), the push with
+ * beta_phi(x) = x in the reference's float / double mix, the move, and the
+ * deposit of J1 (times delta / dt) and Rho[sp] (every step) with plain
+ * float adds in the reference's order (f64 = 1: into double arrays). A
+ * particle outside the bulk is emptied (cell = MAX_CELL). Returns the
+ * number of moves of more than one cell. */
+uint64_t or_update_ptc_1dgap(const or_mesh *m, or_ptc *p, size_t num, float dt,
+                             const float *E3, float *J1, float *const Rho[8],
+                             const float charges[8], const float masses[8]);
+uint64_t or_update_ptc_1dgap_f64(const or_mesh *m, or_ptc *p, size_t num, float dt,
+                                 const float *E3, double *J1, double *const Rho[8],
+                                 const float charges[8], const float masses[8]);
+/* filter_current1d (ptc_updater_1dgap.cu:196-213): one 1-2-1 pass over all
+ * cells [0, dims0) from j into tmp, with the end cells of the bulk clamped
+ * on boundary sides (bnd[0] lower, bnd[1] upper); a neighbour outside the
+ * array (the reference reads past the row there) counts as 0. */
+void or_filter_gap(const or_mesh *m, const float *j, float *tmp, const int bnd[2]);
+/* ptc_updater_1dgap::update_particles (ptc_updater_1dgap.cu:219-272):
+ * E3 = E1, smoothed `smoothing` times through E2; J1 and Rho zeroed; the
+ * push / deposit; then J1 and each Rho smoothed `smoothing` times through
+ * tmp. Returns the number of moves of more than one cell. */
+uint64_t or_update_particles_1dgap(const or_mesh *m, or_ptc *p, size_t num, or_fields *f,
+                                   float dt, int smoothing, int num_species,
+                                   const float charges[8], const float masses[8],
+                                   const int bnd[2]);
+/* field_solver_1dgap::update_fields (field_solver_1dgap.cu:14-40):
+ * E1 += (j0 - J1) dt on cells [guard + 1, dims0 - guard - 1), j0 = B0 1.6. */
+void or_update_fields_1dgap(const or_mesh *m, float *E1, const float *J1, float B0, float dt);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,3 +127,47 @@ def logsph_dt(m, frac=0.4):
 
 LS_CHARGES = [-1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
 LS_MASSES = [1.0, 1.0, 10.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+
+
+# ---------------------------------------------------------------------------
+# 1D gap lab cases (ptc_updater_1dgap.cu): beta_phi(x) = x, so the grid's
+# lower edge decides the sign of beta.
+
+GAP_CHARGES = [-1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+GAP_MASSES = [1.0] * 8
+
+
+def mesh_gap(N, lower=0.0, size=1.0, guard=2):
+    return oracle.make_mesh((N, 1, 1), (guard, 0, 0), lower=(lower, 0.0, 0.0),
+                            size=(size, 1.0, 1.0))
+
+
+def gap_state(m, n, rng, pmax=50.0):
+    """E1 / E3 / J fields and n particles in the bulk of a 1D gap grid:
+    x1 uniform with a share on cell edges, p1 = +-pmax * u^3, E the gamma
+    of p1 at the particle's beta, weights in [0.5, 1.5], e- / e+, a few
+    with ignore_current."""
+    nc = m.dims[0]
+    x = np.arange(nc, dtype=np.float64)
+    E1 = (0.8 * np.sin(2 * np.pi * x / nc) + 0.1 * rng.standard_normal(nc)).astype(np.float32)
+    p = empty_ptc(n)
+    g = m.guard[0]
+    c = rng.integers(g, nc - g, n)
+    p["cell"][:] = c.astype(np.uint32)
+    x1 = rng.random(n, dtype=np.float32)
+    e = rng.random(n) < 0.2
+    edge = np.array([0.0, np.nextafter(np.float32(1), np.float32(0)), 0.5,
+                     np.nextafter(np.float32(0.5), np.float32(0))], np.float32)
+    x1[e] = edge[rng.integers(0, 4, n)[e]]
+    p["x1"][:] = x1
+    p["p1"][:] = (pmax * rng.uniform(-1, 1, n) ** 3).astype(np.float32)
+    beta = (m.lower[0] + m.delta[0] * ((c - g).astype(np.float32) + x1)).astype(np.float32)
+    p["E"][:] = np.sqrt(1.0 + p["p1"].astype(np.float64) ** 2 + beta.astype(np.float64) ** 2
+                        ).astype(np.float32)
+    p["weight"][:] = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    sp = rng.integers(0, 2, n).astype(np.uint32)
+    p["flag"][:] = sp << 29
+    ign = rng.random(n) < 0.05
+    p["flag"][ign] |= np.uint32(1 << 3)
+    p["id"][:] = np.arange(n, dtype=np.uint64)
+    return E1, p

@@ -5,7 +5,8 @@ ptc_updater_logsph.cu / field_solver_logsph.cu kernels and
 grid_log_sph.cpp coefficients), run on the host by oracle/ref_build.
 
 Needs the reference tree (to build oracle/_ref/libapref.so). Run from the
-repository root:  python tests/golden/make_golden.py
+repository root:  python tests/golden/make_golden.py [logsph | gap]
+(gap_*.npz: the 1D gap lab's update_ptc_1dgap, ptc_updater_1dgap.cu).
 Each fixture holds seeded inputs (particles, E/B, backgrounds, J) and the
 reference outputs: particles and J/Rho after push + deposit, and E/B/divE/
 divB after one E update, one B update and compute_divs.
@@ -144,8 +145,46 @@ def main_logsph():
         print(path, os.path.getsize(path))
 
 
+def main_gap():
+    """gap_*.npz: the 1D gap lab's update_ptc_1dgap (oracle/_ref/
+    libapref_gap.so) on seeded particles and E3; outputs are the particles,
+    J1 and Rho after one call."""
+    from _cases import GAP_CHARGES, GAP_MASSES, gap_state, mesh_gap
+    ref = oracle.load_ref_gap(build=True)
+    if ref is None:
+        raise SystemExit("gap pin library unavailable (needs the reference tree)")
+    for name, N, lower, seed in [("gap_a", 256, 0.0, 31), ("gap_b", 300, -0.6, 32)]:
+        rng = np.random.default_rng(seed)
+        m = mesh_gap(N, lower)
+        E3, p = gap_state(m, 500, rng)
+        dt = np.float32(0.5 * m.delta[0])
+        out = {}
+        for k, v in oracle.mesh_dict(m).items():
+            out["mesh_" + k] = np.asarray(v)
+        out["dt"] = dt
+        out["E3"] = E3.copy()
+        for k in p:
+            out["in_" + k] = p[k].copy()
+        J = np.zeros(m.dims[0], np.float32)
+        R = [np.zeros(m.dims[0], np.float32) for _ in range(2)]
+        s_ = oracle.ptc_struct(p)
+        ref.ref_gap_push_deposit(oracle.C.byref(m), oracle.C.byref(s_), len(p["x1"]), dt,
+                                 oracle._p(E3), oracle._p(J), oracle._arr(R, 8), 2,
+                                 oracle._fa(GAP_CHARGES), oracle._fa(GAP_MASSES))
+        for k in p:
+            out["out_" + k] = p[k]
+        out["out_J1"] = J
+        for sp in range(2):
+            out[f"out_Rho{sp}"] = R[sp]
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path))
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "logsph":
         main_logsph()
+    elif len(sys.argv) > 1 and sys.argv[1] == "gap":
+        main_gap()
     else:
         main()
