@@ -10,13 +10,15 @@ loads the library and fails if it is missing.
 """
 from . import _lib  # noqa: F401
 from .sim import (Batch, FLAG_IGNORE_CURRENT, FLAG_IGNORE_EM, ELECTRON, ION, POSITRON, FieldSolver,
-                  FieldSolverLogsph, PtcUpdater, PtcUpdaterLogsph, SimData, SimEnvironment,
-                  SimParams, field_solver, field_solver_logsph, ptc_updater, ptc_updater_logsph,
-                  species_flag)
+                  FieldSolver1dGap, FieldSolverLogsph, PtcUpdater, PtcUpdater1dGap,
+                  PtcUpdaterLogsph, SimData, SimEnvironment, SimParams, field_solver,
+                  field_solver_1dgap, field_solver_logsph, ptc_updater, ptc_updater_1dgap,
+                  ptc_updater_logsph, species_flag)
 
 __all__ = [
     "Batch", "SimParams", "SimEnvironment", "SimData", "ptc_updater", "field_solver", "PtcUpdater",
     "FieldSolver", "ptc_updater_logsph", "field_solver_logsph", "PtcUpdaterLogsph",
-    "FieldSolverLogsph", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
+    "FieldSolverLogsph", "ptc_updater_1dgap", "field_solver_1dgap", "PtcUpdater1dGap",
+    "FieldSolver1dGap", "species_flag", "ELECTRON", "POSITRON", "ION", "FLAG_IGNORE_EM",
     "FLAG_IGNORE_CURRENT",
 ]

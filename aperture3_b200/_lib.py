@@ -88,6 +88,11 @@ class ApPhaseTimes(C.Structure):
                 ("push_deposit_launches", C.c_uint64)]
 
 
+class ApGapParams(C.Structure):
+    """ap_gap_params: SimParams::B0 for the 1D gap lab."""
+    _fields_ = [("B0", C.c_float)]
+
+
 class ApLogsphParams(C.Structure):
     """ap_logsph_params: the dev_params members of the log-spherical kernels."""
     _fields_ = [("compactness", C.c_float), ("omega", C.c_float), ("gravity", C.c_float),
@@ -143,6 +148,8 @@ SIGNATURES = {
     "ap_ctx_create_logsph": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                   C.POINTER(ApLogsphParams), C.POINTER(_vp)]),
     "ap_logsph_coef": (_i, [_vp, _i, C.POINTER(ApArray)]),
+    "ap_ctx_create_1dgap": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams), C.POINTER(ApGapParams),
+                                 C.POINTER(_vp)]),
     "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),
     "ap_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "ap_batch_destroy": (_i, [_vp]),

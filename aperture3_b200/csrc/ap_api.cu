@@ -455,6 +455,76 @@ AP_API int ap_smooth_current(ap_ctx *c, uint32_t step) {
 
 namespace apb {
 
+// ptc_updater_1dgap::update_particles (ptc_updater_1dgap.cu:219-272).
+int update_particles_gap(Ctx *c, double dt, uint32_t step) {
+  (void)step;
+  const ap_params &pr = c->params;
+  // the reference does nothing at all without particles (:226)
+  if (c->number == 0) return finish(c);
+  const int ncomp = 3 + pr.num_species;
+  const int n = c->mesh.dims[0];
+  const int bl = !pr.periodic[0], bu = !pr.periodic[0];  // is_boundary(0), (1)
+  int ph = phase_begin(c, kPhFinalize);
+  // J and Rho are zeroed (:227-230); the finalize writes every component
+  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
+                         c->stream));
+  if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
+  AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  // E3 = E1, smoothed current_smoothing times through E2 (:232-240)
+  float *E1 = c->fields.E[0].ptr, *E2 = c->fields.E[1].ptr, *E3 = c->fields.E[2].ptr;
+  AP_TRY(cudaMemcpyAsync(E3, E1, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  for (int it = 0; it < pr.current_smoothing; ++it) {
+    AP_TRY(launch_gap_filter(*c, E3, E2, bl, bu));
+    AP_TRY(cudaMemcpyAsync(E3, E2, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  phase_end(c, ph);
+  PushDepositParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.m = c->mk;
+  P.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
+             c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
+  P.F[2] = FieldArr{E3, (int)(c->fields.E[2].pitch / 4)};
+  P.acc = c->acc;
+  P.acc_pitch = c->mesh.dims[0];
+  P.acc_comp = c->acc_comp;
+  P.fx_used = c->fx_used;
+  P.n_max = c->n_max;
+  P.wmax = c->wmax;
+  P.number = c->number;
+  P.status = c->status;
+  P.num_species = pr.num_species;
+  P.dt = (float)dt;
+  P.qmax = 0.0f;
+  for (int s = 0; s < AP_MAX_SPECIES; ++s) {
+    P.qmax = fmaxf(P.qmax, fabsf(pr.charges[s]));
+    P.charge[s] = pr.charges[s];
+    P.mass[s] = pr.masses[s];
+  }
+  // J1 contributions carry delta / dt (:143-144)
+  const float kj = c->mesh.delta[0] / (float)dt;
+  if (kj > 1.0f) P.qmax *= kj;
+  ph = phase_begin(c, kPhPushDeposit);
+  AP_TRY(launch_gap_push_deposit(*c, P));
+  phase_end(c, ph);
+  ph = phase_begin(c, kPhFinalize);
+  AP_TRY(launch_finalize_current(*c, ncomp));
+  // J1 and each Rho smoothed current_smoothing times (:254-268)
+  float *tmp = c->tmp_j;
+  for (int it = 0; it < pr.current_smoothing; ++it) {
+    AP_TRY(launch_gap_filter(*c, c->fields.J[0].ptr, tmp, bl, bu));
+    AP_TRY(cudaMemcpyAsync(c->fields.J[0].ptr, tmp, sizeof(float) * n, cudaMemcpyDeviceToDevice,
+                           c->stream));
+    for (int s = 0; s < pr.num_species; ++s) {
+      AP_TRY(launch_gap_filter(*c, c->fields.Rho[s].ptr, tmp, bl, bu));
+      AP_TRY(cudaMemcpyAsync(c->fields.Rho[s].ptr, tmp, sizeof(float) * n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+    }
+  }
+  c->rho_is_zero = false;
+  phase_end(c, ph);
+  return finish(c);
+}
+
 // First part of an update: zero the accumulators, refresh the weight bound
 // and the tile order if needed, and fill the kernel parameters. Returns
 // AP_OK; *has_work is false when there are no particles.
@@ -677,6 +747,7 @@ extern "C" {
 
 AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   if (!c || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  if (c->coord == 2) return update_particles_gap(c, dt, step);
   PushDepositParams P;
   bool has_work = false;
   AP_TRY_ST(update_prepare(c, dt, step, P, &has_work));
@@ -712,6 +783,12 @@ AP_API int ap_compute_divs(ap_ctx *c) {
 AP_API int ap_update_fields(ap_ctx *c, double dt, uint32_t step) {
   if (!c || !c->fields_bound) return AP_ERR_INVALID;
   const int ph = phase_begin(c, kPhFields);
+  if (c->coord == 2) {
+    // field_solver_1dgap::update_fields (field_solver_1dgap.cu:28-40)
+    AP_TRY(launch_gap_update_e(*c, (float)(c->gap.B0 * 1.6), (float)dt));
+    phase_end(c, ph);
+    return finish(c);
+  }
   if (c->coord == 1) {
     // field_solver_logsph::update_fields (field_solver_logsph.cu:354-398):
     // B, then E, then the divergences; no guard exchange on a
@@ -858,6 +935,20 @@ AP_API int ap_ctx_create_logsph(const ap_mesh *mesh, const ap_params *params,
     ap_ctx_destroy(c);
     return st;
   }
+  *out = c;
+  return AP_OK;
+}
+
+AP_API int ap_ctx_create_1dgap(const ap_mesh *mesh, const ap_params *params,
+                               const ap_gap_params *gap, ap_ctx **out) {
+  if (!mesh || !params || !gap || !out) return AP_ERR_INVALID;
+  *out = nullptr;
+  if (make_meshk(*mesh).dim != 1) return AP_ERR_UNSUPPORTED;
+  ap_ctx *c = nullptr;
+  int st = ap_ctx_create(mesh, params, &c);
+  if (st != AP_OK) return st;
+  c->coord = 2;
+  c->gap = *gap;
   *out = c;
   return AP_OK;
 }

@@ -250,7 +250,8 @@ struct Ctx {
   bool compact_direct = false;      // output in the caller's free half, no copy back
 
   // log-spherical grid (ap_ctx_create_logsph)
-  int coord = 0;                // 0 Cartesian, 1 log-spherical
+  int coord = 0;                // 0 Cartesian, 1 log-spherical, 2 1D gap
+  ap_gap_params gap{};          // 1D gap lab parameters
   ap_logsph_params lsp{};
   float *coef = nullptr;        // AP_NUM_COEF arrays of dims[0] x dims[1]
   size_t coef_pitch = 0;        // bytes per row
@@ -314,6 +315,12 @@ int push_number(Ctx *c);
 // log-spherical (k_logsph.cu)
 int logsph_setup(Ctx &c);  // coefficients on the host, upload, J3 bound
 ap_array coef_array(const Ctx &c, int which);
+// 1D gap lab (k_gap.cu)
+cudaError_t launch_gap_push_deposit(Ctx &c, const PushDepositParams &P);
+cudaError_t launch_gap_filter(Ctx &c, const float *src, float *dst, int bnd_lower,
+                              int bnd_upper);
+cudaError_t launch_gap_update_e(Ctx &c, float j0, float dt);
+
 cudaError_t launch_ls_finalize(Ctx &c, float dt, bool do_rho, bool zero_axis);
 cudaError_t launch_ls_smooth(Ctx &c, bool do_rho);
 cudaError_t launch_ls_update_b(Ctx &c, float dt);

@@ -121,7 +121,12 @@ class SimEnvironment:
         self._lib = _lib.lib()
         ctx = C.c_void_p()
         self.logsph = str(params.coord_system).lower() in ("logspherical", "logsph", "log_sph")
-        if self.logsph:
+        self.gap = str(params.coord_system).lower() in ("1dgap", "gap")
+        if self.gap:
+            gp = _lib.ApGapParams(float(params.B0))
+            check(self._lib.ap_ctx_create_1dgap(C.byref(self.mesh), C.byref(ap), C.byref(gp),
+                                                C.byref(ctx)), "ap_ctx_create_1dgap")
+        elif self.logsph:
             lp = ApLogsphParams(float(params.compactness), float(params.omega),
                                 float(params.gravity), float(params.rad_cooling_coef),
                                 float(params.B0), float(params.damping_coef),
@@ -613,8 +618,38 @@ class field_solver_logsph:
         check(self.env._lib.ap_compute_divs(self.env.ctx), "ap_compute_divs")
 
 
+class ptc_updater_1dgap:
+    """ptc_updater_1dgap (src/algorithms/ptc_updater_1dgap.h:11-27), for an
+    environment with coord_system = '1dgap'."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.gap:
+            raise ValueError("ptc_updater_1dgap needs coord_system = '1dgap'")
+        self.env = env
+
+    def update_particles(self, data: SimData, dt: float, step: int = 0):
+        """ptc_updater_1dgap::update_particles (ptc_updater_1dgap.cu:219-272)."""
+        check(self.env._lib.ap_update_particles(self.env.ctx, float(dt), int(step)),
+              "ap_update_particles")
+
+
+class field_solver_1dgap:
+    """field_solver_1dgap (src/algorithms/field_solver_1dgap.h:9-20)."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.gap:
+            raise ValueError("field_solver_1dgap needs coord_system = '1dgap'")
+        self.env = env
+
+    def update_fields(self, data: SimData, dt: float, time: float = 0.0):
+        """E1 += (1.6 B0 - J1) dt (field_solver_1dgap.cu:28-40)."""
+        check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), 0), "ap_update_fields")
+
+
 # Python-style aliases
 PtcUpdater = ptc_updater
 FieldSolver = field_solver
 PtcUpdaterLogsph = ptc_updater_logsph
 FieldSolverLogsph = field_solver_logsph
+PtcUpdater1dGap = ptc_updater_1dgap
+FieldSolver1dGap = field_solver_1dgap

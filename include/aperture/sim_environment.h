@@ -72,6 +72,11 @@ class sim_environment {
       lp.rad_cooling_on = params.rad_cooling_on ? 1 : 0;
       lp.damping_length = params.damping_length;
       ap_check(ap_ctx_create_logsph(&m, &p, &lp, &ctx_), "ap_ctx_create_logsph");
+    } else if (std::strcmp(params.coord_system, "1DGap") == 0) {
+      // the 1D gap lab (labs/1dgap): ptc_updater_1dgap / field_solver_1dgap
+      ap_gap_params gp{};
+      gp.B0 = params.B0;
+      ap_check(ap_ctx_create_1dgap(&m, &p, &gp, &ctx_), "ap_ctx_create_1dgap");
     } else {
       ap_check(ap_ctx_create(&m, &p, &ctx_), "ap_ctx_create");
     }

@@ -258,6 +258,22 @@ AP_API int ap_logsph_coef(ap_ctx *ctx, int which, ap_array *out);
  * damping, and both axes. */
 AP_API int ap_logsph_field_boundary(ap_ctx *ctx, double omega);
 
+/* 1D gap lab (labs/1dgap; src/algorithms/ptc_updater_1dgap.h,
+ * field_solver_1dgap.h). A context made here runs, in ap_update_particles,
+ * ptc_updater_1dgap::update_particles (ptc_updater_1dgap.cu:219-272): E3 is
+ * set to E1 smoothed current_smoothing times (E2 is the scratch), the gap
+ * pusher with beta_phi(x) = x moves the particles (no wrap; a particle
+ * outside the bulk is emptied at the next update), J1 (times delta / dt)
+ * and every species' Rho are deposited on every step and smoothed; and in
+ * ap_update_fields field_solver_1dgap::update_fields (field_solver_1dgap.cu:
+ * 28-40): E1 += (j0 - J1) dt on the bulk cells but the outermost, with
+ * j0 = 1.6 B0. */
+typedef struct {
+  float B0;                  /* SimParams::B0                               */
+} ap_gap_params;
+AP_API int ap_ctx_create_1dgap(const ap_mesh *mesh, const ap_params *params,
+                               const ap_gap_params *gap, ap_ctx **out);
+
 /* ---------------------------------------------------------------------
  * Batched mode (new; the reference runs one simulation per process).
  * A batch advances many independent 2D Cartesian runs, each an ordinary

@@ -24,6 +24,7 @@ def _build(tmp_path, lab="box_lab"):
 def test_dropin_headers_compile(tmp_path):
     _build(tmp_path)
     _build(tmp_path, "pulsar_lab")
+    _build(tmp_path, "gap_lab")
 
 
 @pytest.mark.gpu
@@ -38,3 +39,10 @@ def test_dropin_pulsar_lab_runs(tmp_path):
     exe = _build(tmp_path, "pulsar_lab")
     r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "pulsar_lab ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_dropin_gap_lab_runs(tmp_path):
+    exe = _build(tmp_path, "gap_lab")
+    r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "gap_lab ok" in r.stdout, r.stdout + r.stderr
