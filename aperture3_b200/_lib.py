@@ -151,6 +151,8 @@ SIGNATURES = {
     "ap_ctx_create_1dgap": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams), C.POINTER(ApGapParams),
                                  C.POINTER(_vp)]),
     "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),
+    "ap_logsph_inject": (_i, [_vp, _i, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                              C.c_uint64]),
     "ap_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
     "ap_batch_destroy": (_i, [_vp]),
     "ap_batch_add": (_i, [_vp, _vp]),

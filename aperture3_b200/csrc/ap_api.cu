@@ -299,6 +299,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->gather_tmp);
   cudaFree(c->cell_start);
   cudaFree(c->cell_count);
+  cudaFree(c->ls_surface);
   cudaFree(c->sort_max);
   cudaFree(c->tmp_j);
   cudaFree(c->coef);
@@ -957,6 +958,26 @@ AP_API int ap_logsph_coef(ap_ctx *c, int which, ap_array *out) {
   if (!c || !out || c->coord != 1 || which < 0 || which >= AP_NUM_COEF) return AP_ERR_INVALID;
   *out = coef_array(*c, which);
   return AP_OK;
+}
+
+AP_API int ap_logsph_inject(ap_ctx *c, int inj_per_cell, float p1, float p2, float p3,
+                            float w, float omega, uint64_t seed) {
+  (void)p2;  // the reference's kernel sets p2 from p1 and theta, p3 to 0,
+  (void)p3;  // and leaves omega unused (ptc_updater_logsph.cu:341-367)
+  (void)omega;
+  if (!c || c->coord != 1 || !c->ptc_bound || inj_per_cell < 0) return AP_ERR_INVALID;
+  const int red = c->mesh.dims[1] - 2 * c->mesh.guard[1];
+  const size_t add = (size_t)2 * inj_per_cell * red;
+  if (c->number + add > c->capacity) return fail(c, AP_ERR_CAPACITY);
+  if (!c->ls_surface) AP_TRY(cudaMalloc(&c->ls_surface, sizeof(double) * 2 * red));
+  AP_TRY(launch_ls_inject(*c, inj_per_cell, p1, w, seed, c->inject_calls, c->inject_next_id,
+                          c->ls_surface));
+  c->inject_calls++;
+  c->inject_next_id += add;
+  c->number += add;
+  c->order_valid = false;
+  c->scale_valid = false;
+  return finish(c);
 }
 
 AP_API int ap_logsph_field_boundary(ap_ctx *c, double omega) {

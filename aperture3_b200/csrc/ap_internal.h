@@ -252,6 +252,9 @@ struct Ctx {
   // log-spherical grid (ap_ctx_create_logsph)
   int coord = 0;                // 0 Cartesian, 1 log-spherical, 2 1D gap
   ap_gap_params gap{};          // 1D gap lab parameters
+  double *ls_surface = nullptr;  // log-spherical injection: surface densities
+  uint32_t inject_calls = 0;
+  uint64_t inject_next_id = 1ull << 62;
   ap_logsph_params lsp{};
   float *coef = nullptr;        // AP_NUM_COEF arrays of dims[0] x dims[1]
   size_t coef_pitch = 0;        // bytes per row
@@ -327,6 +330,8 @@ cudaError_t launch_ls_update_b(Ctx &c, float dt);
 cudaError_t launch_ls_update_e(Ctx &c, float dt);
 cudaError_t launch_ls_divs(Ctx &c);
 cudaError_t launch_ls_field_boundary(Ctx &c, float omega);
+cudaError_t launch_ls_inject(Ctx &c, int inj, float p1, float w, uint64_t seed, uint32_t call,
+                             uint64_t first_id, double *surface);
 
 MeshK make_meshk(const ap_mesh &m);
 

@@ -545,6 +545,117 @@ cudaError_t launch_ls_divs(Ctx &c) {
   return cudaGetLastError();
 }
 
+namespace {
+
+// measure_surface_density (ptc_updater_logsph.cu:441-490): electrons and
+// ions in the cells guard0 + 1 .. guard0 + 4, spread 1-4-6-4-1 over theta
+// rows with w / 3 / 16 each, summed in double.
+__global__ void k_ls_surface(MeshK m, PtcK p, size_t num, double *se, double *sp) {
+  const int d0 = m.dims[0], g0 = m.guard[0], g1 = m.guard[1];
+  const int red = m.dims[1] - 2 * g1;
+  const int ic = g0 + 2;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < num;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t c = p.cell[idx];
+    if (c == AP_MAX_CELL) continue;
+    const int c2 = (int)__umul64hi((unsigned long long)c, m.div0);
+    const int c1 = (int)c - c2 * d0;
+    if (!(c1 >= ic - 1 && c1 <= ic - 1 + 3)) continue;
+    const int s = ptc_type(p.flag[idx]);
+    double *a = s == 0 ? se : (s == 2 ? sp : nullptr);
+    if (!a) continue;
+    const float wt = p.w[idx];
+    const int r = c2 - g1;
+    const int at[5] = {max(r - 2, 0), max(r - 1, 0), r, min(r + 1, red - 1), min(r + 2, red - 1)};
+    const float k[5] = {1.0f, 4.0f, 6.0f, 4.0f, 1.0f};
+#pragma unroll
+    for (int q = 0; q < 5; ++q) atomicAdd(a + at[q], (double)(k[q] * wt / 3.0f / 16.0f));
+  }
+}
+
+// inject_ptc (ptc_updater_logsph.cu:301-393) with the library's build
+// semantics: one thread per (bulk theta row r, pair n); pair n of row r
+// takes slots num + 2 (r inj + n) and + 1, empty when the row gets no
+// injection (the outermost rows, or a surface denser than
+// 1.5 sin(theta_c) / dtheta^2 / q_e). x2 from Philox4x32-10 with counter
+// (call, i, n, 0).
+__global__ void k_ls_inject(MeshK m, PtcK p, uint64_t *ids, size_t num, int inj, float p1,
+                            float w, float q_e, float gamma, uint32_t key0, uint32_t key1,
+                            uint32_t call, uint64_t first_id, const double *se,
+                            const double *sp) {
+  const int d0 = m.dims[0], d1 = m.dims[1], g0 = m.guard[0], g1 = m.guard[1];
+  const int red = d1 - 2 * g1;
+  const float inv_d = 1.0f / m.delta[1];
+  const uint32_t key[2] = {key0, key1};
+  const size_t total = (size_t)red * inj;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t / inj), n = (int)(t % inj);
+    const int i = r + g1;
+    const float dens = (float)(se[r] > sp[r] ? se[r] : sp[r]);
+    const float sin_c = sinf(mesh_pos(m.lower[1], m.delta[1], i, g1, 0.5f));
+    const bool on =
+        i >= g1 + 1 && i < d1 - g1 - 1 && !(q_e * dens > 1.5f * (inv_d * inv_d) * sin_c);
+    const size_t s0 = num + 2 * t;
+    float x2 = 0.0f, st = 0.0f, ct = 0.0f;
+    if (on) {
+      const uint32_t ctr[4] = {call, (uint32_t)i, (uint32_t)n, 0u};
+      uint32_t out[4];
+      philox4x32_10(ctr, key, out);
+      x2 = (float)(((double)(out[0] >> 8) + 0.5) * (1.0 / 16777216.0));
+      const float th = mesh_pos(m.lower[1], m.delta[1], i, g1, x2);
+      st = sinf(th);
+      ct = cosf(th);
+    }
+    const float sg = (float)((0.0f < ct) - (ct < 0.0f));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t s = s0 + h;
+      ids[s] = first_id + (s - num);
+      if (!on) {
+        p.cell[s] = AP_MAX_CELL;
+        continue;
+      }
+      p.x1[s] = 0.5f;
+      p.x2[s] = x2;
+      p.x3[s] = 0.0f;
+      p.p1[s] = p1 * 2.0f * fabsf(ct);
+      p.p2[s] = p1 * st * sg;
+      p.p3[s] = 0.0f;
+      p.E[s] = gamma;
+      p.cell[s] = (uint32_t)(g0 + 2 + i * d0);
+      p.w[s] = w * st;
+      p.flag[s] = (1u << 6) | ((uint32_t)h << 29);  // primary; e- then e+
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_ls_inject(Ctx &c, int inj, float p1, float w, uint64_t seed, uint32_t call,
+                             uint64_t first_id, double *surface) {
+  const int red = c.mesh.dims[1] - 2 * c.mesh.guard[1];
+  cudaError_t e = cudaMemsetAsync(surface, 0, sizeof(double) * 2 * red, c.stream);
+  if (e != cudaSuccess) return e;
+  const PtcK p{c.ptc.x1, c.ptc.x2, c.ptc.x3, c.ptc.p1, c.ptc.p2,
+               c.ptc.p3, c.ptc.E,  c.ptc.weight, c.ptc.cell, c.ptc.flag};
+  if (c.number > 0) {
+    size_t g = (c.number + 255) / 256;
+    if (g > (size_t)c.num_sms * 8) g = (size_t)c.num_sms * 8;
+    k_ls_surface<<<(int)g, 256, 0, c.stream>>>(c.mk, p, c.number, surface, surface + red);
+    c.launches++;
+  }
+  const size_t total = (size_t)red * inj;
+  if (total == 0) return cudaGetLastError();
+  // E = sqrt(1.0 + p1 p1 + vphi vphi) with vphi = 0 (ptc_updater_logsph.cu:350)
+  const float gamma = (float)std::sqrt(1.0 + (double)(p1 * p1) + (double)(0.0f * 0.0f));
+  k_ls_inject<<<(int)((total + 255) / 256), 256, 0, c.stream>>>(
+      c.mk, p, c.ptc.id, c.number, inj, p1, w, c.params.charges[1], gamma, (uint32_t)seed,
+      (uint32_t)(seed >> 32), call, first_id, surface, surface + red);
+  c.launches++;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ls_field_boundary(Ctx &c, float omega) {
   const LsGeo G = make_ls_geo(c);
   const LsFields F = make_ls_fields(c);

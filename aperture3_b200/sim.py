@@ -598,6 +598,15 @@ class ptc_updater_logsph:
         """Run by update_particles already (axis current, outflow flags, and
         dropping particles that left the grid)."""
 
+    def inject_ptc(self, data: SimData, inj_per_cell: int, p1: float, p2: float, p3: float,
+                   w: float, omega: float, seed: int = 0x5EED):
+        """inject_ptc (ptc_updater_logsph.cu:849-870): pairs at the stellar
+        surface where it is not yet dense (see ap_logsph_inject)."""
+        check(self.env._lib.ap_logsph_inject(self.env.ctx, int(inj_per_cell), float(p1),
+                                             float(p2), float(p3), float(w), float(omega),
+                                             int(seed)), "ap_logsph_inject")
+        data.refresh_number()
+
 
 class field_solver_logsph:
     """field_solver_logsph (src/algorithms/field_solver_logsph.h:10-20)."""

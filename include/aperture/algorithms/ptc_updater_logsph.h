@@ -24,9 +24,21 @@ class ptc_updater_logsph {
   }
   // Already run by update_particles, as in the reference.
   void apply_boundary(sim_data &, double, uint32_t = 0) {}
+  // inject_ptc (ptc_updater_logsph.cu:849-870): pairs at the stellar
+  // surface where it is not yet dense; see ap_logsph_inject.
+  void inject_ptc(sim_data &data, int inj_per_cell, Scalar p1, Scalar p2, Scalar p3, Scalar w,
+                  Scalar omega) {
+    ap_check(ap_logsph_inject(m_env.ctx(), inj_per_cell, p1, p2, p3, w, omega,
+                              0x5EEDull + inject_calls_++),
+             "inject_ptc");
+    size_t n = 0;
+    ap_check(ap_get_number(m_env.ctx(), &n), "get_number");
+    data.particles.set_num(n);
+  }
 
  private:
   sim_environment &m_env;
+  uint64_t inject_calls_ = 0;
 };
 
 }  // namespace Aperture

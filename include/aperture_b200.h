@@ -257,6 +257,19 @@ AP_API int ap_logsph_coef(ap_ctx *ctx, int which, ap_array *out);
  * (field_solver_logsph.cu:403-428) on one rank: stellar surface, outflow
  * damping, and both axes. */
 AP_API int ap_logsph_field_boundary(ap_ctx *ctx, double omega);
+/* ptc_updater_logsph::inject_ptc (ptc_updater_logsph.cu:301-393, 441-490,
+ * 849-870): measures the electron and ion densities next to the stellar
+ * surface and, in every theta row but the outermost whose density times
+ * q_e stays below 1.5 sin(theta) / dtheta^2, adds inj_per_cell e-/e+ pairs
+ * in cell (guard0 + 2, row): x1 = 0.5, x2 uniform, p1' = 2 p1 |cos theta|,
+ * p2' = p1 sin theta sgn(cos theta), p3' = 0, E = sqrt(1 + p1^2), weight
+ * w sin theta, flag primary. The particle number grows by 2 inj_per_cell
+ * per bulk theta row (rows without injection leave empty slots); x2 is
+ * drawn from Philox4x32-10 keyed by seed with the call count as counter,
+ * in place of the reference's cuRAND states. p2, p3 and omega are accepted
+ * and, as in the reference's kernel, unused. */
+AP_API int ap_logsph_inject(ap_ctx *ctx, int inj_per_cell, float p1, float p2, float p3,
+                            float w, float omega, uint64_t seed);
 
 /* 1D gap lab (labs/1dgap; src/algorithms/ptc_updater_1dgap.h,
  * field_solver_1dgap.h). A context made here runs, in ap_update_particles,

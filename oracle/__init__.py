@@ -156,6 +156,9 @@ for _name, _res, _args in [
     ("or_update_particles_1dgap", _u64, [_vp, _vp, _sz, _vp, C.c_float, C.c_int, C.c_int,
                                          _vp, _vp, _vp]),
     ("or_update_fields_1dgap", None, [_vp, _vp, _vp, C.c_float, C.c_float]),
+    ("or_ls_inject", _sz, [_vp, _vp, _sz, _sz, C.c_int, C.c_float, C.c_float, C.c_float,
+                           C.c_uint64, C.c_uint32, C.c_uint64]),
+    ("or_ls_surface_density", None, [_vp, _vp, _sz, _vp, _vp]),
 ]:
     _f = getattr(lib, _name)
     _f.restype = _res
@@ -524,3 +527,20 @@ def load_ref_gap(build=True):
     r.ref_gap_update_e.argtypes = [_vp, _vp, _vp, C.c_float, C.c_float]
     ref_gap = r
     return ref_gap
+
+
+
+def ls_inject(m, p, num, cap, inj, p1, w, q_e, seed, call, first_id):
+    """Log-spherical surface injection (build semantics, ap_oracle.h);
+    returns the new number."""
+    s = ptc_struct(p)
+    return lib.or_ls_inject(C.byref(m), C.byref(s), num, cap, inj, np.float32(p1),
+                            np.float32(w), np.float32(q_e), seed, call, first_id)
+
+
+def ls_surface_density(m, p, num):
+    red = m.dims[1] - 2 * m.guard[1]
+    se, sp = np.zeros(red), np.zeros(red)
+    s = ptc_struct(p)
+    lib.or_ls_surface_density(C.byref(m), C.byref(s), num, _p(se), _p(sp))
+    return se, sp

@@ -1101,3 +1101,86 @@ void or_update_fields_1dgap(const or_mesh *m, float *E1, const float *J1, float 
   for (int i = m->guard[0] + 1; i < m->dims[0] - m->guard[0] - 1; i++)
     E1[i] += (j0 - J1[i]) * dt;
 }
+
+/* ------------------------------------------------------------------------
+ * Log-spherical surface injection (ptc_updater_logsph.cu:301-393, 441-490,
+ * 849-870), build semantics as documented in ap_oracle.h. */
+
+static inline float ls_pos(const or_mesh *m, int dim, int n, float x) {
+  return m->lower[dim] + m->delta[dim] * ((float)(n - m->guard[dim]) + x);
+}
+
+void or_ls_surface_density(const or_mesh *m, const or_ptc *p, size_t num, double *se,
+                           double *sp_) {
+  const int d0 = m->dims[0], d1 = m->dims[1], g0 = m->guard[0], g1 = m->guard[1];
+  const int red = d1 - 2 * g1;
+  const int ic = g0 + 2;
+  for (int r = 0; r < red; r++) se[r] = sp_[r] = 0.0;
+  for (size_t idx = 0; idx < num; idx++) {
+    const uint32_t c = p->cell[idx];
+    if (c == OR_MAX_CELL) continue;
+    const int c1 = (int)(c % (uint32_t)d0), c2 = (int)(c / (uint32_t)d0);
+    if (!(c1 >= ic - 1 && c1 <= ic - 1 + 3)) continue;
+    const int s = ptc_type(p->flag[idx]);
+    double *a = s == 0 ? se : (s == 2 ? sp_ : NULL);
+    if (!a) continue;
+    const float wt = p->weight[idx];
+    const int r = c2 - g1;
+    const int at[5] = {r - 2 > 0 ? r - 2 : 0, r - 1 > 0 ? r - 1 : 0, r,
+                       r + 1 < red - 1 ? r + 1 : red - 1, r + 2 < red - 1 ? r + 2 : red - 1};
+    const float k[5] = {1.0f, 4.0f, 6.0f, 4.0f, 1.0f};
+    for (int q = 0; q < 5; q++) a[at[q]] += (double)(k[q] * wt / 3.0f / 16.0f);
+  }
+}
+
+size_t or_ls_inject(const or_mesh *m, or_ptc *p, size_t num, size_t cap, int inj, float p1,
+                    float w, float q_e, uint64_t seed, uint32_t call, uint64_t first_id) {
+  const int d0 = m->dims[0], d1 = m->dims[1], g0 = m->guard[0], g1 = m->guard[1];
+  const int red = d1 - 2 * g1;
+  const size_t add = (size_t)2 * inj * red;
+  if (num + add > cap) return num;
+  const int ic = g0 + 2;
+  double *se = (double *)calloc((size_t)red, sizeof(double));
+  double *sp_ = (double *)calloc((size_t)red, sizeof(double));
+  or_ls_surface_density(m, p, num, se, sp_);
+  const float inv_d = 1.0f / m->delta[1];
+  const float gamma = (float)sqrt(1.0 + (double)(p1 * p1) + (double)(0.0f * 0.0f));
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int r = 0; r < red; r++) {
+    const int i = r + g1;
+    const float dens = (float)(se[r] > sp_[r] ? se[r] : sp_[r]);
+    const float sin_c = sinf(ls_pos(m, 1, i, 0.5f));
+    const int on = i >= g1 + 1 && i < d1 - g1 - 1 && !(q_e * dens > 1.5f * (inv_d * inv_d) * sin_c);
+    for (int n = 0; n < inj; n++) {
+      const size_t s0 = num + 2 * ((size_t)r * inj + n);
+      for (int h = 0; h < 2; h++) {
+        const size_t s = s0 + h;
+        p->id[s] = first_id + (s - num);
+        if (!on) {
+          p->cell[s] = OR_MAX_CELL;
+          continue;
+        }
+        const uint32_t ctr[4] = {call, (uint32_t)i, (uint32_t)n, 0u};
+        uint32_t out[4];
+        or_philox4x32_10(ctr, key, out);
+        const float x2 = (float)(((double)(out[0] >> 8) + 0.5) * (1.0 / 16777216.0));
+        const float th = ls_pos(m, 1, i, x2);
+        const float st = sinf(th), ct = cosf(th);
+        const float sg = (float)((0.0f < ct) - (ct < 0.0f));
+        p->x1[s] = 0.5f;
+        p->x2[s] = x2;
+        p->x3[s] = 0.0f;
+        p->p1[s] = p1 * 2.0f * fabsf(ct);
+        p->p2[s] = p1 * st * sg;
+        p->p3[s] = 0.0f;
+        p->E[s] = gamma;
+        p->cell[s] = (uint32_t)(ic + i * d0);
+        p->weight[s] = w * st;
+        p->flag[s] = (1u << 6) | ((uint32_t)h << 29); /* primary; e- then e+ */
+      }
+    }
+  }
+  free(se);
+  free(sp_);
+  return num + add;
+}

@@ -208,6 +208,27 @@ uint64_t or_update_particles_1dgap(const or_mesh *m, or_ptc *p, size_t num, or_f
  * E1 += (j0 - J1) dt on cells [guard + 1, dims0 - guard - 1), j0 = B0 1.6. */
 void or_update_fields_1dgap(const or_mesh *m, float *E1, const float *J1, float B0, float dt);
 
+/* ptc_updater_logsph::inject_ptc (ptc_updater_logsph.cu:301-393 inject_ptc,
+ * 441-490 measure_surface_density, 849-870) with the library's build
+ * semantics: the surface densities of electrons and ions in the cells
+ * guard0 + 1 .. guard0 + 4 (1-4-6-4-1 spread over theta rows, w / 3 / 16
+ * each, summed in double); for every theta row i in [guard1 + 1,
+ * dims1 - guard1 - 1) whose max density times q_e stays below
+ * 1.5 sin(theta_c) / dtheta^2, inj e-/e+ pairs at cell (guard0 + 2, i):
+ * x1 = 0.5, x2 = ((out0 >> 8) + 0.5) / 2^24 of Philox4x32-10 with counter
+ * (call, i, n, 0) and key (seed), p1' = p1 2 |cos th|, p2' = p1 sin th
+ * sgn(cos th), p3 = 0, E = sqrt(1 + p1^2), weight w sin th, flag primary.
+ * Pair n of bulk row r = i - guard1 takes slots num + 2 (r inj + n) and
+ * + 1 (ids first_id + the same offsets); the slots of rows without
+ * injection are empty. Returns num + 2 inj (dims1 - 2 guard1), or num when
+ * that exceeds cap. */
+size_t or_ls_inject(const or_mesh *m, or_ptc *p, size_t num, size_t cap, int inj, float p1,
+                    float w, float q_e, uint64_t seed, uint32_t call, uint64_t first_id);
+/* measure_surface_density (ptc_updater_logsph.cu:441-490) summed in double:
+ * se / sp get dims1 - 2 guard1 values (electrons, ions). */
+void or_ls_surface_density(const or_mesh *m, const or_ptc *p, size_t num, double *se,
+                           double *sp);
+
 #ifdef __cplusplus
 }
 #endif

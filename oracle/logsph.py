@@ -209,6 +209,7 @@ def load_ref(build=True):
         ("ref_ls_filter", [_vp, _vp, _vp, _vp]),
         ("ref_ls_update_fields", [_vp, _vp, _vp, _vp, _f]),
         ("ref_ls_field_boundary", [_vp, _vp, _vp, _f]),
+        ("ref_ls_surface_density", [_vp, _vp, _sz, _vp, _vp]),
     ]:
         fn = getattr(r, name)
         fn.restype = None

@@ -204,6 +204,16 @@ void ref_ls_push(const ref_mesh *m, const ref_ls_params *lp, const ref_ptc *p, s
   Kernels::vay_push_logsph_2d(d, num, dt, &st);
 }
 
+/* measure_surface_density<<<256, 512>>> (ptc_updater_logsph.cu:441-490,
+ * launched at :856-858), one emulated thread; se / sp hold
+ * dims1 - 2 guard1 floats. */
+void ref_ls_surface_density(const ref_mesh *m, const ref_ptc *p, size_t num, float *se,
+                            float *sp) {
+  set_mesh(m);
+  one_thread();
+  Kernels::measure_surface_density(to_pd(p), num, se, sp);
+}
+
 /* deposit_and_move_2d_log_sph<1> (ptc_updater_logsph.cu:715-718). */
 void ref_ls_deposit(const ref_mesh *m, const ref_ls_params *lp, const ref_ptc *p, size_t num,
                     float dt, uint32_t step, int data_interval, float *const J[3],

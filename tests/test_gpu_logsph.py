@@ -268,3 +268,45 @@ def test_multi_step_run(smoothing, data_interval):
         d = np.abs(g["J"][k] - b) / scale
         assert np.percentile(d, 99) < 1e-3, f"J{k + 1}"
     case.close()
+
+
+def test_inject_ptc_matches_oracle():
+    """ptc_updater_logsph::inject_ptc (build semantics, ap_logsph_inject)
+    against the oracle with the same Philox draws: slots, cells, positions,
+    flags, ids and E bit for bit; p1, p2 and the weights, which go through
+    CUDA's sinf / cosf instead of glibc's, within 1e-6; the same rows skip
+    a dense surface."""
+    import test_inject_oracle as tio
+    m = mesh_logsph(64, 48)
+    n, inj = 3000, 2
+    red = m.dims[1] - 2 * m.guard[1]
+    cap = n + 2 * inj * red
+    p = tio._surface_ptc(m, n, np.random.default_rng(4), cap)
+    params, _ = _params(m, 0, 1)
+    params.q_e = 60.0
+    params.max_ptc_number = cap
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=cap)
+    data.set_fields(oracle.new_fields(m, NSP))
+    data.set_particles({k: v[:n] for k, v in p.items()})
+    seed = 0x1234ABCD
+    ptc_updater_logsph(env).inject_ptc(data, inj, 3.0, 0.0, 0.0, 0.5, 0.1, seed=seed)
+    assert data.number == cap
+    new_n = oracle.ls_inject(m, p, n, cap, inj, 3.0, 0.5, 60.0, seed, 0, 1 << 62)
+    assert new_n == cap
+    got = data.particles_host()
+    for k in ("cell", "x1", "x2", "x3", "p3", "E", "flag", "id"):
+        live = p["cell"] != oracle.MAX_CELL
+        a, b = got[k], p[k]
+        if k != "cell" and k != "id":
+            a, b = a[live], b[live]
+        assert_bits(a, b, k)
+    live = p["cell"][n:] != oracle.MAX_CELL
+    assert 0 < live.sum() < live.size
+    for k in ("p1", "p2", "weight"):
+        a = got[k][n:][live].astype(np.float64)
+        b = p[k][n:][live].astype(np.float64)
+        assert np.allclose(a, b, rtol=1e-6, atol=1e-7), k
+    # the injected particles take part in the next update
+    ptc_updater_logsph(env).update_particles(data, float(params.delta_t), 0)
+    env.close()
