@@ -889,6 +889,15 @@ AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
   return AP_OK;
 }
 
+AP_API int ap_diagnostics_async(ap_ctx *c, double *host_out) {
+  if (!c || !host_out || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
+  if (c->pstate && c->mk.dim == 1 && c->number_stale) return fail(c, AP_ERR_INVALID);
+  AP_TRY(launch_diagnostics(*c, c->diag_dev));
+  AP_TRY(cudaMemcpyAsync(host_out, c->diag_dev, sizeof(double) * 6, cudaMemcpyDeviceToHost,
+                         c->stream));
+  return AP_OK;
+}
+
 AP_API int ap_set_profiling(ap_ctx *c, int on) {
   if (!c) return AP_ERR_INVALID;
   c->profiling = on != 0;

@@ -117,9 +117,11 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_fields(const DiagParams P
 
 cudaError_t launch_diagnostics(Ctx &c, double *out) {
   DiagParams P;
-  P.p = PtcK{c.ptc.x1, c.ptc.x2, c.ptc.x3, c.ptc.p1, c.ptc.p2,
-             c.ptc.p3, c.ptc.E,  c.ptc.weight, c.ptc.cell, c.ptc.flag};
-  P.number = c.number;
+  // the occupied slots [store_base, number)
+  const size_t b = c.store_base;
+  P.p = PtcK{c.ptc.x1 + b, c.ptc.x2 + b, c.ptc.x3 + b, c.ptc.p1 + b,     c.ptc.p2 + b,
+             c.ptc.p3 + b, c.ptc.E + b,  c.ptc.weight + b, c.ptc.cell + b, c.ptc.flag + b};
+  P.number = c.number - b;
   for (int s = 0; s < AP_MAX_SPECIES; ++s) {
     P.mass[s] = c.params.masses[s];
     P.charge[s] = c.params.charges[s];

@@ -671,8 +671,11 @@ def run_served(args):
 
 
 def run_e2e(args, env, data, pusher, solver, dt, stream, n):
+    import ctypes as C
+
+    import numpy as np
     import torch
-    from aperture3_b200._lib import ApDiag, check
+    from aperture3_b200._lib import check
     from aperture3_b200.sim import PTC_FIELDS
 
     names = [k for k, _ in PTC_FIELDS]
@@ -695,7 +698,9 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
         sum(t.numel() * t.element_size() for k in ("E", "B") for t in fhost[k])
     d2h = sum(t.numel() * t.element_size() for t in host.values()) + \
         sum(t.numel() * t.element_size() for v in fhost.values() for t in v)
-    diag = ApDiag()
+    # per-step FP64 diagnostics copied into pinned host memory without a
+    # host synchronisation per step (ap_diagnostics_async)
+    diag_host = torch.zeros((args.steps, 6), dtype=torch.float64).pin_memory()
     d2h_diag = 48
     lib = env._lib
     e0 = torch.cuda.Event(enable_timing=True)
@@ -714,7 +719,8 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
             solver.update_fields(data, dt, s)
             if s % args.sort_interval == 0 and s != 0:
                 data.sort_particles()
-            check(lib.ap_diagnostics(env.ctx, diag), "ap_diagnostics")
+            check(lib.ap_diagnostics_async(env.ctx, C.c_void_p(diag_host[s].data_ptr())),
+                  "ap_diagnostics_async")
         first, end = data.slot_range()  # host-side bounds, no synchronisation
         for k in names:
             host[k][:end - first].copy_(data.particles[k][first:end], non_blocking=True)
@@ -728,6 +734,9 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
     live = int((host["cell"][:end - first] != -1).sum())  # int32 view of MAX_CELL
     if live != n:
         raise RuntimeError(f"end-to-end run returned {live} particles, expected {n}")
+    kin = diag_host[:, 0].numpy()
+    if not (np.all(np.isfinite(kin)) and np.all(kin > 0)):
+        raise RuntimeError("end-to-end run: per-step kinetic energy not finite and positive")
     return {"value": n * args.steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": h2d / args.steps,
             "d2h_bytes_per_step": d2h / args.steps + d2h_diag, "ms": ms,

@@ -210,6 +210,12 @@ AP_API int ap_get_stats(ap_ctx *ctx, ap_step_stats *stats);
 /* FP64 energy / charge / Gauss-law diagnostics (new; the reference only
  * computes per-particle gamma, cuda/core/particles.cu:10-22). */
 AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
+/* The same reductions without waiting: the six values (in ap_diag's member
+ * order) are copied to host_out, which should be pinned host memory, on the
+ * context's stream; they are there after the next ap_sync. A 1D context
+ * whose particle count moved on the device (pair injection) must be synced
+ * first. */
+AP_API int ap_diagnostics_async(ap_ctx *ctx, double *host_out);
 
 /* ---------------------------------------------------------------------
  * Log-spherical (ln r, theta) grids: ptc_updater_logsph and

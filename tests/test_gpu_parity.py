@@ -377,3 +377,45 @@ def test_coupled_steps_within_tolerance():
         a, b = got[k].astype(np.float64), pr.p[k].astype(np.float64)
         scale = np.maximum(np.abs(b), 1e-3)
         assert (np.abs(a - b) / scale).max() <= 1e-5, k
+
+
+def test_fp64_diagnostics_sync_and_async():
+    """ap_diagnostics (and ap_diagnostics_async into pinned memory) against
+    the same reductions in numpy FP64 on the copied state: kinetic energy
+    sum w m (gamma - 1), total charge, field energy 1/2 sum(E^2 + B^2) dV
+    over the bulk, max |rho|, max |divE - rho|, max |J|."""
+    import ctypes as C
+
+    import torch
+    pr = _setup((64, 48), 20000, seed=31, tile=(8, 8), capacity=40000)
+    pr.env.set_compaction(2)
+    for step in range(3):
+        pr.both_update_particles(step)
+        pr.both_update_fields(step)
+    d = pr.data.diagnostics()
+    host = torch.zeros(6, dtype=torch.float64).pin_memory()
+    check_status = pr.env._lib.ap_diagnostics_async(pr.env.ctx, C.c_void_p(host.data_ptr()))
+    assert check_status == 0
+    pr.env.sync()
+    got = pr.data.particles_host()
+    live = got["cell"] != oracle.MAX_CELL
+    sp = (got["flag"][live] >> 29).astype(np.int64)
+    p2 = sum(got[k][live].astype(np.float64) ** 2 for k in ("p1", "p2", "p3"))
+    w = got["weight"][live].astype(np.float64)
+    charges = np.array(pr.env.charges, np.float64)
+    masses = np.array(pr.env.masses, np.float64)
+    kin = np.sum(w * masses[sp] * (p2 / (np.sqrt(1.0 + p2) + 1.0)))
+    q = np.sum(w * charges[sp])
+    g = pr.data.fields_host()
+    m = pr.m
+    sl = (slice(m.guard[1], m.dims[1] - m.guard[1]), slice(m.guard[0], m.dims[0] - m.guard[0]))
+    en = 0.5 * sum(np.sum(g[k][c][sl].astype(np.float64) ** 2)
+                   for k in ("E", "B") for c in range(3)) * float(m.delta[0]) * float(m.delta[1])
+    rho = sum(g["Rho"][s][sl].astype(np.float64) for s in range(len(g["Rho"])))
+    ref = [kin, q, en, np.abs(rho).max(), np.abs(g["divE"][sl].astype(np.float64) - rho).max(),
+           max(np.abs(g["J"][c][sl]).max() for c in range(3))]
+    vals = [d.kinetic, d.charge, d.field_energy, d.max_abs_rho, d.gauss_residual, d.max_abs_j]
+    for name, a, b, c in zip(("kinetic", "charge", "field", "rho", "gauss", "J"), vals,
+                             host.numpy(), ref):
+        assert np.isclose(a, c, rtol=1e-10, atol=1e-12), (name, a, c)
+        assert np.isclose(b, c, rtol=1e-10, atol=1e-12), (name, b, c)
