@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--tile", type=int, nargs=2, default=(16, 16))
     ap.add_argument("--sort-interval", type=int, default=20)
     ap.add_argument("--chunk", type=int, default=0)
-    ap.add_argument("--compact", type=int, default=4,
+    ap.add_argument("--compact", type=int, default=2,
                     help="rewrite the particle store in tile order every n steps (0: never); "
                          "particles keep their values, only their slots change")
     ap.add_argument("--no-e2e", action="store_true")
