@@ -299,6 +299,8 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->gather_tmp);
   cudaFree(c->cell_start);
   cudaFree(c->cell_count);
+  cudaFree(c->chunk_count);
+  cudaFree(c->big_tiles);
   cudaFree(c->ls_surface);
   cudaFree(c->sort_max);
   cudaFree(c->tmp_j);
@@ -624,6 +626,27 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
         P.id = c->ptc.id;
         c->compact_now = true;
         c->since_compact = 0;
+      }
+      // per-chunk direction counts for the one-pass order update
+      c->chunk_count_ok = false;
+      if (incremental_order(*c)) {
+        const size_t need = c->order_cap / (size_t)chunk_of(*c) + c->tiles.ntiles + 2;
+        if (c->chunk_count_cap < need) {
+          cudaFree(c->chunk_count);
+          c->chunk_count = nullptr;
+          c->chunk_count_cap = 0;
+          AP_TRY(cudaMalloc(&c->chunk_count, sizeof(uint32_t) * 10 * need));
+          c->chunk_count_cap = need;
+        }
+        if (c->big_tiles_cap < (size_t)c->tiles.ntiles + 1) {
+          cudaFree(c->big_tiles);
+          c->big_tiles = nullptr;
+          c->big_tiles_cap = 0;
+          AP_TRY(cudaMalloc(&c->big_tiles, sizeof(uint32_t) * (c->tiles.ntiles + 1)));
+          c->big_tiles_cap = c->tiles.ntiles + 1;
+        }
+        P.chunk_count = c->chunk_count;
+        c->chunk_count_ok = true;
       }
       P.t = c->tiles;
       P.order = c->order[c->cur];

@@ -102,8 +102,7 @@ std::vector<Group> make_groups(const ap_batch *b, const std::vector<bool> &activ
     if (only_class && (*only_class)[r] != cls) continue;
     const Ctx *c = b->runs[r];
     const int dim = c->mk.dim;
-    const int pc = c->params.chunk;
-    const int chunk = dim == 1 ? kChunk1DSlots : (pc == 2048 || pc == 1024 ? pc : 512);
+    const int chunk = dim == 1 ? kChunk1DSlots : chunk_of(*c);
     const int tx = dim == 1 ? 0 : c->tiles.tx, ty = dim == 1 ? 0 : c->tiles.ty;
     const bool tma = dim == 1 ? false : c->use_tma;
     auto key = std::make_tuple(dim, tx, ty, chunk, tma);

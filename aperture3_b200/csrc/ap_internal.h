@@ -93,6 +93,9 @@ struct PushDepositParams {
   const uint32_t *tile_start;
   uint8_t *dir;
   uint32_t *dir_count;   // ntiles * 10
+  // per staged chunk of the tile lists, its direction counts (10 each):
+  // chunk k of tile t is entry tile_start[t] / CH + t + k (null: not kept)
+  uint32_t *chunk_count;
   uint32_t *queue;
   DevStatus *status;
   size_t number;         // 1D: particle slots (an upper bound when d_number is set)
@@ -208,6 +211,12 @@ struct Ctx {
   uint32_t *newcount = nullptr;  // per-tile population after the step
   uint32_t *queue = nullptr;
   size_t order_cap = 0;
+  // per-chunk direction counts of the push / deposit (one-pass order update)
+  uint32_t *chunk_count = nullptr;
+  size_t chunk_count_cap = 0;  // entries of 10 counts
+  uint32_t *big_tiles = nullptr;  // count, then tiles left to the two-pass kernel
+  size_t big_tiles_cap = 0;
+  bool chunk_count_ok = false;  // the last push / deposit recorded them
 
   // rebuild / sort scratch
   uint32_t *keys[2] = {nullptr, nullptr};
@@ -334,6 +343,14 @@ cudaError_t launch_ls_inject(Ctx &c, int inj, float p1, float w, uint64_t seed, 
                              uint64_t first_id, double *surface);
 
 MeshK make_meshk(const ap_mesh &m);
+
+// Particles staged per chunk by the 2D push / deposit of this context: 1024
+// for log-spherical grids, else the configured 256, 1024 or 2048, or 512.
+inline int chunk_of(const Ctx &c) {
+  if (c.coord == 1) return 1024;
+  const int ch = c.params.chunk;
+  return (ch == 256 || ch == 1024 || ch == 2048) ? ch : 512;
+}
 
 // The update of one context in three parts (ap_api.cu): prepare (zeroing,
 // tile-order rebuild, kernel parameters), the push / deposit launch, and

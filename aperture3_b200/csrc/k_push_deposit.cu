@@ -331,6 +331,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
       cp_async_commit();
     };
     int buf = 0;
+    uint32_t cnt_prev = 0;  // threads < 10: the tile's direction count so far
     if (G::NBUF == 2 && n_t > 0) issue(0, 0);
     for (int c0 = 0; c0 < n_t; c0 += CH) {
       const int nch = min(CH, n_t - c0);
@@ -585,6 +586,12 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
         if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[dir], (uint32_t)__popc(peers));
       }
       __syncthreads();
+      // direction counts of this chunk, for the one-pass order update
+      if (P.chunk_count && tid < 10) {
+        const uint32_t v = s_cnt[tid];
+        P.chunk_count[((size_t)(base / CH + t) + c0 / CH) * 10 + tid] = v - cnt_prev;
+        cnt_prev = v;
+      }
       // 3c. coalesced write-back of the chunk
 #pragma unroll
       for (int k = 0; k < PER_THREAD; ++k) {
@@ -919,10 +926,12 @@ cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
   // log-spherical: chunk 1024, two CTAs per SM (more registers per thread
   // for the transcendental move)
   if (c.coord == 1) return launch_2d_tiles<TX, TY, 1024, 2, true>(c, P);
-  if (c.params.chunk == 2048) return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
-  if (c.params.chunk == 1024) return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
-  if (c.params.chunk == 256) return launch_2d_tiles<TX, TY, 256, 4>(c, P);
-  return launch_2d_tiles<TX, TY, 512, 4>(c, P);
+  switch (chunk_of(c)) {
+    case 2048: return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
+    case 1024: return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
+    case 256: return launch_2d_tiles<TX, TY, 256, 4>(c, P);
+    default: return launch_2d_tiles<TX, TY, 512, 4>(c, P);
+  }
 }
 
 // Largest |weight| over slots [0, n) (non-negative floats order like their
@@ -1005,6 +1014,9 @@ cudaError_t launch_batch_chunk(cudaStream_t stream, int num_sms, int chunk, bool
   if (chunk == 1024)
     return launch_batch_tiles<TX, TY, 1024, 3>(stream, num_sms, tma, do_rho, max_species, runs,
                                                base, nruns, total, queue);
+  if (chunk == 256)
+    return launch_batch_tiles<TX, TY, 256, 4>(stream, num_sms, tma, do_rho, max_species, runs,
+                                              base, nruns, total, queue);
   return launch_batch_tiles<TX, TY, 512, 4>(stream, num_sms, tma, do_rho, max_species, runs,
                                             base, nruns, total, queue);
 }

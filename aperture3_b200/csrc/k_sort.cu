@@ -128,14 +128,18 @@ __global__ void __launch_bounds__(kScatterThreads)
     k_order_scatter(int ntiles, const uint32_t *__restrict__ old_start,
                     const uint32_t *__restrict__ old_order, const uint8_t *__restrict__ dir,
                     const uint32_t *__restrict__ grp_off, uint32_t *__restrict__ new_order,
-                    uint32_t capacity, uint32_t slot0, DevStatus *status) {
+                    uint32_t capacity, uint32_t slot0, const uint32_t *__restrict__ tile_list,
+                    DevStatus *status) {
   constexpr int kWarps = kScatterThreads / 32;
   constexpr int kU = 4;  // 32-entry steps per batch of loads
   __shared__ uint32_t s_cnt[kWarps][10];
   __shared__ uint32_t s_base[kWarps][10];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t lt = (1u << lane) - 1u;
-  for (int s = blockIdx.x; s < ntiles; s += gridDim.x) {
+  // all tiles, or the count and indices in tile_list
+  const int nlist = tile_list ? (int)tile_list[0] : ntiles;
+  for (int li = blockIdx.x; li < nlist; li += gridDim.x) {
+    const int s = tile_list ? (int)tile_list[1 + li] : li;
     const uint32_t b = old_start[s], e = old_start[s + 1];
     const uint32_t n = e - b;
     const uint32_t seg = ((n + kWarps * 32 - 1) / (kWarps * 32)) * 32;
@@ -227,6 +231,90 @@ __global__ void __launch_bounds__(kScatterThreads)
             atomicAdd(&status->tile_faults, 1ull);
         }
       }
+    }
+    __syncthreads();
+  }
+}
+
+// One pass of the same stable placement, using the per-chunk direction
+// counts the push / deposit kernel recorded (chunk k of source tile s is
+// list entries [k CH, (k + 1) CH) of the tile, its counts at entry
+// old_start[s] / CH + s + k of chunk_count). The CTA turns them into the
+// group offset of every (chunk, direction); warp w then places chunks w,
+// w + 8, ... with the ballot / __match_any_sync ranking of pass 2 above.
+// Tiles of more than kMaxChunks chunks take the two-pass kernel.
+constexpr int kMaxChunks = 128;
+
+__global__ void __launch_bounds__(kScatterThreads)
+    k_order_scatter1(int ntiles, int ch, const uint32_t *__restrict__ old_start,
+                     const uint32_t *__restrict__ old_order, const uint8_t *__restrict__ dir,
+                     const uint32_t *__restrict__ chunk_count, const uint32_t *__restrict__ grp_off,
+                     uint32_t *__restrict__ new_order, uint32_t capacity, uint32_t slot0,
+                     uint32_t *__restrict__ big_tiles, DevStatus *status) {
+  constexpr int kWarps = kScatterThreads / 32;
+  constexpr int kU = 4;
+  __shared__ uint32_t s_cb[kMaxChunks][9];  // group offset of each (chunk, direction)
+  __shared__ uint32_t s_base[kWarps][9];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int s = blockIdx.x; s < ntiles; s += gridDim.x) {
+    const uint32_t b = old_start[s], e = old_start[s + 1];
+    const uint32_t n = e - b;
+    const int nch = (int)((n + ch - 1) / ch);
+    if (nch > kMaxChunks) {  // left to the two-pass kernel
+      if (tid == 0) big_tiles[1 + atomicAdd(big_tiles, 1u)] = (uint32_t)s;
+      continue;
+    }
+    const size_t c0 = (size_t)(b / ch) + s;
+    if (tid < 9) {
+      uint32_t run = grp_off[s * 9 + tid];
+      for (int k = 0; k < nch; ++k) {
+        s_cb[k][tid] = run;
+        run += chunk_count[(c0 + k) * 10 + tid];
+      }
+    }
+    __syncthreads();
+    for (int k = warp; k < nch; k += kWarps) {
+      if (lane < 9) s_base[warp][lane] = s_cb[k][lane];
+      __syncwarp();
+      uint32_t base4 = s_base[warp][4];
+      const uint32_t w0 = b + (uint32_t)k * ch, w1 = min(e, w0 + ch);
+      for (uint32_t q = w0; q < w1; q += 32 * kU) {
+        uint32_t d[kU], src[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const uint32_t p = q + 32 * u + lane;
+          d[u] = p < w1 ? dir[p] : 10u;
+          src[u] = p < w1 ? (old_order ? old_order[p] : slot0 + p) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          if (q + 32 * u >= w1) break;
+          const uint32_t dk = d[u];
+          const uint32_t stay = __ballot_sync(0xffffffffu, dk == 4u);
+          const uint32_t other = __ballot_sync(0xffffffffu, dk < 9u && dk != 4u);
+          uint32_t dst = 0xffffffffu;
+          if (dk == 4u) dst = base4 + __popc(stay & lt);
+          base4 += __popc(stay);
+          if (other) {
+            if ((other >> lane) & 1u) {
+              const uint32_t peers = __match_any_sync(other, dk);
+              const uint32_t bs = s_base[warp][dk];
+              dst = bs + __popc(peers & lt);
+              __syncwarp(other);
+              if ((peers & lt) == 0u) s_base[warp][dk] = bs + __popc(peers);
+            }
+            __syncwarp();
+          }
+          if (dst != 0xffffffffu) {
+            if (dst < capacity)
+              new_order[dst] = src[u];
+            else
+              atomicAdd(&status->tile_faults, 1ull);
+          }
+        }
+      }
+      __syncwarp();
     }
     __syncthreads();
   }
@@ -424,10 +512,24 @@ cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start, const uint32
                                  const uint8_t *dir, const uint32_t *grp_off,
                                  uint32_t *new_order, uint32_t slot0) {
   int grid = c.tiles.ntiles < c.num_sms * 8 ? c.tiles.ntiles : c.num_sms * 8;
-  k_order_scatter<<<grid, kScatterThreads, 0, c.stream>>>(c.tiles.ntiles, old_start, old_order,
-                                                          dir, grp_off, new_order,
-                                                          (uint32_t)c.order_cap, slot0, c.status);
-  c.launches++;
+  if (!c.chunk_count_ok) {
+    k_order_scatter<<<grid, kScatterThreads, 0, c.stream>>>(
+        c.tiles.ntiles, old_start, old_order, dir, grp_off, new_order, (uint32_t)c.order_cap,
+        slot0, nullptr, c.status);
+    c.launches++;
+    return cudaGetLastError();
+  }
+  // one pass from the push / deposit kernel's chunk counts; tiles of more
+  // than kMaxChunks chunks are listed in big_tiles for the two-pass kernel
+  cudaError_t e = cudaMemsetAsync(c.big_tiles, 0, sizeof(uint32_t), c.stream);
+  if (e != cudaSuccess) return e;
+  k_order_scatter1<<<grid, kScatterThreads, 0, c.stream>>>(
+      c.tiles.ntiles, chunk_of(c), old_start, old_order, dir, c.chunk_count, grp_off, new_order,
+      (uint32_t)c.order_cap, slot0, c.big_tiles, c.status);
+  k_order_scatter<<<c.num_sms, kScatterThreads, 0, c.stream>>>(
+      c.tiles.ntiles, old_start, old_order, dir, grp_off, new_order, (uint32_t)c.order_cap,
+      slot0, c.big_tiles, c.status);
+  c.launches += 2;
   return cudaGetLastError();
 }
 

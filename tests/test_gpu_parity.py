@@ -143,6 +143,36 @@ def test_2d_tile_order_is_stable_counting_sort():
         order = order_ref
 
 
+@pytest.mark.parametrize("chunk", [0, 256])
+def test_2d_tile_order_with_crowded_tiles(chunk):
+    """The one-pass order update (chunk counts from the push / deposit) and
+    its two-pass fallback for tiles of more than 128 staged chunks give the
+    stable counting sort: one of the 3 x 3 tiles holds 70,000 particles."""
+    tile = (16, 16)
+    n_bg, n_crowd = 9 * 4000, 70000
+    pr = _setup((48, 48), n_bg + n_crowd, seed=13, tile=tile, chunk=chunk)
+    m = pr.m
+    rng = np.random.default_rng(14)
+    g0, g1 = m.guard[0], m.guard[1]
+    c1 = rng.integers(g0 + 16, g0 + 32, n_crowd)
+    c2 = rng.integers(g1 + 16, g1 + 32, n_crowd)
+    pr.p["cell"][n_bg:] = (c1 + c2 * m.dims[0]).astype(np.uint32)
+    pr.data.set_particles(pr.p)
+    cells0 = pr.p["cell"]
+    keys = np.array([oracle.tile_key(m, tile, int(c)) for c in cells0], np.uint32)
+    nt = oracle.tile_key(m, tile, oracle.MAX_CELL)
+    order = oracle.stable_counting_sort(keys, nt + 1)
+    order = order[keys[order] < nt]
+    for step in range(3):
+        pr.both_update_particles(step)
+        order_ref, start_ref = oracle.tile_order(m, tile, pr.p["cell"], order)
+        order_gpu, start_gpu = pr.data.tile_order()
+        assert_bits(start_gpu, start_ref, f"tile_start step {step}")
+        assert_bits(order_gpu, order_ref, f"tile order step {step}")
+        order = order_ref
+        pr.check_particles()
+
+
 def test_1d_push_deposit_bitexact():
     params = make_params((512,), periodic=(True,), capacity=4096)
     m = oracle.make_mesh(params.N, params.guard, size=params.size)
