@@ -155,6 +155,7 @@ SIGNATURES = {
     "ap_logsph_inject": (_i, [_vp, _i, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                               C.c_uint64]),
     "ap_batch_create": (_i, [C.POINTER(_vp), _i, C.POINTER(_vp)]),
+    "ap_batch_set_capture": (_i, [_vp, _i]),
     "ap_batch_destroy": (_i, [_vp]),
     "ap_batch_add": (_i, [_vp, _vp]),
     "ap_batch_remove": (_i, [_vp, _vp]),

@@ -67,6 +67,10 @@ struct ap_batch {
   };
   Slot ring[8];
   int ring_next = 0;
+  // graph capture (ap_batch_set_capture): every staging copy comes from its
+  // own host / device block, kept until the mode is turned off
+  bool capture = false;
+  std::vector<unsigned char *> arena_h, arena_d;
   // autotuning: time the push / deposit per class when set
   bool tuning = false;
   std::vector<int> tune_class;   // class of each run
@@ -76,8 +80,16 @@ struct ap_batch {
 
 namespace {
 
+void free_arena(ap_batch *b) {
+  for (unsigned char *h : b->arena_h) cudaFreeHost(h);
+  for (unsigned char *d : b->arena_d) cudaFree(d);
+  b->arena_h.clear();
+  b->arena_d.clear();
+}
+
 void release(ap_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
+  free_arena(b);
   for (int i = 0; i < 2; ++i) {
     if (b->h_stage[i]) cudaFreeHost(b->h_stage[i]);
     if (b->stage_ev[i]) cudaEventDestroy(b->stage_ev[i]);
@@ -135,7 +147,25 @@ int fail_cuda(cudaError_t e) {
 
 // Copies `bytes` from src to a device staging slot, in stream order; the
 // slot's host buffer is reused only after its previous copy completed.
+// A host / device block pair of the capture arena.
+int arena_block(ap_batch *b, size_t bytes, unsigned char **h, unsigned char **d) {
+  *h = *d = nullptr;
+  B_TRY(cudaMallocHost(reinterpret_cast<void **>(h), bytes));
+  b->arena_h.push_back(*h);
+  B_TRY(cudaMalloc(reinterpret_cast<void **>(d), bytes));
+  b->arena_d.push_back(*d);
+  return AP_OK;
+}
+
 int stage(ap_batch *b, const void *src, size_t bytes, const unsigned char **dptr) {
+  if (b->capture) {
+    unsigned char *h, *d;
+    B_TRY_ST(arena_block(b, bytes, &h, &d));
+    std::memcpy(h, src, bytes);
+    B_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, b->stream));
+    *dptr = d;
+    return AP_OK;
+  }
   auto &s = b->ring[b->ring_next];
   b->ring_next = (b->ring_next + 1) % 8;
   if (!s.ev) B_TRY(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
@@ -187,11 +217,17 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
                   const std::vector<PushDepositParams> &P, bool do_rho) {
   if (gs.empty()) return AP_OK;
   const int s = b->slot;
-  b->slot ^= 1;
-  B_TRY(cudaEventSynchronize(b->stage_ev[s]));  // the copy that last used this slot is done
-  RunDesc *hd = reinterpret_cast<RunDesc *>(b->h_stage[s]);
   const size_t nr = b->cap_runs;
-  uint32_t *hbase = reinterpret_cast<uint32_t *>(b->h_stage[s] + sizeof(RunDesc) * nr);
+  unsigned char *hblk = nullptr, *dblk = b->d_stage;
+  if (b->capture) {
+    B_TRY_ST(arena_block(b, b->stage_bytes, &hblk, &dblk));
+  } else {
+    b->slot ^= 1;
+    B_TRY(cudaEventSynchronize(b->stage_ev[s]));  // the copy that last used this slot is done
+    hblk = b->h_stage[s];
+  }
+  RunDesc *hd = reinterpret_cast<RunDesc *>(hblk);
+  uint32_t *hbase = reinterpret_cast<uint32_t *>(hblk + sizeof(RunDesc) * nr);
   size_t k = 0, kb = 0;
   std::vector<size_t> desc_off, base_off;
   std::vector<uint32_t> totals;
@@ -213,13 +249,12 @@ int launch_groups(ap_batch *b, const std::vector<Group> &gs,
     totals.push_back(total);
     max_sp.push_back(msp);
   }
-  B_TRY(cudaMemcpyAsync(b->d_stage, b->h_stage[s], sizeof(RunDesc) * k, cudaMemcpyHostToDevice,
-                        b->stream));
-  B_TRY(cudaMemcpyAsync(b->d_stage + sizeof(RunDesc) * nr, b->h_stage[s] + sizeof(RunDesc) * nr,
+  B_TRY(cudaMemcpyAsync(dblk, hblk, sizeof(RunDesc) * k, cudaMemcpyHostToDevice, b->stream));
+  B_TRY(cudaMemcpyAsync(dblk + sizeof(RunDesc) * nr, hblk + sizeof(RunDesc) * nr,
                         sizeof(uint32_t) * kb, cudaMemcpyHostToDevice, b->stream));
-  B_TRY(cudaEventRecord(b->stage_ev[s], b->stream));
-  const RunDesc *dd = reinterpret_cast<const RunDesc *>(b->d_stage);
-  const uint32_t *db = reinterpret_cast<const uint32_t *>(b->d_stage + sizeof(RunDesc) * nr);
+  if (!b->capture) B_TRY(cudaEventRecord(b->stage_ev[s], b->stream));
+  const RunDesc *dd = reinterpret_cast<const RunDesc *>(dblk);
+  const uint32_t *db = reinterpret_cast<const uint32_t *>(dblk + sizeof(RunDesc) * nr);
   for (size_t gi = 0; gi < gs.size(); ++gi) {
     const Group &g = gs[gi];
     if (g.dim == 1)
@@ -417,6 +452,18 @@ AP_API int ap_batch_set_stream(ap_batch *b, void *stream) {
   b->stream = static_cast<cudaStream_t>(stream);
   for (Ctx *c : b->runs) ap_set_stream(static_cast<ap_ctx *>(c), b->stream);
   for (int i = 0; i < 2; ++i) B_TRY(cudaEventRecord(b->stage_ev[i], b->stream));
+  return AP_OK;
+}
+
+AP_API int ap_batch_set_capture(ap_batch *b, int on) {
+  if (!b) return AP_ERR_INVALID;
+  if (on) {
+    b->capture = true;
+    return AP_OK;
+  }
+  B_TRY(cudaStreamSynchronize(b->stream));
+  free_arena(b);
+  b->capture = false;
   return AP_OK;
 }
 

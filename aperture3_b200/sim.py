@@ -517,6 +517,10 @@ class Batch:
         vals = [int(steps)] * len(self.runs) if np.isscalar(steps) else [int(x) for x in steps]
         return (C.c_uint32 * len(self.runs))(*vals)
 
+    def set_capture(self, on: bool):
+        """Graph-capture mode (ap_batch_set_capture)."""
+        check(self._lib.ap_batch_set_capture(self.handle, int(bool(on))), "ap_batch_set_capture")
+
     def set_stream(self, stream: torch.cuda.Stream):
         check(self._lib.ap_batch_set_stream(self.handle, C.c_void_p(stream.cuda_stream)),
               "ap_batch_set_stream")

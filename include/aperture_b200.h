@@ -328,6 +328,18 @@ AP_API int ap_batch_sort_by_cell(ap_batch *batch);
 /* Waits for the batch and returns the first non-OK device status of a run
  * (run index in *failed_run, -1 if none; may be NULL). */
 AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
+/* Graph capture. While on, every batched call stages its launch
+ * descriptors in host / device blocks of its own, kept until the mode is
+ * turned off, and waits for nothing on the host, so that a sequence of
+ * ap_batch_update_particles / _update_fields / _inject_pairs calls can be
+ * captured into a CUDA graph on the batch's stream (stream capture in
+ * relaxed mode; the first step after adding runs or changing tile shapes
+ * allocates, so run it before capturing) and the graph replayed. The host
+ * side of the captured calls runs once, at capture: a replay repeats those
+ * steps' parameters, so capture whole cycles (an even number of steps;
+ * compaction intervals and charge-deposition steps that repeat). Turning
+ * the mode off (after the graphs are destroyed) frees the blocks. */
+AP_API int ap_batch_set_capture(ap_batch *batch, int on);
 /* Project autotuner: advances the batch by *steps_used complete steps
  * (particle update, then field update) starting at steps[r], timing the
  * push / deposit of each class of runs (same grid size) over three steps
