@@ -128,6 +128,7 @@ SIGNATURES = {
     "ap_get_number": (_i, [_vp, C.POINTER(C.c_size_t)]),
     "ap_get_slot_range": (_i, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "ap_diagnostics_async": (_i, [_vp, _vp]),
+    "ap_selftest_wait_timeout": (_i, [_vp]),
     "ap_update_particles": (_i, [_vp, C.c_double, C.c_uint32]),
     "ap_smooth_current": (_i, [_vp, C.c_uint32]),
     "ap_smooth_array": (_i, [_vp, ApArray]),

@@ -921,6 +921,13 @@ AP_API int ap_diagnostics_async(ap_ctx *c, double *host_out) {
   return AP_OK;
 }
 
+AP_API int ap_selftest_wait_timeout(ap_ctx *c) {
+  if (!c) return AP_ERR_INVALID;
+  AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  AP_TRY(launch_selftest_wait(*c, 1u << 12));
+  return check_status(c);
+}
+
 AP_API int ap_set_profiling(ap_ctx *c, int on) {
   if (!c) return AP_ERR_INVALID;
   c->profiling = on != 0;

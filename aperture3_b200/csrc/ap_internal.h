@@ -288,6 +288,7 @@ struct Ctx {
 // --- launchers (defined in the .cu files) ---
 cudaError_t launch_push_deposit_2d(Ctx &c, const PushDepositParams &P);
 cudaError_t launch_push_deposit_1d(Ctx &c, const PushDepositParams &P);
+cudaError_t launch_selftest_wait(Ctx &c, uint32_t limit);
 cudaError_t launch_tile_scan(Ctx &c, const uint32_t *dir_count,
                              uint32_t *new_start, uint32_t *grp_off);
 // old_order null: the particle at list position p sits in slot slot0 + p.

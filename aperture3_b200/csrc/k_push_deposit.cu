@@ -60,9 +60,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 }
 
 // Bounded wait on an mbarrier phase; returns false when the limit is hit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          uint32_t limit = kMbarSpinLimit) {
   uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < kMbarSpinLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -670,6 +671,19 @@ __global__ void __launch_bounds__(kThreads2D, MINB)
 }
 
 // ---------------------------------------------------------------------------
+// Self-test of the bounded wait: an mbarrier that announces bytes no copy
+// will bring is waited on with the field-tile wait above; the give-up is
+// recorded as a timeout in the status word. No asynchronous copy is
+// issued, so nothing is left in flight when the kernel returns.
+__global__ void k_selftest_wait(DevStatus *status, uint32_t limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, 64u);
+    if (!mbar_wait(&bar, 0u, limit)) atomicAdd(&status->timeouts, 1ull);
+  }
+}
+
 // 1D: the whole line is small, so each CTA takes a contiguous chunk of
 // particle slots, finds the cell range it touches, and deposits into a
 // shared-memory window over that range (or straight to the global
@@ -1050,6 +1064,12 @@ cudaError_t launch_push_deposit_1d_batch(cudaStream_t stream, int num_sms, bool 
     k_push_deposit_1d_batch<true><<<grid, kThreads1D, 0, stream>>>(runs, base, nruns);
   else
     k_push_deposit_1d_batch<false><<<grid, kThreads1D, 0, stream>>>(runs, base, nruns);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_selftest_wait(Ctx &c, uint32_t limit) {
+  k_selftest_wait<<<1, 32, 0, c.stream>>>(c.status, limit);
+  c.launches++;
   return cudaGetLastError();
 }
 

@@ -680,16 +680,18 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
 
     names = [k for k, _ in PTC_FIELDS]
     # the initial state of the end-to-end run: the current particles, sorted
-    # by cell into slots [0, n) (the periodic box loses none)
+    # by cell into one contiguous slot range (the lower or the upper half of
+    # the doubled capacity; the periodic box loses none)
     data.sort_particles()
-    if data.number != n:
-        raise RuntimeError(f"expected {n} particles after the sort, found {data.number}")
+    s0, s1 = data.slot_range()
+    if s1 - s0 != n:
+        raise RuntimeError(f"expected {n} particles after the sort, found {s1 - s0}")
     host = {k: torch.empty_like(data.particles[k][:n], device="cpu").pin_memory() for k in names}
     fhost = {k: [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in getattr(data, k)]
              for k in ("E", "B", "J")}
     with torch.cuda.stream(stream):
         for k in names:
-            host[k].copy_(data.particles[k][:n], non_blocking=True)
+            host[k].copy_(data.particles[k][s0:s1], non_blocking=True)
         for k in fhost:
             for h, a in zip(fhost[k], getattr(data, k)):
                 h.copy_(a, non_blocking=True)

@@ -216,6 +216,11 @@ AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
  * whose particle count moved on the device (pair injection) must be synced
  * first. */
 AP_API int ap_diagnostics_async(ap_ctx *ctx, double *host_out);
+/* Failure-detection self-test: waits, with the bounded wait the 2D kernel
+ * uses for its field tiles and a short limit, on a barrier that nothing
+ * completes, and returns the status the give-up produces (AP_ERR_TIMEOUT).
+ * Nothing is left running; the context stays usable. */
+AP_API int ap_selftest_wait_timeout(ap_ctx *ctx);
 
 /* ---------------------------------------------------------------------
  * Log-spherical (ln r, theta) grids: ptc_updater_logsph and

@@ -367,6 +367,19 @@ def test_moved_far_is_reported():
     assert e.value.status == 4
 
 
+def test_bounded_wait_timeout_is_reported_and_context_survives():
+    """A device-side wait that nothing completes gives up after its limit and
+    comes back as AP_ERR_TIMEOUT; the same context then steps bit-exactly."""
+    pr = _setup((32, 32), 800, seed=15, tile=(8, 8))
+    st = pr.env._lib.ap_selftest_wait_timeout(pr.env.ctx)
+    assert st == 6
+    assert pr.env._lib.ap_last_error(pr.env.ctx) == 6
+    for step in range(2):
+        pr.both_update_particles(step)
+        pr.check_particles()
+        pr.check_current(J_TOL, rho=True)
+
+
 def test_continuity_residual():
     """Esirkepov charge conservation through the ABI: rho(t+1) - rho(t) +
     div J = 0 on the bulk, within 1e-6 of max|rho|."""
