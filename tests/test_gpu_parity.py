@@ -252,10 +252,9 @@ def test_sort_by_cell_bitexact():
 
 @pytest.mark.parametrize("tile,crowd", [((8, 8), 0), ((16, 16), 0), ((16, 8), 5000)])
 def test_sort_by_cell_after_updates_bitexact(tile, crowd):
-    """sort_by_cell right after updates (the tile-local path: per-tile cell
-    histograms, ranks by slot within each cell, one gather) gives the
-    oracle's stable sort slot for slot; a cell holding more than 4096
-    particles (crowd) takes the radix path, with the same result."""
+    """sort_by_cell right after updates (stable radix sort of the cell keys,
+    one gather per member) gives the oracle's stable sort slot for slot,
+    also with one cell holding `crowd` more particles than the rest."""
     pr = _setup((64, 48), 12000, seed=21, tile=tile, capacity=12000 + crowd)
     if crowd:
         # `crowd` more particles at rest in one cell
