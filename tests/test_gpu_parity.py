@@ -282,6 +282,43 @@ def test_sort_by_cell_after_updates_bitexact(tile, crowd):
     pr.check_particles()
 
 
+@pytest.mark.parametrize("N,tile,crowd,spare", [
+    ((64, 48), (8, 8), 0, 2), ((64, 48), (16, 8), 0, 2), ((64, 64), (16, 16), 3000, 2),
+    ((128, 64), (32, 16), 0, 2), ((64, 48), (8, 8), 0, 1)])
+def test_sort_by_cell_is_stable_sort_of_the_store(N, tile, crowd, spare):
+    """After compacting updates, sort_by_cell gives, slot for slot and for
+    every member, the stable sort by cell of the slots it started from (into
+    the free half with spare 2, back into slots [0, live) with spare 1),
+    also with one cell holding `crowd` more particles."""
+    n = N[0] * N[1] * 6
+    pr = _setup(N, n, seed=31, tile=tile, capacity=spare * (n + crowd))
+    if crowd:
+        rng = np.random.default_rng(4)
+        extra = random_particles(pr.m, crowd, rng, gamma_max=1.0)
+        extra["cell"][:] = pr.p["cell"][0]
+        for k in ("p1", "p2", "p3"):
+            extra[k][:] = 0
+        extra["id"][:] = np.arange(n, n + crowd, dtype=np.uint64)
+        pr.p = {k: np.concatenate([pr.p[k], extra[k]]) for k in pr.p}
+        pr.data.set_particles(pr.p)
+    pr.env.set_compaction(2)
+    for step in range(3):
+        pr.pusher.update_particles(pr.data, pr.dt, step)
+    first, end = pr.data.slot_range()
+    seg = {k: v[first:end].copy() for k, v in pr.data.particles_host().items()}
+    live = np.flatnonzero(seg["cell"] != oracle.MAX_CELL)
+    order = live[np.argsort(seg["cell"][live], kind="stable")]
+    pr.data.sort_particles()
+    f2, e2 = pr.data.slot_range()
+    assert e2 - f2 == len(order) and (spare == 1 or f2 != first)
+    got = {k: v[f2:e2] for k, v in pr.data.particles_host().items()}
+    for k in PTC_KEYS:
+        assert_bits(got[k], seg[k][order], f"sorted {k}")
+    # the tile order after the sort covers exactly the sorted slots
+    o, _ = pr.data.tile_order()
+    assert np.array_equal(np.sort(o), np.arange(f2, e2, dtype=np.uint32))
+
+
 def test_tile_order_after_sort_by_cell():
     """sort_by_cell leaves the tile order equal to a stable counting sort by
     tile of the cell-sorted slots, and the next steps stay bit-exact."""
