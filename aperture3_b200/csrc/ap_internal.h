@@ -350,7 +350,7 @@ MeshK make_meshk(const ap_mesh &m);
 inline int chunk_of(const Ctx &c) {
   if (c.coord == 1) return 1024;
   const int ch = c.params.chunk;
-  return (ch == 256 || ch == 1024 || ch == 2048) ? ch : 512;
+  return (ch == 512 || ch == 1024 || ch == 2048) ? ch : 256;
 }
 
 // The update of one context in three parts (ap_api.cu): prepare (zeroing,

@@ -156,8 +156,11 @@ struct TileGeom {
   static constexpr int HDR = 128;     // mbarrier, tile id, abort flag, counters
   static constexpr size_t stage_bytes() { return 10 * 4 * SP + 2 * SP; }
   static constexpr int NBUF = pipelined<CH>() ? 2 : 1;
+  // double-buffered chunks: the order indices of the next two chunks
+  static constexpr size_t order_bytes() { return NBUF == 2 ? 2 * 4 * CH : 0; }
   static size_t smem_bytes(int nrho, bool ls = false) {
-    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + NBUF * stage_bytes() + (ls ? 4 * JSZ : 0);
+    return HDR + 4 * 6 * FSZ + 8 * (3 + nrho) * JSZ + NBUF * stage_bytes() + (ls ? 4 * JSZ : 0) +
+           order_bytes();
   }
 };
 
@@ -248,6 +251,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     // log-spherical: cell volumes over the J tile window
     float *s_dv = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(st) +
                                             G::NBUF * G::stage_bytes());
+    uint32_t *s_ord = reinterpret_cast<uint32_t *>(s_dv + (kLS ? G::JSZ : 0));
     const int dims0 = P.m.dims[0], dims1 = P.m.dims[1];
     const int g0 = P.m.guard[0], g1 = P.m.guard[1];
     const int nacc = ncomp * G::JSZ;
@@ -262,6 +266,22 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     const int x0 = g0 + tix * TX, y0 = g1 + tiy * TY;
     const int xs = (x0 - 1) & ~3, ys = y0 - 1;
     const int jx0 = x0 - 2, jy0 = y0 - 2;
+
+    // the tile's particle list; with double-buffered chunks the order
+    // indices run two chunks ahead (slot (chunk index) & 1 of s_ord), so
+    // the gathers of the next chunk never wait for them
+    const uint32_t base = P.tile_start[t];
+    const int n_t = (int)(P.tile_start[t + 1] - base);
+    auto prefetch_order = [&](int c0) {
+      uint32_t *dst = s_ord + ((c0 / CH) & 1) * CH;
+      const int nch = min(CH, n_t - c0);
+      for (int e = tid; e < nch; e += kThreads2D) cp_async4(dst + e, P.order + base + c0 + e);
+      cp_async_commit();
+    };
+    if (G::NBUF == 2) {
+      if (n_t > 0) prefetch_order(0);
+      if (CH < n_t) prefetch_order(CH);
+    }
 
     // 1. field tile
     if (kTMA) {
@@ -294,6 +314,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     if (kTMA) {
       if (!mbar_wait(mbar, phase)) atomicExch(s_abort, 1);
     }
+    cp_async_wait_group<0>();
     __syncthreads();
     if (*s_abort) {
       if (tid == 0) {
@@ -304,8 +325,6 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     }
 
     // 3. particles of this tile, CH at a time
-    const uint32_t base = P.tile_start[t];
-    const int n_t = (int)(P.tile_start[t + 1] - base);
     constexpr int kStageFloats = (int)(G::stage_bytes() / 4);
     // 3a. coalesced asynchronous load of the chunk at c0 into buffer b
     auto issue = [&](int c0, int b) {
@@ -316,7 +335,8 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
         const int e = tid + k * kThreads2D;
         if (e < nch) {
           const int s = spos(e);
-          const uint32_t idx = P.order[base + c0 + e];
+          const uint32_t idx =
+              G::NBUF == 2 ? s_ord[((c0 / CH) & 1) * CH + e] : P.order[base + c0 + e];
           reinterpret_cast<uint32_t *>(sb + 9 * SP)[s] = idx;
           cp_async4(sb + 7 * SP + s, P.p.cell + idx);
           cp_async4(sb + 8 * SP + s, P.p.flag + idx);
@@ -333,21 +353,23 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
     };
     int buf = 0;
     uint32_t cnt_prev = 0;  // threads < 10: the tile's direction count so far
-    if (G::NBUF == 2 && n_t > 0) issue(0, 0);
+    if (G::NBUF == 2 && n_t > 0) {
+      issue(0, 0);
+      cp_async_wait_group<0>();
+      __syncthreads();
+    }
     for (int c0 = 0; c0 < n_t; c0 += CH) {
       const int nch = min(CH, n_t - c0);
       if (G::NBUF == 2) {
-        if (c0 + CH < n_t) {
-          issue(c0 + CH, buf ^ 1);
-          cp_async_wait_group<1>();
-        } else {
-          cp_async_wait_group<0>();
-        }
+        // this chunk landed at the end of the previous one; start the next
+        // chunk's gathers and the order indices of the one after
+        if (c0 + CH < n_t) issue(c0 + CH, buf ^ 1);
+        if (c0 + 2 * CH < n_t) prefetch_order(c0 + 2 * CH);
       } else {
         issue(c0, 0);
         cp_async_wait_group<0>();
+        __syncthreads();
       }
-      __syncthreads();
       float *stc = st + buf * kStageFloats;
       float *s_x1 = stc, *s_x2 = stc + SP, *s_x3 = stc + 2 * SP;
       float *s_p1 = stc + 3 * SP, *s_p2 = stc + 4 * SP, *s_p3 = stc + 5 * SP;
@@ -634,6 +656,7 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
           P.dir[base + c0 + e] = s_dir[s];
         }
       }
+      if (G::NBUF == 2) cp_async_wait_group<0>();  // the next chunk and order indices
       __syncthreads();
       if (G::NBUF == 2) buf ^= 1;
     }
@@ -932,9 +955,11 @@ cudaError_t launch_2d_tiles(Ctx &c, const PushDepositParams &P) {
                   : run(k_push_deposit_2d<TX, TY, CH, MINB, false, false, kLS>);
 }
 
-// Staged chunk of 512 particles with four CTAs per SM (default: 64
-// registers, no spills; measured 6% faster than 1024 with three CTAs on the
-// 1024^2 box), 256 double-buffered with four, 1024 with three, 2048 with two.
+// Staged chunks of 256 particles, double-buffered, with four CTAs per SM
+// (default: 64 registers, no spills; the order indices run two chunks ahead
+// and the gathers one chunk ahead, so no global load is waited on inside a
+// tile; measured 3 % faster than 512 single-buffered on the 1024^2 box),
+// 512 single-buffered with four, 1024 with three, 2048 with two.
 template <int TX, int TY>
 cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
   // log-spherical: chunk 1024, two CTAs per SM (more registers per thread
@@ -943,8 +968,8 @@ cudaError_t launch_2d_chunk(Ctx &c, const PushDepositParams &P) {
   switch (chunk_of(c)) {
     case 2048: return launch_2d_tiles<TX, TY, 2048, 2>(c, P);
     case 1024: return launch_2d_tiles<TX, TY, 1024, 3>(c, P);
-    case 256: return launch_2d_tiles<TX, TY, 256, 4>(c, P);
-    default: return launch_2d_tiles<TX, TY, 512, 4>(c, P);
+    case 512: return launch_2d_tiles<TX, TY, 512, 4>(c, P);
+    default: return launch_2d_tiles<TX, TY, 256, 4>(c, P);
   }
 }
 
@@ -1028,10 +1053,10 @@ cudaError_t launch_batch_chunk(cudaStream_t stream, int num_sms, int chunk, bool
   if (chunk == 1024)
     return launch_batch_tiles<TX, TY, 1024, 3>(stream, num_sms, tma, do_rho, max_species, runs,
                                                base, nruns, total, queue);
-  if (chunk == 256)
-    return launch_batch_tiles<TX, TY, 256, 4>(stream, num_sms, tma, do_rho, max_species, runs,
+  if (chunk == 512)
+    return launch_batch_tiles<TX, TY, 512, 4>(stream, num_sms, tma, do_rho, max_species, runs,
                                               base, nruns, total, queue);
-  return launch_batch_tiles<TX, TY, 512, 4>(stream, num_sms, tma, do_rho, max_species, runs,
+  return launch_batch_tiles<TX, TY, 256, 4>(stream, num_sms, tma, do_rho, max_species, runs,
                                             base, nruns, total, queue);
 }
 
