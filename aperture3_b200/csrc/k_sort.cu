@@ -266,11 +266,18 @@ __global__ void __launch_bounds__(kScatterThreads)
       continue;
     }
     const size_t c0 = (size_t)(b / ch) + s;
+    // the tile's chunk counts, loaded by all threads, then scanned per
+    // direction in shared memory
+    for (int i = tid; i < nch * 9; i += kScatterThreads)
+      s_cb[i / 9][i % 9] = chunk_count[(c0 + i / 9) * 10 + i % 9];
+    const uint32_t off = tid < 9 ? grp_off[s * 9 + tid] : 0u;
+    __syncthreads();
     if (tid < 9) {
-      uint32_t run = grp_off[s * 9 + tid];
+      uint32_t run = off;
       for (int k = 0; k < nch; ++k) {
+        const uint32_t v = s_cb[k][tid];
         s_cb[k][tid] = run;
-        run += chunk_count[(c0 + k) * 10 + tid];
+        run += v;
       }
     }
     __syncthreads();
