@@ -264,8 +264,28 @@ class SimData:
         self.particles: Dict[str, torch.Tensor] = {
             name: torch.zeros(max(cap, 1), dtype=dt, device=dev) for name, dt in PTC_FIELDS}
         self.particles["cell"].fill_(-1)  # MAX_CELL
+        self._number_stale = False
         self.number = 0
         self._bind()
+
+    @property
+    def number(self) -> int:
+        """Particle count (slots [0, number) or the occupied slot range's
+        end). After a batched step that may have changed it on the device it
+        is read back on first use."""
+        if self._number_stale:
+            self.refresh_number()
+        return self._number
+
+    @number.setter
+    def number(self, n: int):
+        self._number = int(n)
+        self._number_stale = False
+
+    def mark_number_stale(self):
+        """The device-side count may have changed (batched pair injection or
+        sort); the next read of `number` fetches it."""
+        self._number_stale = True
 
     def _bind(self):
         f = ApFields()
@@ -365,8 +385,9 @@ class SimData:
 
     def sort_particles_async(self):
         """sort_by_cell without reading the new count back (1D runs with pair
-        injection keep it on the device)."""
+        injection keep it on the device; `number` fetches it on next use)."""
         check(self.env._lib.ap_sort_by_cell(self.env.ctx), "ap_sort_by_cell")
+        self.mark_number_stale()
 
     def inject_pairs(self, dt: float, step: int):
         """Pair injection after the particle update of `step` (see
@@ -538,17 +559,18 @@ class Batch:
               "ap_batch_update_fields")
 
     def inject_pairs(self, steps, dt=None):
-        """Pair injection of every run that has it enabled (one device
-        synchronisation); refreshes each run's particle number."""
+        """Pair injection of every run that has it enabled, without a host
+        synchronisation; each run's particle number is read back when it is
+        next used."""
         check(self._lib.ap_batch_inject_pairs(self.handle, self._dts(dt), self._steps(steps)),
               "ap_batch_inject_pairs")
         for d in self.runs:
-            d.refresh_number()
+            d.mark_number_stale()
 
     def sort_particles(self):
         check(self._lib.ap_batch_sort_by_cell(self.handle), "ap_batch_sort_by_cell")
         for d in self.runs:
-            d.refresh_number()
+            d.mark_number_stale()
 
     def sync(self):
         bad = C.c_int(-1)

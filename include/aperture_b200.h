@@ -400,7 +400,9 @@ AP_API int ap_get_pair_stats(ap_ctx *ctx, uint64_t *particle_steps, uint64_t *em
 AP_API int ap_inject_pairs(ap_ctx *ctx, double dt, uint32_t step, uint64_t *emitted,
                            uint64_t *dropped);
 /* The same for every run of a batch that has pair injection enabled (dt[r]
- * and steps[r] per run), with one synchronisation for the whole batch. */
+ * and steps[r] per run). 1D runs are served by three batched launches and
+ * no host synchronisation: their counts stay on the device until
+ * ap_get_number or another call that needs them reads them back. */
 AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32_t *steps);
 
 /* Device time per phase of the update, from CUDA events recorded on the
