@@ -729,6 +729,57 @@ __device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weigh
   return acc;
 }
 
+// Warp-collective deposit of one node into the 1D window (every lane of the
+// warp calls it; `act` lanes contribute a1 to J1 at window offset o + 1 and
+// a2, a3 to J2, J3 at o). In a cell-sorted run neighbouring lanes hold
+// particles of the same cell, so their atomics would all hit one address:
+// when the active lanes touch at most kAgg1D distinct offsets, each
+// offset's fixed-point words are summed across its lanes (integer sums, so
+// the result is the same bits) and one lane adds them.
+constexpr int kAgg1D = 4;
+
+__device__ __forceinline__ void deposit_1d_node(bool act, int o, float a1, float a2, float a3,
+                                                int *hi, unsigned *lo, int win_comp,
+                                                float scale, int L) {
+  if (__ballot_sync(0xffffffffu, act) == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned mask = (1u << L) - 1u;
+  unsigned h[3], l[3];
+  const float a[3] = {a1, a2, a3};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const long long X = act ? __float2ll_rn(a[c] * scale) : 0ll;  // exact scaling
+    h[c] = (unsigned)(int)(X >> L);
+    l[c] = (unsigned)X & mask;
+  }
+  const int dst[3] = {o + 1, win_comp + o, 2 * win_comp + o};
+  const unsigned key = act ? (unsigned)o : (0x80000000u | (unsigned)lane);
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  const unsigned leaders = __ballot_sync(0xffffffffu, act && lane == __ffs(peers) - 1);
+  if (__popc(leaders) <= kAgg1D) {
+    for (unsigned m = leaders; m != 0u; m &= m - 1u) {
+      const int ld = __ffs(m) - 1;
+      const int ko = __shfl_sync(0xffffffffu, o, ld);  // every lane takes part
+      const bool in = act && o == ko;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const unsigned sh = __reduce_add_sync(0xffffffffu, in ? h[c] : 0u);
+        const unsigned sl = __reduce_add_sync(0xffffffffu, in ? l[c] : 0u);
+        if (lane == ld) {
+          atomicAdd(hi + dst[c], (int)sh);
+          atomicAdd(lo + dst[c], sl);
+        }
+      }
+    }
+  } else if (act) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      atomicAdd(hi + dst[c], (int)h[c]);
+      atomicAdd(lo + dst[c], l[c]);
+    }
+  }
+}
+
 // One chunk of kChunk1D particle slots of a 1D run: push, deposit into a
 // shared-memory window over the cells the chunk touches (or straight into
 // the global accumulators when the window would not fit), move.
@@ -778,27 +829,56 @@ __device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P
   const int wlen = s_hi - s_lo + 5;
   const bool use_smem = (s_lo <= s_hi) && wlen <= win_comp;
   if (use_smem)
-    for (int i = tid; i < ncomp * win_comp; i += kThreads1D) {
-      sWhi[i] = 0;
-      sWlo[i] = 0u;
+    for (int i = tid; i < ncomp * wlen; i += kThreads1D) {
+      const int si = (i / wlen) * win_comp + i % wlen;
+      sWhi[si] = 0;
+      sWlo[si] = 0u;
     }
   __syncthreads();
 
+  // The members of item k + 1 are loaded while item k is pushed and
+  // deposited (the items of one thread are distinct slots).
+  struct Item1D {
+    uint32_t flag;
+    float x1, x2, x3, p1, p2, p3, w;
+  };
+  auto load_item = [&](int k, Item1D &it) {
+    const uint32_t c = cells[k];
+    if (c == AP_MAX_CELL || (int)c < g0 || (int)c >= n0 - g0) return;
+    const size_t idx = first + (size_t)k * kThreads1D + tid;
+    it.flag = P.p.flag[idx];
+    it.x1 = P.p.x1[idx];
+    it.x2 = P.p.x2[idx];
+    it.x3 = P.p.x3[idx];
+    it.p1 = P.p.p1[idx];
+    it.p2 = P.p.p2[idx];
+    it.p3 = P.p.p3[idx];
+    it.w = P.p.w[idx];
+  };
+  Item1D cur{}, nxt{};
+  load_item(0, cur);
 #pragma unroll 1
   for (int k = 0; k < kItems1D; ++k) {
+    if (k + 1 < kItems1D) load_item(k + 1, nxt);
+    // deposit inputs of this item; the deposit runs after the item, with
+    // every lane of the warp present
+    bool dep = false;
+    float d_x1 = 0.0f, d_nx1 = 0.0f, d_w = 0.0f, d_v2 = 0.0f, d_v3 = 0.0f;
+    int d_c1 = 0, d_dc1 = 0, d_sp = 0;
+    do {  // one item; `break` skips to the next
     const size_t idx = first + (size_t)k * kThreads1D + tid;
     uint32_t c = cells[k];
-    if (c == AP_MAX_CELL) continue;
+    if (c == AP_MAX_CELL) break;
     if ((int)c < g0 || (int)c >= n0 - g0) {  // ptc_updater.cu:30-33
       P.p.cell[idx] = AP_MAX_CELL;
-      continue;
+      break;
     }
-    const uint32_t flag = P.p.flag[idx];
-    float x1 = P.p.x1[idx];
-    float p1 = P.p.p1[idx], p2 = P.p.p2[idx], p3 = P.p.p3[idx];
+    const uint32_t flag = cur.flag;
+    float x1 = cur.x1;
+    float p1 = cur.p1, p2 = cur.p2, p3 = cur.p3;
     if (p1 != p1 || p2 != p2 || p3 != p3) {
       atomicAdd(&P.status->nan_momenta, 1ull);
-      continue;
+      break;
     }
     const int sp = ptc_type(flag);
     const int c1 = (int)c;
@@ -821,8 +901,8 @@ __device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P
       gamma = P.p.E[idx];
     }
     // deposit_current_cart_1d (ptc_updater.cu:220-293)
-    const float w = P.p.w[idx];
-    const float x2 = P.p.x2[idx], x3 = P.p.x3[idx];
+    const float w = cur.w;
+    const float x2 = cur.x2, x3 = cur.x3;
     const float v1 = p1 / gamma, v2 = p2 / gamma, v3 = p3 / gamma;
     float nx1 = x1 + (v1 * P.dt) / P.m.delta[0];
     const int dc1 = (int)floorf(nx1);
@@ -832,28 +912,46 @@ __device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P
     P.p.x2[idx] = x2 + v2 * P.dt;
     P.p.x3[idx] = x3 + v3 * P.dt;
     if (!far && !(flag & kFlagIgnoreCurrent)) {
-      const float weight = P.charge[sp] * w;
-      const int i0 = (dc1 == -1 ? -2 : -1), i1 = (dc1 == 1 ? 1 : 0);
+      dep = true;
+      d_x1 = x1;
+      d_nx1 = nx1;
+      d_w = P.charge[sp] * w;
+      d_v2 = v2;
+      d_v3 = v3;
+      d_c1 = c1;
+      d_dc1 = dc1;
+      d_sp = sp;
+    }
+    int cn = c1 + dc1;
+    bool keep = !far && wrap_coord(cn, g0, n0, P.m.red[0], P.periodic[0]);
+    if (!keep) atomicAdd(far ? &P.status->moved_far : &P.status->lost, 1ull);
+    P.p.cell[idx] = keep ? (uint32_t)cn : AP_MAX_CELL;
+    } while (false);
+    {
+      const float weight = d_w;
+      const int i0 = (d_dc1 == -1 ? -2 : -1), i1 = (d_dc1 == 1 ? 1 : 0);
       float djx = 0.0f;
 #pragma unroll
       for (int i = -2; i <= 1; ++i) {
-        if (i < i0 || i > i1) continue;
-        const float sx0 = cic(-x1 + i + 1);
-        const float sx1 = cic(-nx1 + (i + 1 - dc1));
-        const int off = i + c1;
-        djx += sx1 - sx0;
-        const float a1 = -weight * djx;
-        const float val1 = 0.5f * (sx0 + sx1);
-        const float a2 = weight * v2 * val1;
-        const float a3 = weight * v3 * val1;
+        const bool act = dep && i >= i0 && i <= i1;
+        float sx1 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+        const int off = i + d_c1;
+        if (act) {
+          const float sx0 = cic(-d_x1 + i + 1);
+          sx1 = cic(-d_nx1 + (i + 1 - d_dc1));
+          djx += sx1 - sx0;
+          a1 = -weight * djx;
+          const float val1 = 0.5f * (sx0 + sx1);
+          a2 = weight * d_v2 * val1;
+          a3 = weight * d_v3 * val1;
+        }
         if (use_smem) {
-          const Acc32 W{sWhi, sWlo};
-          add_fixed(W, off + 1 - wlo, a1, fscale, fx.L);
-          add_fixed(W, win_comp + off - wlo, a2, fscale, fx.L);
-          add_fixed(W, 2 * win_comp + off - wlo, a3, fscale, fx.L);
-          if (kRho && P.do_rho && sp < P.num_species)
-            add_fixed(W, (3 + sp) * win_comp + off - wlo, weight * sx1, fscale, fx.L);
-        } else {
+          deposit_1d_node(act, off - wlo, a1, a2, a3, sWhi, sWlo, win_comp, fscale, fx.L);
+          if (act && kRho && P.do_rho && d_sp < P.num_species) {
+            const Acc32 W{sWhi, sWlo};
+            add_fixed(W, (3 + d_sp) * win_comp + off - wlo, weight * sx1, fscale, fx.L);
+          }
+        } else if (act) {
           auto gadd = [&](int k2, int x, float v) {
             atomicAdd(P.acc + k2 * P.acc_comp + x,
                       (unsigned long long)__float2ll_rn(v * fscale));
@@ -861,14 +959,11 @@ __device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P
           gadd(0, off + 1, a1);
           gadd(1, off, a2);
           gadd(2, off, a3);
-          if (kRho && P.do_rho && sp < P.num_species) gadd(3 + sp, off, weight * sx1);
+          if (kRho && P.do_rho && d_sp < P.num_species) gadd(3 + d_sp, off, weight * sx1);
         }
       }
     }
-    int cn = c1 + dc1;
-    bool keep = !far && wrap_coord(cn, g0, n0, P.m.red[0], P.periodic[0]);
-    if (!keep) atomicAdd(far ? &P.status->moved_far : &P.status->lost, 1ull);
-    P.p.cell[idx] = keep ? (uint32_t)cn : AP_MAX_CELL;
+    cur = nxt;
   }
   __syncthreads();
   if (use_smem) {
