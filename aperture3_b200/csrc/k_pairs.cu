@@ -52,14 +52,27 @@ __device__ __forceinline__ bool emit_test(const PairK &K, const PtcK &p, const u
 __device__ __forceinline__ void mark_chunk(const PairK &K, const PtcK &p, const uint64_t *ids,
                                            size_t number, uint32_t step, uint8_t *emit,
                                            uint32_t *chunk_count, uint32_t ch) {
-  int cnt = 0;
+  // the cells and gammas of all items are loaded first, so their latencies
+  // overlap; only the rare hot particles go on to the momentum and the draw
+  uint32_t cell[kPairPerThread];
+  float gam[kPairPerThread];
 #pragma unroll
   for (int k = 0; k < kPairPerThread; ++k) {
     const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
-    const bool e = idx < number && emit_test(K, p, ids, idx, step);
-    if (idx < number) emit[idx] = e ? 1 : 0;
-    cnt += __syncthreads_count(e);
+    cell[k] = idx < number ? p.cell[idx] : AP_MAX_CELL;
+    gam[k] = idx < number ? p.E[idx] : 0.0f;
   }
+  bool e[kPairPerThread];
+#pragma unroll
+  for (int k = 0; k < kPairPerThread; ++k) {
+    const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
+    e[k] = cell[k] != AP_MAX_CELL && gam[k] > K.gamma_thr &&
+           emit_test(K, p, ids, idx, step);
+    if (idx < number) emit[idx] = e[k] ? 1 : 0;
+  }
+  int cnt = 0;
+#pragma unroll
+  for (int k = 0; k < kPairPerThread; ++k) cnt += __syncthreads_count(e[k]);
   if (threadIdx.x == 0) chunk_count[ch] = (uint32_t)cnt;
 }
 
