@@ -733,15 +733,17 @@ __device__ __forceinline__ float interp_1d_global(const FieldArr &f, const Weigh
 // warp calls it; `act` lanes contribute a1 to J1 at window offset o + 1 and
 // a2, a3 to J2, J3 at o). In a cell-sorted run neighbouring lanes hold
 // particles of the same cell, so their atomics would all hit one address:
-// when the active lanes touch at most kAgg1D distinct offsets, each
-// offset's fixed-point words are summed across its lanes (integer sums, so
-// the result is the same bits) and one lane adds them.
+// when more than kAgg1D lanes are active but they touch at most kAgg1D
+// distinct offsets, each offset's fixed-point words are summed across its
+// lanes (integer sums, so the result is the same bits) and one lane adds
+// them; a few active lanes add directly.
 constexpr int kAgg1D = 4;
 
 __device__ __forceinline__ void deposit_1d_node(bool act, int o, float a1, float a2, float a3,
                                                 int *hi, unsigned *lo, int win_comp,
                                                 float scale, int L) {
-  if (__ballot_sync(0xffffffffu, act) == 0u) return;
+  const unsigned am = __ballot_sync(0xffffffffu, act);
+  if (am == 0u) return;
   const int lane = threadIdx.x & 31;
   const unsigned mask = (1u << L) - 1u;
   unsigned h[3], l[3];
@@ -753,6 +755,16 @@ __device__ __forceinline__ void deposit_1d_node(bool act, int o, float a1, float
     l[c] = (unsigned)X & mask;
   }
   const int dst[3] = {o + 1, win_comp + o, 2 * win_comp + o};
+  if (__popc(am) <= kAgg1D) {  // few lanes (the outer nodes of crossing particles): add directly
+    if (act) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        atomicAdd(hi + dst[c], (int)h[c]);
+        atomicAdd(lo + dst[c], l[c]);
+      }
+    }
+    return;
+  }
   const unsigned key = act ? (unsigned)o : (0x80000000u | (unsigned)lane);
   const unsigned peers = __match_any_sync(0xffffffffu, key);
   const unsigned leaders = __ballot_sync(0xffffffffu, act && lane == __ffs(peers) - 1);
