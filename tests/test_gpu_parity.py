@@ -46,10 +46,11 @@ def test_2d_push_deposit_bitexact(tile):
         pr.check_current(J_TOL, rho=True)
 
 
-@pytest.mark.parametrize("chunk", [256, 1024, 2048])
+@pytest.mark.parametrize("chunk", [256, 512, 1024, 2048])
 def test_2d_push_deposit_bitexact_chunks(chunk):
-    """The staged-chunk variants (512 double-buffered, 2048) give the same
-    bits; tiles of 16 x 16 with 64 particles per cell need several chunks."""
+    """Every staged-chunk variant (256 and 512 double-buffered, 1024 and 2048
+    single-buffered) gives the same bits; tiles of 16 x 16 with 64 particles
+    per cell need several chunks."""
     pr = _setup((64, 48), 64 * 48 * 64, seed=7, tile=(16, 16), chunk=chunk)
     for step in range(3):
         pr.both_update_particles(step)
