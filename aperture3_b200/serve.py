@@ -209,7 +209,7 @@ class GapServer:
             # a round of steps over the resident runs, each at its own step
             rounds = min(self.round_steps, min(r.req.steps - r.step for r in active))
             for _ in range(rounds):
-                steps = [r.step for r in active]
+                steps = batch.step_array([r.step for r in active])
                 batch.update_particles(steps)
                 batch.update_fields(steps)
                 batch.inject_pairs(steps)

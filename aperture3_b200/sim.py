@@ -515,6 +515,7 @@ class Batch:
         b = C.c_void_p()
         check(self._lib.ap_batch_create(arr, len(self.runs), C.byref(b)), "ap_batch_create")
         self.handle = b
+        self._dt_arr = None  # each run's own delta_t as a ctypes array (membership cache)
 
     @property
     def dt(self):
@@ -524,19 +525,30 @@ class Batch:
     def add(self, data: "SimData"):
         check(self._lib.ap_batch_add(self.handle, data.env.ctx), "ap_batch_add")
         self.runs.append(data)
+        self._dt_arr = None
 
     def remove(self, data: "SimData"):
         check(self._lib.ap_batch_remove(self.handle, data.env.ctx), "ap_batch_remove")
         self.runs.remove(data)
+        self._dt_arr = None
 
     def _dts(self, dt):
-        vals = self.dt if dt is None else (
-            [float(dt)] * len(self.runs) if np.isscalar(dt) else [float(x) for x in dt])
+        if dt is None:
+            if self._dt_arr is None:
+                self._dt_arr = (C.c_double * len(self.runs))(*self.dt)
+            return self._dt_arr
+        vals = [float(dt)] * len(self.runs) if np.isscalar(dt) else [float(x) for x in dt]
         return (C.c_double * len(self.runs))(*vals)
 
-    def _steps(self, steps):
+    def step_array(self, steps):
+        """Per-run step numbers as the ctypes array the batched calls take;
+        a loop that makes several calls per step can build it once."""
+        if isinstance(steps, C.Array):
+            return steps
         vals = [int(steps)] * len(self.runs) if np.isscalar(steps) else [int(x) for x in steps]
         return (C.c_uint32 * len(self.runs))(*vals)
+
+    _steps = step_array
 
     def set_capture(self, on: bool):
         """Graph-capture mode (ap_batch_set_capture)."""
