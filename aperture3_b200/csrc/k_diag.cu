@@ -58,17 +58,36 @@ struct DiagParams {
 __global__ void __launch_bounds__(kDiagThreads) k_diag_particles(const DiagParams P) {
   __shared__ double sh[kDiagThreads / 32];
   double kin = 0.0, q = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < P.number;
-       i += (size_t)gridDim.x * blockDim.x) {
-    if (P.p.cell[i] == AP_MAX_CELL) continue;
-    const int sp = ptc_type(P.p.flag[i]);
-    const double p1 = P.p.p1[i], p2 = P.p.p2[i], p3 = P.p.p3[i];
+  auto add = [&](uint32_t cell, uint32_t flag, double p1, double p2, double p3, double w) {
+    if (cell == AP_MAX_CELL) return;
+    const int sp = ptc_type(flag);
     const double pp = p1 * p1 + p2 * p2 + p3 * p3;
     const double gm1 = pp / (sqrt(1.0 + pp) + 1.0);  // gamma - 1 without cancellation
-    const double w = P.p.w[i];
     kin += w * P.mass[sp] * gm1;
     q += w * P.charge[sp];
+  };
+  // four particles' loads in flight per thread (a streaming read)
+  constexpr int U = 4;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (; i + (U - 1) * stride < P.number; i += U * stride) {
+    uint32_t c[U], f[U];
+    float p1[U], p2[U], p3[U], w[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const size_t k = i + u * stride;
+      c[u] = P.p.cell[k];
+      f[u] = P.p.flag[k];
+      p1[u] = P.p.p1[k];
+      p2[u] = P.p.p2[k];
+      p3[u] = P.p.p3[k];
+      w[u] = P.p.w[k];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) add(c[u], f[u], p1[u], p2[u], p3[u], w[u]);
   }
+  for (; i < P.number; i += stride)
+    add(P.p.cell[i], P.p.flag[i], P.p.p1[i], P.p.p2[i], P.p.p3[i], P.p.w[i]);
   const double sk = block_sum(kin, sh);
   const double sq = block_sum(q, sh);
   if (threadIdx.x == 0) {
@@ -144,7 +163,7 @@ cudaError_t launch_diagnostics(Ctx &c, double *out) {
   P.out = out;
   cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * 6, c.stream);
   if (e != cudaSuccess) return e;
-  int grid = c.num_sms * 4;
+  int grid = c.num_sms * 8;
   if (c.number > 0) {
     k_diag_particles<<<grid, kDiagThreads, 0, c.stream>>>(P);
     c.launches++;
