@@ -348,7 +348,7 @@ MeshK make_meshk(const ap_mesh &m);
 // Particles staged per chunk by the 2D push / deposit of this context: 1024
 // for log-spherical grids, else the configured 256, 1024 or 2048, or 512.
 inline int chunk_of(const Ctx &c) {
-  if (c.coord == 1) return 1024;
+  if (c.coord == 1) return 256;
   const int ch = c.params.chunk;
   return (ch == 512 || ch == 1024 || ch == 2048) ? ch : 256;
 }
