@@ -258,3 +258,53 @@ def _stats(requests, admitted, finished, particle_steps, makespan):
             "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)),
             "latency_mean_s": float(lat.mean())}
+
+
+def resident_steps(nsteps: int, requests: int = 24, seed: int = 5, warmup: int = 5,
+                   device=None) -> Dict[str, float]:
+    """Every request of the stream resident in one batch, `nsteps` batched
+    steps timed after `warmup` (the full phase of a served run, without
+    arrivals or departures): for profiling the batched serving step."""
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    reqs = request_stream(requests, seed=seed, rate=50.0, steps=(200, 5000))
+    runs = [GapRun(r, device) for r in reqs]
+    batch = Batch()
+    for r in runs:
+        batch.add(r.data)
+
+    def step():
+        steps = batch.step_array([r.step for r in runs])
+        batch.update_particles(steps)
+        batch.update_fields(steps)
+        batch.inject_pairs(steps)
+        for r in runs:
+            if r.step % SORT_INTERVAL == 0 and r.step != 0:
+                r.data.sort_particles_async()
+            r.step += 1
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    n = sum(r.req.cells * r.req.ppc for r in runs)
+    for r in runs:
+        batch.remove(r.data)
+        r.close()
+    batch.close()
+    return {"particles": n, "ms_per_step": 1e3 * dt / max(nsteps, 1),
+            "particle_steps_per_s": n * nsteps / dt if dt > 0 else 0.0}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="batched serving step with every request resident")
+    ap.add_argument("--resident-steps", type=int, default=200)
+    ap.add_argument("--requests", type=int, default=24)
+    a = ap.parse_args()
+    print(json.dumps(resident_steps(a.resident_steps, a.requests)))
