@@ -146,12 +146,20 @@ __device__ __forceinline__ void append_chunk(const PairK &K, const PtcK &p, uint
   const float Eph = K.pair_energy;
   float q = sqrtf(0.25f * Eph * Eph - 1.0f);
   if (q != q) q = 0.0f;
-  // thread t ranks slots ch * kPairChunk + t * kPairPerThread + [0, 4)
+  const uint32_t off_ch = offs[ch];
+  // thread t ranks slots ch * kPairChunk + t * kPairPerThread + [0, 4); the
+  // four emit bytes are read as one word (first is a multiple of 4)
+  static_assert(kPairPerThread == 4, "one 32-bit word of emit bytes per thread");
   const size_t first = (size_t)ch * kPairChunk + (size_t)threadIdx.x * kPairPerThread;
-  uint32_t mine = 0;
+  uint32_t e4 = 0;
+  if (first + kPairPerThread <= number) {
+    e4 = *reinterpret_cast<const uint32_t *>(emit + first);
+  } else {
 #pragma unroll
-  for (int k = 0; k < kPairPerThread; ++k)
-    if (first + k < number) mine += emit[first + k];
+    for (int k = 0; k < kPairPerThread; ++k)
+      if (first + k < number) e4 |= (uint32_t)emit[first + k] << (8 * k);
+  }
+  const uint32_t mine = (e4 * 0x01010101u) >> 24;  // sum of the four 0/1 bytes
   uint32_t x = mine;
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -161,12 +169,12 @@ __device__ __forceinline__ void append_chunk(const PairK &K, const PtcK &p, uint
   __syncthreads();
   uint32_t before = 0;
   for (int w = 0; w < warp; ++w) before += s_warp[w];
-  uint32_t rank = offs[ch] + before + x - mine;
+  uint32_t rank = off_ch + before + x - mine;
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kPairPerThread; ++k) {
     const size_t idx = first + k;
-    if (idx >= number || !emit[idx]) continue;
+    if (idx >= number || !((e4 >> (8 * k)) & 0xffu)) continue;
     const uint32_t r = rank++;
     if (r >= emitted) continue;  // over capacity: this parent keeps its energy
     const float gamma = p.E[idx];
