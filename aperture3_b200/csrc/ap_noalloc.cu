@@ -11,6 +11,8 @@
 // that pool. The caller passes the particle and field arrays; the only other
 // device memory used is the fixed-size file-scope array below, which every
 // GPU that loads this library keeps until the process exits.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -30,25 +32,66 @@ constexpr size_t kTailWords = 32;  // format word, weight maximum, status counte
 // cleared at the start of each call.
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kAccWords + kTailWords];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned long long *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device. The host-side
+// Device address of g_noalloc_scratch per CUDA context. The host-side
 // symbol is only a stand-in: kernels must be given the address that
-// cudaGetSymbolAddress returns, looked up once per device with that device
-// current.
-int scratch_on_current_device(unsigned long long **out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return AP_ERR_CUDA;
-  if (dev < 0 || dev >= kMaxDevices) return AP_ERR_CAPACITY;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
+// cudaGetSymbolAddress returns in the context they run in. The cache is
+// keyed by the context's unique id (cuCtxGetId), not by the device
+// ordinal, so a context that is destroyed and re-created (cudaDeviceReset,
+// or a caller's own driver-API context on the same device) gets its own
+// lookup instead of a stale address.
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  unsigned long long *ptr;
+};
+constexpr int kMaxContexts = 64;
+std::mutex g_mu;
+ScratchEntry g_scratch_cache[kMaxContexts] = {};
+int g_scratch_cached = 0;
+int g_scratch_next = 0;
+
+// The two driver calls, reached through the runtime's entry-point query so
+// that the library does not link the driver library directly.
+template <typename F>
+F driver_fn(const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(p);
+}
+
+int scratch_in_current_context(unsigned long long **out) {
+  static const PFN_cuCtxGetCurrent_v4000 get_current =
+      driver_fn<PFN_cuCtxGetCurrent_v4000>("cuCtxGetCurrent");
+  static const PFN_cuCtxGetId_v12000 get_id = driver_fn<PFN_cuCtxGetId_v12000>("cuCtxGetId");
+  if (!get_current || !get_id) return AP_ERR_CUDA;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return AP_ERR_CUDA;
+  void *p = nullptr;
+  if (!ctx) {
+    // No context current on this thread yet: the runtime call below makes
+    // the device's primary context current.
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return AP_ERR_CUDA;
-    g_scratch_ptr[dev] = static_cast<unsigned long long *>(p);
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return AP_ERR_CUDA;
   }
-  *out = g_scratch_ptr[dev];
+  unsigned long long id = 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return AP_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_mu);
+  for (int i = 0; i < g_scratch_cached; ++i)
+    if (g_scratch_cache[i].ctx_id == id) {
+      *out = g_scratch_cache[i].ptr;
+      return AP_OK;
+    }
+  if (!p && (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p))
+    return AP_ERR_CUDA;
+  // a full table is reused round-robin; a dropped entry is looked up again
+  ScratchEntry &slot = g_scratch_cache[g_scratch_cached < kMaxContexts ? g_scratch_cached++
+                                                                       : g_scratch_next];
+  if (g_scratch_cached == kMaxContexts) g_scratch_next = (g_scratch_next + 1) % kMaxContexts;
+  slot.ctx_id = id;
+  slot.ptr = static_cast<unsigned long long *>(p);
+  *out = slot.ptr;
   return AP_OK;
 }
 
@@ -86,7 +129,7 @@ extern "C" AP_API int ap_update_particles_1d_noalloc(const ap_mesh *mesh,
     if (!array_ok(fields->Rho[s], *mesh)) return AP_ERR_INVALID;
 
   unsigned long long *scratch = nullptr;
-  int st = scratch_on_current_device(&scratch);
+  int st = scratch_in_current_context(&scratch);
   if (st != AP_OK) return st;
 
   // A context on the stack: only plain fields, no allocation.
@@ -162,7 +205,12 @@ extern "C" AP_API int ap_update_particles_1d_noalloc(const ap_mesh *mesh,
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&hs, c.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
-  if (e != cudaSuccess) return AP_ERR_CUDA;
+  if (e != cudaSuccess) {
+    // Work enqueued before the failure may still use the shared array: wait
+    // for it, so that a retry (on any stream) cannot overlap with it.
+    cudaStreamSynchronize(c.stream);
+    return AP_ERR_CUDA;
+  }
   if (hs.timeouts) return AP_ERR_TIMEOUT;
   if (hs.nan_momenta) return AP_ERR_NAN;
   if (hs.moved_far) return AP_ERR_MOVED_FAR;
