@@ -28,6 +28,25 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+
+def _ref_tree() -> str:
+    """The reference tree the pin libraries are built from: REF of
+    ref_build/Makefile (APERTURE_REF in the environment overrides it)."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref_build"), "print-ref"],
+                             check=True, capture_output=True, text=True).stdout.strip()
+    except Exception:
+        out = ""
+    return out
+
+
+REF_TREE = _ref_tree()
+
+
+def ref_tree_present() -> bool:
+    return bool(REF_TREE) and os.path.isdir(os.path.join(REF_TREE, "src"))
 MAX_CELL = 0xFFFFFFFF
 
 PTC_FIELDS = (
@@ -361,7 +380,7 @@ def load_ref(build=True):
     global ref
     if ref is not None:
         return ref
-    if not os.path.exists(_REF_PATH) and build and os.path.isdir("/root/reference/src"):
+    if not os.path.exists(_REF_PATH) and build and ref_tree_present():
         try:
             _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref.so")
         except Exception:
@@ -427,7 +446,7 @@ def load_ref_mt(build=True):
     global ref_mt
     if ref_mt is not None:
         return ref_mt
-    if not os.path.exists(_REF_MT_PATH) and build and os.path.isdir("/root/reference/src"):
+    if not os.path.exists(_REF_MT_PATH) and build and ref_tree_present():
         try:
             _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_mt.so")
         except Exception:
@@ -510,7 +529,7 @@ def load_ref_gap(build=True):
     global ref_gap
     if ref_gap is not None:
         return ref_gap
-    if not os.path.exists(_REF_GAP_PATH) and build and os.path.isdir("/root/reference/src"):
+    if not os.path.exists(_REF_GAP_PATH) and build and ref_tree_present():
         try:
             _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_gap.so")
         except Exception:

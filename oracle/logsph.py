@@ -16,7 +16,7 @@ import os
 
 import numpy as np
 
-from . import (PTC_FIELDS, _HERE, _arr, _build, _fa, _p, fields_struct, lib,
+from . import (PTC_FIELDS, _HERE, _arr, _build, _fa, _p, fields_struct, lib, ref_tree_present,
                ptc_struct)
 
 COEF_NAMES = ("l1_e", "l2_e", "l3_e", "l1_b", "l2_b", "l3_b",
@@ -191,7 +191,7 @@ def load_ref(build=True):
     global ref
     if ref is not None:
         return ref
-    if not os.path.exists(_REF_PATH) and build and os.path.isdir("/root/reference/src"):
+    if not os.path.exists(_REF_PATH) and build and ref_tree_present():
         try:
             _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_ls.so")
         except Exception:
