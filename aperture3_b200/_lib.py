@@ -78,7 +78,8 @@ class ApStepStats(C.Structure):
 class ApDiag(C.Structure):
     _fields_ = [("kinetic", C.c_double), ("charge", C.c_double),
                 ("field_energy", C.c_double), ("max_abs_rho", C.c_double),
-                ("gauss_residual", C.c_double), ("max_abs_j", C.c_double)]
+                ("gauss_residual", C.c_double), ("max_abs_j", C.c_double),
+                ("continuity_residual", C.c_double)]
 
 
 class ApPhaseTimes(C.Structure):
@@ -166,10 +167,12 @@ SIGNATURES = {
     "ap_batch_update_fields": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "ap_batch_sort_by_cell": (_i, [_vp]),
     "ap_batch_sync": (_i, [_vp, C.POINTER(_i)]),
+    "ap_batch_advance": (_i, [_vp, _vp, _vp, _i, _i, _i]),
     "ap_batch_autotune": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
                                C.POINTER(_i)]),
     "ap_set_tile_shape": (_i, [_vp, _i, _i]),
     "ap_set_compaction": (_i, [_vp, _i]),
+    "ap_set_continuity_check": (_i, [_vp, _i]),
     "ap_get_tile_shape": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
     "ap_set_pair_params": (_i, [_vp, C.POINTER(ApPairParams)]),
     "ap_get_pair_stats": (_i, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),

@@ -273,6 +273,7 @@ AP_API int ap_ctx_create(const ap_mesh *mesh, const ap_params *params, ap_ctx **
     return AP_ERR_NOMEM;
   }
   cudaMemset(c->status, 0, sizeof(DevStatus));
+  cudaMemset(c->diag_dev, 0xFF, sizeof(double) * 16);  // NaN: nothing recorded yet
   std::memset(c->status_host, 0, sizeof(DevStatus));
   cudaMemset(c->fx_used, 0, sizeof(FixedFmt));
   cudaMemset(c->n_max, 0, sizeof(uint32_t));
@@ -295,7 +296,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->grp_off);
   cudaFree(c->newcount);
   cudaFree(c->queue);
-  cudaFree(c->cub_tmp);
+  cudaFree(c->rx_counts);
   cudaFree(c->gather_tmp);
   cudaFree(c->cell_start);
   cudaFree(c->cell_count);
@@ -315,6 +316,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->wmax);
   cudaFree(c->status);
   cudaFree(c->diag_dev);
+  cudaFree(c->rho_prev);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->diag_host) cudaFreeHost(c->diag_host);
   for (int i = 0; i < c->ev_cap; ++i) {
@@ -551,6 +553,12 @@ int update_prepare(Ctx *c, double dt, uint32_t step, PushDepositParams &P, bool 
     c->rho_is_zero = true;
   }
   if (!batched) AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  // continuity check: rho(t) of the previous update, before it is replaced
+  c->cont_snap = false;
+  if (c->cont_on && !batched && !ls && do_rho && c->last_rho_step == (long long)step - 1) {
+    AP_TRY(launch_rho_snapshot(*c));
+    c->cont_snap = true;
+  }
   phase_end(c, ph);
 
   std::memset(&P, 0, sizeof(P));
@@ -706,6 +714,13 @@ int update_complete(Ctx *c, double dt, uint32_t step, bool had_work, bool batche
     AP_TRY(launch_finalize_current(*c, ncomp));
     phase_end(c, ph);
     AP_TRY_ST(smooth_current_async(c, step));
+    if (c->cont_on && !batched) {
+      if (c->cont_snap)
+        AP_TRY(launch_continuity(*c, c->diag_dev + 6));
+      else
+        AP_TRY(cudaMemsetAsync(c->diag_dev + 6, 0xFF, sizeof(double), c->stream));  // NaN
+      c->last_rho_step = do_rho ? (long long)step : -2;
+    }
   }
   return AP_OK;
 }
@@ -900,7 +915,7 @@ AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
   if (!c || !out || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
   AP_TRY_ST(refresh_number(c));
   AP_TRY(launch_diagnostics(*c, c->diag_dev));
-  AP_TRY(cudaMemcpyAsync(c->diag_host, c->diag_dev, sizeof(double) * 6, cudaMemcpyDeviceToHost,
+  AP_TRY(cudaMemcpyAsync(c->diag_host, c->diag_dev, sizeof(double) * 7, cudaMemcpyDeviceToHost,
                          c->stream));
   AP_TRY(cudaStreamSynchronize(c->stream));
   out->kinetic = c->diag_host[0];
@@ -909,6 +924,7 @@ AP_API int ap_diagnostics(ap_ctx *c, ap_diag *out) {
   out->max_abs_rho = c->diag_host[3];
   out->gauss_residual = c->diag_host[4];
   out->max_abs_j = c->diag_host[5];
+  out->continuity_residual = c->diag_host[6];
   return AP_OK;
 }
 
@@ -916,7 +932,7 @@ AP_API int ap_diagnostics_async(ap_ctx *c, double *host_out) {
   if (!c || !host_out || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
   if (c->pstate && c->mk.dim == 1 && c->number_stale) return fail(c, AP_ERR_INVALID);
   AP_TRY(launch_diagnostics(*c, c->diag_dev));
-  AP_TRY(cudaMemcpyAsync(host_out, c->diag_dev, sizeof(double) * 6, cudaMemcpyDeviceToHost,
+  AP_TRY(cudaMemcpyAsync(host_out, c->diag_dev, sizeof(double) * 7, cudaMemcpyDeviceToHost,
                          c->stream));
   return AP_OK;
 }
@@ -1073,6 +1089,21 @@ AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitte
   AP_TRY_ST(refresh_number(c));
   if (emitted) *emitted = c->pstate_host->emitted;
   if (dropped) *dropped = c->pstate_host->dropped;
+  return AP_OK;
+}
+
+AP_API int ap_set_continuity_check(ap_ctx *c, int on) {
+  if (!c) return AP_ERR_INVALID;
+  if (c->coord != 0) return AP_ERR_UNSUPPORTED;
+  if (on && !c->rho_prev) {
+    const size_t n = (size_t)c->mesh.dims[0] * (c->mk.dim > 1 ? c->mesh.dims[1] : 1);
+    if (cudaMalloc(&c->rho_prev, sizeof(double) * n) != cudaSuccess) {
+      c->rho_prev = nullptr;
+      return fail(c, AP_ERR_NOMEM);
+    }
+  }
+  c->cont_on = on != 0;
+  c->last_rho_step = -2;
   return AP_OK;
 }
 

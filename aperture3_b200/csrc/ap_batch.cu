@@ -543,6 +543,23 @@ AP_API int ap_batch_inject_pairs(ap_batch *b, const double *dt, const uint32_t *
   return AP_OK;
 }
 
+AP_API int ap_batch_advance(ap_batch *b, const double *dt, const uint32_t *steps0, int nsteps,
+                            int sort_interval, int inject) {
+  if (!b || !dt || !steps0 || nsteps < 0 || sort_interval < 0) return AP_ERR_INVALID;
+  std::vector<uint32_t> st(steps0, steps0 + b->runs.size());
+  for (int s = 0; s < nsteps; ++s) {
+    B_TRY_ST(batch_update(b, dt, st.data()));
+    B_TRY_ST(ap_batch_update_fields(b, dt, st.data()));
+    if (inject) B_TRY_ST(ap_batch_inject_pairs(b, dt, st.data()));
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+      if (sort_interval > 0 && st[r] != 0 && st[r] % (uint32_t)sort_interval == 0)
+        B_TRY_ST(ap_sort_by_cell(static_cast<ap_ctx *>(b->runs[r])));
+      ++st[r];
+    }
+  }
+  return AP_OK;
+}
+
 AP_API int ap_batch_sync(ap_batch *b, int *failed_run) {
   if (!b) return AP_ERR_INVALID;
   if (failed_run) *failed_run = -1;
@@ -579,11 +596,15 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *step
   b->tune_ev.assign(2 * ncls, nullptr);
   for (auto &e : b->tune_ev) B_TRY(cudaEventCreate(&e));
   b->tune_ms.assign(ncls, 0.0f);
-  // Candidates: smaller tiles look faster right after the order rebuild
-  // but lose in steady state (more particles change tiles each step and
-  // more halo per particle), so only 16x16 and 32x16 are tried.
-  constexpr int kCand = 2, kSteps = 4;
-  const int cand[kCand][2] = {{16, 16}, {32, 16}};
+  // Candidates: every compiled tile shape with 256-particle chunks, and the
+  // two large shapes with 512-particle chunks. Each runs kSteps steps; the
+  // first includes the order rebuild after the shape change and the next
+  // one still reads a freshly sorted store (which flatters small tiles,
+  // whose particles change tiles more often in steady state), so only the
+  // last kSteps - 2 are timed.
+  constexpr int kCand = 7, kSteps = 5;
+  const int cand[kCand][3] = {{16, 16, 256}, {32, 16, 256}, {16, 8, 256}, {8, 8, 256},
+                              {4, 4, 256},   {16, 16, 512}, {32, 16, 512}};
   std::vector<float> best(ncls, 1e30f);
   std::vector<int> best_k(ncls, 0);
   int used = 0;
@@ -601,6 +622,7 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *step
         ok[b->tune_class[r]] = true;
         st = ap_set_tile_shape(static_cast<ap_ctx *>(b->runs[r]), cand[k][0], cand[k][1]);
         if (st != AP_OK) break;
+        b->runs[r]->params.chunk = cand[k][2];
       }
     }
     // the first step after a shape change includes the order rebuild: time
@@ -611,7 +633,7 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *step
       if (st == AP_OK) st = ap_batch_update_fields(b, dt, cur.data());
       for (uint32_t &x : cur) ++x;
       ++used;
-      if (rep > 0)
+      if (rep > 1)
         for (int cl = 0; cl < ncls; ++cl) sum[cl] += b->tune_ms[cl];
     }
     if (st != AP_OK) break;
@@ -630,6 +652,7 @@ AP_API int ap_batch_autotune(ap_batch *b, const double *dt, const uint32_t *step
       ap_get_tile_shape(static_cast<ap_ctx *>(b->runs[r]), &tx, &ty);
       if (tx != cand[k][0] || ty != cand[k][1])
         st = ap_set_tile_shape(static_cast<ap_ctx *>(b->runs[r]), cand[k][0], cand[k][1]);
+      b->runs[r]->params.chunk = cand[k][2];
     }
   if (steps_used) *steps_used = used;
   return st;

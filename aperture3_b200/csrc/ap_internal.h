@@ -221,8 +221,7 @@ struct Ctx {
   // rebuild / sort scratch
   uint32_t *keys[2] = {nullptr, nullptr};
   uint32_t *vals[2] = {nullptr, nullptr};
-  void *cub_tmp = nullptr;
-  size_t cub_tmp_bytes = 0;
+  uint32_t *rx_counts = nullptr;  // radix sort: per-CTA digit counts
   void *gather_tmp = nullptr;
   size_t scratch_cap = 0;
   uint32_t *cell_start = nullptr;  // ncells + 1 entries, set by sort_by_cell
@@ -283,6 +282,12 @@ struct Ctx {
   DevStatus *status_host = nullptr;  // pinned
   double *diag_dev = nullptr;
   double *diag_host = nullptr;
+  // FP64 continuity check (ap_set_continuity_check): the total charge
+  // density of the last update with Rho output, and its step
+  bool cont_on = false;
+  double *rho_prev = nullptr;  // dims[0] * dims[1] doubles
+  long long last_rho_step = -2;
+  bool cont_snap = false;      // this update took the snapshot
 };
 
 // --- launchers (defined in the .cu files) ---
@@ -297,6 +302,11 @@ cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start,
                                  const uint32_t *grp_off, uint32_t *new_order,
                                  uint32_t slot0 = 0);
 cudaError_t rebuild_tile_order(Ctx &c);
+// Stable LSD radix sort of (c.keys[0], c.vals[0])[0, n) by the low end_bit
+// bits of the keys, ping-ponging with keys[1] / vals[1] (k_radix.cu).
+cudaError_t radix_sort_pairs(Ctx &c, size_t n, int end_bit, uint32_t **keys_out,
+                             uint32_t **vals_out);
+size_t radix_count_words(int num_sms);
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number);
 // Compaction: the scratch store the push / deposit writes into (allocated on
 // first use), and the copy back into the caller's arrays; `live` is the
@@ -314,6 +324,10 @@ cudaError_t launch_zero(Ctx &c, ap_array a);
 cudaError_t launch_finalize_current(Ctx &c, int ncomp);
 cudaError_t launch_fixed_scale(Ctx &c);
 cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
+// rho_prev = sum over species of Rho (FP64)
+cudaError_t launch_rho_snapshot(Ctx &c);
+// *out = max over the bulk of |sum_s Rho_s - rho_prev + div J| (FP64)
+cudaError_t launch_continuity(Ctx &c, double *out);
 
 // pair injection (k_pairs.cu): enqueue mark / scan / append on the device
 // count (no host synchronisation); refresh_number reads the device state

@@ -132,7 +132,94 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_fields(const DiagParams P
   }
 }
 
+struct ContParams {
+  FieldArr Rho[AP_MAX_SPECIES], J1, J2;
+  double *prev;
+  int n0, n1, g0, g1, dim, num_species, per0, per1;
+  double *out;
+};
+
+__global__ void __launch_bounds__(kDiagThreads) k_rho_snapshot(const ContParams P) {
+  const size_t total = (size_t)P.n0 * P.n1;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % P.n0), j = (int)(t / P.n0);
+    double rho = 0.0;
+    for (int sp = 0; sp < P.num_species; ++sp)
+      rho += P.Rho[sp].ptr[(size_t)j * P.Rho[sp].pitch + i];
+    P.prev[t] = rho;
+  }
+}
+
+// Discrete continuity of the Esirkepov deposit: J1 at index i + 1 is the
+// flux through the upper x face of cell i (ptc_updater.cu:364-371), J2 at
+// j + 1 through the upper y face; the face past the last bulk cell of a
+// periodic side is the first bulk face (the guard cells keep the raw
+// deposit).
+__global__ void __launch_bounds__(kDiagThreads) k_continuity(const ContParams P) {
+  __shared__ double sh[kDiagThreads / 32];
+  const int r0 = P.n0 - 2 * P.g0;
+  const int r1 = P.dim > 1 ? P.n1 - 2 * P.g1 : 1;
+  const int g1 = P.dim > 1 ? P.g1 : 0;
+  const size_t total = (size_t)r0 * r1;
+  double mres = 0.0;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = P.g0 + (int)(t % r0), j = g1 + (int)(t / r0);
+    double rho = 0.0;
+    for (int sp = 0; sp < P.num_species; ++sp)
+      rho += P.Rho[sp].ptr[(size_t)j * P.Rho[sp].pitch + i];
+    const int ip = (i + 1 == P.n0 - P.g0 && P.per0) ? P.g0 : i + 1;
+    double div = (double)P.J1.ptr[(size_t)j * P.J1.pitch + ip] -
+                 (double)P.J1.ptr[(size_t)j * P.J1.pitch + i];
+    if (P.dim > 1) {
+      const int jp = (j + 1 == P.n1 - P.g1 && P.per1) ? P.g1 : j + 1;
+      div += (double)P.J2.ptr[(size_t)jp * P.J2.pitch + i] -
+             (double)P.J2.ptr[(size_t)j * P.J2.pitch + i];
+    }
+    mres = fmax(mres, fabs(rho - P.prev[(size_t)j * P.n0 + i] + div));
+  }
+  const double m = block_max(mres, sh);
+  if (threadIdx.x == 0) atomic_max_nonneg(P.out, m);
+}
+
+ContParams cont_params(const Ctx &c) {
+  ContParams P;
+  auto fa = [](const ap_array &a) { return FieldArr{a.ptr, (int)(a.pitch / 4)}; };
+  for (int s = 0; s < c.params.num_species; ++s) P.Rho[s] = fa(c.fields.Rho[s]);
+  P.J1 = fa(c.fields.J[0]);
+  P.J2 = fa(c.fields.J[1]);
+  P.prev = c.rho_prev;
+  P.n0 = c.mesh.dims[0];
+  P.n1 = c.mk.dim > 1 ? c.mesh.dims[1] : 1;
+  P.g0 = c.mesh.guard[0];
+  P.g1 = c.mesh.guard[1];
+  P.dim = c.mk.dim;
+  P.num_species = c.params.num_species;
+  P.per0 = c.params.periodic[0];
+  P.per1 = c.params.periodic[1];
+  P.out = nullptr;
+  return P;
+}
+
 }  // namespace
+
+cudaError_t launch_rho_snapshot(Ctx &c) {
+  const ContParams P = cont_params(c);
+  k_rho_snapshot<<<c.num_sms * 4, kDiagThreads, 0, c.stream>>>(P);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_continuity(Ctx &c, double *out) {
+  ContParams P = cont_params(c);
+  P.out = out;
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), c.stream);
+  if (e != cudaSuccess) return e;
+  k_continuity<<<c.num_sms * 4, kDiagThreads, 0, c.stream>>>(P);
+  c.launches++;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_diagnostics(Ctx &c, double *out) {
   DiagParams P;

@@ -137,6 +137,16 @@ __device__ __forceinline__ void add_fixed(const Acc32 &a, int o, float v, float 
   atomicAdd(a.lo + o, (unsigned)X & ((1u << L) - 1u));
 }
 
+// The same for a contribution already scaled by 2^S. Scaling by a power of
+// two commutes with rounding, so for a product a * b the value
+// (a * 2^S) * b equals (a * b) * 2^S bit for bit whenever the result is a
+// normal float; a result below the normal range rounds to X = 0 either way.
+__device__ __forceinline__ void add_fixed_scaled(const Acc32 &a, int o, float vs, int L) {
+  const long long X = __float2ll_rn(vs);
+  atomicAdd(a.hi + o, (int)(X >> L));
+  atomicAdd(a.lo + o, (unsigned)X & ((1u << L) - 1u));
+}
+
 // Chunks of at most 256 particles are double-buffered: the loads of the
 // next chunk run while the current one is pushed and deposited.
 template <int CH>
@@ -518,6 +528,10 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
             // zero up to rounding); the reference adds that rounding residue,
             // these sites are skipped.
             const float weight = -P.charge[sp] * w;
+            // the deposit's factors pre-scaled by 2^S (exact): weight, and
+            // -weight * v3 as the reference forms it before the site loop
+            const float wsc = weight * fscale;
+            const float w3s = -wsc * v3;
             const int ib = (dc1 == -1 ? -2 : -1), nib = (dc1 == 0 ? 2 : 3);
             const int jb = (dc2 == -1 ? -2 : -1), njb = (dc2 == 0 ? 2 : 3);
             float sx0[3], sx1[3];
@@ -545,17 +559,17 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
                 if (jv && a < nib) {
                   const int o = obase + b * G::JX + a;
                   djx += movement2d(sy0, sy1, sx0[a], sx1[a]);
-                  if (a < 2) add_fixed(J1, o + 1, weight * djx, fscale, fx.L);
+                  if (a < 2) add_fixed_scaled(J1, o + 1, wsc * djx, fx.L);
                   djy[a] += movement2d(sx0[a], sx1[a], sy0, sy1);
-                  if (b < 2) add_fixed(J2, o + G::JX, weight * djy[a], fscale, fx.L);
+                  if (b < 2) add_fixed_scaled(J2, o + G::JX, wsc * djy[a], fx.L);
                   const float val2 = center2d(sx0[a], sx1[a], sy0, sy1);
                   if constexpr (kLS)
-                    add_fixed(J3, o, -weight * v3 * val2 / s_dv[o], fscale, fx.L);
+                    add_fixed_scaled(J3, o, w3s * val2 / s_dv[o], fx.L);
                   else
-                    add_fixed(J3, o, -weight * v3 * val2, fscale, fx.L);
+                    add_fixed_scaled(J3, o, w3s * val2, fx.L);
                   if (rho) {
                     const float s1 = sx1[a] * sy1;
-                    add_fixed(R, o, -weight * s1, fscale, fx.L);
+                    add_fixed_scaled(R, o, -wsc * s1, fx.L);
                   }
                 }
               }

@@ -19,7 +19,6 @@
 //
 // Full rebuild (after binding or external changes) and sort_by_cell
 // (cuda/core/particle_base_impl.cu:435-487) use a stable LSD radix sort.
-#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include "ap_device.cuh"
@@ -485,19 +484,10 @@ int grid_for(Ctx &c, size_t n, int threads) {
   return (int)g;
 }
 
-// Stable radix sort of (keys[0], vals[0]) -> result pointers.
+// Stable radix sort of (keys[0], vals[0]) -> result pointers (k_radix.cu).
 cudaError_t radix_pairs(Ctx &c, size_t n, int end_bit, uint32_t **keys_out,
                         uint32_t **vals_out) {
-  cub::DoubleBuffer<uint32_t> k(c.keys[0], c.keys[1]);
-  cub::DoubleBuffer<uint32_t> v(c.vals[0], c.vals[1]);
-  size_t bytes = c.cub_tmp_bytes;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(c.cub_tmp, bytes, k, v, (int64_t)n, 0,
-                                                   end_bit, c.stream);
-  if (e != cudaSuccess) return e;
-  *keys_out = k.Current();
-  *vals_out = v.Current();
-  c.launches += (uint64_t)((end_bit + 7) / 8) * 3;
-  return cudaSuccess;
+  return radix_sort_pairs(c, n, end_bit, keys_out, vals_out);
 }
 
 }  // namespace
@@ -541,7 +531,7 @@ cudaError_t launch_order_scatter(Ctx &c, const uint32_t *old_start, const uint32
 }
 
 // Scratch for the radix sorts: two key and two value buffers of n entries,
-// CUB's temporary storage, and an 8-byte-per-slot gather buffer.
+// the per-CTA digit counts, and an 8-byte-per-slot gather buffer.
 int ensure_scratch(Ctx &c, size_t n) {
   if (n <= c.scratch_cap && c.keys[0]) return AP_OK;
   for (int i = 0; i < 2; ++i) {
@@ -549,21 +539,17 @@ int ensure_scratch(Ctx &c, size_t n) {
     cudaFree(c.vals[i]);
     c.keys[i] = c.vals[i] = nullptr;
   }
-  cudaFree(c.cub_tmp);
+  cudaFree(c.rx_counts);
   cudaFree(c.gather_tmp);
-  c.cub_tmp = c.gather_tmp = nullptr;
+  c.rx_counts = nullptr;
+  c.gather_tmp = nullptr;
   size_t cap = n < 1024 ? 1024 : n;
   for (int i = 0; i < 2; ++i) {
     if (cudaMalloc(&c.keys[i], cap * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
     if (cudaMalloc(&c.vals[i], cap * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
   }
-  cub::DoubleBuffer<uint32_t> k(c.keys[0], c.keys[1]);
-  cub::DoubleBuffer<uint32_t> v(c.vals[0], c.vals[1]);
-  size_t bytes = 0;
-  if (cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int64_t)cap, 0, 32) != cudaSuccess)
-    return AP_ERR_CUDA;
-  if (cudaMalloc(&c.cub_tmp, bytes) != cudaSuccess) return AP_ERR_NOMEM;
-  c.cub_tmp_bytes = bytes;
+  if (cudaMalloc(&c.rx_counts, radix_count_words(c.num_sms) * sizeof(uint32_t)) != cudaSuccess)
+    return AP_ERR_NOMEM;
   if (cudaMalloc(&c.gather_tmp, cap * sizeof(uint64_t)) != cudaSuccess) return AP_ERR_NOMEM;
   c.scratch_cap = cap;
   return AP_OK;

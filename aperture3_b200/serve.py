@@ -6,9 +6,9 @@ amplitude `ramp`, and pair injection for particles above gamma 1e6
 (ap_pair_params). The server keeps every admitted run's particles and
 fields resident on the device, admits queued requests in arrival order while
 their HBM footprint fits the budget, and advances all resident runs
-together through one batch (ap_batch_*): one batched push / deposit launch,
-then the per-run field updates and one pair-injection pass with a single
-synchronisation, each run at its own step. A run leaves the batch when it
+together through one batch (ap_batch_*), a round of steps per call
+(ap_batch_advance): per step one batched push / deposit launch, batched
+field updates and one pair-injection pass, each run at its own step. A run leaves the batch when it
 has done its steps; the batch is rebuilt when its membership changes.
 
 Each run computes exactly what it computes alone through the plain path
@@ -208,15 +208,12 @@ class GapServer:
                 continue
             # a round of steps over the resident runs, each at its own step
             rounds = min(self.round_steps, min(r.req.steps - r.step for r in active))
-            for _ in range(rounds):
-                steps = batch.step_array([r.step for r in active])
-                batch.update_particles(steps)
-                batch.update_fields(steps)
-                batch.inject_pairs(steps)
-                for r in active:
-                    if r.step % SORT_INTERVAL == 0 and r.step != 0:
-                        r.data.sort_particles_async()
-                    r.step += 1
+            # the lab loop of every resident run for `rounds` steps in one
+            # call: update_particles, update_fields, inject_pairs, sort every
+            # SORT_INTERVAL steps (ap_batch_advance)
+            batch.advance([r.step for r in active], rounds, SORT_INTERVAL, inject=True)
+            for r in active:
+                r.step += rounds
             for r in [r for r in active if r.step >= r.req.steps]:
                 batch.remove(r.data)  # waits for the batch's stream
                 finished[r.req.rid] = time.perf_counter() - t0
@@ -273,13 +270,8 @@ def resident_steps(nsteps: int, requests: int = 24, seed: int = 5, warmup: int =
         batch.add(r.data)
 
     def step():
-        steps = batch.step_array([r.step for r in runs])
-        batch.update_particles(steps)
-        batch.update_fields(steps)
-        batch.inject_pairs(steps)
+        batch.advance([r.step for r in runs], 1, SORT_INTERVAL, inject=True)
         for r in runs:
-            if r.step % SORT_INTERVAL == 0 and r.step != 0:
-                r.data.sort_particles_async()
             r.step += 1
 
     for _ in range(warmup):

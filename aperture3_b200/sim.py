@@ -202,6 +202,18 @@ class SimEnvironment:
         updates (0: never). Particles change slots, not values."""
         check(self._lib.ap_set_compaction(self.ctx, int(interval)), "ap_set_compaction")
 
+    def set_tile_shape(self, tx: int, ty: int):
+        """Tile shape of the 2D particle update (16x16, 32x16, 16x8, 8x8 or
+        4x4); the tile order is rebuilt at the next update."""
+        check(self._lib.ap_set_tile_shape(self.ctx, int(tx), int(ty)), "ap_set_tile_shape")
+
+    def set_continuity_check(self, on: bool = True):
+        """Record max |rho(t+1) - rho(t) + div J| (FP64, on the device) on
+        every update with charge output that follows one; read it from
+        SimData.diagnostics().continuity_residual (NaN when not recorded)."""
+        check(self._lib.ap_set_continuity_check(self.ctx, int(bool(on))),
+              "ap_set_continuity_check")
+
     def logsph_coef(self, which: int) -> np.ndarray:
         """Host copy of one Grid_LogSph coefficient array (grid_log_sph.h:45-47),
         shape (dims[1], dims[0])."""
@@ -581,6 +593,15 @@ class Batch:
 
     def sort_particles(self):
         check(self._lib.ap_batch_sort_by_cell(self.handle), "ap_batch_sort_by_cell")
+
+    def advance(self, steps, nsteps: int, sort_interval: int = 0, inject: bool = False,
+                dt=None):
+        """`nsteps` lab-loop steps of every run in one call (ap_batch_advance):
+        run r goes from step steps[r] to steps[r] + nsteps - 1; runs whose
+        step is a positive multiple of sort_interval are sorted after it."""
+        check(self._lib.ap_batch_advance(self.handle, self._dts(dt), self._steps(steps),
+                                         int(nsteps), int(sort_interval), int(bool(inject))),
+              "ap_batch_advance")
         for d in self.runs:
             d.mark_number_stale()
 
@@ -635,6 +656,12 @@ class ptc_updater_logsph:
     def apply_boundary(self, data: SimData, dt: float, step: int = 0):
         """Run by update_particles already (axis current, outflow flags, and
         dropping particles that left the grid)."""
+
+    def smooth_current(self, data: SimData, step: int = 0):
+        """The smoothing passes of update_particles alone (filter_current_logsph
+        weighted by face areas / cell volumes, then the axis current;
+        ptc_updater_logsph.cu:616-666, 414-438) on the fields as they are."""
+        check(self.env._lib.ap_smooth_current(self.env.ctx, int(step)), "ap_smooth_current")
 
     def inject_ptc(self, data: SimData, inj_per_cell: int, p1: float, p2: float, p3: float,
                    w: float, omega: float, seed: int = 0x5EED):

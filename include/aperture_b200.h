@@ -116,6 +116,9 @@ typedef struct {
   double max_abs_rho;    /* max |rho_total| over the bulk                    */
   double gauss_residual; /* max |divE - sum rho| over the bulk               */
   double max_abs_j;      /* max |J| over the bulk, all components            */
+  double continuity_residual; /* max |rho(t+1) - rho(t) + div J| over the bulk,
+                               * from the last update (ap_set_continuity_check);
+                               * NaN when it was not recorded               */
 } ap_diag;
 
 typedef struct ap_ctx ap_ctx;
@@ -191,6 +194,17 @@ AP_API int ap_send_add_guard_cells(ap_ctx *ctx, ap_array a);
  * This bounds the scatter of the particle accesses that grows as particles
  * cross tiles. */
 AP_API int ap_set_compaction(ap_ctx *ctx, int interval);
+/* FP64 continuity check (new; derived from the deposit of
+ * ptc_updater.cu:295-386 and the divergence of compute_divs_2d,
+ * field_solver.cu:237-288). While on (1), every Cartesian update_particles
+ * that deposits Rho right after an update that also deposited it records,
+ * on the device and in FP64, max |sum_s Rho_s(t+1) - sum_s Rho_s(t) +
+ * J1(i+1) - J1(i) + J2(j+1) - J2(j)| over the bulk cells (the face past the
+ * last bulk cell is the first one's periodic image on periodic sides), in
+ * the deposit's own units; ap_diagnostics reports it as
+ * continuity_residual. Other updates report NaN. Off by default; costs one
+ * FP64 copy of the charge density per output step while on. */
+AP_API int ap_set_continuity_check(ap_ctx *ctx, int on);
 
 /* sim_data::sort_particles -> particle_base::sort_by_cell
  * (sim_data_impl.hpp:78-89, cuda/core/particle_base_impl.cu:435-487):
@@ -210,7 +224,7 @@ AP_API int ap_get_stats(ap_ctx *ctx, ap_step_stats *stats);
 /* FP64 energy / charge / Gauss-law diagnostics (new; the reference only
  * computes per-particle gamma, cuda/core/particles.cu:10-22). */
 AP_API int ap_diagnostics(ap_ctx *ctx, ap_diag *out);
-/* The same reductions without waiting: the six values (in ap_diag's member
+/* The same reductions without waiting: the seven values (in ap_diag's member
  * order) are copied to host_out, which should be pinned host memory, on the
  * context's stream; they are there after the next ap_sync. A 1D context
  * whose particle count moved on the device (pair injection) must be synced
@@ -333,6 +347,17 @@ AP_API int ap_batch_sort_by_cell(ap_batch *batch);
 /* Waits for the batch and returns the first non-OK device status of a run
  * (run index in *failed_run, -1 if none; may be NULL). */
 AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
+/* nsteps steps of the lab loop for every run without returning between
+ * steps (new; the loop of labs/box/src/main.cpp:69-92 and
+ * labs/1dgap/src/main.cpp:61-98 over a batch): step s calls
+ * ap_batch_update_particles, ap_batch_update_fields and, when inject is
+ * nonzero, ap_batch_inject_pairs with run r at step steps0[r] + s, then
+ * sorts each run whose step is a positive multiple of sort_interval (0:
+ * never). Exactly the calls a caller would make step by step, so every run
+ * computes the same; what it saves is the caller's per-step work on the
+ * host. Nothing waits for the device unless a 2D run sorts. */
+AP_API int ap_batch_advance(ap_batch *batch, const double *dt, const uint32_t *steps0,
+                            int nsteps, int sort_interval, int inject);
 /* Graph capture. While on, every batched call stages its launch
  * descriptors in host / device blocks of its own, kept until the mode is
  * turned off, and waits for nothing on the host, so that a sequence of
@@ -346,12 +371,14 @@ AP_API int ap_batch_sync(ap_batch *batch, int *failed_run);
  * the mode off (after the graphs are destroyed) frees the blocks. */
 AP_API int ap_batch_set_capture(ap_batch *batch, int on);
 /* Project autotuner: advances the batch by *steps_used complete steps
- * (particle update, then field update) starting at steps[r], timing the
- * push / deposit of each class of runs (same grid size) over three steps
- * with each candidate tile shape (16x16, 32x16), and keeps the fastest
- * shape per class. Particle
- * results do not depend on the tile shape; J can differ in the last bits
- * (the fixed-point scale follows the largest tile population). */
+ * (particle update, then field update; 5 per candidate) starting at
+ * steps[r], timing the push / deposit of each class of runs (same grid
+ * size) over the last three steps of each candidate -- every tile shape
+ * (16x16, 32x16, 16x8, 8x8, 4x4) with 256-particle chunks, and 16x16 and
+ * 32x16 with 512-particle chunks -- and keeps the fastest per class.
+ * Particle results do not depend on the shape or chunk; J can differ in
+ * the last bits (the fixed-point scale follows the largest tile
+ * population). */
 AP_API int ap_batch_autotune(ap_batch *batch, const double *dt, const uint32_t *steps,
                              int *steps_used);
 /* Tile shape of one run (16x16, 32x16, 16x8, 8x8 or 4x4); rebuilds its
@@ -439,13 +466,16 @@ AP_API int ap_get_phase_times(ap_ctx *ctx, ap_phase_times *out, int reset);
  * until the process exits. Grids with more than AP_NOALLOC_MAX_CELLS cells
  * (AP_ERR_CAPACITY), more than AP_NOALLOC_MAX_SPECIES species
  * (AP_ERR_CAPACITY), current smoothing (AP_ERR_UNSUPPORTED) or other than
- * 1D (AP_ERR_UNSUPPORTED) are rejected. The first call on a device looks up
- * the array's device address with cudaGetSymbolAddress, so make that first
- * call before any stream capture. All calls share the array and clear it
- * at their start: calls that overlap on the GPU (on different streams, or
- * from different threads) race and must not be issued. The call enqueues
- * its work on cuda_stream (0 = legacy default stream) and synchronises that
- * stream before returning. */
+ * 1D (AP_ERR_UNSUPPORTED) are rejected. The first call in each CUDA
+ * context (normally once per device: the device's primary context) looks
+ * up the array's device address with cudaGetSymbolAddress and caches it
+ * under that context's id, so make that first call before any stream
+ * capture; a context that is destroyed and re-created is looked up afresh.
+ * All calls share the array and clear it at their start: calls that
+ * overlap on the GPU (on different streams, or from different threads)
+ * race and must not be issued. The call enqueues its work on cuda_stream
+ * (0 = legacy default stream) and synchronises that stream before
+ * returning, also when it fails after enqueueing work. */
 AP_API int ap_update_particles_1d_noalloc(const ap_mesh *mesh, const ap_params *params,
                                           const ap_particles *ptc, size_t number,
                                           const ap_fields *fields, double dt,

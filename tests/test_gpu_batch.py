@@ -106,7 +106,7 @@ def test_batch_autotune_then_steps():
         batch.update_fields(step)
     batch.sync()
     shapes = batch.tile_shapes()
-    assert all(s in ((16, 16), (32, 16)) for s in shapes)
+    assert all(s in ((16, 16), (32, 16), (16, 8), (8, 8), (4, 4)) for s in shapes)
     _compare(alone, batched, tol=1e-6)
     _close(batch, alone, batched)
 
@@ -167,4 +167,24 @@ def test_batch_compaction_equals_alone(tile, spare):
         for key in ("J", "E", "B"):
             for c in range(3):
                 assert_bits(fb[key][c], fa[key][c], f"run {r}: {key}{c + 1}")
+    _close(batch, alone, batched)
+
+
+def test_batch_advance_equals_alone_with_sorts():
+    """ap_batch_advance (a whole round of lab-loop steps in one call, with
+    sort_by_cell every 3 steps and compaction on) leaves every run as the
+    same steps taken alone through the plain path."""
+    specs = _specs(5, 6)
+    alone = [_make(s, spare=2, compact=2) for s in specs]
+    batched = [_make(s, spare=2, compact=2) for s in specs]
+    batch = Batch([d for _, d in batched])
+    for step in range(7):
+        _step_alone(alone, step)
+        if step % 3 == 0 and step != 0:
+            for _, d in alone:
+                d.sort_particles()
+    batch.advance([0] * len(specs), 4, sort_interval=3)
+    batch.advance([4] * len(specs), 3, sort_interval=3)
+    batch.sync()
+    _compare(alone, batched)
     _close(batch, alone, batched)

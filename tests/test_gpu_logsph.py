@@ -310,3 +310,35 @@ def test_inject_ptc_matches_oracle():
     # the injected particles take part in the next update
     ptc_updater_logsph(env).update_particles(data, float(params.delta_t), 0)
     env.close()
+
+
+@pytest.mark.parametrize("passes,data_interval", [(1, 1), (3, 1), (2, 2)])
+def test_smoothing_bit_exact(passes, data_interval):
+    """smooth_current of the log-spherical updater (filter_current_logsph,
+    ptc_updater_logsph.cu:616-666, weighted by the face areas and the cell
+    volume, then axis_rho, :414-438) on the same J and Rho equals the
+    oracle's passes bit for bit: the filter has no transcendental, so the
+    loose bound of the coupled run is not needed here."""
+    case = LsCase((96, 64), 10, 12, smoothing=passes, data_interval=data_interval)
+    rng = np.random.default_rng(13)
+    for key, n in (("J", 3), ("Rho", NSP)):
+        for k in range(n):
+            case.f[key][k][:] = rng.standard_normal(case.f[key][k].shape).astype(np.float32)
+    case.data.set_fields(case.f)
+    case.pusher.smooth_current(case.data, 0)
+    m = case.m
+    tmp = np.zeros_like(case.f["J"][0])
+    for _ in range(passes):
+        for k in range(3):
+            ls.filter_current(m, case.f["J"][k], tmp, case.c32[ls.A1E + k])
+        if data_interval == 1:
+            for k in range(NSP):
+                ls.filter_current(m, case.f["Rho"][k], tmp, case.c32[ls.DV])
+    ls.axis_rho(m, case.f["J"][2])
+    g = case.data.fields_host()
+    sl = (slice(m.guard[1], m.dims[1] - m.guard[1]), slice(m.guard[0], m.dims[0] - m.guard[0]))
+    for k in range(3):
+        assert_bits(g["J"][k][sl], case.f["J"][k][sl], f"J{k + 1}")
+    for k in range(NSP):
+        assert_bits(g["Rho"][k][sl], case.f["Rho"][k][sl], f"Rho{k}")
+    case.close()

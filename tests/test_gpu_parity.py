@@ -454,7 +454,9 @@ def test_continuity_residual():
     """Esirkepov charge conservation through the ABI: rho(t+1) - rho(t) +
     div J = 0 on the bulk, within 1e-6 of max|rho|."""
     pr = _setup((48, 48), 8000, seed=15, tile=(8, 8))
+    pr.env.set_continuity_check(True)
     pr.pusher.update_particles(pr.data, pr.dt, 0)
+    assert np.isnan(pr.data.diagnostics().continuity_residual)  # no rho(t) yet
     rho0 = sum(r.cpu().double() for r in pr.data.Rho).numpy()
     pr.pusher.update_particles(pr.data, pr.dt, 1)
     g = pr.data.fields_host()
@@ -469,6 +471,9 @@ def test_continuity_residual():
     div = (np.roll(j1, -1, axis=1) - j1) + (np.roll(j2, -1, axis=0) - j2)
     res = np.abs(rho1[ys, xs] - rho0[ys, xs] + div).max()
     assert res <= 1e-6 * np.abs(rho1).max(), res
+    # the same reduction on the device, in FP64 (ap_set_continuity_check)
+    dev = pr.data.diagnostics().continuity_residual
+    assert np.isclose(dev, res, rtol=1e-12, atol=1e-300), (dev, res)
 
 
 def test_coupled_steps_within_tolerance():
@@ -506,7 +511,7 @@ def test_fp64_diagnostics_sync_and_async():
         pr.both_update_particles(step)
         pr.both_update_fields(step)
     d = pr.data.diagnostics()
-    host = torch.zeros(6, dtype=torch.float64).pin_memory()
+    host = torch.zeros(7, dtype=torch.float64).pin_memory()
     check_status = pr.env._lib.ap_diagnostics_async(pr.env.ctx, C.c_void_p(host.data_ptr()))
     assert check_status == 0
     pr.env.sync()
@@ -532,3 +537,62 @@ def test_fp64_diagnostics_sync_and_async():
                              host.numpy(), ref):
         assert np.isclose(a, c, rtol=1e-10, atol=1e-12), (name, a, c)
         assert np.isclose(b, c, rtol=1e-10, atol=1e-12), (name, b, c)
+
+
+@pytest.mark.parametrize("N,periodic", [((64, 48), (True, True)), ((64, 48), (False, True)),
+                                        ((96,), (True, True)), ((96,), (False, False))])
+def test_smooth_array_bitexact(N, periodic):
+    """smooth_current(multi_array&) (filter_current_cart_{1,2}d,
+    ptc_updater.cu:501-560) on one array: the bulk equals the oracle's
+    binomial filter bit for bit, with and without boundary sides."""
+    pr = _setup(N, 10, seed=41, periodic=periodic)
+    rng = np.random.default_rng(42)
+    a = rng.standard_normal(pr.f["J"][0].shape).astype(np.float32)
+    import torch
+    dev = pr.data.J[0]
+    dev.copy_(torch.from_numpy(a).reshape(dev.shape))
+    pr.pusher.smooth_current(dev)
+    got = dev.cpu().numpy().reshape(a.shape)
+    ref = a.copy()
+    bnd = (int(not pr.periodic[0]), int(not pr.periodic[0]), int(not pr.periodic[1]),
+           int(not pr.periodic[1]))
+    oracle.filter_current(pr.m, ref, np.zeros_like(ref), bnd)
+    m = pr.m
+    sl = (slice(m.guard[1], m.dims[1] - m.guard[1]) if m.dimension > 1 else slice(0, 1),
+          slice(m.guard[0], m.dims[0] - m.guard[0]))
+    assert_bits(got[sl], ref[sl], "filtered bulk")
+
+
+@pytest.mark.parametrize("N", [(64, 48), (512,)])
+@pytest.mark.parametrize("smoothing", [1, 2, 3])
+def test_update_with_current_smoothing(N, smoothing):
+    """update_particles with current_smoothing passes (smooth_current,
+    ptc_updater.cu:852-873): J and Rho equal the oracle's filter passes
+    (each followed by the periodic guard copy) applied to the same
+    update's unsmoothed current, bit for bit; the particles are unchanged
+    by the smoothing."""
+    n = 8000
+    raw = _setup(N, n, seed=43)
+    params = make_params(N, smoothing=smoothing, capacity=n)
+    sm = Pair(params, raw.f, raw.p)
+    for step in range(2):
+        raw.pusher.update_particles(raw.data, raw.dt, step)
+        sm.pusher.update_particles(sm.data, sm.dt, step)
+        assert_bits(sm.data.particles_host()["p1"], raw.data.particles_host()["p1"], "p1")
+        g_raw, g_sm = raw.data.fields_host(), sm.data.fields_host()
+        m = raw.m
+        bnd = (int(not raw.periodic[0]),) * 2 + (int(not raw.periodic[1]),) * 2
+        J = [g_raw["J"][c].copy() for c in range(3)]
+        R = [r.copy() for r in g_raw["Rho"]]
+        tmp = np.zeros_like(J[0])
+        for _ in range(smoothing):
+            for c in range(3):
+                oracle.filter_current(m, J[c], tmp, bnd)
+                oracle.send_guard_cells(m, J[c], raw.periodic)
+            for r in R:  # data_interval 1: every step has charge output
+                oracle.filter_current(m, r, tmp, bnd)
+                oracle.send_guard_cells(m, r, raw.periodic)
+        for c in range(3):
+            assert_bits(g_sm["J"][c], J[c], f"step {step}: J{c + 1}")
+        for s, r in enumerate(R):
+            assert_bits(g_sm["Rho"][s], r, f"step {step}: Rho{s}")
