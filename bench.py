@@ -57,10 +57,12 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="batched workload: keep every run's tile shape")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="box workload: skip the bounded runs of the other configurations")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
     ap.add_argument("--workload", default="box",
-                    choices=["box", "batched", "served", "logsph"],
+                    choices=["box", "box1d", "batched", "config4", "served", "logsph"],
                     help="box: the 2D box (headline line); batched: many uneven boxes "
                          "through ap_batch_* against the same runs one at a time; served: "
                          "a Poisson stream of 1D gap runs, continuous batching against "
@@ -71,6 +73,7 @@ def parse():
     ap.add_argument("--hbm-budget", type=float, default=60.0,
                     help="served: GB of device memory the resident runs may occupy")
     ap.add_argument("--runs", type=int, default=24, help="batched: number of runs")
+    ap.add_argument("--run-steps", type=int, default=500, help="config4: steps of every run")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="seconds for the whole --impl reference run")
     return ap.parse_args()
@@ -110,7 +113,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", sel, f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -436,12 +439,11 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches, "clocks": clocks,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     env.close()
+    return line
 
 
-AUTOTUNE_STEPS = 8  # 2 candidate tile shapes x 4 steps (ap_batch_autotune)
+AUTOTUNE_STEPS = 35  # 7 candidate shapes / chunks x 5 steps (ap_batch_autotune)
 
 
 def check_live(data, n, what):
@@ -452,7 +454,7 @@ def check_live(data, n, what):
         raise RuntimeError(f"{what}: {live} particles in the store, expected {n}")
 
 
-def run_batched(args):
+def run_batched(args, emit=True):
     """Batched uneven boxes: `runs` independent periodic boxes, side uniform
     in {128, 192, 256, 384, 512}, 16-128 particles per cell (even), the
     box2d field setup, each with its own dt. Two legs from the same seeded
@@ -556,12 +558,414 @@ def run_batched(args):
         "one_at_a_time": alone, "speedup_vs_one_at_a_time": batched / alone,
         "autotune_steps": used, "tile_shapes": shapes,
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
     for env, _, _ in runs:
         env.close()
+    return line
 
 
-def run_logsph(args):
+def run_config4(args, emit=True):
+    """Batched uneven boxes at their stated size: `runs` periodic boxes
+    (default 256), side uniform in {128, 192, 256, 384, 512}, 16-128
+    particles per cell, box2d fields, `run_steps` steps each (default 500),
+    compaction every 2 into a doubled capacity. The runs need more device
+    memory than one B200 has, so aperture3_b200.batching.BoxBatcher admits
+    them in order while their footprint fits `hbm_budget`, tunes the tile
+    shape per box size, and advances the resident runs in rounds of 50
+    steps. The one-at-a-time leg runs every k-th request through the plain
+    path (synchronous lab loop), k = runs / 32, and its rate stands for all
+    of them. Wall clock; aggregate particle-steps/s."""
+    import torch
+    from aperture3_b200 import batching
+
+    dev = torch.device("cuda", 0)
+    reqs = batching.box_requests(args.runs, steps=args.run_steps)
+    total = sum(r.side * r.side * r.ppc for r in reqs)
+    # warm the code paths
+    batching.run_alone(batching.BoxRequest(-1, 128, 16, 3, 1), dev, args.compact)
+    bb = batching.BoxBatcher(dev, hbm_budget=args.hbm_budget * 1e9, compact=args.compact,
+                             sort_interval=args.sort_interval)
+    st = bb.run(reqs)
+    k = max(1, len(reqs) // 32)
+    sample = reqs[::k]
+    t = time.perf_counter()
+    ps = sum(batching.run_alone(r, dev, args.compact, args.sort_interval) for r in sample)
+    alone = ps / (time.perf_counter() - t)
+    line = {
+        "metric": "aggregate particle-steps/s (batched uneven boxes, HBM admission)",
+        "value": st["throughput"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic (seeded, aperture3_b200.ic.box2d per run)",
+        "config": {"workload": f"{args.runs} periodic boxes, side in {{128,192,256,384,512}}, "
+                               f"16-128 ppc, random-mode fields, {args.run_steps} steps each",
+                   "runs": args.runs, "particles": total, "compaction_interval": args.compact,
+                   "hbm_budget_gb": args.hbm_budget},
+        "batched": {k2: v for k2, v in st.items() if k2 != "schedule"},
+        "admission_schedule": st["schedule"],
+        "one_at_a_time": alone,
+        "one_at_a_time_sample": f"every {k}-th run ({len(sample)} runs), plain path",
+        "speedup_vs_one_at_a_time": st["throughput"] / alone,
+    }
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def run_box1d(args, emit=True):
+    """1D periodic plain PIC (the CPU-runnable configuration): 4096 cells,
+    dx = 1/4096, dt = dx/2, 2^20 particles (e-/e+ pairs at shared positions,
+    weight 1), x uniform, p ~ N(0, 0.1^2) per component, E1 = 0.5 sin(2 pi
+    x), B1 = 1 (aperture3_b200.ic.box1d, seed 0); one step is update_particles
+    (Vay push + 1D charge-conserving deposit, Rho every step) and
+    update_fields. The 100 steps of the configuration are timed from the
+    seeded initial state, after a warm-up on a separate copy: device time
+    with the inputs resident (value), and end to end through the C ABI from
+    pinned host memory (e2e). The CPU baseline runs the reference's own 1D
+    kernels compiled for the host on all host threads over the same 100
+    steps, and the line states how far the GPU's final state is from it."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from aperture3_b200 import SimData, SimEnvironment, field_solver, ic, ptc_updater
+    from aperture3_b200._lib import ApPhaseTimes, check
+    from aperture3_b200.sim import PTC_FIELDS
+
+    steps = 100
+    dev = torch.device("cuda", 0)
+    params, fields, ptc = ic.box1d(seed=0, device=dev)
+    n = ptc["x1"].numel()
+    names = [k for k, _ in PTC_FIELDS]
+    stream = torch.cuda.Stream()
+
+    def make():
+        env = SimEnvironment(params)
+        data = SimData(env, capacity=n)
+        env.set_stream(stream)
+        env.set_sync(False)
+        return env, data, ptc_updater(env), field_solver(env)
+
+    dt = params.delta_t
+    # warm-up on a separate copy (first launches, module loads)
+    env, data, pusher, solver = make()
+    data.set_fields_device(fields)
+    data.set_particles_device(ptc)
+    # the initial state in the store's own dtypes, for the end-to-end leg
+    host = {k: data.particles[k][:n].cpu().pin_memory() for k in names}
+    with torch.cuda.stream(stream):
+        for s in range(max(args.warmup, 3)):
+            pusher.update_particles(data, dt, s)
+            solver.update_fields(data, dt, s)
+    env.sync()
+    env.close()
+    del data
+
+    # device-timed: the configuration's 100 steps, inputs resident
+    env, data, pusher, solver = make()
+    data.set_fields_device(fields)
+    data.set_particles_device(ptc)
+    lib = env._lib
+    check(lib.ap_set_profiling(env.ctx, 1), "profiling")
+    launches0 = env.launch_count()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for s in range(steps):
+            pusher.update_particles(data, dt, s)
+            solver.update_fields(data, dt, s)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    env.sync()
+    ms = e0.elapsed_time(e1)
+    launches = env.launch_count() - launches0
+    pt = ApPhaseTimes()
+    check(lib.ap_get_phase_times(env.ctx, pt, 1), "phase times")
+    gpu_final = {k: data.particles[k][:n].cpu().numpy() for k in names}
+    env.close()
+    del data
+
+    G = params.N[0] + 2 * params.guard[0]
+    k_ms = pt.push_deposit_ms / max(pt.push_deposit_launches, 1)
+    achieved = (ALG_BYTES_PER_PARTICLE * n + ALG_BYTES_PER_CELL * G) / (k_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # end to end: upload, 100 steps with a per-step FP64 diagnostics
+    # read-back, download of particles and fields
+    fh = {k: [f.cpu().pin_memory() for f in fields[k]] for k in ("E", "B")}
+    diag_host = torch.zeros((steps, 7), dtype=torch.float64).pin_memory()
+    env, data, pusher, solver = make()
+    lib = env._lib
+    out_p = {k: torch.empty_like(host[k]).pin_memory() for k in names}
+    out_f = {k: [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in getattr(data, k)]
+             for k in ("E", "B", "J")}
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for k in names:
+            data.particles[k][:n].copy_(host[k], non_blocking=True)
+        for k in ("E", "B"):
+            for h, a in zip(fh[k], getattr(data, k)):
+                a.copy_(h, non_blocking=True)
+        data.particles_modified(n)
+        for s in range(steps):
+            pusher.update_particles(data, dt, s)
+            solver.update_fields(data, dt, s)
+            check(lib.ap_diagnostics_async(env.ctx, C.c_void_p(diag_host[s].data_ptr())),
+                  "ap_diagnostics_async")
+        for k in names:
+            out_p[k].copy_(data.particles[k][:n], non_blocking=True)
+        for k in out_f:
+            for h, a in zip(out_f[k], getattr(data, k)):
+                h.copy_(a, non_blocking=True)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    env.sync()
+    ms_e2e = e0.elapsed_time(e1)
+    env.close()
+    del data
+    h2d = sum(t.numel() * t.element_size() for t in host.values()) + \
+        sum(t.numel() * t.element_size() for k in fh for t in fh[k])
+    d2h = sum(t.numel() * t.element_size() for t in out_p.values()) + \
+        sum(t.numel() * t.element_size() for k in out_f for t in out_f[k])
+    for k in names:
+        if not np.array_equal(out_p[k].numpy().view(np.uint8), gpu_final[k].view(np.uint8)):
+            raise RuntimeError(f"1D e2e run differs from the device-timed run in {k}")
+
+    # CPU: the reference's own 1D kernels on all host threads, same 100 steps
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        threads = cpu_threads()
+        m = oracle.make_mesh(params.N, params.guard, params.lower, params.size)
+        f = oracle.new_fields(m, params.num_species)
+        for c in range(3):
+            f["E"][c][:] = fields["E"][c].cpu().numpy()
+            f["B"][c][:] = fields["B"][c].cpu().numpy()
+        p = ic.to_numpy_ptc({k: v.cpu() for k, v in ptc.items()})
+        charges, masses = [-1.0] + [1.0] * 7, [1.0] * 8
+        per = [1, 0, 0]
+        ref = oracle.load_ref_mt(build=False) is not None
+        t = time.perf_counter()
+        for s in range(steps):
+            if ref:
+                oracle.ref_update_particles_mt(m, p, n, f, dt, s, params.data_interval, 2,
+                                               charges, masses, per, threads)
+            else:
+                oracle.update_particles(m, p, n, f, dt, s, params.data_interval, 2, 0, charges,
+                                        masses, per, threads)
+            oracle.update_fields(m, f, dt, s, per)
+        el = time.perf_counter() - t
+        same_cell = float(np.mean(p["cell"] == gpu_final["cell"]))
+        rel = 0.0
+        for k in ("p1", "p2", "p3"):
+            a, b = gpu_final[k].astype(np.float64), p[k].astype(np.float64)
+            rel = max(rel, float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-3))))
+        cpu = {"value": n * steps / el, "unit": UNIT, "cores": threads,
+               "kind": "reference" if ref else "port",
+               "sample": f"the whole configuration ({n} particles, {steps} steps), "
+                         + ("the reference's 1D push and deposit kernels compiled for the "
+                            "host (oracle/_ref)" if ref else "C restatement (oracle)"),
+               "final_state_vs_gpu": {"same_cell_fraction": same_cell,
+                                      "max_momentum_rel_diff": rel,
+                                      "note": "free-running 100 steps; the CPU sums J with "
+                                              "float atomics in particle order, the GPU "
+                                              "exactly, so the runs drift apart at FP32 "
+                                              "rounding level"}}
+    value = n * steps / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded initial state, aperture3_b200.ic.box1d, seed 0)",
+        "config": {"workload": "1D periodic plain PIC, 4096 cells, 2^20 particles (e-/e+), "
+                               "E1 = 0.5 sin(2 pi x), B1 = 1, 100 steps of Vay push + 1D "
+                               "charge-conserving deposit + Yee update, seed 0",
+                   "cells": params.N[0], "particles": n, "steps": steps,
+                   "l2": "inputs (50 MB of particles) fit in L2: no flush between steps; "
+                         "the line is a throughput of the configuration as specified"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "kernel": "k_push_deposit_1d", "kernel_ms": k_ms},
+        "phases_ms_per_step": {"push_deposit": pt.push_deposit_ms / steps,
+                               "finalize": pt.finalize_ms / steps,
+                               "fields": pt.fields_ms / steps},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n * steps / (ms_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps + 56,
+                "includes": "initial-state upload, 100 steps with a per-step FP64 diagnostics "
+                            "read-back, final particle and field download"},
+        "gpu_launches": launches,
+    }
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def box_parity(ppc=4, N=1024, seed=77):
+    """One update_particles step of the 2D box on the GPU against the
+    reference's own push and deposit kernels compiled for the host
+    (oracle/_ref, all threads) on the same seeded state: a 1024 x 1024 grid
+    at `ppc` particles per cell (the full grid; fewer particles per cell
+    than the benchmark so that the CPU step takes a second), 16 x 16 tiles,
+    charge output on. Counts particle members that differ in any bit, and
+    the current's largest difference relative to max |J| against the
+    reference (which sums in FP32 with atomics) and against the FP64 sum
+    of the same contributions (the parity bar, 1e-6)."""
+    import numpy as np
+    import torch
+    import oracle
+    from aperture3_b200 import SimData, SimEnvironment, ic, ptc_updater
+
+    dev = torch.device("cuda", 0)
+    params, fields, ptc = ic.box2d(seed=seed, N=N, ppc=ppc, device="cpu", tile=(16, 16),
+                                   data_interval=1)
+    n = ptc["x1"].numel()
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=n)
+    data.set_fields_device({k: [c.to(dev) for c in v] for k, v in fields.items()})
+    data.set_particles_device({k: v.to(dev) for k, v in ptc.items()})
+    dt = params.delta_t
+    ptc_updater(env).update_particles(data, dt, 0)
+    got = data.particles_host()
+    g = data.fields_host()
+    env.close()
+    m = oracle.make_mesh(params.N, params.guard, params.lower, params.size)
+    f = oracle.new_fields(m, params.num_species)
+    for c in range(3):
+        f["E"][c][:] = fields["E"][c].numpy()
+        f["B"][c][:] = fields["B"][c].numpy()
+    p0 = ic.to_numpy_ptc(ptc)
+    charges, masses = [-1.0] + [1.0] * 7, [1.0] * 8
+    per = [1, 1, 0]
+    # FP64 sum of the reference's FP32 contributions
+    p64 = oracle.copy_ptc(p0)
+    oracle.push(m, p64, n, np.float32(dt), f["E"] + f["B"], charges, masses)
+    J64 = [np.zeros(f["J"][0].shape) for _ in range(3)]
+    R64 = [np.zeros(f["J"][0].shape) for _ in range(params.num_species)]
+    oracle.deposit(m, p64, n, np.float32(dt), 0, 1, J64, R64, charges, f64=True)
+    for a in J64:
+        oracle.send_add_guard_cells(m, a, per)
+    ref = oracle.load_ref_mt(build=False) is not None
+    pr = oracle.copy_ptc(p0)
+    if ref:
+        oracle.ref_update_particles_mt(m, pr, n, f, dt, 0, 1, params.num_species, charges,
+                                       masses, per, cpu_threads())
+    else:
+        oracle.update_particles(m, pr, n, f, dt, 0, 1, params.num_species, 0, charges, masses,
+                                per, cpu_threads())
+    diff = {}
+    for k in ("x1", "x2", "x3", "p1", "p2", "p3", "E", "cell", "flag", "weight", "id"):
+        a = np.ascontiguousarray(got[k][:n]).view(np.uint8).reshape(n, -1)
+        b = np.ascontiguousarray(pr[k][:n]).view(np.uint8).reshape(n, -1)
+        diff[k] = int(np.count_nonzero((a != b).any(axis=1)))
+    jr, j64 = 0.0, 0.0
+    for c in range(3):
+        gj = g["J"][c].astype(np.float64)
+        jr = max(jr, float(np.abs(gj - f["J"][c]).max() / max(np.abs(f["J"][c]).max(), 1e-30)))
+        j64 = max(j64, float(np.abs(gj - J64[c]).max() / max(np.abs(J64[c]).max(), 1e-30)))
+    return {"grid": [N, N], "ppc": ppc, "particles": n, "tile": [16, 16],
+            "against": ("the reference's push and deposit kernels compiled for the host"
+                        if ref else "the C restatement"),
+            "particle_members_differing": diff,
+            "J_max_rel_diff_vs_reference_fp32": jr, "J_max_rel_diff_vs_fp64_sum": j64,
+            "J_bar": 1e-6}
+
+
+def logsph_fp64_error(N=64, steps=2000, seed=11):
+    """The log-spherical configuration on a reduced N x N grid (the same
+    seeded setup, aperture3_b200.ic.logsph, with as many particles as N^2
+    cells hold) advanced `steps` coupled steps three ways: on the GPU, by the
+    FP32 CPU restatement and by its FP64 build (Scalar = double, the truth).
+    Errors against FP64 of the GPU and of the FP32 restatement, over the
+    particles alive in both (position in cells, momentum relative) and over
+    the fields (relative to each field's maximum)."""
+    import numpy as np
+    import torch
+    import oracle
+    from oracle import logsph as ls
+    from aperture3_b200 import (SimData, SimEnvironment, field_solver_logsph, ic,
+                                ptc_updater_logsph)
+
+    dev = torch.device("cuda", 0)
+    params, fields, ptc = ic.logsph(seed=seed, N=N, ppc=32, device="cpu")
+    n = ptc["x1"].numel()
+    env = SimEnvironment(params)
+    data = SimData(env, capacity=n)
+    data.set_fields_device({k: [c.to(dev) for c in v] for k, v in fields.items()})
+    data.set_particles_device({k: v.to(dev) for k, v in ptc.items()})
+    pusher, solver = ptc_updater_logsph(env), field_solver_logsph(env)
+    m = oracle.make_mesh(params.N, params.guard, params.lower, params.size)
+    f32 = oracle.new_fields(m, params.num_species)
+    for k in ("E", "B", "Ebg", "Bbg"):
+        for c in range(3):
+            f32[k][c][:] = fields[k][c].numpy()
+    p32 = ic.to_numpy_ptc(ptc)
+    lp = ls.ls_params(compactness=params.compactness, omega=params.omega,
+                      gravity=params.gravity, rad_cooling_coef=params.rad_cooling_coef,
+                      B0=params.B0, damping_coef=params.damping_coef,
+                      rad_cooling_on=params.rad_cooling_on, damping_length=params.damping_length)
+    c32, c64 = ls.coef(m), ls.coef(m, f64=True)
+    p64, f64 = ls.to_f64(p32), ls.fields_to_f64(f32)
+    dt = np.float32(params.delta_t)
+    om = np.float32(params.omega)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        pusher.update_particles(data, float(dt), s)
+        solver.update_fields(data, float(dt), s * float(dt))
+        solver.apply_boundary(data, params.omega, s * float(dt))
+        for p, f, c in ((p32, f32, c32), (p64, f64, c64)):
+            ls.update_particles(m, lp, p, n, f, c, dt, s, params.data_interval,
+                                params.num_species, params.current_smoothing, env.charges,
+                                env.masses)
+            ls.update_fields(m, lp, f, c, dt)
+            ls.field_boundary(m, lp, f, om)
+    got = data.particles_host()
+    g = data.fields_host()
+    env.close()
+
+    def phys(p):
+        cc = p["cell"].astype(np.int64)
+        live = p["cell"] != oracle.MAX_CELL
+        return (live, cc % m.dims[0] + p["x1"].astype(np.float64),
+                cc // m.dims[0] + p["x2"].astype(np.float64))
+
+    def perr(a, ref):
+        # particles keep their slots here (no sort), so slot i is particle i
+        la, xa, ya = phys(a)
+        lr, xr, yr = phys(ref)
+        both = la & lr
+        pos = np.hypot(xa - xr, ya - yr)[both]
+        pa = np.stack([a[k] for k in ("p1", "p2", "p3")]).astype(np.float64)[:, both]
+        pr = np.stack([ref[k] for k in ("p1", "p2", "p3")]).astype(np.float64)[:, both]
+        mom = np.linalg.norm(pa - pr, axis=0) / np.maximum(np.linalg.norm(pr, axis=0), 1e-30)
+        q = lambda v: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),  # noqa: E731
+                       "p99.9": float(np.percentile(v, 99.9)), "max": float(v.max())}
+        return {"position_cells": q(pos), "momentum_rel": q(mom),
+                "alive_in_one_only": float(np.mean(la != lr)), "alive": int(both.sum())}
+
+    def ferr(fa):
+        out = {}
+        for key in ("E", "B", "J"):
+            for c in range(3):
+                ref = f64[key][c]
+                scale = max(float(np.abs(ref).max()), 1e-30)
+                out[f"{key}{c + 1}"] = float(np.abs(fa[key][c].astype(np.float64) - ref).max()
+                                             / scale)
+        return out
+
+    return {"grid": [N, N], "particles": n, "steps": steps, "seed": seed,
+            "seconds": time.perf_counter() - t0,
+            "gpu_vs_fp64": {"particles": perr(got, p64), "fields_max_rel": ferr(g)},
+            "fp32_cpu_vs_fp64": {"particles": perr(p32, p64), "fields_max_rel": ferr(f32)},
+            "note": "reduced grid of the log-spherical configuration (same seeded setup); "
+                    "the FP64 truth is the C restatement built with Scalar = double"}
+
+
+def run_logsph(args, emit=True, fp64_error=True):
     """Log-spherical grid 1024 x 1024, r in [1, 50], dipole B with corotation
     E, 32 particles per cell scaled by exp(-(r - 1) / 0.5), gamma up to 1e6
     along B (aperture3_b200.ic.logsph). A step is the pulsar lab's loop body:
@@ -632,11 +1036,15 @@ def run_logsph(args):
                                "fields": pt.fields_ms / args.steps,
                                "sort_by_cell": pt.sort_ms / args.steps},
     }
-    print(json.dumps(line), flush=True)
     env.close()
+    if fp64_error:
+        line["fp64_error_after_2000_steps"] = logsph_fp64_error()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
-def run_served(args):
+def run_served(args, emit=True):
     """Served stream of 1D gap runs: `runs` requests with Poisson arrivals
     (50/s), 512-16384 cells, 32-256 particles per cell, 200-5000 steps
     scaled by --steps-scale, E_parallel ramp amplitude in [0.1, 10], pair
@@ -667,7 +1075,9 @@ def run_served(args):
         "served": st_b, "one_at_a_time": st_a,
         "speedup_vs_one_at_a_time": st_b["throughput"] / st_a["throughput"],
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_e2e(args, env, data, pusher, solver, dt, stream, n):
@@ -702,8 +1112,8 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
         sum(t.numel() * t.element_size() for v in fhost.values() for t in v)
     # per-step FP64 diagnostics copied into pinned host memory without a
     # host synchronisation per step (ap_diagnostics_async)
-    diag_host = torch.zeros((args.steps, 6), dtype=torch.float64).pin_memory()
-    d2h_diag = 48
+    diag_host = torch.zeros((args.steps, 7), dtype=torch.float64).pin_memory()
+    d2h_diag = 56
     lib = env._lib
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -746,6 +1156,42 @@ def run_e2e(args, env, data, pusher, solver, dt, stream, n):
                         "readback, final particle and field download"}
 
 
+def run_extras(args):
+    """The other configurations, bounded, for the default single-GPU line:
+    parity of one box step against the reference's kernels, the 1D
+    configuration (its own roofline, CPU baseline and e2e), the
+    log-spherical grid (throughput at 1024^2 over 20 steps, and the error
+    against the FP64 build after 2000 steps on a reduced grid), the batched
+    boxes (24 runs, 20 timed steps) and the served stream (24 requests,
+    p50/p99 completion latency against one at a time)."""
+    import copy
+    out = {}
+    t0 = time.perf_counter()
+
+    def timed(name, fn):
+        t = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # reported, not hidden: the key carries the error
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        if isinstance(out[name], dict):
+            out[name]["bench_seconds"] = time.perf_counter() - t
+
+    a = copy.copy(args)
+    a.warmup, a.steps = 3, 20
+    timed("parity_box_one_step", box_parity)
+    timed("config_1d", lambda: run_box1d(args, emit=False))
+    timed("logsph", lambda: run_logsph(a, emit=False))
+    ab = copy.copy(a)
+    ab.runs = 24
+    timed("batched", lambda: run_batched(ab, emit=False))
+    asv = copy.copy(a)
+    asv.runs, asv.steps_scale, asv.hbm_budget = 24, 1.0, 60.0
+    timed("served", lambda: run_served(asv, emit=False))
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -762,12 +1208,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.workload in ("batched", "served", "logsph"):
+        if args.workload in ("batched", "served", "logsph", "box1d", "config4"):
             if rank == 0:
-                {"batched": run_batched, "served": run_served,
-                 "logsph": run_logsph}[args.workload](args)
+                {"batched": run_batched, "served": run_served, "logsph": run_logsph,
+                 "box1d": run_box1d, "config4": run_config4}[args.workload](args)
             return
-        run_ours(args, rank, world, local_rank)
+        line = run_ours(args, rank, world, local_rank)
+        if rank == 0:
+            if world == 1 and not args.no_extras:
+                line["other_configs"] = run_extras(args)
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist
