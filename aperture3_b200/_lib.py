@@ -94,6 +94,23 @@ class ApGapParams(C.Structure):
     _fields_ = [("B0", C.c_float)]
 
 
+class ApGrParams(C.Structure):
+    """ap_gr_params: SimParams::a, omega, B0 for the 1D GR lab."""
+    _fields_ = [("a", C.c_float), ("omega", C.c_float), ("B0", C.c_float)]
+
+
+class ApGrTable(C.Structure):
+    """ap_gr_table: the tabulated field-line data of the 1D GR lab."""
+    _fields_ = [("r", C.c_void_p), ("B1", C.c_void_p), ("B3", C.c_void_p), ("jr", C.c_void_p),
+                ("rho", C.c_void_p), ("theta", C.c_void_p), ("dpsidth", C.c_void_p),
+                ("n", C.c_size_t)]
+
+
+GR_TABLE_KEYS = ("r", "B1", "B3", "jr", "rho", "theta", "dpsidth")
+GR_COEF_NAMES = ("D1", "D2", "D3", "alpha", "theta", "K1", "K1_j", "j0", "agrr", "agrf", "rho0",
+                 "gamma_rr", "gamma_ff", "beta_phi", "B3B1")
+
+
 class ApLogsphParams(C.Structure):
     """ap_logsph_params: the dev_params members of the log-spherical kernels."""
     _fields_ = [("compactness", C.c_float), ("omega", C.c_float), ("gravity", C.c_float),
@@ -151,6 +168,9 @@ SIGNATURES = {
     "ap_ctx_create_logsph": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                   C.POINTER(ApLogsphParams), C.POINTER(_vp)]),
     "ap_logsph_coef": (_i, [_vp, _i, C.POINTER(ApArray)]),
+    "ap_gr_coef": (_i, [_vp, _i, C.POINTER(ApArray)]),
+    "ap_ctx_create_1dgr": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams), C.POINTER(ApGrParams),
+                                C.POINTER(ApGrTable), C.POINTER(_vp)]),
     "ap_ctx_create_1dgap": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams), C.POINTER(ApGapParams),
                                  C.POINTER(_vp)]),
     "ap_logsph_field_boundary": (_i, [_vp, C.c_double]),

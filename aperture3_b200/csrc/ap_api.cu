@@ -5,6 +5,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -530,6 +531,90 @@ int update_particles_gap(Ctx *c, double dt, uint32_t step) {
   return finish(c);
 }
 
+// ptc_updater_1dgr::update_particles (ptc_updater_1dgr.cu:418-473).
+int update_particles_gr(Ctx *c, double dt, uint32_t step) {
+  const ap_params &pr = c->params;
+  if (c->number == 0) return finish(c);  // nothing at all without particles (:422)
+  const int ncomp = 3 + pr.num_species;
+  const int n = c->mesh.dims[0];
+  const int bl = !pr.periodic[0], bu = !pr.periodic[0];  // is_boundary(0), (1)
+  const float *K1 = coef_array(*c, AP_GR_K1).ptr, *K1j = coef_array(*c, AP_GR_K1_J).ptr;
+  int ph = phase_begin(c, kPhFinalize);
+  // J and Rho are zeroed (:423-426); the finalize writes every component
+  AP_TRY(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * c->acc_comp * ncomp,
+                         c->stream));
+  if (!c->scale_valid) AP_TRY(launch_fixed_scale(*c));
+  AP_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
+  // E3 = E1, smoothed current_smoothing times through E2 with K1_j (:428-435)
+  float *E1 = c->fields.E[0].ptr, *E2 = c->fields.E[1].ptr, *E3 = c->fields.E[2].ptr;
+  AP_TRY(cudaMemcpyAsync(E3, E1, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  for (int it = 0; it < pr.current_smoothing; ++it) {
+    AP_TRY(launch_gr_filter(*c, E3, E2, K1j, bl, bu));
+    AP_TRY(cudaMemcpyAsync(E3, E2, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  phase_end(c, ph);
+  PushDepositParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.m = c->mk;
+  P.p = PtcK{c->ptc.x1, c->ptc.x2, c->ptc.x3, c->ptc.p1, c->ptc.p2,
+             c->ptc.p3, c->ptc.E,  c->ptc.weight, c->ptc.cell, c->ptc.flag};
+  P.F[2] = FieldArr{E3, (int)(c->fields.E[2].pitch / 4)};
+  P.acc = c->acc;
+  P.acc_pitch = c->mesh.dims[0];
+  P.acc_comp = c->acc_comp;
+  P.fx_used = c->fx_used;
+  P.n_max = c->n_max;
+  P.wmax = c->wmax;
+  P.number = c->number;
+  P.status = c->status;
+  P.num_species = pr.num_species;
+  P.dt = (float)dt;
+  P.qmax = 0.0f;
+  for (int s = 0; s < AP_MAX_SPECIES; ++s) {
+    P.qmax = fmaxf(P.qmax, fabsf(pr.charges[s]));
+    P.charge[s] = pr.charges[s];
+    P.mass[s] = pr.masses[s];
+  }
+  // J1 contributions carry delta / (dt K1_j), Rho ones 1 / K1 (:280-288)
+  const float kj = c->gr_kfac * c->mesh.delta[0] / (float)dt;
+  P.qmax *= fmaxf(1.0f, fmaxf(kj, c->gr_kfac));
+  GrK G;
+  G.D1 = coef_array(*c, AP_GR_D1).ptr;
+  G.D2 = coef_array(*c, AP_GR_D2).ptr;
+  G.D3 = coef_array(*c, AP_GR_D3).ptr;
+  G.alpha = coef_array(*c, AP_GR_ALPHA).ptr;
+  G.theta = coef_array(*c, AP_GR_THETA).ptr;
+  G.K1 = K1;
+  G.K1_j = K1j;
+  G.agrr = coef_array(*c, AP_GR_AGRR).ptr;
+  G.B3B1 = coef_array(*c, AP_GR_B3B1).ptr;
+  G.a = c->gr.a;
+  G.omega = c->gr.omega;
+  G.step = step;
+  G.data_interval = pr.data_interval;
+  ph = phase_begin(c, kPhPushDeposit);
+  AP_TRY(launch_gr_push_deposit(*c, P, G));
+  phase_end(c, ph);
+  ph = phase_begin(c, kPhFinalize);
+  AP_TRY(launch_finalize_current(*c, ncomp));
+  // J1 (K1_j) and each Rho (K1) smoothed current_smoothing times (:447-466)
+  float *tmp = c->tmp_j;
+  for (int it = 0; it < pr.current_smoothing; ++it) {
+    AP_TRY(launch_gr_filter(*c, c->fields.J[0].ptr, tmp, K1j, bl, bu));
+    AP_TRY(cudaMemcpyAsync(c->fields.J[0].ptr, tmp, sizeof(float) * n, cudaMemcpyDeviceToDevice,
+                           c->stream));
+    for (int s = 0; s < pr.num_species; ++s) {
+      AP_TRY(launch_gr_filter(*c, c->fields.Rho[s].ptr, tmp, K1, bl, bu));
+      AP_TRY(cudaMemcpyAsync(c->fields.Rho[s].ptr, tmp, sizeof(float) * n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+    }
+  }
+  c->rho_is_zero = false;
+  phase_end(c, ph);
+  if (!c->sync) return AP_OK;
+  return check_status(c);  // AP_ERR_MOVED_FAR
+}
+
 // First part of an update: zero the accumulators, refresh the weight bound
 // and the tile order if needed, and fill the kernel parameters. Returns
 // AP_OK; *has_work is false when there are no particles.
@@ -787,6 +872,7 @@ extern "C" {
 AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   if (!c || !c->fields_bound || !c->ptc_bound) return AP_ERR_INVALID;
   if (c->coord == 2) return update_particles_gap(c, dt, step);
+  if (c->coord == 3) return update_particles_gr(c, dt, step);
   PushDepositParams P;
   bool has_work = false;
   AP_TRY_ST(update_prepare(c, dt, step, P, &has_work));
@@ -825,6 +911,12 @@ AP_API int ap_update_fields(ap_ctx *c, double dt, uint32_t step) {
   if (c->coord == 2) {
     // field_solver_1dgap::update_fields (field_solver_1dgap.cu:28-40)
     AP_TRY(launch_gap_update_e(*c, (float)(c->gap.B0 * 1.6), (float)dt));
+    phase_end(c, ph);
+    return finish(c);
+  }
+  if (c->coord == 3) {
+    // field_solver_1dgr::update_fields (field_solver_1dgr.cu:29-44)
+    AP_TRY(launch_gr_update_e(*c, coef_array(*c, AP_GR_J0).ptr, (float)dt));
     phase_end(c, ph);
     return finish(c);
   }
@@ -1006,6 +1098,50 @@ AP_API int ap_ctx_create_1dgap(const ap_mesh *mesh, const ap_params *params,
   c->coord = 2;
   c->gap = *gap;
   *out = c;
+  return AP_OK;
+}
+
+AP_API int ap_ctx_create_1dgr(const ap_mesh *mesh, const ap_params *params,
+                              const ap_gr_params *gr, const ap_gr_table *table, ap_ctx **out) {
+  if (!mesh || !params || !gr || !table || !out) return AP_ERR_INVALID;
+  *out = nullptr;
+  if (make_meshk(*mesh).dim != 1) return AP_ERR_UNSUPPORTED;
+  if (table->n < 2 || !table->r || !table->B1 || !table->B3 || !table->jr || !table->rho ||
+      !table->theta || !table->dpsidth)
+    return AP_ERR_INVALID;
+  std::vector<float> co[AP_GR_NCOEF];
+  host_gr_coef(*mesh, *gr, *table, co);
+  // largest 1 / |K1| and 1 / |K1_j| the deposit can divide by
+  float kfac = 0.0f;
+  for (int k : {AP_GR_K1, AP_GR_K1_J})
+    for (float v : co[k])
+      if (v != 0.0f && std::isfinite(1.0f / v)) kfac = fmaxf(kfac, fabsf(1.0f / v));
+  ap_ctx *c = nullptr;
+  int st = ap_ctx_create(mesh, params, &c);
+  if (st != AP_OK) return st;
+  c->coord = 3;
+  c->gr = *gr;
+  c->gr_kfac = kfac > 0.0f ? kfac : 1.0f;
+  const size_t n0 = (size_t)mesh->dims[0];
+  c->coef_pitch = n0 * sizeof(float);
+  if (cudaMalloc(&c->coef, c->coef_pitch * AP_GR_NCOEF) != cudaSuccess) {
+    c->coef = nullptr;
+    ap_ctx_destroy(c);
+    return AP_ERR_NOMEM;
+  }
+  for (int k = 0; k < AP_GR_NCOEF; ++k)
+    if (cudaMemcpy(reinterpret_cast<char *>(c->coef) + k * c->coef_pitch, co[k].data(),
+                   c->coef_pitch, cudaMemcpyHostToDevice) != cudaSuccess) {
+      ap_ctx_destroy(c);
+      return AP_ERR_CUDA;
+    }
+  *out = c;
+  return AP_OK;
+}
+
+AP_API int ap_gr_coef(ap_ctx *c, int which, ap_array *out) {
+  if (!c || !out || c->coord != 3 || which < 0 || which >= AP_GR_NCOEF) return AP_ERR_INVALID;
+  *out = coef_array(*c, which);
   return AP_OK;
 }
 

@@ -4,6 +4,8 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <vector>
 #include <stdint.h>
 
 #include "../../include/aperture_b200.h"
@@ -258,8 +260,10 @@ struct Ctx {
   bool compact_direct = false;      // output in the caller's free half, no copy back
 
   // log-spherical grid (ap_ctx_create_logsph)
-  int coord = 0;                // 0 Cartesian, 1 log-spherical, 2 1D gap
+  int coord = 0;                // 0 Cartesian, 1 log-spherical, 2 1D gap, 3 1D GR
   ap_gap_params gap{};          // 1D gap lab parameters
+  ap_gr_params gr{};            // 1D GR lab parameters (coefficients in coef)
+  float gr_kfac = 1.0f;         // bound of |J1, Rho contribution| / (|q| w) in the GR deposit
   double *ls_surface = nullptr;  // log-spherical injection: surface densities
   uint32_t inject_calls = 0;
   uint64_t inject_next_id = 1ull << 62;
@@ -347,6 +351,20 @@ cudaError_t launch_gap_push_deposit(Ctx &c, const PushDepositParams &P);
 cudaError_t launch_gap_filter(Ctx &c, const float *src, float *dst, int bnd_lower,
                               int bnd_upper);
 cudaError_t launch_gap_update_e(Ctx &c, float j0, float dt);
+
+// 1D GR lab (k_gr.cu): coefficient pointers and parameters of the pusher.
+struct GrK {
+  const float *D1, *D2, *D3, *alpha, *theta, *K1, *K1_j, *agrr, *B3B1;
+  float a, omega;
+  uint32_t step;
+  int data_interval;
+};
+void host_gr_coef(const ap_mesh &m, const ap_gr_params &gp, const ap_gr_table &t,
+                  std::vector<float> *co);
+cudaError_t launch_gr_push_deposit(Ctx &c, const PushDepositParams &P, const GrK &G);
+cudaError_t launch_gr_filter(Ctx &c, const float *src, float *dst, const float *k1,
+                             int bnd_lower, int bnd_upper);
+cudaError_t launch_gr_update_e(Ctx &c, const float *j0, float dt);
 
 cudaError_t launch_ls_finalize(Ctx &c, float dt, bool do_rho, bool zero_axis);
 cudaError_t launch_ls_smooth(Ctx &c, bool do_rho);

@@ -67,6 +67,8 @@ class SimParams:
     rad_cooling_coef: float = 1.0
     damping_length: int = 30
     damping_coef: float = 0.002
+    # 1D GR lab (coord_system "1DGR"): black hole spin (src/sim_params.h:63)
+    a: float = 0.0
 
     @classmethod
     def from_toml(cls, path: str) -> "SimParams":
@@ -92,7 +94,11 @@ def _pad3(v, fill):
 class SimEnvironment:
     """sim_environment (src/sim_environment.h) for one rank."""
 
-    def __init__(self, params: SimParams, device: Optional[int] = None):
+    def __init__(self, params: SimParams, device: Optional[int] = None,
+                 gr_table: Optional[Dict[str, np.ndarray]] = None):
+        """gr_table (1D GR lab only): the tabulated field-line data the
+        reference reads from coef.h5 -- arrays r, B1, B3, jr, rho, theta and
+        dpsidth of equal length, r increasing."""
         self.params = params
         if device is not None:
             torch.cuda.set_device(device)
@@ -122,7 +128,20 @@ class SimEnvironment:
         ctx = C.c_void_p()
         self.logsph = str(params.coord_system).lower() in ("logspherical", "logsph", "log_sph")
         self.gap = str(params.coord_system).lower() in ("1dgap", "gap")
-        if self.gap:
+        self.gr = str(params.coord_system).lower() in ("1dgr", "gr")
+        if self.gr:
+            if gr_table is None:
+                raise ValueError("a 1D GR environment needs gr_table")
+            cols = [np.ascontiguousarray(gr_table[k], dtype=np.float32)
+                    for k in _lib.GR_TABLE_KEYS]
+            if len({len(c) for c in cols}) != 1:
+                raise ValueError("gr_table arrays differ in length")
+            self._gr_cols = cols  # kept alive for the call
+            tab = _lib.ApGrTable(*[c.ctypes.data for c in cols], len(cols[0]))
+            gp = _lib.ApGrParams(float(params.a), float(params.omega), float(params.B0))
+            check(self._lib.ap_ctx_create_1dgr(C.byref(self.mesh), C.byref(ap), C.byref(gp),
+                                               C.byref(tab), C.byref(ctx)), "ap_ctx_create_1dgr")
+        elif self.gap:
             gp = _lib.ApGapParams(float(params.B0))
             check(self._lib.ap_ctx_create_1dgap(C.byref(self.mesh), C.byref(ap), C.byref(gp),
                                                 C.byref(ctx)), "ap_ctx_create_1dgap")
@@ -222,6 +241,14 @@ class SimEnvironment:
         d0, d1 = self.mesh.dims[0], self.mesh.dims[1]
         rows = device_to_host(a.ptr, a.pitch * d1).view(np.float32).reshape(d1, -1)
         return rows[:, :d0].copy()
+
+    def gr_coef(self, which) -> np.ndarray:
+        """Host copy of one Grid_1dGR coefficient array (grid_1dgr.h:16-20),
+        by index or by its name in _lib.GR_COEF_NAMES."""
+        k = _lib.GR_COEF_NAMES.index(which) if isinstance(which, str) else int(which)
+        a = ApArray()
+        check(self._lib.ap_gr_coef(self.ctx, k, C.byref(a)), "ap_gr_coef")
+        return device_to_host(a.ptr, 4 * self.mesh.dims[0]).view(np.float32).copy()
 
     def launch_count(self) -> int:
         return int(self._lib.ap_launch_count(self.ctx))
@@ -717,6 +744,34 @@ class field_solver_1dgap:
 
     def update_fields(self, data: SimData, dt: float, time: float = 0.0):
         """E1 += (1.6 B0 - J1) dt (field_solver_1dgap.cu:28-40)."""
+        check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), 0), "ap_update_fields")
+
+
+class ptc_updater_1dgr:
+    """ptc_updater_1dgr (src/algorithms/ptc_updater_1dgr.h:11-30), for an
+    environment with coord_system = '1DGR'."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.gr:
+            raise ValueError("ptc_updater_1dgr needs coord_system = '1DGR'")
+        self.env = env
+
+    def update_particles(self, data: SimData, dt: float, step: int = 0):
+        """ptc_updater_1dgr::update_particles (ptc_updater_1dgr.cu:418-473)."""
+        check(self.env._lib.ap_update_particles(self.env.ctx, float(dt), int(step)),
+              "ap_update_particles")
+
+
+class field_solver_1dgr:
+    """field_solver_1dgr (src/algorithms/field_solver_1dgr.h:11-22)."""
+
+    def __init__(self, env: SimEnvironment):
+        if not env.gr:
+            raise ValueError("field_solver_1dgr needs coord_system = '1DGR'")
+        self.env = env
+
+    def update_fields(self, data: SimData, dt: float, time: float = 0.0):
+        """E1 += (j0 - J1) dt (field_solver_1dgr.cu:14-44)."""
         check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), 0), "ap_update_fields")
 
 

@@ -26,8 +26,12 @@ class Grid {
 class sim_environment {
  public:
   // The reference constructor (int*, char***) initialises MPI and parses
-  // the configuration file; this one takes the parsed parameters.
-  explicit sim_environment(const SimParams &params, int device = -1) : params_(params) {
+  // the configuration file; this one takes the parsed parameters. A 1D GR
+  // environment (coord_system "1DGR") also takes the field-line table the
+  // reference's Grid_1dGR reads from coef.h5 (grid_1dgr.cpp:41-66).
+  explicit sim_environment(const SimParams &params, int device = -1,
+                           const ap_gr_table *gr_table = nullptr)
+      : params_(params) {
     if (device >= 0) cuda_check(cudaSetDevice(device), "cudaSetDevice");
     // Grid::init (src/core/grid.cpp:31-48)
     Quadmesh &m = grid_.mesh();
@@ -72,6 +76,14 @@ class sim_environment {
       lp.rad_cooling_on = params.rad_cooling_on ? 1 : 0;
       lp.damping_length = params.damping_length;
       ap_check(ap_ctx_create_logsph(&m, &p, &lp, &ctx_), "ap_ctx_create_logsph");
+    } else if (std::strcmp(params.coord_system, "1DGR") == 0) {
+      // the 1D GR lab (labs/1dgr): ptc_updater_1dgr / field_solver_1dgr
+      if (!gr_table) throw ap_error(AP_ERR_INVALID, "1DGR environment without a coef table");
+      ap_gr_params gp{};
+      gp.a = params.a;
+      gp.omega = params.omega;
+      gp.B0 = params.B0;
+      ap_check(ap_ctx_create_1dgr(&m, &p, &gp, gr_table, &ctx_), "ap_ctx_create_1dgr");
     } else if (std::strcmp(params.coord_system, "1DGap") == 0) {
       // the 1D gap lab (labs/1dgap): ptc_updater_1dgap / field_solver_1dgap
       ap_gap_params gp{};

@@ -37,6 +37,8 @@ struct SimParams {
   Scalar rad_cooling_coef = 1.0;
   int damping_length = 30;
   float damping_coef = 0.002;
+  // 1D GR lab: black hole spin (src/sim_params.h:63)
+  float a = 0.0;
 };
 
 }  // namespace Aperture

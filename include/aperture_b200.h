@@ -312,6 +312,56 @@ typedef struct {
 AP_API int ap_ctx_create_1dgap(const ap_mesh *mesh, const ap_params *params,
                                const ap_gap_params *gap, ap_ctx **out);
 
+/* 1D GR lab (labs/1dgr; src/algorithms/ptc_updater_1dgr.h,
+ * field_solver_1dgr.h, src/grids/grid_1dgr.h). A context made here holds
+ * the metric coefficients of Grid_1dGR::compute_coef (grid_1dgr.cpp:21-187),
+ * computed on the host as the reference does from the tabulated field-line
+ * data it reads from coef.h5 (radius r, B^1, B^3, j^1, rho, theta and
+ * dpsi/dtheta, table.n entries each, r increasing), so no HDF5 is needed.
+ * ap_update_particles then runs ptc_updater_1dgr::update_particles
+ * (ptc_updater_1dgr.cu:418-473): E3 = E1 smoothed current_smoothing times
+ * by the K1_j-weighted filter (E2 is the scratch), the GR pusher
+ * (update_ptc_1dgr, :137-300; tracked particles get the lower u_0 in p2
+ * every data_interval steps), J1 through K1_j times delta / dt and every
+ * species' Rho through K1 on every step, then J1 and Rho smoothed; and
+ * ap_update_fields field_solver_1dgr::update_fields (field_solver_1dgr.cu:
+ * 14-44): E1 += (j0 - J1) dt on cells [guard + 1, dims - guard - 5). A
+ * particle that would move more than one cell (which the reference reports
+ * and follows past the coefficient arrays) is emptied and counted as
+ * AP_ERR_MOVED_FAR. */
+typedef struct {
+  float a;      /* SimParams::a, the black hole's spin */
+  float omega;  /* SimParams::omega, the field line's angular velocity */
+  float B0;     /* SimParams::B0 */
+} ap_gr_params;
+typedef struct {
+  const float *r, *B1, *B3, *jr, *rho, *theta, *dpsidth; /* host arrays of n floats */
+  size_t n;
+} ap_gr_table;
+/* Coefficient arrays of Grid_1dGR, in the order of its mesh_ptrs
+ * (grid_1dgr.h:16-20); theta and agrf stay zero, as compute_coef leaves
+ * them. */
+#define AP_GR_D1 0
+#define AP_GR_D2 1
+#define AP_GR_D3 2
+#define AP_GR_ALPHA 3
+#define AP_GR_THETA 4
+#define AP_GR_K1 5
+#define AP_GR_K1_J 6
+#define AP_GR_J0 7
+#define AP_GR_AGRR 8
+#define AP_GR_AGRF 9
+#define AP_GR_RHO0 10
+#define AP_GR_GAMMA_RR 11
+#define AP_GR_GAMMA_FF 12
+#define AP_GR_BETA_PHI 13
+#define AP_GR_B3B1 14
+#define AP_GR_NCOEF 15
+AP_API int ap_ctx_create_1dgr(const ap_mesh *mesh, const ap_params *params,
+                              const ap_gr_params *gr, const ap_gr_table *table, ap_ctx **out);
+/* Device array of one coefficient (which = AP_GR_*). */
+AP_API int ap_gr_coef(ap_ctx *ctx, int which, ap_array *out);
+
 /* ---------------------------------------------------------------------
  * Batched mode (new; the reference runs one simulation per process).
  * A batch advances many independent 2D Cartesian runs, each an ordinary

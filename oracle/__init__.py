@@ -169,6 +169,17 @@ for _name, _res, _args in [
     ("or_philox4x32_10", None, [_vp, _vp, _vp]),
     ("or_inject_pairs", _sz, [_vp, _sz, _sz, C.c_float, C.c_uint32, C.c_float, C.c_float,
                               C.c_float, C.c_uint64, C.c_uint64, _vp, _vp]),
+    ("or_gr_coef", None, [_vp, C.c_float, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp,
+                          _vp, _sz, _vp]),
+    ("or_update_ptc_1dgr", _u64, [_vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int, C.c_float,
+                                  C.c_float, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("or_update_ptc_1dgr_f64", _u64, [_vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int, C.c_float,
+                                      C.c_float, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("or_filter_gr", None, [_vp, _vp, _vp, _vp, _vp]),
+    ("or_update_particles_1dgr", _u64, [_vp, _vp, _sz, _vp, C.c_float, C.c_uint32, C.c_int,
+                                        C.c_int, C.c_int, C.c_float, C.c_float, _vp, _vp, _vp,
+                                        _vp]),
+    ("or_update_e_1dgr", None, [_vp, _vp, _vp, _vp, C.c_float]),
     ("or_update_ptc_1dgap", _u64, [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, _vp, _vp]),
     ("or_update_ptc_1dgap_f64", _u64, [_vp, _vp, _sz, C.c_float, _vp, _vp, _vp, _vp, _vp]),
     ("or_filter_gap", None, [_vp, _vp, _vp, _vp]),
@@ -492,6 +503,53 @@ def ref_update_particles_mt(m, p, num, f, dt, step, data_interval, num_species, 
 
 
 # ---------------------------------------------------------------------------
+# 1D GR lab (ap_gr.c: grid_1dgr.cpp, ptc_updater_1dgr.cu, field_solver_1dgr.cu).
+
+GR_NCOEF = 15
+GR_COEF_NAMES = ("D1", "D2", "D3", "alpha", "theta", "K1", "K1_j", "j0", "agrr", "agrf", "rho0",
+                 "gamma_rr", "gamma_ff", "beta_phi", "B3B1")
+GR_TABLE_KEYS = ("r", "B1", "B3", "jr", "rho", "theta", "dpsidth")
+
+
+def gr_coef(m, a, omega, B0, table):
+    """Grid_1dGR::compute_coef from the tabulated arrays; returns the 15
+    coefficient arrays (float32, dims[0] each) in mesh_ptrs order."""
+    cols = [np.ascontiguousarray(table[k], dtype=np.float32) for k in GR_TABLE_KEYS]
+    out = [np.zeros(m.dims[0], np.float32) for _ in range(GR_NCOEF)]
+    lib.or_gr_coef(C.byref(m), np.float32(a), np.float32(omega), np.float32(B0),
+                   *[_p(c) for c in cols], len(cols[0]), _arr(out, GR_NCOEF))
+    return out
+
+
+def update_ptc_1dgr(m, p, num, dt, step, data_interval, a, omega, E3, co, J1, Rho, charges,
+                    masses, f64=False):
+    s = ptc_struct(p)
+    fn = lib.or_update_ptc_1dgr_f64 if f64 else lib.or_update_ptc_1dgr
+    return fn(C.byref(m), C.byref(s), num, np.float32(dt), int(step), int(data_interval),
+              np.float32(a), np.float32(omega), _p(E3), _arr(co, GR_NCOEF), _p(J1),
+              _arr(Rho, 8), _fa(charges), _fa(masses))
+
+
+def filter_gr(m, j, tmp, k1, bnd):
+    lib.or_filter_gr(C.byref(m), _p(j), _p(tmp), _p(k1), _fa(bnd, C.c_int, 2))
+
+
+def update_particles_1dgr(m, p, num, f, dt, step, data_interval, smoothing, num_species, a,
+                          omega, co, charges, masses, bnd):
+    s = ptc_struct(p)
+    fs = fields_struct(f)
+    return lib.or_update_particles_1dgr(C.byref(m), C.byref(s), num, C.byref(fs),
+                                        np.float32(dt), int(step), int(data_interval),
+                                        int(smoothing), int(num_species), np.float32(a),
+                                        np.float32(omega), _arr(co, GR_NCOEF), _fa(charges),
+                                        _fa(masses), _fa(bnd, C.c_int, 2))
+
+
+def update_e_1dgr(m, E1, J1, j0, dt):
+    lib.or_update_e_1dgr(C.byref(m), _p(E1), _p(J1), _p(j0), np.float32(dt))
+
+
+# ---------------------------------------------------------------------------
 # 1D gap lab (ptc_updater_1dgap.cu, field_solver_1dgap.cu).
 
 def update_ptc_1dgap(m, p, num, dt, E3, J1, Rho, charges, masses, f64=False):
@@ -547,6 +605,38 @@ def load_ref_gap(build=True):
     ref_gap = r
     return ref_gap
 
+
+
+_REF_GR_PATH = os.path.join(_HERE, "_ref", "libapref_gr.so")
+ref_gr = None
+
+
+def load_ref_gr(build=True):
+    """The 1D GR lab's own kernels and Grid_1dGR::compute_coef on the host
+    (pin library), or None."""
+    global ref_gr
+    if ref_gr is not None:
+        return ref_gr
+    if not os.path.exists(_REF_GR_PATH) and build and ref_tree_present():
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_gr.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_GR_PATH):
+        return None
+    r = C.CDLL(_REF_GR_PATH)
+    r.ref_gr_coef.restype = None
+    r.ref_gr_coef.argtypes = [_vp, C.c_float, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp, _vp,
+                              _vp, _sz, _vp]
+    r.ref_gr_push.restype = None
+    r.ref_gr_push.argtypes = [_vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int, C.c_float,
+                              C.c_float, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp]
+    r.ref_gr_filter.restype = None
+    r.ref_gr_filter.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_int]
+    r.ref_gr_update_e.restype = None
+    r.ref_gr_update_e.argtypes = [_vp, _vp, _vp, _vp, C.c_float]
+    ref_gr = r
+    return ref_gr
 
 
 def ls_inject(m, p, num, cap, inj, p1, w, q_e, seed, call, first_id):

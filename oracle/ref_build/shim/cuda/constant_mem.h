@@ -13,6 +13,7 @@ struct ap_ref_params {
   bool rad_cooling_on;
   int damping_length;
   float q_e, r_cutoff, track_percent;
+  float a;  /* 1D GR lab: spin */
   bool inject_ions;
 };
 extern Quadmesh dev_mesh;

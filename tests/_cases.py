@@ -171,3 +171,67 @@ def gap_state(m, n, rng, pmax=50.0):
     p["flag"][ign] |= np.uint32(1 << 3)
     p["id"][:] = np.arange(n, dtype=np.uint64)
     return E1, p
+
+
+# ---------------------------------------------------------------------------
+# 1D GR lab cases (labs/1dgr/config.toml grid: lower -6.273, size 6.138,
+# guard 3; spin a = 0.99, field-line angular velocity 0.211765; q_e 1.2).
+
+GR_A, GR_OMEGA = 0.99, 0.211765
+
+
+def gr_table(n=600, rmin=1.15, rmax=14.0):
+    """A synthetic field-line table (the reference reads one from coef.h5):
+    B^3 / B^1 large enough near the horizon that u_0 is real in every cell."""
+    a, om = GR_A, GR_OMEGA
+    r = np.geomspace(rmin, rmax, n)
+    theta = 0.3 + 0.2 / r
+    Sigma = r * r + a * a * np.cos(theta) ** 2
+    Delta = r * r - 2 * r + a * a
+    A = (r * r + a * a) ** 2 - Delta * a * a * np.sin(theta) ** 2
+    w = 2 * a * r / A
+    g11, g33, al2 = Sigma / Delta, A * np.sin(theta) ** 2 / Sigma, Delta * Sigma / A
+    b31 = 1.5 * np.sqrt(np.maximum(0.0, g11 * (g33 * (om - w) ** 2 - al2) / (g33 * al2))) + 0.1
+    B1 = 1.0 / r ** 2
+    tab = {"r": r, "B1": B1, "B3": b31 * B1, "jr": 0.5 / r ** 2, "rho": 0.2 / r ** 2,
+           "theta": theta, "dpsidth": 0.5 * np.sin(theta)}
+    return {k: v.astype(np.float32) for k, v in tab.items()}
+
+
+def gr_mesh(N, guard=3):
+    return oracle.make_mesh((N, 1, 1), (guard, 0, 0), lower=(-6.273, 0, 0), size=(6.138, 1, 1))
+
+
+def gr_particles(m, co, n, rng, p_sigma=2.0, tracked_frac=0.1, ignore_frac=0.05):
+    """n particles in bulk cells away from the ends, momenta N(0, p_sigma),
+    u_0 = E consistent with p1 at each position (as the lab's initial
+    condition sets it, ptc_updater_1dgr.cu:37-39)."""
+    p = empty_ptc(n)
+    g = m.guard[0]
+    c = rng.integers(g + 2, m.dims[0] - g - 2, n)
+    x1 = rng.random(n, dtype=np.float32)
+    p["cell"][:] = c.astype(np.uint32)
+    p["x1"][:] = x1
+    p1 = (p_sigma * rng.standard_normal(n)).astype(np.float32)
+    p["p1"][:] = p1
+    nx = 1.0 - x1.astype(np.float64)
+    it = lambda k: co[k][c] * x1 + co[k][c - 1] * nx  # noqa: E731
+    D1, D2, D3, al = it(0), it(1), it(2), it(3)
+    u0 = np.sqrt((D2 + p1.astype(np.float64) ** 2) / (D2 * (al * al - D3) + D1 * D1))
+    p["E"][:] = u0.astype(np.float32)
+    p["weight"][:] = (0.5 + rng.random(n)).astype(np.float32)
+    sp = rng.integers(0, 2, n).astype(np.uint32)
+    flag = sp << np.uint32(29)
+    flag |= ((rng.random(n) < tracked_frac).astype(np.uint32) << np.uint32(1))  # tracked
+    flag |= ((rng.random(n) < ignore_frac).astype(np.uint32) << np.uint32(3))  # ignore_current
+    p["flag"][:] = flag
+    p["id"][:] = np.arange(n, dtype=np.uint64)
+    return p
+
+
+def gr_dt(m, co, p):
+    """A time step that moves the fastest particle half a cell."""
+    c = p["cell"].astype(np.int64)
+    D1, D2 = co[0][c], co[1][c]
+    vr = np.abs((p["p1"] / p["E"] - D1) / D2).max()
+    return float(np.float32(0.5 * m.delta[0] / max(vr, 1e-6)))

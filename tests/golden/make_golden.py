@@ -5,8 +5,9 @@ ptc_updater_logsph.cu / field_solver_logsph.cu kernels and
 grid_log_sph.cpp coefficients), run on the host by oracle/ref_build.
 
 Needs the reference tree (to build oracle/_ref/libapref.so). Run from the
-repository root:  python tests/golden/make_golden.py [logsph | gap]
-(gap_*.npz: the 1D gap lab's update_ptc_1dgap, ptc_updater_1dgap.cu).
+repository root:  python tests/golden/make_golden.py [logsph | gap | gr]
+(gap_*.npz: the 1D gap lab's update_ptc_1dgap, ptc_updater_1dgap.cu;
+gr_a.npz: the 1D GR lab's compute_coef and update_ptc_1dgr).
 Each fixture holds seeded inputs (particles, E/B, backgrounds, J) and the
 reference outputs: particles and J/Rho after push + deposit, and E/B/divE/
 divB after one E update, one B update and compute_divs.
@@ -181,10 +182,54 @@ def main_gap():
         print(path, os.path.getsize(path))
 
 
+def main_gr():
+    """gr_a.npz: the 1D GR lab's Grid_1dGR::compute_coef and
+    update_ptc_1dgr (oracle/_ref/libapref_gr.so) on a synthetic field-line
+    table and seeded particles (tracked ones included, output step);
+    outputs are the coefficients, the particles, J1 and Rho after one call."""
+    from _cases import GR_A, GR_OMEGA, gr_dt, gr_mesh, gr_particles, gr_table
+    ref = oracle.load_ref_gr(build=True)
+    if ref is None:
+        raise SystemExit("GR pin library unavailable (needs the reference tree)")
+    N, B0, seed, step = 384, 2.0, 41, 8
+    m = gr_mesh(N)
+    tab = gr_table(n=200)
+    cols = [np.ascontiguousarray(tab[k], np.float32) for k in oracle.GR_TABLE_KEYS]
+    co = [np.zeros(m.dims[0], np.float32) for _ in range(oracle.GR_NCOEF)]
+    ref.ref_gr_coef(oracle.C.byref(m), np.float32(GR_A), np.float32(GR_OMEGA), np.float32(B0),
+                    *[oracle._p(c) for c in cols], len(cols[0]), oracle._arr(co, 15))
+    rng = np.random.default_rng(seed)
+    p = gr_particles(m, co, 700, rng)
+    dt = np.float32(gr_dt(m, co, p))
+    E3 = (0.05 * np.sin(0.013 * np.arange(m.dims[0]))).astype(np.float32)
+    out = {"N": np.int64(N), "B0": np.float32(B0), "dt": dt, "step": np.int64(step),
+           "E3": E3, "coef": np.stack(co)}
+    for k in oracle.GR_TABLE_KEYS:
+        out["tab_" + k] = tab[k]
+    for k in p:
+        out["in_" + k] = p[k].copy()
+    charges, masses = [-1.2, 1.2] + [1.2] * 6, [1.2] * 8
+    J = np.zeros(m.dims[0], np.float32)
+    R = [np.zeros(m.dims[0], np.float32) for _ in range(2)]
+    ref.ref_gr_push(oracle.C.byref(m), oracle.C.byref(oracle.ptc_struct(p)), len(p["x1"]), dt,
+                    step, 4, np.float32(GR_A), np.float32(GR_OMEGA), oracle._p(E3),
+                    oracle._arr(co, 15), oracle._p(J), oracle._arr(R, 8), 2,
+                    oracle._fa(charges), oracle._fa(masses))
+    for k in p:
+        out["out_" + k] = p[k]
+    out["J1"] = J
+    out["Rho"] = np.stack(R)
+    path = os.path.join(HERE, "gr_a.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path))
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "logsph":
         main_logsph()
     elif len(sys.argv) > 1 and sys.argv[1] == "gap":
         main_gap()
+    elif len(sys.argv) > 1 and sys.argv[1] == "gr":
+        main_gr()
     else:
         main()

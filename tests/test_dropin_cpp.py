@@ -25,6 +25,7 @@ def test_dropin_headers_compile(tmp_path):
     _build(tmp_path)
     _build(tmp_path, "pulsar_lab")
     _build(tmp_path, "gap_lab")
+    _build(tmp_path, "gr_lab")
 
 
 @pytest.mark.gpu
@@ -46,3 +47,10 @@ def test_dropin_gap_lab_runs(tmp_path):
     exe = _build(tmp_path, "gap_lab")
     r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "gap_lab ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_dropin_gr_lab_runs(tmp_path):
+    exe = _build(tmp_path, "gr_lab")
+    r = subprocess.run([exe, "12"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "gr_lab ok" in r.stdout, r.stdout + r.stderr
