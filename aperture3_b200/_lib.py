@@ -126,6 +126,32 @@ class ApPairParams(C.Structure):
                 ("first_id", C.c_uint64)]
 
 
+class ApPhotons(C.Structure):
+    """ap_photons: photon_data (particle_data.h:68-80)."""
+    _fields_ = [
+        ("x1", C.c_void_p), ("x2", C.c_void_p), ("x3", C.c_void_p),
+        ("p1", C.c_void_p), ("p2", C.c_void_p), ("p3", C.c_void_p),
+        ("E", C.c_void_p), ("weight", C.c_void_p), ("path_left", C.c_void_p),
+        ("cell", C.c_void_p), ("id", C.c_void_p), ("flag", C.c_void_p),
+    ]
+
+
+class ApRadParams(C.Structure):
+    """ap_rad_params: radiative transfer model and parameters."""
+    _fields_ = [("model", C.c_int), ("delta_t", C.c_float), ("gamma_thr", C.c_float),
+                ("E_secondary", C.c_float), ("photon_path", C.c_float),
+                ("r_cutoff", C.c_float), ("track_percent", C.c_float), ("e_curv", C.c_float),
+                ("l_curv", C.c_float), ("BQ", C.c_float), ("omega", C.c_float),
+                ("seed", C.c_uint64), ("first_photon_id", C.c_uint64),
+                ("first_particle_id", C.c_uint64)]
+
+
+class ApRadCounts(C.Structure):
+    _fields_ = [("marked", C.c_uint64), ("written", C.c_uint64), ("dropped", C.c_uint64)]
+
+
+RAD_DEFAULT, RAD_PULSAR = 0, 1
+
 COEF_NAMES = ("l1_e", "l2_e", "l3_e", "l1_b", "l2_b", "l3_b",
               "A1_e", "A2_e", "A3_e", "A1_b", "A2_b", "A3_b", "dV")
 
@@ -200,6 +226,12 @@ SIGNATURES = {
     "ap_inject_pairs": (_i, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64),
                              C.POINTER(C.c_uint64)]),
     "ap_batch_inject_pairs": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
+    "ap_bind_photons": (_i, [_vp, C.POINTER(ApPhotons), C.c_size_t, C.c_size_t]),
+    "ap_get_photon_number": (_i, [_vp, C.POINTER(C.c_size_t)]),
+    "ap_set_rad_params": (_i, [_vp, C.POINTER(ApRadParams)]),
+    "ap_emit_photons": (_i, [_vp, ApArray, C.POINTER(ApRadCounts)]),
+    "ap_produce_pairs": (_i, [_vp, ApArray, C.POINTER(ApRadCounts)]),
+    "ap_move_photons": (_i, [_vp, C.c_double]),
     "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                             C.POINTER(ApParticles), C.c_size_t,
                                             C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),

@@ -318,6 +318,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->status);
   cudaFree(c->diag_dev);
   cudaFree(c->rho_prev);
+  rad_free(*c);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->diag_host) cudaFreeHost(c->diag_host);
   for (int i = 0; i < c->ev_cap; ++i) {
@@ -883,6 +884,9 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
     c->pd_launches++;
   }
   AP_TRY_ST(update_complete(c, dt, step, has_work));
+  // photons move after the particles (ptc_updater.cu:814-833,
+  // ptc_updater_logsph.cu:793-803)
+  if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt));
   if (!c->sync) return AP_OK;
   return check_status(c);
 }
@@ -960,6 +964,12 @@ AP_API int ap_sort_by_cell(ap_ctx *c) {
   if (!device_count) AP_TRY_ST(refresh_number(c));
   const int ph = phase_begin(c, kPhSort);
   AP_TRY(sort_by_cell(*c, &n));  // also leaves the 2D tile order of the sorted store
+  if (c->ph_bound) {
+    // sim_data::sort_particles sorts the photons too (sim_data_impl.hpp:78-82)
+    size_t nph = 0;
+    AP_TRY(sort_photons(*c, &nph));
+    c->ph_number = nph;
+  }
   phase_end(c, ph);
   if (!device_count) {
     c->number = n;  // sort_by_cell set store_base
@@ -1226,6 +1236,76 @@ AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitte
   if (emitted) *emitted = c->pstate_host->emitted;
   if (dropped) *dropped = c->pstate_host->dropped;
   return AP_OK;
+}
+
+AP_API int ap_bind_photons(ap_ctx *c, const ap_photons *ph, size_t number, size_t capacity) {
+  if (!c || !ph) return AP_ERR_INVALID;
+  if (c->coord != 0 && c->coord != 1) return fail(c, AP_ERR_UNSUPPORTED);
+  if (number > capacity || capacity >= (size_t)UINT32_MAX) return fail(c, AP_ERR_CAPACITY);
+  if (!ph->x1 || !ph->x2 || !ph->x3 || !ph->p1 || !ph->p2 || !ph->p3 || !ph->E ||
+      !ph->weight || !ph->path_left || !ph->cell || !ph->id || !ph->flag)
+    return fail(c, AP_ERR_INVALID);
+  c->ph = *ph;
+  c->ph_number = number;
+  c->ph_capacity = capacity;
+  c->ph_bound = true;
+  return AP_OK;
+}
+
+AP_API int ap_get_photon_number(const ap_ctx *c, size_t *n) {
+  if (!c || !n) return AP_ERR_INVALID;
+  *n = c->ph_bound ? c->ph_number : 0;
+  return AP_OK;
+}
+
+AP_API int ap_set_rad_params(ap_ctx *c, const ap_rad_params *rp) {
+  if (!c || !rp) return AP_ERR_INVALID;
+  if (rp->model != AP_RAD_DEFAULT && rp->model != AP_RAD_PULSAR) return fail(c, AP_ERR_INVALID);
+  // the pulsar lab's functions read (ln r, theta) positions and Rho[0], Rho[1]
+  if (rp->model == AP_RAD_PULSAR && (c->coord != 1 || c->params.num_species < 2))
+    return fail(c, AP_ERR_UNSUPPORTED);
+  if (c->coord != 0 && c->coord != 1) return fail(c, AP_ERR_UNSUPPORTED);
+  c->rad = *rp;
+  c->rad_on = true;
+  c->rad_emit_calls = c->rad_pair_calls = 0;
+  c->rad_next_photon_id = rp->first_photon_id;
+  c->rad_next_ptc_id = rp->first_particle_id;
+  return AP_OK;
+}
+
+static bool produced_ok(const Ctx *c, ap_array a) {
+  return a.ptr == nullptr || valid_array(a, c->mesh);
+}
+
+AP_API int ap_emit_photons(ap_ctx *c, ap_array produced, ap_rad_counts *out) {
+  if (!c || !out || !c->rad_on || !c->ph_bound || !c->ptc_bound || !c->fields_bound ||
+      !produced_ok(c, produced))
+    return AP_ERR_INVALID;
+  AP_TRY_ST(refresh_number(c));
+  AP_TRY_ST(rad_emit_photons(*c, produced, out));
+  return AP_OK;
+}
+
+AP_API int ap_produce_pairs(ap_ctx *c, ap_array produced, ap_rad_counts *out) {
+  if (!c || !out || !c->rad_on || !c->ph_bound || !c->ptc_bound || !c->fields_bound ||
+      !produced_ok(c, produced))
+    return AP_ERR_INVALID;
+  AP_TRY_ST(refresh_number(c));
+  const size_t before = c->number;
+  AP_TRY_ST(rad_produce_pairs(*c, produced, out));
+  if (c->number != before) {
+    // the new pairs are in no tile list and may carry a larger weight
+    c->order_valid = false;
+    c->scale_valid = false;
+    AP_TRY_ST(push_number(c));
+  }
+  return AP_OK;
+}
+
+AP_API int ap_move_photons(ap_ctx *c, double dt) {
+  if (!c || !c->ph_bound) return AP_ERR_INVALID;
+  AP_TRY_ST(rad_move_photons(*c, (float)dt));
+  return finish(c);
 }
 
 AP_API int ap_set_continuity_check(ap_ctx *c, int on) {

@@ -272,6 +272,23 @@ struct Ctx {
   size_t coef_pitch = 0;        // bytes per row
   float ls_kfac = 1.0f;         // bound of |J3 contribution| / (|q| w)
 
+  // photons and pair production (ap_bind_photons, ap_set_rad_params)
+  bool ph_bound = false;
+  ap_photons ph{};
+  size_t ph_number = 0;
+  size_t ph_capacity = 0;
+  bool rad_on = false;
+  ap_rad_params rad{};
+  uint32_t rad_emit_calls = 0;
+  uint32_t rad_pair_calls = 0;
+  uint64_t rad_next_photon_id = 0;
+  uint64_t rad_next_ptc_id = 0;
+  uint8_t *rad_mark = nullptr;     // one byte per slot of the larger store
+  size_t rad_mark_cap = 0;
+  uint32_t *rad_chunks = nullptr;  // per-chunk counts, offsets, then the total
+  size_t rad_chunks_cap = 0;
+  uint32_t *rad_total_host = nullptr;  // pinned: marked count of the last pass
+
   // per-phase event timing (ap_set_profiling)
   bool profiling = false;
   struct EventPair {
@@ -312,6 +329,7 @@ cudaError_t radix_sort_pairs(Ctx &c, size_t n, int end_bit, uint32_t **keys_out,
                              uint32_t **vals_out);
 size_t radix_count_words(int num_sms);
 cudaError_t sort_by_cell(Ctx &c, size_t *new_number);
+cudaError_t sort_photons(Ctx &c, size_t *new_number);
 // Compaction: the scratch store the push / deposit writes into (allocated on
 // first use), and the copy back into the caller's arrays; `live` is the
 // device-side count of written slots, the slots after it become empty.
@@ -332,6 +350,14 @@ cudaError_t launch_diagnostics(Ctx &c, double *out_dev);
 cudaError_t launch_rho_snapshot(Ctx &c);
 // *out = max over the bulk of |sum_s Rho_s - rho_prev + div J| (FP64)
 cudaError_t launch_continuity(Ctx &c, double *out);
+
+// photons and pair production (k_rad.cu): the photon move of an update, and
+// the emit / produce passes; *marked receives the emitters of the pass
+// (waits for the stream).
+int rad_move_photons(Ctx &c, float dt);
+int rad_emit_photons(Ctx &c, ap_array produced, ap_rad_counts *out);
+int rad_produce_pairs(Ctx &c, ap_array produced, ap_rad_counts *out);
+void rad_free(Ctx &c);
 
 // pair injection (k_pairs.cu): enqueue mark / scan / append on the device
 // count (no host synchronisation); refresh_number reads the device state

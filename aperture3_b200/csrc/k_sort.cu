@@ -814,4 +814,59 @@ cudaError_t sort_by_cell(Ctx &c, size_t *new_number) {
   return cudaSuccess;
 }
 
+// photons.sort_by_cell (sim_data_impl.hpp:81; particle_base_impl.cu:435-487
+// for photon_data): the same stable sort of the photon slots [0, number),
+// each of the twelve members gathered through the scratch buffer, and the
+// empty slots trimmed.
+cudaError_t sort_photons(Ctx &c, size_t *new_number) {
+  const size_t n = c.ph_number;
+  *new_number = 0;
+  if (n == 0) return cudaSuccess;
+  if (ensure_scratch(c, n) != AP_OK) return cudaErrorMemoryAllocation;
+  const uint32_t ncells =
+      (uint32_t)c.mesh.dims[0] * (uint32_t)c.mesh.dims[1] * (uint32_t)c.mesh.dims[2];
+  k_cell_keys<<<grid_for(c, n, 256), 256, 0, c.stream>>>(c.ph.cell, 0, n, ncells, c.keys[0],
+                                                        c.vals[0], nullptr);
+  c.launches++;
+  uint32_t *ko, *vo;
+  cudaError_t e = radix_pairs(c, n, bits_for(ncells), &ko, &vo);
+  if (e != cudaSuccess) return e;
+  const int g = grid_for(c, n, 256);
+#define AP_GATHER_PH(FIELD, T)                                                                \
+  do {                                                                                        \
+    k_gather<T><<<g, 256, 0, c.stream>>>(c.ph.FIELD, vo, n, (T *)c.gather_tmp);               \
+    e = cudaMemcpyAsync(c.ph.FIELD, c.gather_tmp, n * sizeof(T), cudaMemcpyDeviceToDevice,    \
+                        c.stream);                                                            \
+    if (e != cudaSuccess) return e;                                                           \
+    c.launches++;                                                                             \
+  } while (0)
+  AP_GATHER_PH(x1, float);
+  AP_GATHER_PH(x2, float);
+  AP_GATHER_PH(x3, float);
+  AP_GATHER_PH(p1, float);
+  AP_GATHER_PH(p2, float);
+  AP_GATHER_PH(p3, float);
+  AP_GATHER_PH(E, float);
+  AP_GATHER_PH(weight, float);
+  AP_GATHER_PH(path_left, float);
+  AP_GATHER_PH(cell, uint32_t);
+  AP_GATHER_PH(id, uint64_t);
+  AP_GATHER_PH(flag, uint32_t);
+#undef AP_GATHER_PH
+  if (!c.cell_start) {
+    e = cudaMalloc(&c.cell_start, sizeof(uint32_t) * ((size_t)ncells + 1));
+    if (e != cudaSuccess) return e;
+  }
+  k_segment_starts<<<grid_for(c, n + 1, 256), 256, 0, c.stream>>>(ko, n, ncells, c.cell_start);
+  c.launches++;
+  uint32_t live = 0;
+  e = cudaMemcpyAsync(&live, c.cell_start + ncells, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                      c.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return e;
+  *new_number = live;
+  return cudaSuccess;
+}
+
 }  // namespace apb

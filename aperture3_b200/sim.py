@@ -17,7 +17,8 @@ import torch
 
 from . import _lib
 from ._lib import (AP_MAX_CELL, AP_MAX_SPECIES, ApArray, ApDiag, ApFields, ApLogsphParams,
-                   ApMesh, ApParams, ApParticles, ApStepStats, check)
+                   ApMesh, ApParams, ApParticles, ApPhotons, ApRadCounts, ApRadParams,
+                   ApStepStats, check)
 
 PTC_FIELDS = (
     ("x1", torch.float32), ("x2", torch.float32), ("x3", torch.float32),
@@ -26,6 +27,13 @@ PTC_FIELDS = (
     ("cell", torch.int32), ("id", torch.int64), ("flag", torch.int32),
 )
 NP_DTYPES = {"cell": np.uint32, "id": np.uint64, "flag": np.uint32}
+# photon_data (src/data/particle_data.h:68-80)
+PH_FIELDS = (
+    ("x1", torch.float32), ("x2", torch.float32), ("x3", torch.float32),
+    ("p1", torch.float32), ("p2", torch.float32), ("p3", torch.float32),
+    ("E", torch.float32), ("weight", torch.float32), ("path_left", torch.float32),
+    ("cell", torch.int32), ("id", torch.int64), ("flag", torch.int32),
+)
 
 ELECTRON, POSITRON, ION = 0, 1, 2
 FLAG_IGNORE_CURRENT = 1 << 3
@@ -69,6 +77,22 @@ class SimParams:
     damping_coef: float = 0.002
     # 1D GR lab (coord_system "1DGR"): black hole spin (src/sim_params.h:63)
     a: float = 0.0
+    # photons and pair production (src/sim_params.h:23, 50-83); rad_model
+    # selects the user radiative functions: "default" (src/cuda/radiation/
+    # user_radiative_functions.cu) or "pulsar" (the pulsar lab's); rad_seed
+    # keys the counter-based random stream that replaces cuRAND
+    max_photon_number: int = 100
+    create_pairs: bool = False
+    gamma_thr: float = 20.0
+    track_percent: float = 0.2
+    BQ: float = 1.0
+    photon_path: float = 1.0
+    E_secondary: float = 4.0
+    r_cutoff: float = 4.0
+    l_curv: float = 6.0
+    e_curv: float = 6.4e-9
+    rad_model: str = "default"
+    rad_seed: int = 1
 
     @classmethod
     def from_toml(cls, path: str) -> "SimParams":
@@ -271,6 +295,10 @@ def array_view(t: torch.Tensor) -> ApArray:
     return ApArray(t.data_ptr(), pitch)
 
 
+def _view_or_null(t: Optional[torch.Tensor]) -> ApArray:
+    return array_view(t) if t is not None else ApArray(None, 0)
+
+
 def _alloc_field(dims, device, row_align=4):
     rows = dims[1] * dims[2]
     padded = (dims[0] + row_align - 1) // row_align * row_align
@@ -281,11 +309,13 @@ def _alloc_field(dims, device, row_align=4):
 class SimData:
     """sim_data (src/sim_data.h:14-70): fields and the particle store."""
 
-    def __init__(self, env: SimEnvironment, capacity: Optional[int] = None, row_align: int = 4):
+    def __init__(self, env: SimEnvironment, capacity: Optional[int] = None, row_align: int = 4,
+                 photon_capacity: Optional[int] = None):
         """row_align: field rows are padded to a multiple of this many floats
         (4 gives the 16-byte row pitch the TMA field loads need; 1 packs the
         rows, which makes the kernels read the field tiles with plain loads
-        when dims[0] is not a multiple of 4)."""
+        when dims[0] is not a multiple of 4). photon_capacity: photon slots
+        (default max_photon_number when create_pairs is set, else none)."""
         self.env = env
         dims = env.dims
         dev = env.device
@@ -305,6 +335,19 @@ class SimData:
         self.particles["cell"].fill_(-1)  # MAX_CELL
         self._number_stale = False
         self.number = 0
+        # photons (sim_data.h: photons, photon_produced, pair_produced) when
+        # the run creates pairs or a photon capacity is given
+        if photon_capacity is None:
+            photon_capacity = env.params.max_photon_number if env.params.create_pairs else 0
+        self.photon_capacity = int(photon_capacity)
+        self.photons: Optional[Dict[str, torch.Tensor]] = None
+        self.photon_produced = self.pair_produced = None
+        if self.photon_capacity > 0:
+            self.photons = {name: torch.zeros(self.photon_capacity, dtype=dt, device=dev)
+                            for name, dt in PH_FIELDS}
+            self.photons["cell"].fill_(-1)
+            self.photon_produced = mk()
+            self.pair_produced = mk()
         self._bind()
 
     @property
@@ -343,6 +386,46 @@ class SimData:
             setattr(p, name, self.particles[name].data_ptr())
         check(lib.ap_bind_particles(self.env.ctx, C.byref(p), self.number, self.capacity),
               "ap_bind_particles")
+        if self.photons is not None:
+            self._bind_photons(0)
+
+    def _bind_photons(self, number: int):
+        ph = ApPhotons()
+        for name, _ in PH_FIELDS:
+            setattr(ph, name, self.photons[name].data_ptr())
+        check(self.env._lib.ap_bind_photons(self.env.ctx, C.byref(ph), int(number),
+                                            self.photon_capacity), "ap_bind_photons")
+
+    # -- photons ---------------------------------------------------------
+    @property
+    def photon_number(self) -> int:
+        n = C.c_size_t()
+        check(self.env._lib.ap_get_photon_number(self.env.ctx, C.byref(n)),
+              "ap_get_photon_number")
+        return int(n.value)
+
+    def set_photons(self, host: Dict[str, np.ndarray]):
+        """Copies host photon arrays into slots [0, n)."""
+        if self.photons is None:
+            raise _lib.ApError(1, "set_photons: no photon storage")
+        n = len(host["x1"])
+        if n > self.photon_capacity:
+            raise _lib.ApError(5, "set_photons")
+        for name, dt in PH_FIELDS:
+            a = np.ascontiguousarray(host[name])
+            t = torch.from_numpy(a.view(np.int32) if dt == torch.int32 else
+                                 (a.view(np.int64) if dt == torch.int64 else a))
+            self.photons[name][:n].copy_(t)
+        self._bind_photons(n)
+
+    def photons_host(self) -> Dict[str, np.ndarray]:
+        n = self.photon_number
+        torch.cuda.synchronize()
+        out = {}
+        for name, _ in PH_FIELDS:
+            a = self.photons[name][:n].cpu().numpy()
+            out[name] = a.view(NP_DTYPES[name]) if name in NP_DTYPES else a
+        return out
 
     # -- particles -------------------------------------------------------
     def set_particles(self, host: Dict[str, np.ndarray]):
@@ -773,6 +856,61 @@ class field_solver_1dgr:
     def update_fields(self, data: SimData, dt: float, time: float = 0.0):
         """E1 += (j0 - J1) dt (field_solver_1dgr.cu:14-44)."""
         check(self.env._lib.ap_update_fields(self.env.ctx, float(dt), 0), "ap_update_fields")
+
+
+class radiative_transfer:
+    """radiative_transfer (src/radiation/radiative_transfer.h:11-29): photon
+    emission and pair production with the user radiative functions that
+    SimParams.rad_model names ("default": src/cuda/radiation/
+    user_radiative_functions.cu; "pulsar": the pulsar lab's). The photon
+    move itself is part of update_particles, as in the reference."""
+
+    MODELS = {"default": _lib.RAD_DEFAULT, "pulsar": _lib.RAD_PULSAR}
+
+    def __init__(self, env: SimEnvironment, first_photon_id: int = 1 << 60,
+                 first_particle_id: int = (1 << 60) + (1 << 59)):
+        self.env = env
+        pr = env.params
+        rp = ApRadParams()
+        rp.model = self.MODELS[pr.rad_model]
+        rp.delta_t = pr.delta_t
+        rp.gamma_thr = pr.gamma_thr
+        rp.E_secondary = pr.E_secondary
+        rp.photon_path = pr.photon_path
+        rp.r_cutoff = pr.r_cutoff
+        rp.track_percent = pr.track_percent
+        rp.e_curv = pr.e_curv
+        rp.l_curv = pr.l_curv
+        rp.BQ = pr.BQ
+        rp.omega = pr.omega
+        rp.seed = int(pr.rad_seed)
+        rp.first_photon_id = int(first_photon_id)
+        rp.first_particle_id = int(first_particle_id)
+        check(env._lib.ap_set_rad_params(env.ctx, C.byref(rp)), "ap_set_rad_params")
+        self.last: Dict[str, int] = {}
+
+    @staticmethod
+    def _counts(c: ApRadCounts) -> Dict[str, int]:
+        return {"marked": int(c.marked), "written": int(c.written), "dropped": int(c.dropped)}
+
+    def emit_photons(self, data: SimData) -> Dict[str, int]:
+        """radiative_transfer::emit_photons (radiative_transfer.cu:196-243);
+        photon_produced accumulates the emitters' weights per cell."""
+        cnt = ApRadCounts()
+        check(self.env._lib.ap_emit_photons(self.env.ctx, _view_or_null(data.photon_produced),
+                                             C.byref(cnt)), "ap_emit_photons")
+        self.last = self._counts(cnt)
+        return self.last
+
+    def produce_pairs(self, data: SimData) -> Dict[str, int]:
+        """radiative_transfer::produce_pairs (radiative_transfer.cu:245-301);
+        pair_produced accumulates the converted photons' weights per cell."""
+        cnt = ApRadCounts()
+        check(self.env._lib.ap_produce_pairs(self.env.ctx, _view_or_null(data.pair_produced),
+                                             C.byref(cnt)), "ap_produce_pairs")
+        data.refresh_number()
+        self.last = self._counts(cnt)
+        return self.last
 
 
 # Python-style aliases

@@ -59,9 +59,54 @@ class particles_t {
   size_t num_ = 0, cap_;
 };
 
+// photon_data (src/data/particle_data.h:68-80): device SoA pointers.
+struct photon_data {
+  Pos_t *x1, *x2, *x3;
+  Scalar *p1, *p2, *p3, *E, *weight, *path_left;
+  uint32_t *cell;
+  uint64_t *id;
+  uint32_t *flag;
+};
+
+// photons_t (src/core/photons.h): fixed-capacity device SoA.
+class photons_t {
+ public:
+  explicit photons_t(size_t capacity) : cap_(capacity ? capacity : 1) {
+    auto alloc = [&](void **p, size_t b) { cuda_check(cudaMalloc(p, b * cap_), "photons"); };
+    void **f[] = {(void **)&d_.x1, (void **)&d_.x2, (void **)&d_.x3, (void **)&d_.p1,
+                  (void **)&d_.p2, (void **)&d_.p3, (void **)&d_.E, (void **)&d_.weight,
+                  (void **)&d_.path_left, (void **)&d_.cell, (void **)&d_.flag};
+    for (void **p : f) alloc(p, 4);
+    alloc((void **)&d_.id, 8);
+    cuda_check(cudaMemset(d_.cell, 0xff, 4 * cap_), "photons");  // MAX_CELL
+  }
+  ~photons_t() {
+    void *ps[] = {d_.x1, d_.x2, d_.x3, d_.p1, d_.p2, d_.p3, d_.E, d_.weight, d_.path_left,
+                  d_.cell, d_.id, d_.flag};
+    for (void *p : ps) cudaFree(p);
+  }
+  photons_t(const photons_t &) = delete;
+  photons_t &operator=(const photons_t &) = delete;
+  photon_data &data() { return d_; }
+  size_t number() const { return num_; }
+  size_t size() const { return cap_; }
+  void set_num(size_t n) { num_ = n; }
+  ap_photons view() const {
+    return ap_photons{d_.x1, d_.x2, d_.x3, d_.p1, d_.p2, d_.p3, d_.E, d_.weight, d_.path_left,
+                      d_.cell, d_.id, d_.flag};
+  }
+
+ private:
+  photon_data d_{};
+  size_t num_ = 0, cap_;
+};
+
 struct sim_data {
   explicit sim_data(sim_environment &e)
-      : env(e), particles((size_t)e.params().max_ptc_number), num_species(e.params().num_species) {
+      : env(e),
+        particles((size_t)e.params().max_ptc_number),
+        photons(e.params().create_pairs ? (size_t)e.params().max_photon_number : 1),
+        num_species(e.params().num_species) {
     const Quadmesh &m = e.mesh();
     E.resize(m, FieldType::E);
     B.resize(m, FieldType::B);
@@ -72,6 +117,8 @@ struct sim_data {
     for (auto &r : Rho) r.resize(m, FieldType::Scalar, 0b111);
     divE.resize(m, FieldType::Scalar, 0b111);
     divB.resize(m, FieldType::Scalar, 0b000);
+    photon_produced.resize(m, FieldType::Scalar, 0b111);
+    pair_produced.resize(m, FieldType::Scalar, 0b111);
     bind();
   }
 
@@ -167,6 +214,8 @@ struct sim_data {
   std::vector<scalar_field<Scalar>> Rho;
   scalar_field<Scalar> divE, divB;
   particles_t particles;
+  photons_t photons;  // bound to the library when SimParams::create_pairs is set
+  scalar_field<Scalar> photon_produced, pair_produced;
   int num_species;
 
  private:
@@ -186,6 +235,11 @@ struct sim_data {
     ap_particles p = particles.view();
     ap_check(ap_bind_particles(env.ctx(), &p, particles.number(), particles.size()),
              "bind_particles");
+    if (env.params().create_pairs) {
+      ap_photons ph = photons.view();
+      ap_check(ap_bind_photons(env.ctx(), &ph, photons.number(), photons.size()),
+               "bind_photons");
+    }
   }
 };
 

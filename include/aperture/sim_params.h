@@ -39,6 +39,23 @@ struct SimParams {
   float damping_coef = 0.002;
   // 1D GR lab: black hole spin (src/sim_params.h:63)
   float a = 0.0;
+  // photons and pair production (src/sim_params.h:23, 50-83)
+  uint64_t max_photon_number = 100;
+  bool create_pairs = false;
+  float gamma_thr = 20.0;
+  float track_percent = 0.2;
+  float BQ = 1.0;
+  float photon_path = 1.0;
+  float E_secondary = 4.0;
+  float r_cutoff = 4.0;
+  float l_curv = 6.0;
+  float e_curv = 6.4e-9;
+  // which user radiative functions (AP_RAD_DEFAULT: src/cuda/radiation/
+  // user_radiative_functions.cu; AP_RAD_PULSAR: the pulsar lab's; the
+  // reference picks them at build time by lab shadowing) and the key of the
+  // counter-based random stream that replaces cuRAND
+  int rad_model = 0;
+  uint64_t rad_seed = 1;
 };
 
 }  // namespace Aperture

@@ -208,7 +208,8 @@ AP_API int ap_set_continuity_check(ap_ctx *ctx, int on);
 
 /* sim_data::sort_particles -> particle_base::sort_by_cell
  * (sim_data_impl.hpp:78-89, cuda/core/particle_base_impl.cu:435-487):
- * stable sort of all SoA members by cell, empty slots last and trimmed. */
+ * stable sort of all SoA members by cell, empty slots last and trimmed;
+ * bound photons are sorted the same way. */
 AP_API int ap_sort_by_cell(ap_ctx *ctx);
 
 /* The device tile order maintained by the per-step counting sort: order has
@@ -481,6 +482,84 @@ AP_API int ap_inject_pairs(ap_ctx *ctx, double dt, uint32_t step, uint64_t *emit
  * no host synchronisation: their counts stay on the device until
  * ap_get_number or another call that needs them reads them back. */
 AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32_t *steps);
+
+/* ---------------------------------------------------------------------
+ * Photons and pair production: radiative_transfer (src/radiation/
+ * radiative_transfer.h:11-29, src/cuda/radiation/radiative_transfer.cu)
+ * with the user radiative functions of the framework
+ * (src/cuda/radiation/user_radiative_functions.cu, AP_RAD_DEFAULT) or of
+ * the pulsar lab (labs/pulsar/src/cuda/radiation/
+ * user_radiative_functions.cu, AP_RAD_PULSAR), and the photon movers of
+ * the particle updaters (ptc_updater.cu:627-690, ptc_updater_logsph.cu:
+ * 58-131), which ap_update_particles runs after the particles when photons
+ * are bound, followed by the exchange: photons leaving the bulk wrap
+ * through periodic sides (Cartesian) or are removed.
+ *
+ * Each pass ranks its emitters in slot order and appends: photon k of an
+ * emit_photons call at slot number + k (the photon count then grows by the
+ * emitters + 1, the reference's padding), pair k of a produce_pairs call at
+ * particle slots number + 20 + 2k and + 1 (the count grows by 2 x the
+ * converted photons + 50). Random numbers: each particle (photon) draws
+ * four uniforms in (0, 1] from Philox4x32-10 keyed on `seed` with counter
+ * (call, id, 1) for emission (2 for conversion), call counting the passes
+ * of its kind since ap_set_rad_params (the reference draws cuRAND XORWOW in
+ * thread order). Every new photon and particle gets an id (photons from
+ * first_photon_id, particles from first_particle_id, in rank order); the
+ * tracked flag keeps the reference's meaning (a draw below track_percent).
+ * An emission past the photon capacity leaves its parent unchanged and a
+ * pair whose second slot is past the particle capacity removes its photon;
+ * both are counted as dropped. Empty slots that a pass leaves in its range
+ * (a photon the model does not keep) have cell = MAX_CELL. */
+#define AP_RAD_DEFAULT 0
+#define AP_RAD_PULSAR 1
+typedef struct {
+  float *x1, *x2, *x3;
+  float *p1, *p2, *p3;
+  float *E, *weight, *path_left;
+  uint32_t *cell;
+  uint64_t *id;
+  uint32_t *flag;
+} ap_photons; /* photon_data (src/data/particle_data.h:68-80) */
+typedef struct {
+  int model;            /* AP_RAD_DEFAULT or AP_RAD_PULSAR                 */
+  float delta_t;        /* SimParams::delta_t (the pulsar emission rate)   */
+  float gamma_thr;      /* default model: emission threshold               */
+  float E_secondary;    /* default model: photon energy scale              */
+  float photon_path;    /* default model: free path scale                  */
+  float r_cutoff;       /* default: longest path; log-spherical mover:
+                           photons beyond this radius are removed          */
+  float track_percent;  /* fraction of new photons / pairs flagged tracked */
+  float e_curv, l_curv; /* pulsar model: curvature photon energy and rate  */
+  float BQ;             /* pulsar model: critical field                    */
+  float omega;          /* pulsar model: emission only inside 0.6 / omega  */
+  uint64_t seed;
+  uint64_t first_photon_id;
+  uint64_t first_particle_id;
+} ap_rad_params;
+typedef struct {
+  uint64_t marked;   /* particles (photons) that passed the model's check  */
+  uint64_t written;  /* appended within the capacity                      */
+  uint64_t dropped;  /* over the capacity                                 */
+} ap_rad_counts;
+
+/* Binds caller-owned photon arrays of `capacity` slots, `number` in use. */
+AP_API int ap_bind_photons(ap_ctx *ctx, const ap_photons *ph, size_t number, size_t capacity);
+AP_API int ap_get_photon_number(const ap_ctx *ctx, size_t *number);
+/* Sets the model and its parameters; resets the pass counters. */
+AP_API int ap_set_rad_params(ap_ctx *ctx, const ap_rad_params *params);
+/* radiative_transfer::emit_photons (radiative_transfer.cu:196-243):
+ * particles in the bulk (ions excepted) that pass check_emit_photon emit
+ * one photon each; photon_produced (ptr may be NULL; a 2D field array)
+ * accumulates their weights per cell. Waits for the stream. */
+AP_API int ap_emit_photons(ap_ctx *ctx, ap_array photon_produced, ap_rad_counts *out);
+/* radiative_transfer::produce_pairs (radiative_transfer.cu:245-301):
+ * photons in the bulk that pass check_produce_pair become an e-/e+ pair;
+ * pair_produced (ptr may be NULL) accumulates their weights per cell.
+ * Waits for the stream. */
+AP_API int ap_produce_pairs(ap_ctx *ctx, ap_array pair_produced, ap_rad_counts *out);
+/* The photon move of one update (also run by ap_update_particles when
+ * photons are bound). */
+AP_API int ap_move_photons(ap_ctx *ctx, double dt);
 
 /* Device time per phase of the update, from CUDA events recorded on the
  * context's stream around each phase while profiling is on. */

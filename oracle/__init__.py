@@ -128,7 +128,8 @@ def _build(target_dir, target):
 def _load_oracle():
     path = os.path.join(_HERE, "liboracle.so")
     srcs = [os.path.join(_HERE, n) for n in ("ap_oracle.c", "ap_oracle.h", "ap_logsph.c",
-                                              "ap_logsph.h")]
+                                              "ap_logsph.h", "ap_gr.c", "ap_gr.h", "ap_rad.c",
+                                              "ap_rad.h")]
     if not os.path.exists(path) or any(os.path.getmtime(path) < os.path.getmtime(s)
                                        for s in srcs):
         _build(_HERE, "liboracle.so")

@@ -1,0 +1,207 @@
+"""CPU oracle for photons and pair production -- TEST INFRASTRUCTURE ONLY.
+
+Wraps ``ap_rad.c`` of ``liboracle.so`` (the restatement of the photon movers
+and of ``radiative_transfer`` with the default and the pulsar lab's user
+radiative functions) and the pin library ``_ref/libapref_rad.so`` that runs
+the reference's own user functions on the host (built by
+``ref_build/Makefile`` when the reference tree is present), plus the photon
+movers of ``_ref/libapref.so`` and ``_ref/libapref_ls.so``.
+
+Photons are dicts of numpy arrays with the members of ``photon_data``
+(``particle_data.h:68-80``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import (_HERE, _arr, _build, _p, _vp, _sz, fields_struct, lib, load_ref as _load_ref_cart,
+               ptc_struct, ref_tree_present)
+from . import logsph as _ls
+
+PH_FIELDS = (
+    ("x1", np.float32), ("x2", np.float32), ("x3", np.float32),
+    ("p1", np.float32), ("p2", np.float32), ("p3", np.float32),
+    ("E", np.float32), ("weight", np.float32), ("path_left", np.float32),
+    ("cell", np.uint32), ("id", np.uint64), ("flag", np.uint32),
+)
+
+RAD_DEFAULT, RAD_PULSAR = 0, 1
+
+
+class Photons(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n, _ in PH_FIELDS]
+
+
+class RadParams(C.Structure):
+    """or_rad_params (ap_rad.h)."""
+    _fields_ = [
+        ("model", C.c_int), ("delta_t", C.c_float), ("gamma_thr", C.c_float),
+        ("E_secondary", C.c_float), ("photon_path", C.c_float), ("r_cutoff", C.c_float),
+        ("track_percent", C.c_float), ("e_curv", C.c_float), ("l_curv", C.c_float),
+        ("BQ", C.c_float), ("omega", C.c_float), ("seed", C.c_uint64),
+    ]
+
+
+class RadCounts(C.Structure):
+    _fields_ = [("marked", C.c_uint64), ("written", C.c_uint64), ("dropped", C.c_uint64)]
+
+
+def rad_params(model=RAD_DEFAULT, delta_t=0.01, gamma_thr=20.0, E_secondary=4.0,
+               photon_path=1.0, r_cutoff=4.0, track_percent=0.2, e_curv=6.4e-9, l_curv=6.0,
+               BQ=1.0, omega=0.2, seed=1):
+    """RadParams with the reference's SimParams defaults (sim_params.h:50-83)."""
+    return RadParams(model, delta_t, gamma_thr, E_secondary, photon_path, r_cutoff,
+                     track_percent, e_curv, l_curv, BQ, omega, seed)
+
+
+for _name, _res, _args in [
+    ("or_rad_uniforms", None, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _vp]),
+    ("or_move_photons_cart", None, [_vp, _vp, _sz, C.c_float, _vp]),
+    ("or_move_photons_logsph", None, [_vp, _vp, _vp, _sz, C.c_float]),
+    ("or_emit_photons", None, [_vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, C.c_uint32,
+                               C.c_uint64, _vp]),
+    ("or_produce_pairs", None, [_vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, C.c_uint32,
+                                C.c_uint64, _vp]),
+]:
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def new_photons(cap):
+    ph = {n: np.zeros(cap, dt) for n, dt in PH_FIELDS}
+    ph["cell"][:] = 0xFFFFFFFF
+    return ph
+
+
+def copy_photons(ph):
+    return {k: v.copy() for k, v in ph.items()}
+
+
+def photons_struct(ph):
+    s = Photons()
+    for name, dt in PH_FIELDS:
+        a = ph[name]
+        assert a.dtype == dt and a.flags.c_contiguous, name
+        setattr(s, name, a.ctypes.data)
+    return s
+
+
+def uniforms(seed, tag, call, ids):
+    """The four build uniforms of each id (or_rad_uniforms), shape (n, 4)."""
+    out = np.zeros((len(ids), 4), np.float32)
+    u = (C.c_float * 4)()
+    for k, i in enumerate(ids):
+        lib.or_rad_uniforms(seed, tag, call, int(i), u)
+        out[k] = np.frombuffer(u, np.float32)
+    return out
+
+
+def move_photons_cart(m, ph, num, dt, periodic):
+    s = photons_struct(ph)
+    lib.or_move_photons_cart(C.byref(m), C.byref(s), num, dt,
+                             (C.c_int * 3)(*[int(bool(x)) for x in periodic]))
+
+
+def move_photons_logsph(m, rp, ph, num, dt):
+    s = photons_struct(ph)
+    lib.or_move_photons_logsph(C.byref(m), C.byref(rp), C.byref(s), num, dt)
+
+
+def emit_photons(m, rp, p, ptc_num, ph, ph_num, ph_cap, f, photon_produced, call, first_id):
+    """Returns (new photon number, RadCounts)."""
+    sp, sph, sf = ptc_struct(p), photons_struct(ph), fields_struct(f)
+    n = C.c_size_t(ph_num)
+    cnt = RadCounts()
+    lib.or_emit_photons(C.byref(m), C.byref(rp), C.byref(sp), ptc_num, C.byref(sph), C.byref(n),
+                        ph_cap, C.byref(sf), _p(photon_produced), call, first_id, C.byref(cnt))
+    return n.value, cnt
+
+
+def produce_pairs(m, rp, ph, ph_num, p, ptc_num, ptc_cap, f, pair_produced, call, first_id):
+    """Returns (new particle number, RadCounts)."""
+    sp, sph, sf = ptc_struct(p), photons_struct(ph), fields_struct(f)
+    n = C.c_size_t(ptc_num)
+    cnt = RadCounts()
+    lib.or_produce_pairs(C.byref(m), C.byref(rp), C.byref(sph), ph_num, C.byref(sp), C.byref(n),
+                         ptc_cap, C.byref(sf), _p(pair_produced), call, first_id, C.byref(cnt))
+    return n.value, cnt
+
+
+# ---------------------------------------------------------------------------
+# The reference's own functions on the host (pin libraries).
+
+_REF_PATH = os.path.join(_HERE, "_ref", "libapref_rad.so")
+ref = None
+
+
+def load_ref(build=True):
+    """The reference's user radiative functions on the host, or None."""
+    global ref
+    if ref is not None:
+        return ref
+    if not os.path.exists(_REF_PATH) and build and ref_tree_present():
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_rad.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_PATH):
+        return None
+    r = C.CDLL(_REF_PATH)
+    for name in ("ref_rad_emit_photons", "ref_rad_produce_pairs"):
+        fn = getattr(r, name)
+        fn.restype = C.c_int
+        fn.argtypes = [_vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, _vp, C.c_uint64, _vp]
+    ref = r
+    return ref
+
+
+def ref_emit_photons(m, rp, p, ptc_num, ph, ph_num, ph_cap, f, photon_produced, call, first_id):
+    u4 = uniforms(rp.seed, 1, call, p["id"][:ptc_num])
+    sp, sph, sf = ptc_struct(p), photons_struct(ph), fields_struct(f)
+    n = C.c_size_t(ph_num)
+    cnt = RadCounts()
+    rc = load_ref().ref_rad_emit_photons(C.byref(m), C.byref(rp), C.byref(sp), ptc_num,
+                                         C.byref(sph), C.byref(n), ph_cap, C.byref(sf),
+                                         _p(photon_produced), _p(u4), first_id, C.byref(cnt))
+    assert rc == 0, "a user function drew more uniforms than the build gives it"
+    return n.value, cnt
+
+
+def ref_produce_pairs(m, rp, ph, ph_num, p, ptc_num, ptc_cap, f, pair_produced, call, first_id):
+    u4 = uniforms(rp.seed, 2, call, ph["id"][:ph_num])
+    sp, sph, sf = ptc_struct(p), photons_struct(ph), fields_struct(f)
+    n = C.c_size_t(ptc_num)
+    cnt = RadCounts()
+    rc = load_ref().ref_rad_produce_pairs(C.byref(m), C.byref(rp), C.byref(sph), ph_num,
+                                          C.byref(sp), C.byref(n), ptc_cap, C.byref(sf),
+                                          _p(pair_produced), _p(u4), first_id, C.byref(cnt))
+    assert rc == 0, "a user function drew more uniforms than the build gives it"
+    return n.value, cnt
+
+
+def ref_move_photons_cart(m, ph, num, dt):
+    """The reference's move_photons_cart_1d / _2d (no wrap)."""
+    r = _load_ref_cart()
+    fn = r.ref_move_photons_cart
+    fn.restype = None
+    fn.argtypes = [_vp, _vp, _sz, C.c_float]
+    s = photons_struct(ph)
+    fn(C.byref(m), C.byref(s), num, dt)
+
+
+def ref_move_photons_logsph(m, r_cutoff, ph, num, dt):
+    """The reference's log-spherical move_photons (no guard clearing)."""
+    r = _ls.load_ref()
+    fn = r.ref_ls_move_photons
+    fn.restype = None
+    fn.argtypes = [_vp, C.c_float, _vp, _sz, C.c_float]
+    s = photons_struct(ph)
+    fn(C.byref(m), r_cutoff, C.byref(s), num, dt)
+
+
+def ref_available():
+    return (ref_tree_present() or os.path.exists(_REF_PATH)) and load_ref() is not None

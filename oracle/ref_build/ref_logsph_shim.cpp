@@ -297,4 +297,26 @@ void ref_ls_field_boundary(const ref_mesh *m, const ref_ls_params *lp, const ref
   Kernels::axis_boundary_upper(d);
 }
 
+/* Same layout as or_photons (oracle/ap_rad.h). */
+typedef struct {
+  float *x1, *x2, *x3, *p1, *p2, *p3, *E, *weight, *path_left;
+  uint32_t *cell; uint64_t *id; uint32_t *flag;
+} ref_photons;
+
+/* move_photons<<<256, 512>>> (ptc_updater_logsph.cu:58-131, launched at
+ * :797-800), one emulated thread. send_particles and clear_guard_cells
+ * that follow are not compiled; the caller removes what left the bulk. */
+void ref_ls_move_photons(const ref_mesh *m, float r_cutoff, const ref_photons *ph, size_t num,
+                         float dt) {
+  set_mesh(m);
+  dev_params.r_cutoff = r_cutoff;
+  photon_data d;
+  d.x1 = ph->x1; d.x2 = ph->x2; d.x3 = ph->x3;
+  d.p1 = ph->p1; d.p2 = ph->p2; d.p3 = ph->p3;
+  d.E = ph->E; d.weight = ph->weight; d.path_left = ph->path_left;
+  d.cell = ph->cell; d.id = ph->id; d.flag = ph->flag;
+  one_thread();
+  Kernels::move_photons(d, num, dt, true, true);
+}
+
 }  // extern "C"

@@ -297,4 +297,27 @@ void ref_deposit_mt(const ref_mesh *m, const ref_ptc *p, size_t num, float dt,
 }
 #endif
 
+/* Same layout as or_photons (oracle/ap_rad.h). */
+typedef struct {
+  float *x1, *x2, *x3, *p1, *p2, *p3, *E, *weight, *path_left;
+  uint32_t *cell; uint64_t *id; uint32_t *flag;
+} ref_photons;
+
+/* move_photons_cart_1d / _2d<<<256, 512>>> (ptc_updater.cu:627-690,
+ * launched at :822-831), one emulated thread. The MPI exchange that follows
+ * (send_particles) is not compiled; the caller applies the wrap. */
+void ref_move_photons_cart(const ref_mesh *m, const ref_photons *ph, size_t num, float dt) {
+  set_mesh(m);
+  photon_data d;
+  d.x1 = ph->x1; d.x2 = ph->x2; d.x3 = ph->x3;
+  d.p1 = ph->p1; d.p2 = ph->p2; d.p3 = ph->p3;
+  d.E = ph->E; d.weight = ph->weight; d.path_left = ph->path_left;
+  d.cell = ph->cell; d.id = ph->id; d.flag = ph->flag;
+  one_thread();
+  if (m->dimension == 1)
+    Kernels::move_photons_cart_1d(d, num, dt);
+  else
+    Kernels::move_photons_cart_2d(d, num, dt);
+}
+
 }  // extern "C"

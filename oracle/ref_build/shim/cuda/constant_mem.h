@@ -15,6 +15,9 @@ struct ap_ref_params {
   float q_e, r_cutoff, track_percent;
   float a;  /* 1D GR lab: spin */
   bool inject_ions;
+  /* radiative transfer (user_radiative_functions.cu of src/ and of the
+   * pulsar lab) */
+  float delta_t, gamma_thr, E_secondary, photon_path, l_curv, e_curv, BQ;
 };
 extern Quadmesh dev_mesh;
 extern ap_ref_params dev_params;

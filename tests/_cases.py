@@ -235,3 +235,47 @@ def gr_dt(m, co, p):
     D1, D2 = co[0][c], co[1][c]
     vr = np.abs((p["p1"] / p["E"] - D1) / D2).max()
     return float(np.float32(0.5 * m.delta[0] / max(vr, 1e-6)))
+
+
+# ---------------------------------------------------------------------------
+# Photons and pair production (radiative_transfer with the default and the
+# pulsar lab's user functions).
+
+def rad_photons(m, n, cap, rng, E_range=(2.5, 200.0), path_range=(-0.2, 1.0), holes=0.2,
+                first_id=10_000_000):
+    """cap photon slots, the first n in use: random bulk cells (a fifth of
+    them holes), direction isotropic, energy log-uniform in E_range."""
+    from oracle import rad
+    ph = rad.new_photons(cap)
+    g0, g1 = m.guard[0], m.guard[1]
+    c1 = rng.integers(g0, m.dims[0] - g0, n)
+    c2 = rng.integers(g1, m.dims[1] - g1, n) if m.dimension > 1 else np.zeros(n, np.int64)
+    cell = (c1 + c2 * m.dims[0]).astype(np.uint32)
+    cell[rng.random(n) < holes] = np.uint32(0xFFFFFFFF)
+    ph["cell"][:n] = cell
+    ph["x1"][:n] = rng.random(n, dtype=np.float32)
+    ph["x2"][:n] = rng.random(n, dtype=np.float32)
+    ph["x3"][:n] = (np.pi * (2 * rng.random(n) - 1)).astype(np.float32)
+    E = np.exp(np.log(E_range[0]) + rng.random(n) * np.log(E_range[1] / E_range[0]))
+    ct = 2 * rng.random(n) - 1
+    st = np.sqrt(1 - ct * ct)
+    phi = 2 * np.pi * rng.random(n)
+    ph["p1"][:n] = (E * st * np.cos(phi)).astype(np.float32)
+    ph["p2"][:n] = (E * st * np.sin(phi)).astype(np.float32)
+    ph["p3"][:n] = (E * ct).astype(np.float32)
+    ph["E"][:n] = E.astype(np.float32)
+    ph["weight"][:n] = (0.5 + rng.random(n)).astype(np.float32)
+    ph["path_left"][:n] = (path_range[0] + (path_range[1] - path_range[0]) * rng.random(n)
+                           ).astype(np.float32)
+    ph["id"][:n] = np.arange(first_id, first_id + n, dtype=np.uint64)
+    return ph
+
+
+def rad_rho(f, rng, frac_dense=0.3):
+    """Charge densities with a multiplicity |rho0| + |rho1| over |rho0 + rho1|
+    above 50 in about frac_dense of the cells."""
+    shape = f["Rho"][0].shape
+    a = rng.random(shape) + 0.1
+    dense = rng.random(shape) < frac_dense
+    f["Rho"][0][:] = (-a).astype(np.float32)
+    f["Rho"][1][:] = np.where(dense, a * (1 + 1e-3), a * 3.0).astype(np.float32)

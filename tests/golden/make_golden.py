@@ -5,9 +5,11 @@ ptc_updater_logsph.cu / field_solver_logsph.cu kernels and
 grid_log_sph.cpp coefficients), run on the host by oracle/ref_build.
 
 Needs the reference tree (to build oracle/_ref/libapref.so). Run from the
-repository root:  python tests/golden/make_golden.py [logsph | gap | gr]
+repository root:  python tests/golden/make_golden.py [logsph | gap | gr | rad]
 (gap_*.npz: the 1D gap lab's update_ptc_1dgap, ptc_updater_1dgap.cu;
-gr_a.npz: the 1D GR lab's compute_coef and update_ptc_1dgr).
+gr_a.npz: the 1D GR lab's compute_coef and update_ptc_1dgr; rad_a.npz: the
+pulsar lab's user radiative functions through emit_photons and
+produce_pairs).
 Each fixture holds seeded inputs (particles, E/B, backgrounds, J) and the
 reference outputs: particles and J/Rho after push + deposit, and E/B/divE/
 divB after one E update, one B update and compute_divs.
@@ -224,6 +226,48 @@ def main_gr():
     print(path, os.path.getsize(path))
 
 
+def main_rad():
+    """rad_a.npz: the pulsar lab's check_emit_photon / emit_photon and
+    check_produce_pair / produce_pair (oracle/_ref/libapref_rad.so, run by
+    the pin driver with the build's draws) on a small seeded log-spherical
+    state: inputs are the particles, photons and B / Rho fields; outputs the
+    particles and photons after emit_photons, then after produce_pairs."""
+    from oracle import rad
+    from _cases import logsph_fields, logsph_particles, mesh_logsph, rad_photons, rad_rho
+    if rad.load_ref(build=True) is None:
+        raise SystemExit("radiation pin library unavailable (needs the reference tree)")
+    seed, N, n, ph_n = 12, 40, 1000, 500
+    m = mesh_logsph(N, N, rmax=8.0)
+    rng = np.random.default_rng(seed)
+    f = logsph_fields(m, rng, omega=0.1, noise=0.0, num_species=2)
+    rad_rho(f, rng)
+    p = logsph_particles(m, n, rng, gamma_max=3e4)
+    ph = rad_photons(m, ph_n, 3 * ph_n, rng, E_range=(2.5, 500.0))
+    rp = rad.rad_params(rad.RAD_PULSAR, delta_t=0.01, e_curv=2e-8, l_curv=2.0, BQ=0.05,
+                        omega=0.1, r_cutoff=6.0, track_percent=0.3, seed=77)
+    out = {"N": np.int64(N), "ph_num": np.int64(ph_n), "ph_cap": np.int64(ph["x1"].size),
+           "B": np.stack(f["B"]), "Rho": np.stack(f["Rho"])}
+    for k in p:
+        out["in_ptc_" + k] = p[k].copy()
+    for k in ph:
+        out["in_ph_" + k] = ph[k][:ph_n].copy()
+    no, _ = rad.ref_emit_photons(m, rp, p, n, ph, ph_n, ph["x1"].size, f, None, 4, 700)
+    for k in ("p1", "p2", "p3", "E"):
+        out["emit_ptc_" + k] = p[k].copy()
+    for k in ph:
+        out["emit_ph_" + k] = ph[k][:no].copy()
+    cap = n + 2 * no + 60
+    big = {k: np.concatenate([v, np.zeros(cap - n, v.dtype)]) for k, v in p.items()}
+    big["cell"][n:] = oracle.MAX_CELL
+    nb, _ = rad.ref_produce_pairs(m, rp, ph, no, big, n, cap, f, None, 4, 123_456)
+    out["pairs_ph_cell"] = ph["cell"][:no].copy()
+    for k in big:
+        out["pairs_ptc_" + k] = big[k][n:nb].copy()
+    path = os.path.join(HERE, "rad_a.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path))
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "logsph":
         main_logsph()
@@ -231,5 +275,7 @@ if __name__ == "__main__":
         main_gap()
     elif len(sys.argv) > 1 and sys.argv[1] == "gr":
         main_gr()
+    elif len(sys.argv) > 1 and sys.argv[1] == "rad":
+        main_rad()
     else:
         main()
