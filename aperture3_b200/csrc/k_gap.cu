@@ -142,8 +142,9 @@ __device__ void gap_chunk(const PushDepositParams &P, size_t ch, int *sWhi, unsi
       const bool rho = sp < ns;
       float djx = 0.0f;
 #pragma unroll
-      for (int i = -2; i <= 1; ++i) {
-        if (i < i0 || i > i1) continue;
+      for (int j = 0; j < 3; ++j) {  // the 2 or 3 nodes i0 .. i1, in order
+        const int i = i0 + j;
+        if (i > i1) continue;
         const float sx0 = cic(-x1 + i + 1);
         const float sx1 = cic(-new_x1 + (i + 1 - dc1));
         djx += sx1 - sx0;

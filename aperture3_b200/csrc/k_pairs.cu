@@ -35,51 +35,90 @@ __device__ __forceinline__ double uniform_of(uint32_t step, uint64_t id, const u
   return ((double)(out[0] >> 8) + 0.5) * (1.0 / 16777216.0);
 }
 
-// The emission test of one live particle (no writes).
-__device__ __forceinline__ bool emit_test(const PairK &K, const PtcK &p, const uint64_t *ids,
-                                          size_t idx, uint32_t step) {
-  if (p.cell[idx] == AP_MAX_CELL) return false;
-  const float gamma = p.E[idx];
-  if (!(gamma > K.gamma_thr)) return false;
-  const float p1 = p.p1[idx], p2 = p.p2[idx], p3 = p.p3[idx];
+// The emission decision of a hot particle (gamma > gamma_thr) from its
+// momentum and id.
+__device__ __forceinline__ bool emit_decide(const PairK &K, float gamma, float p1, float p2,
+                                            float p3, uint64_t id, uint32_t step) {
   const float pm = sqrtf(p1 * p1 + p2 * p2 + p3 * p3);
   const float ds = (pm / gamma) * K.dt;
+  const double u = uniform_of(step, id, K.key);
+  // The decision is u < 1 - exp(-ds / free_path) evaluated in double. A
+  // float estimate decides it first: expm1f is within 1 ulp and the float
+  // quotient within half an ulp, so it is within 4e-7 relative of the exact
+  // value, and the double expression within 1e-15 absolute of it; only a u
+  // inside that band goes on to the double expression.
+  const double pf = -(double)expm1f(-(ds / K.free_path));
+  const double band = pf * 1e-5 + 1e-15;
+  if (u < pf - band) return true;
+  if (u > pf + band) return false;
   const double prob = 1.0 - exp(-(double)ds / (double)K.free_path);
-  return uniform_of(step, ids[idx], K.key) < prob;
+  return u < prob;
 }
 
-// Marks the emitters of chunk ch and stores the chunk's count.
+// Marks the emitters of chunk ch and adds the chunk's count to
+// chunk_count[ch] (one atomic per warp; the scan resets the counts).
+// Thread t takes the four consecutive slots ch * kPairChunk + 4 t + [0, 4):
+// their cells and gammas arrive in one 16-byte load each (when the arrays
+// are 16-byte aligned), then the momenta and ids of the hot ones, and the
+// four emit bytes leave as one word.
 __device__ __forceinline__ void mark_chunk(const PairK &K, const PtcK &p, const uint64_t *ids,
                                            size_t number, uint32_t step, uint8_t *emit,
                                            uint32_t *chunk_count, uint32_t ch) {
-  // the cells and gammas of all items are loaded first, so their latencies
-  // overlap; only the rare hot particles go on to the momentum and the draw
-  uint32_t cell[kPairPerThread];
-  float gam[kPairPerThread];
+  static_assert(kPairPerThread == 4, "four consecutive slots per thread");
+  const size_t first = (size_t)ch * kPairChunk + (size_t)threadIdx.x * kPairPerThread;
+  uint32_t cell[4] = {AP_MAX_CELL, AP_MAX_CELL, AP_MAX_CELL, AP_MAX_CELL};
+  float gam[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  const bool vec = ((reinterpret_cast<uintptr_t>(p.cell) | reinterpret_cast<uintptr_t>(p.E)) &
+                    15u) == 0;
+  if (vec && first + 4 <= number) {
+    const uint4 c4 = *reinterpret_cast<const uint4 *>(p.cell + first);
+    const float4 g4 = *reinterpret_cast<const float4 *>(p.E + first);
+    cell[0] = c4.x; cell[1] = c4.y; cell[2] = c4.z; cell[3] = c4.w;
+    gam[0] = g4.x; gam[1] = g4.y; gam[2] = g4.z; gam[3] = g4.w;
+  } else {
 #pragma unroll
-  for (int k = 0; k < kPairPerThread; ++k) {
-    const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
-    cell[k] = idx < number ? p.cell[idx] : AP_MAX_CELL;
-    gam[k] = idx < number ? p.E[idx] : 0.0f;
+    for (int k = 0; k < 4; ++k)
+      if (first + k < number) {
+        cell[k] = p.cell[first + k];
+        gam[k] = p.E[first + k];
+      }
   }
-  bool e[kPairPerThread];
+  bool hot[4];
+  float q1[4], q2[4], q3[4];
+  uint64_t id[4];
 #pragma unroll
-  for (int k = 0; k < kPairPerThread; ++k) {
-    const size_t idx = (size_t)ch * kPairChunk + (size_t)k * kPairThreads + threadIdx.x;
-    e[k] = cell[k] != AP_MAX_CELL && gam[k] > K.gamma_thr &&
-           emit_test(K, p, ids, idx, step);
-    if (idx < number) emit[idx] = e[k] ? 1 : 0;
+  for (int k = 0; k < 4; ++k) {
+    hot[k] = cell[k] != AP_MAX_CELL && gam[k] > K.gamma_thr;
+    q1[k] = hot[k] ? p.p1[first + k] : 0.0f;
+    q2[k] = hot[k] ? p.p2[first + k] : 0.0f;
+    q3[k] = hot[k] ? p.p3[first + k] : 0.0f;
+    id[k] = hot[k] ? ids[first + k] : 0ull;
   }
+  uint32_t e4 = 0;
   int cnt = 0;
+  if (hot[0] | hot[1] | hot[2] | hot[3]) {
 #pragma unroll
-  for (int k = 0; k < kPairPerThread; ++k) cnt += __syncthreads_count(e[k]);
-  if (threadIdx.x == 0) chunk_count[ch] = (uint32_t)cnt;
+    for (int k = 0; k < 4; ++k) {
+      const bool e = hot[k] && emit_decide(K, gam[k], q1[k], q2[k], q3[k], id[k], step);
+      e4 |= (e ? 1u : 0u) << (8 * k);
+      cnt += e ? 1 : 0;
+    }
+  }
+  if (first + 4 <= number) {
+    *reinterpret_cast<uint32_t *>(emit + first) = e4;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (first + k < number) emit[first + k] = (uint8_t)((e4 >> (8 * k)) & 1u);
+  }
+  cnt = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(chunk_count + ch, (uint32_t)cnt);
 }
 
 // One CTA of 1024 threads: exclusive scan of the chunk counts into offs; the
 // total is clamped to the free capacity and the device state moves on; the
 // old count and next id go to tot[] for the append pass.
-__device__ __forceinline__ void scan_chunks(const uint32_t *chunk_count, uint32_t nchunks,
+__device__ __forceinline__ void scan_chunks(uint32_t *chunk_count, uint32_t nchunks,
                                             uint32_t *offs, size_t capacity, PairState *st,
                                             uint32_t *tot) {
   __shared__ uint32_t s_warp[32];
@@ -90,6 +129,7 @@ __device__ __forceinline__ void scan_chunks(const uint32_t *chunk_count, uint32_
   for (uint32_t b0 = 0; b0 < nchunks; b0 += blockDim.x) {
     const uint32_t i = b0 + threadIdx.x;
     const uint32_t v = i < nchunks ? chunk_count[i] : 0u;
+    if (i < nchunks) chunk_count[i] = 0u;  // ready for the next mark pass
     uint32_t x = v;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -114,6 +154,7 @@ __device__ __forceinline__ void scan_chunks(const uint32_t *chunk_count, uint32_
   }
   if (threadIdx.x == 0) {
     const uint32_t total = s_carry;
+    offs[nchunks] = total;  // so that chunk ch holds offs[ch + 1] - offs[ch] emitters
     const uint32_t old = st->number;
     const size_t free_slots = capacity > old ? capacity - old : 0;
     const uint32_t room = (uint32_t)(free_slots / 2 > 0xffffffffu ? 0xffffffffu : free_slots / 2);
@@ -135,10 +176,17 @@ __device__ __forceinline__ void scan_chunks(const uint32_t *chunk_count, uint32_
 }
 
 // Appends the pairs of the emitters of chunk ch (ranked in slot order).
-__device__ __forceinline__ void append_chunk(const PairK &K, const PtcK &p, uint64_t *ids,
+// Returns false, having done nothing, for a chunk without emitters (the same
+// answer in every thread of the CTA). The warp totals alternate between two
+// shared buffers by `parity` (the count of chunks this CTA appended so far),
+// so one barrier per chunk suffices: a buffer is rewritten only after the
+// barrier of the chunk in between.
+__device__ __forceinline__ bool append_chunk(const PairK &K, const PtcK &p, uint64_t *ids,
                                              const uint8_t *emit, const uint32_t *offs,
-                                             const uint32_t *tot, uint32_t ch) {
-  __shared__ uint32_t s_warp[kPairThreads / 32];
+                                             const uint32_t *tot, uint32_t ch, int parity) {
+  __shared__ uint32_t s_warp2[2][kPairThreads / 32];
+  if (offs[ch + 1] == offs[ch]) return false;
+  uint32_t *s_warp = s_warp2[parity & 1];
   const uint32_t emitted = tot[0];
   const size_t number = tot[1];
   const uint64_t id_base = (uint64_t)tot[2] | ((uint64_t)tot[3] << 32);
@@ -170,7 +218,6 @@ __device__ __forceinline__ void append_chunk(const PairK &K, const PtcK &p, uint
   uint32_t before = 0;
   for (int w = 0; w < warp; ++w) before += s_warp[w];
   uint32_t rank = off_ch + before + x - mine;
-  __syncthreads();
 #pragma unroll
   for (int k = 0; k < kPairPerThread; ++k) {
     const size_t idx = first + k;
@@ -215,7 +262,7 @@ __global__ void __launch_bounds__(kPairThreads)
 }
 
 __global__ void __launch_bounds__(1024)
-    k_pair_scan(const uint32_t *chunk_count, uint32_t nchunks, uint32_t *offs, size_t capacity,
+    k_pair_scan(uint32_t *chunk_count, uint32_t nchunks, uint32_t *offs, size_t capacity,
                 PairState *st, uint32_t *tot) {
   scan_chunks(chunk_count, nchunks, offs, capacity, st, tot);
 }
@@ -223,8 +270,9 @@ __global__ void __launch_bounds__(1024)
 __global__ void __launch_bounds__(kPairThreads)
     k_pair_append(PairK K, PtcK p, uint64_t *ids, const uint8_t *emit, const uint32_t *offs,
                   const uint32_t *tot, uint32_t nchunks) {
+  int parity = 0;
   for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
-    append_chunk(K, p, ids, emit, offs, tot, ch);
+    parity += append_chunk(K, p, ids, emit, offs, tot, ch, parity) ? 1 : 0;
 }
 
 // Batched over 1D runs: work item g is chunk g - base[r] of run r.
@@ -273,10 +321,13 @@ __global__ void __launch_bounds__(kPairThreads)
     k_b1_pair_append(const Run1D *__restrict__ runs, const uint32_t *__restrict__ base,
                      int nruns) {
   const uint32_t total = base[nruns];
+  int parity = 0;
   for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
     const int r = run_of(base, nruns, g);
     const Run1D &R = runs[r];
-    append_chunk(pairk_of(R), R.p, R.ids, R.emit, R.offs, R.tot, g - base[r]);
+    parity += append_chunk(pairk_of(R), R.p, R.ids, R.emit, R.offs, R.tot, g - base[r], parity)
+                  ? 1
+                  : 0;
   }
 }
 
@@ -330,6 +381,9 @@ int ensure_pair_scratch(Ctx &c) {
   const size_t cap = (size_t)nchunks + 64;
   if (cudaMalloc(&c.pair_chunks, sizeof(uint32_t) * (2 * cap + 8)) != cudaSuccess)
     return AP_ERR_NOMEM;
+  // the mark pass adds into the counts, the scan resets them
+  if (cudaMemset(c.pair_chunks, 0, sizeof(uint32_t) * (2 * cap + 8)) != cudaSuccess)
+    return AP_ERR_CUDA;
   c.pair_cap_chunks = cap;
   return AP_OK;
 }

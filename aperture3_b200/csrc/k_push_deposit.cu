@@ -955,11 +955,15 @@ __device__ __forceinline__ void push_deposit_1d_chunk(const PushDepositParams &P
     } while (false);
     {
       const float weight = d_w;
+      // the reference's node range [i0, i1] has 2 or 3 nodes; every lane
+      // walks three node slots i0, i0 + 1, i0 + 2 (the third active only for
+      // a cell crossing), in the reference's order
       const int i0 = (d_dc1 == -1 ? -2 : -1), i1 = (d_dc1 == 1 ? 1 : 0);
       float djx = 0.0f;
 #pragma unroll
-      for (int i = -2; i <= 1; ++i) {
-        const bool act = dep && i >= i0 && i <= i1;
+      for (int j = 0; j < 3; ++j) {
+        const int i = i0 + j;
+        const bool act = dep && i <= i1;
         float sx1 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         const int off = i + d_c1;
         if (act) {

@@ -254,6 +254,27 @@ __device__ void produce_pair(const PhK &ph, size_t tid, const PtcK &p, size_t of
   ph.cell[tid] = AP_MAX_CELL;
 }
 
+// photon_produced / pair_produced (cell) += w for the lanes with `on`.
+// Lanes hold consecutive slots, mostly sorted by cell, so many of them add
+// to one cell: each group of lanes with the same cell sums its weights in
+// lane order and its lowest lane adds once (the reference adds per particle
+// with float atomics, radiative_transfer.cu:57-58, 126-130).
+__device__ __forceinline__ void add_produced(const RadK &K, uint32_t cell, float w, bool on) {
+  const unsigned any = __ballot_sync(0xffffffffu, on);
+  if (!any) return;
+  const uint32_t key = on ? cell : AP_MAX_CELL;
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  float sum = 0.0f;
+  for (int o = 0; o < 32; ++o) {
+    const float v = __shfl_sync(0xffffffffu, w, o);
+    if ((peers >> o) & 1u) sum += v;
+  }
+  const int lane = threadIdx.x & 31;
+  if (on && lane == __ffs(peers) - 1)
+    atomicAdd(K.produced.ptr + (size_t)c2_of(K.m, cell) * K.produced.pitch + c1_of(K.m, cell),
+              sum);
+}
+
 // Exclusive scan of the chunk counts (one CTA of 1024 threads); the total
 // goes to offs[nchunks].
 __global__ void __launch_bounds__(1024) k_rad_scan(const uint32_t *counts, uint32_t nchunks,
@@ -330,19 +351,17 @@ __global__ void __launch_bounds__(kRadThreads)
     for (int k = 0; k < kRadPer; ++k) {
       const size_t idx = (size_t)ch * kRadChunk + (size_t)k * kRadThreads + threadIdx.x;
       bool e = false;
+      uint32_t cell = AP_MAX_CELL;
       if (idx < number) {
-        const uint32_t cell = p.cell[idx];
+        cell = p.cell[idx];
         if (cell != AP_MAX_CELL && in_bulk(K.m, cell) && (p.flag[idx] >> 29) != 2u) {
           float u[4];
           uniforms(K, 1u, ids[idx], u);
           e = check_emit(K, p, idx, cell, u);
-          if (e && K.produced.ptr)
-            atomicAdd(K.produced.ptr + (size_t)c2_of(K.m, cell) * K.produced.pitch +
-                          c1_of(K.m, cell),
-                      p.w[idx]);
         }
         mark[idx] = e ? 1 : 0;
       }
+      if (K.produced.ptr) add_produced(K, cell, e ? p.w[idx] : 0.0f, e);
       cnt += __syncthreads_count(e);
     }
     if (threadIdx.x == 0) counts[ch] = (uint32_t)cnt;
@@ -383,17 +402,13 @@ __global__ void __launch_bounds__(kRadThreads)
     for (int k = 0; k < kRadPer; ++k) {
       const size_t idx = (size_t)ch * kRadChunk + (size_t)k * kRadThreads + threadIdx.x;
       bool e = false;
+      uint32_t cell = AP_MAX_CELL;
       if (idx < number) {
-        const uint32_t cell = ph.cell[idx];
-        if (cell != AP_MAX_CELL && in_bulk(K.m, cell)) {
-          e = check_pair(K, ph, idx, cell);
-          if (e && K.produced.ptr)
-            atomicAdd(K.produced.ptr + (size_t)c2_of(K.m, cell) * K.produced.pitch +
-                          c1_of(K.m, cell),
-                      ph.w[idx]);
-        }
+        cell = ph.cell[idx];
+        if (cell != AP_MAX_CELL && in_bulk(K.m, cell)) e = check_pair(K, ph, idx, cell);
         mark[idx] = e ? 1 : 0;
       }
+      if (K.produced.ptr) add_produced(K, cell, e ? ph.w[idx] : 0.0f, e);
       cnt += __syncthreads_count(e);
     }
     if (threadIdx.x == 0) counts[ch] = (uint32_t)cnt;
@@ -622,9 +637,15 @@ int rad_move_photons(Ctx &c, float dt) {
   return cudaGetLastError() == cudaSuccess ? AP_OK : AP_ERR_CUDA;
 }
 
+// Scratch for either store at its capacity, allocated once: an allocation
+// inside a pass would stall the device between its launches.
+static size_t rad_scratch_slots(const Ctx &c) {
+  return c.capacity > c.ph_capacity ? c.capacity : c.ph_capacity;
+}
+
 int rad_emit_photons(Ctx &c, ap_array produced, ap_rad_counts *out) {
   const size_t number = c.number;
-  if (ensure_rad_scratch(c, number) != AP_OK) return AP_ERR_NOMEM;
+  if (ensure_rad_scratch(c, rad_scratch_slots(c)) != AP_OK) return AP_ERR_NOMEM;
   const uint32_t nchunks = (uint32_t)((number + kRadChunk - 1) / kRadChunk);
   uint32_t marked = 0;
   if (nchunks > 0) {
@@ -659,7 +680,7 @@ int rad_emit_photons(Ctx &c, ap_array produced, ap_rad_counts *out) {
 
 int rad_produce_pairs(Ctx &c, ap_array produced, ap_rad_counts *out) {
   const size_t number = c.ph_number;
-  if (ensure_rad_scratch(c, number) != AP_OK) return AP_ERR_NOMEM;
+  if (ensure_rad_scratch(c, rad_scratch_slots(c)) != AP_OK) return AP_ERR_NOMEM;
   const uint32_t nchunks = (uint32_t)((number + kRadChunk - 1) / kRadChunk);
   uint32_t marked = 0;
   const size_t base = c.number + 20;  // produce_pairs starts at number + 20 (:281)

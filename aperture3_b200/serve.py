@@ -179,6 +179,12 @@ class GapServer:
         self.round_steps = int(round_steps)
         self.keep = keep_results
         self.results: Dict[int, Dict[str, object]] = {}
+        # per round: (start s, resident runs, resident particles, steps, wall s);
+        # per admission ("admit", rid, start s, s) and retirement ("retire",
+        # rid, start s, s waiting for the batch, s reading the run's counters,
+        # s releasing the run)
+        self.trace: List[tuple] = []
+        self.events: List[tuple] = []
 
     def serve(self, requests: List[GapRequest], realtime: bool = True) -> Dict[str, object]:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
@@ -196,8 +202,10 @@ class GapServer:
             while pending and pending[0].arrival <= now() and used + footprint_bytes(
                     pending[0]) <= self.budget:
                 req = pending.pop(0)
+                t_adm = time.perf_counter()
                 run = GapRun(req, self.device)
                 batch.add(run.data)
+                self.events.append(("admit", req.rid, t_adm - t0, time.perf_counter() - t_adm))
                 active.append(run)
                 used += run.fp
                 admitted[req.rid] = now() if realtime else 0.0
@@ -211,18 +219,29 @@ class GapServer:
             # the lab loop of every resident run for `rounds` steps in one
             # call: update_particles, update_fields, inject_pairs, sort every
             # SORT_INTERVAL steps (ap_batch_advance)
+            t_round = time.perf_counter()
             batch.advance([r.step for r in active], rounds, SORT_INTERVAL, inject=True)
             for r in active:
                 r.step += rounds
+            self.trace.append((t_round - t0, len(active),
+                               sum(r.req.cells * r.req.ppc for r in active), rounds,
+                               time.perf_counter() - t_round))
             for r in [r for r in active if r.step >= r.req.steps]:
+                t_ret = time.perf_counter()
                 batch.remove(r.data)  # waits for the batch's stream
+                t_rem = time.perf_counter() - t_ret
+                t_ps = time.perf_counter()
                 finished[r.req.rid] = time.perf_counter() - t0
                 particle_steps += r.particle_steps()
                 if self.keep:
                     self.results[r.req.rid] = r.result()
                 active.remove(r)
                 used -= r.fp
+                t_cl = time.perf_counter()
                 r.close()
+                t_end = time.perf_counter()
+                self.events.append(("retire", r.req.rid, t_ret - t0, t_rem, t_cl - t_ps,
+                                    t_end - t_cl))
         batch.close()
         torch.cuda.synchronize()
         makespan = time.perf_counter() - t0

@@ -1039,9 +1039,71 @@ def run_logsph(args, emit=True, fp64_error=True):
     env.close()
     if fp64_error:
         line["fp64_error_after_2000_steps"] = logsph_fp64_error()
+        line["radiation"] = logsph_radiation(args)
     if emit:
         print(json.dumps(line), flush=True)
     return line
+
+
+def logsph_radiation(args, passes=4):
+    """Photon emission and pair production (radiative_transfer with the
+    pulsar lab's user functions) on the log-spherical state of run_logsph,
+    the reference's SimParams defaults for the radiation constants: one
+    emit_photons + produce_pairs pass per round, device time of each pass
+    (CUDA events on the library's stream around the three launches), the
+    first pass untimed."""
+    import dataclasses
+
+    import torch
+    from aperture3_b200 import SimData, SimEnvironment, ic, radiative_transfer
+
+    dev = torch.device("cuda", 0)
+    params, fields, ptc = ic.logsph(seed=11, N=args.N, ppc=32, device=dev)
+    n = ptc["x1"].numel()
+    ph_cap = 2 * n
+    params = dataclasses.replace(params, create_pairs=True, rad_model="pulsar",
+                                 max_photon_number=ph_cap, max_ptc_number=n + 4 * n, rad_seed=7)
+    env = SimEnvironment(params)
+    data = SimData(env)
+    data.set_fields_device(fields)
+    data.set_particles_device(ptc)
+    del ptc
+    stream = torch.cuda.Stream()
+    env.set_stream(stream)
+    rt = radiative_transfer(env)
+    rows = []
+    with torch.cuda.stream(stream):
+        for r in range(passes + 1):
+            n_ptc, n_ph = data.number, data.photon_number
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            em = rt.emit_photons(data)
+            e[1].record(stream)
+            pr = rt.produce_pairs(data)
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            data.sort_particles()  # trims the photons and the empty particle slots
+            if r == 0:
+                continue
+            rows.append({"particles": n_ptc, "photons_in": n_ph + em["written"],
+                         "emitted": em["written"], "pairs": pr["written"],
+                         "emit_ms": e[0].elapsed_time(e[1]), "pairs_ms": e[1].elapsed_time(e[2])})
+    env.close()
+    emit_ms = sum(r["emit_ms"] for r in rows) / len(rows)
+    pair_ms = sum(r["pairs_ms"] for r in rows) / len(rows)
+    scanned = sum(r["particles"] for r in rows) / len(rows)
+    ph_scanned = sum(r["photons_in"] for r in rows) / len(rows)
+    return {
+        "model": "pulsar lab (labs/pulsar/src/cuda/radiation/user_radiative_functions.cu), "
+                 "SimParams defaults e_curv 6.4e-9, l_curv 6, BQ 1",
+        "passes": rows,
+        "emit_ms": emit_ms, "produce_ms": pair_ms,
+        "emit_particles_per_s": scanned / (emit_ms / 1e3),
+        "produce_photons_per_s": ph_scanned / (pair_ms / 1e3),
+        # mark reads cell, flag, E, x1, x2 (20 B) per particle; the append
+        # reads the emitter again and writes a 52 B photon
+        "emit_algorithmic_gbs": scanned * 20 / (emit_ms / 1e3) / 1e9,
+    }
 
 
 def run_served(args, emit=True):
