@@ -152,8 +152,10 @@ class GapRun:
         self.env.close()
 
 
-def run_alone(req: GapRequest, device, keep_result: bool = True):
-    """The plain path: the lab loop of one run, synchronous calls."""
+def run_alone(req: GapRequest, device, keep_result: bool = True, retired=None):
+    """The plain path: the lab loop of one run, synchronous calls. With a
+    `retired` list the finished run is appended to it instead of being
+    released (the caller releases it later, as the server does)."""
     run = GapRun(req, device)
     pusher, solver = ptc_updater(run.env), field_solver(run.env)
     for s in range(req.steps):
@@ -165,12 +167,17 @@ def run_alone(req: GapRequest, device, keep_result: bool = True):
     torch.cuda.synchronize()
     out = run.result() if keep_result else None
     ps = run.particle_steps()
-    run.close()
+    if retired is None:
+        run.close()
+    else:
+        retired.append(run)
     return out, ps
 
 
 class GapServer:
-    """Continuous batching of gap runs under an HBM budget."""
+    """Continuous batching of gap runs under an HBM budget. Finished runs
+    leave the batch at once; their device memory is released when a later
+    admission needs the room, or after the last request."""
 
     def __init__(self, device=None, hbm_budget: float = 40e9, round_steps: int = 16,
                  keep_results: bool = False):
@@ -185,6 +192,8 @@ class GapServer:
         # s releasing the run)
         self.trace: List[tuple] = []
         self.events: List[tuple] = []
+        self.retired: List["GapRun"] = []  # finished runs whose memory is not yet released
+        self.retired_bytes = 0
 
     def serve(self, requests: List[GapRequest], realtime: bool = True) -> Dict[str, object]:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
@@ -203,6 +212,7 @@ class GapServer:
                     pending[0]) <= self.budget:
                 req = pending.pop(0)
                 t_adm = time.perf_counter()
+                self._release_if_needed(footprint_bytes(req))
                 run = GapRun(req, self.device)
                 batch.add(run.data)
                 self.events.append(("admit", req.rid, t_adm - t0, time.perf_counter() - t_adm))
@@ -238,32 +248,61 @@ class GapServer:
                 active.remove(r)
                 used -= r.fp
                 t_cl = time.perf_counter()
-                r.close()
+                # the run's device memory is released off the critical path:
+                # when a later admission needs the room, else after the last
+                # request (cudaFree waits for the whole device and can take
+                # tens of milliseconds per run)
+                self.retired.append(r)
+                self.retired_bytes += r.fp
+                if self.retired_bytes > self.budget:
+                    self._release()
                 t_end = time.perf_counter()
                 self.events.append(("retire", r.req.rid, t_ret - t0, t_rem, t_cl - t_ps,
                                     t_end - t_cl))
         batch.close()
         torch.cuda.synchronize()
         makespan = time.perf_counter() - t0
+        self._release()
         return _stats(requests, admitted, finished, particle_steps, makespan)
+
+    def _release(self):
+        for r in self.retired:
+            r.close()
+        self.retired.clear()
+        self.retired_bytes = 0
+
+    def _release_if_needed(self, need: int):
+        """Frees the retired runs when the device lacks room for `need` bytes
+        and a 2 GB reserve."""
+        if self.retired and torch.cuda.mem_get_info(self.device)[0] < need + (2 << 30):
+            self._release()
 
 
 def serve_one_at_a_time(requests: List[GapRequest], device=None, realtime: bool = True):
     """The same requests served first come, first served, one at a time
-    through the plain path."""
+    through the plain path. Finished runs are released off the critical
+    path, as by the server: when the next request needs the room, else at
+    the end."""
     device = device or torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
     admitted, finished, total = {}, {}, 0
+    retired: List[GapRun] = []
     for req in sorted(requests, key=lambda r: (r.arrival, r.rid)):
         if realtime:
             wait = req.arrival - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
         admitted[req.rid] = time.perf_counter() - t0
-        _, ps = run_alone(req, device, keep_result=False)
+        if retired and torch.cuda.mem_get_info(device)[0] < footprint_bytes(req) + (2 << 30):
+            for r in retired:
+                r.close()
+            retired.clear()
+        _, ps = run_alone(req, device, keep_result=False, retired=retired)
         total += ps
         finished[req.rid] = time.perf_counter() - t0
     makespan = time.perf_counter() - t0
+    for r in retired:
+        r.close()
     return _stats(requests, admitted, finished, total, makespan)
 
 

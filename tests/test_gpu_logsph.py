@@ -243,30 +243,59 @@ def test_field_boundary():
     case.close()
 
 
+def _live_by_id(p):
+    live = p["cell"] != oracle.MAX_CELL
+    order = np.argsort(p["id"][live], kind="stable")
+    return {k: v[live][order] for k, v in p.items()}
+
+
+def _errors_by_id(m, a, ref):
+    """_errors over the particles live in both, matched by id (the GPU run
+    sorts its store, the oracles do not)."""
+    a, ref = _live_by_id(a), _live_by_id(ref)
+    _, ia, ir = np.intersect1d(a["id"], ref["id"], assume_unique=True, return_indices=True)
+    a = {k: v[ia] for k, v in a.items()}
+    ref = {k: v[ir] for k, v in ref.items()}
+    _, xa, ya = _phys(m, a)
+    _, xr, yr = _phys(m, ref)
+    pos = np.hypot(xa - xr, ya - yr)
+    pa, pr = _p(a), _p(ref)
+    mom = np.linalg.norm(pa - pr, axis=0) / np.maximum(np.linalg.norm(pr, axis=0), 1e-30)
+    return pos, mom
+
+
 @pytest.mark.parametrize("smoothing,data_interval", [(0, 2), (2, 1)])
 def test_multi_step_run(smoothing, data_interval):
-    """Ten coupled steps (particles, fields, boundaries, a sort): particle
-    error against FP64 stays at the FP32 oracle's level, and the live count,
-    total charge and J agree with the FP32 oracle."""
+    """Ten coupled steps (particles, fields, boundaries, a sort on the GPU):
+    against the FP64 oracle run alongside, the GPU's particle errors (p50,
+    p99, matched by id) and current errors (maximum and 99.9th percentile of
+    the cells, relative to max|J|) stay within ERR_FACTOR of the FP32
+    oracle's own; the live count and the total weight agree with the FP32
+    oracle."""
     case = LsCase((96, 64), 30000, 9, gamma_max=1e4, smoothing=smoothing,
                   data_interval=data_interval, compactness=0.2)
     for step in range(10):
         case.step_particles(step)
         case.step_fields(omega=0.05)
         if step == 4:
-            case.data.sort_particles()  # the checks below do not depend on slot order
+            case.data.sort_particles()
     got = case.data.particles_host()
     live_g = int((got["cell"] != oracle.MAX_CELL).sum())
     live_o = int((case.p["cell"] != oracle.MAX_CELL).sum())
     assert abs(live_g - live_o) <= max(3, live_o // 1000), (live_g, live_o)
     w = lambda p: float((p["weight"].astype(np.float64) * (p["cell"] != oracle.MAX_CELL)).sum())
     assert abs(w(got) - w(case.p)) <= 1e-3 * w(case.p)
-    g = case.data.fields_host()
-    for k in range(3):
-        b = case.f["J"][k].astype(np.float64)
-        scale = max(np.abs(b).max(), 1e-30)
-        d = np.abs(g["J"][k] - b) / scale
-        assert np.percentile(d, 99) < 1e-3, f"J{k + 1}"
+    pos_g, mom_g = _errors_by_id(case.m, got, case.p64)
+    pos_o, mom_o = _errors_by_id(case.m, case.p, case.p64)
+    for name, g, o in (("position", pos_g, pos_o), ("momentum", mom_g, mom_o)):
+        for q in (50, 99):
+            eg, eo = np.percentile(g, q), np.percentile(o, q)
+            print(f"{name} p{q}: GPU {eg:.3g}, FP32 oracle {eo:.3g}")
+            assert eg <= ERR_FACTOR * eo + ERR_FLOOR, f"{name} p{q}: {eg:.3g} vs {eo:.3g}"
+    for name, (eg, eo, dg, do) in _current_errors(case).items():
+        print(f"{name}: max {eg:.3g} (FP32 oracle {eo:.3g}), p99.9 {dg:.3g} ({do:.3g})")
+        assert eg <= ERR_FACTOR * eo + 1e-5, f"{name}: {eg:.3g} vs FP32 oracle {eo:.3g}"
+        assert dg <= ERR_FACTOR * do + 1e-6, f"{name}: p99.9 {dg:.3g} vs FP32 oracle {do:.3g}"
     case.close()
 
 
