@@ -282,3 +282,25 @@ def test_sort_particles_sorts_photons():
     for k in before:
         assert_bits(after[k], before[k][perm][:live], f"sorted photon {k}")
     case.close()
+
+
+def test_empty_passes_keep_the_reference_padding():
+    """A conversion pass over no photons and an emission pass with no
+    emitter still grow the counts by the reference's padding (50 particle
+    slots, one photon slot), on both sides."""
+    case = RadCase("cart2d", 41, n=3000, ph_n=0, ph_cap=1000)
+    c2, _ = case.pairs()
+    assert c2.marked == 0 and case.data.number == 3000 + 50
+    case.rp.gamma_thr = 1e9  # no particle is above it: the oracle's copy, the library's below
+    import ctypes as C
+    from aperture3_b200._lib import ApRadParams, check
+    rp = ApRadParams()
+    for name, _ in ApRadParams._fields_:
+        setattr(rp, name, getattr(case.rp, name) if hasattr(case.rp, name) else 0)
+    rp.first_photon_id, rp.first_particle_id = FIRST_PH, FIRST_PTC
+    check(case.env._lib.ap_set_rad_params(case.env.ctx, C.byref(rp)), "ap_set_rad_params")
+    case.emit_calls = case.pair_calls = 0
+    case.next_ph, case.next_ptc = FIRST_PH, FIRST_PTC
+    c, _ = case.emit()
+    assert c.marked == 0 and case.data.photon_number == 1
+    case.close()
