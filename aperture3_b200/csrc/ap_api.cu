@@ -175,6 +175,14 @@ int alloc_particle_state(Ctx *c, size_t cap) {
     if (cudaMalloc(&c->order[i], n * sizeof(uint32_t)) != cudaSuccess) return AP_ERR_NOMEM;
   if (cudaMalloc(&c->dir, n) != cudaSuccess) return AP_ERR_NOMEM;
   c->order_cap = n;
+  // sort_by_cell's cell starts, here rather than at the first sort, so that
+  // no allocation falls between the updates of a run
+  if (!c->cell_start) {
+    const size_t ncells =
+        (size_t)c->mesh.dims[0] * (size_t)c->mesh.dims[1] * (size_t)c->mesh.dims[2];
+    if (cudaMalloc(&c->cell_start, sizeof(uint32_t) * (ncells + 1)) != cudaSuccess)
+      return AP_ERR_NOMEM;
+  }
   return ensure_scratch(*c, n);
 }
 

@@ -106,25 +106,45 @@ __device__ __forceinline__ float mesh_pos(float lower, float delta, int n, int g
   return lower + delta * ((float)(n - guard) + x);
 }
 
-// beta_phi (field_solver_logsph.cu:16-20).
+// beta_phi (field_solver_logsph.cu:16-20); beta_phi_s takes sin(theta).
+__device__ __forceinline__ float beta_phi_s(float compactness, float omega, float r,
+                                            float sin_theta) {
+  return -0.4f * compactness * omega * sin_theta / (r * r);
+}
 __device__ __forceinline__ float beta_phi(float compactness, float omega, float r, float theta) {
-  return -0.4f * compactness * omega * sinf(theta) / (r * r);
+  return beta_phi_s(compactness, omega, r, sinf(theta));
 }
 
-// logsph2cart / cart2logsph (ptc_updater_logsph.cu:26-44).
-__device__ __forceinline__ void logsph2cart(float &v1, float &v2, float &v3, float x2, float x3) {
+// sinf(x) and cosf(x) (.x, .y) from one out-of-line copy. The fused
+// log-spherical kernel takes the sine and cosine of four angles per
+// particle; inlined, every copy carries the functions' full argument
+// reduction and the kernel's code grows past what the instruction cache
+// holds. The values are those of inline sinf / cosf.
+static __device__ __noinline__ float2 sin_cos_ool(float x) {
+  return make_float2(sinf(x), cosf(x));
+}
+
+// logsph2cart / cart2logsph (ptc_updater_logsph.cu:26-44); the _sc forms
+// take cos x2, sin x2, cos x3, sin x3.
+__device__ __forceinline__ void logsph2cart_sc(float &v1, float &v2, float &v3, float c2,
+                                               float s2, float c3, float s3) {
   const float v1n = v1, v2n = v2, v3n = v3;
-  const float c2 = cosf(x2), s2 = sinf(x2), c3 = cosf(x3), s3 = sinf(x3);
   v1 = v1n * s2 * c3 + v2n * c2 * c3 - v3n * s3;
   v2 = v1n * s2 * s3 + v2n * c2 * s3 + v3n * c3;
   v3 = v1n * c2 - v2n * s2;
 }
-__device__ __forceinline__ void cart2logsph(float &v1, float &v2, float &v3, float x2, float x3) {
+__device__ __forceinline__ void cart2logsph_sc(float &v1, float &v2, float &v3, float c2,
+                                               float s2, float c3, float s3) {
   const float v1n = v1, v2n = v2, v3n = v3;
-  const float c2 = cosf(x2), s2 = sinf(x2), c3 = cosf(x3), s3 = sinf(x3);
   v1 = v1n * s2 * c3 + v2n * s2 * s3 + v3n * c2;
   v2 = v1n * c2 * c3 + v2n * c2 * s3 - v3n * s2;
   v3 = -v1n * s3 + v2n * c3;
+}
+__device__ __forceinline__ void logsph2cart(float &v1, float &v2, float &v3, float x2, float x3) {
+  logsph2cart_sc(v1, v2, v3, cosf(x2), sinf(x2), cosf(x3), sinf(x3));
+}
+__device__ __forceinline__ void cart2logsph(float &v1, float &v2, float &v3, float x2, float x3) {
+  cart2logsph_sc(v1, v2, v3, cosf(x2), sinf(x2), cosf(x3), sinf(x3));
 }
 
 // sync_kill_perp (sync_cooling.cuh:59-86); B1..B3 are the pusher's scaled

@@ -136,7 +136,11 @@ __device__ __forceinline__ float pos1(const LsGeo &G, int n, float x) {
 }
 __device__ __forceinline__ float alpha_gr(float) { return 1.0f; }
 
-// compute_b_update_logsph (field_solver_logsph.cu:117-185).
+// compute_b_update_logsph (field_solver_logsph.cu:117-185). The three new
+// values are computed before any of them is stored: the arrays are distinct,
+// but the compiler cannot know that, and a store between two expressions
+// would make it reload the second one's inputs after the store instead of
+// issuing all loads up front.
 __global__ void k_ls_update_b(LsGeo G, LsFields F, LsCoef K, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -145,29 +149,37 @@ __global__ void k_ls_update_b(LsGeo G, LsFields F, LsCoef K, float dt) {
   const float r1 = expf(pos0(G, n1, 1.0f));
   const float r0 = expf(pos0(G, n1 - 1, 1.0f));
   const float r = expf(pos0(G, n1, 0.5f));
-  F.B1(n1, n2) += -dt *
-                  ((F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2) -
-                   (F.E3(n1, n2 - 1) - F.Eb3(n1, n2 - 1)) * alpha_gr(r1) * l3e(n1, n2 - 1)) /
-                  K.c[AP_COEF_A1B](n1, n2);
-  F.B2(n1, n2) += -dt *
-                  ((F.E3(n1 - 1, n2) - F.Eb3(n1 - 1, n2)) * alpha_gr(r0) * l3e(n1 - 1, n2) -
-                   (F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2)) /
-                  K.c[AP_COEF_A2B](n1, n2);
-  F.B3(n1, n2) +=
+  const float v1 =
+      F.B1(n1, n2) +
       -dt *
-      ((((F.E2(n1, n2) - F.Eb2(n1, n2)) * alpha_gr(r1) +
-         F.Bb1(n1, n2) * beta_phi(G.compactness, G.omega, r1, pos1(G, n2, 0.5f))) *
-            l2e(n1, n2) -
-        ((F.E2(n1 - 1, n2) - F.Eb2(n1 - 1, n2)) * alpha_gr(r0) +
-         F.Bb1(n1 - 1, n2) * beta_phi(G.compactness, G.omega, r0, pos1(G, n2, 0.5f))) *
-            l2e(n1 - 1, n2) +
-        ((F.E1(n1, n2 - 1) - F.Eb1(n1, n2 - 1)) * alpha_gr(r) -
-         F.Bb2(n1, n2 - 1) * beta_phi(G.compactness, G.omega, r, pos1(G, n2 - 1, 1.0f))) *
-            l1e(n1, n2 - 1) -
-        ((F.E1(n1, n2) - F.Eb1(n1, n2)) * alpha_gr(r) -
-         F.Bb2(n1, n2) * beta_phi(G.compactness, G.omega, r, pos1(G, n2, 1.0f))) *
-            l1e(n1, n2)) /
-       K.c[AP_COEF_A3B](n1, n2));
+          ((F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2) -
+           (F.E3(n1, n2 - 1) - F.Eb3(n1, n2 - 1)) * alpha_gr(r1) * l3e(n1, n2 - 1)) /
+          K.c[AP_COEF_A1B](n1, n2);
+  const float v2 =
+      F.B2(n1, n2) +
+      -dt *
+          ((F.E3(n1 - 1, n2) - F.Eb3(n1 - 1, n2)) * alpha_gr(r0) * l3e(n1 - 1, n2) -
+           (F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2)) /
+          K.c[AP_COEF_A2B](n1, n2);
+  const float v3 =
+      F.B3(n1, n2) +
+      -dt *
+          ((((F.E2(n1, n2) - F.Eb2(n1, n2)) * alpha_gr(r1) +
+             F.Bb1(n1, n2) * beta_phi(G.compactness, G.omega, r1, pos1(G, n2, 0.5f))) *
+                l2e(n1, n2) -
+            ((F.E2(n1 - 1, n2) - F.Eb2(n1 - 1, n2)) * alpha_gr(r0) +
+             F.Bb1(n1 - 1, n2) * beta_phi(G.compactness, G.omega, r0, pos1(G, n2, 0.5f))) *
+                l2e(n1 - 1, n2) +
+            ((F.E1(n1, n2 - 1) - F.Eb1(n1, n2 - 1)) * alpha_gr(r) -
+             F.Bb2(n1, n2 - 1) * beta_phi(G.compactness, G.omega, r, pos1(G, n2 - 1, 1.0f))) *
+                l1e(n1, n2 - 1) -
+            ((F.E1(n1, n2) - F.Eb1(n1, n2)) * alpha_gr(r) -
+             F.Bb2(n1, n2) * beta_phi(G.compactness, G.omega, r, pos1(G, n2, 1.0f))) *
+                l1e(n1, n2)) /
+           K.c[AP_COEF_A3B](n1, n2));
+  F.B1(n1, n2) = v1;
+  F.B2(n1, n2) = v2;
+  F.B3(n1, n2) = v3;
   // axis at theta = 0: written by the threads of the first bulk row; no
   // thread of this kernel reads B
   if (fabsf(pos1(G, n2, 1.0f) - G.d1) < 1.0e-5) {
@@ -176,7 +188,8 @@ __global__ void k_ls_update_b(LsGeo G, LsFields F, LsCoef K, float dt) {
   }
 }
 
-// compute_e_update_logsph (field_solver_logsph.cu:29-114).
+// compute_e_update_logsph (field_solver_logsph.cu:29-114); the new values
+// are computed before any is stored, as in k_ls_update_b.
 __global__ void k_ls_update_e(LsGeo G, LsFields F, LsCoef K, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -185,30 +198,36 @@ __global__ void k_ls_update_e(LsGeo G, LsFields F, LsCoef K, float dt) {
   const float r = expf(pos0(G, n1, 1.0f));
   const float r1 = expf(pos0(G, n1 + 1, 0.5f));
   const float r0 = expf(pos0(G, n1, 0.5f));
+  float v1;
   if (fabs((double)pos1(G, n2, 1.0f) - kPi) < 1.0e-5) {
-    F.E1(n1, n2) += dt * (-4.0f * (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) /
-                              (G.d1 * r0) -
-                          F.J1(n1, n2));
+    v1 = F.E1(n1, n2) + dt * (-4.0f * (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) /
+                                  (G.d1 * r0) -
+                              F.J1(n1, n2));
   } else {
-    F.E1(n1, n2) += dt * (((F.B3(n1, n2 + 1) - F.Bb3(n1, n2 + 1)) * alpha_gr(r0) *
-                               l3b(n1, n2 + 1) -
-                           (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2)) /
-                              K.c[AP_COEF_A1E](n1, n2) -
-                          F.J1(n1, n2));
+    v1 = F.E1(n1, n2) + dt * (((F.B3(n1, n2 + 1) - F.Bb3(n1, n2 + 1)) * alpha_gr(r0) *
+                                   l3b(n1, n2 + 1) -
+                               (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2)) /
+                                  K.c[AP_COEF_A1E](n1, n2) -
+                              F.J1(n1, n2));
   }
-  F.E2(n1, n2) += dt * (((F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2) -
-                         (F.B3(n1 + 1, n2) - F.Bb3(n1 + 1, n2)) * alpha_gr(r1) *
-                             l3b(n1 + 1, n2)) /
-                            K.c[AP_COEF_A2E](n1, n2) -
-                        F.J2(n1, n2));
-  F.E3(n1, n2) += dt * (((F.B2(n1 + 1, n2) - F.Bb2(n1 + 1, n2)) * alpha_gr(r1) *
-                             l2b(n1 + 1, n2) -
-                         (F.B2(n1, n2) - F.Bb2(n1, n2)) * alpha_gr(r0) * l2b(n1, n2) +
-                         (F.B1(n1, n2) - F.Bb1(n1, n2)) * alpha_gr(r) * l1b(n1, n2) -
-                         (F.B1(n1, n2 + 1) - F.Bb1(n1, n2 + 1)) * alpha_gr(r) *
-                             l1b(n1, n2 + 1)) /
-                            K.c[AP_COEF_A3E](n1, n2) -
-                        F.J3(n1, n2));
+  const float v2 =
+      F.E2(n1, n2) + dt * (((F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2) -
+                            (F.B3(n1 + 1, n2) - F.Bb3(n1 + 1, n2)) * alpha_gr(r1) *
+                                l3b(n1 + 1, n2)) /
+                               K.c[AP_COEF_A2E](n1, n2) -
+                           F.J2(n1, n2));
+  const float v3 =
+      F.E3(n1, n2) + dt * (((F.B2(n1 + 1, n2) - F.Bb2(n1 + 1, n2)) * alpha_gr(r1) *
+                                l2b(n1 + 1, n2) -
+                            (F.B2(n1, n2) - F.Bb2(n1, n2)) * alpha_gr(r0) * l2b(n1, n2) +
+                            (F.B1(n1, n2) - F.Bb1(n1, n2)) * alpha_gr(r) * l1b(n1, n2) -
+                            (F.B1(n1, n2 + 1) - F.Bb1(n1, n2 + 1)) * alpha_gr(r) *
+                                l1b(n1, n2 + 1)) /
+                               K.c[AP_COEF_A3E](n1, n2) -
+                           F.J3(n1, n2));
+  F.E1(n1, n2) = v1;
+  F.E2(n1, n2) = v2;
+  F.E3(n1, n2) = v3;
   // axis at theta = 0; these cells are read by no thread of this kernel
   if (fabsf(pos1(G, n2, 1.0f) - G.d1) < 1.0e-5) {
     const int a = G.g1 - 1;
@@ -219,32 +238,37 @@ __global__ void k_ls_update_e(LsGeo G, LsFields F, LsCoef K, float dt) {
   }
 }
 
-// compute_divs_logsph (field_solver_logsph.cu:188-250).
+// compute_divs_logsph (field_solver_logsph.cu:188-250); both values are
+// computed before either is stored, as in k_ls_update_b.
 __global__ void k_ls_divs(LsGeo G, LsFields F, LsCoef K) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0 || n2 >= G.n1 - G.g1) return;
   const Arr &A1e = K.c[AP_COEF_A1E], &A2e = K.c[AP_COEF_A2E];
   const Arr &A1b = K.c[AP_COEF_A1B], &A2b = K.c[AP_COEF_A2B], &dV = K.c[AP_COEF_DV];
-  if (pos0(G, n1, 1.0f) > G.d0) {
-    F.divE(n1, n2) = ((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
-                      (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2) +
-                      (F.E2(n1, n2 + 1) - F.Eb2(n1, n2 + 1)) * A2e(n1, n2 + 1) -
-                      (F.E2(n1, n2) - F.Eb2(n1, n2)) * A2e(n1, n2)) /
-                     (dV(n1, n2) * G.d0 * G.d1);
+  const bool has_e = pos0(G, n1, 1.0f) > G.d0;
+  float de = 0.0f;
+  if (has_e) {
     if (fabsf(pos1(G, n2, 1.0f) - G.size1 + G.lower1) < 1.0e-5) {
-      F.divE(n1, n2) =
-          (float)(((double)((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
-                            (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2)) -
-                   2.0 * (double)(F.E2(n1, n2) - F.Eb2(n1, n2)) * (double)A2e(n1, n2)) /
-                  (double)(dV(n1, n2) * G.d0 * G.d1));
+      de = (float)(((double)((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
+                             (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2)) -
+                    2.0 * (double)(F.E2(n1, n2) - F.Eb2(n1, n2)) * (double)A2e(n1, n2)) /
+                   (double)(dV(n1, n2) * G.d0 * G.d1));
+    } else {
+      de = ((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
+            (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2) +
+            (F.E2(n1, n2 + 1) - F.Eb2(n1, n2 + 1)) * A2e(n1, n2 + 1) -
+            (F.E2(n1, n2) - F.Eb2(n1, n2)) * A2e(n1, n2)) /
+           (dV(n1, n2) * G.d0 * G.d1);
     }
   }
-  F.divB(n1, n2) = ((F.B1(n1, n2) - F.Bb1(n1, n2)) * A1b(n1, n2) -
+  const float db = ((F.B1(n1, n2) - F.Bb1(n1, n2)) * A1b(n1, n2) -
                     (F.B1(n1 - 1, n2) - F.Bb1(n1 - 1, n2)) * A1b(n1 - 1, n2) +
                     (F.B2(n1, n2) - F.Bb2(n1, n2)) * A2b(n1, n2) -
                     (F.B2(n1, n2 - 1) - F.Bb2(n1, n2 - 1)) * A2b(n1, n2 - 1)) /
                    (dV(n1, n2) * G.d0 * G.d1);
+  if (has_e) F.divE(n1, n2) = de;
+  F.divB(n1, n2) = db;
   // the reference tests |pos| - delta here (not |pos - delta|)
   if (fabsf(pos1(G, n2, 1.0f)) - G.d1 < 1.0e-5) {
     const int a = G.g1 - 1;
@@ -277,6 +301,45 @@ __global__ void k_ls_bnd_radial(LsGeo G, LsFields F, float omega, int damping_le
     F.B3(i, j) = F.Bb3(i, j);
   }
   for (int i = 0; i < damping_length; ++i) {
+    const int n1 = G.n0 - damping_length + i;
+    const float q = (float)i / (float)damping_length;
+    const float lambda = 1.0f - damping_coef * (q * q);
+    F.E1(n1, j) = lambda * (F.E1(n1, j) - F.Eb1(n1, j)) + F.Eb1(n1, j);
+    F.E2(n1, j) = lambda * (F.E2(n1, j) - F.Eb2(n1, j)) + F.Eb2(n1, j);
+    F.E3(n1, j) = lambda * (F.E3(n1, j) - F.Eb3(n1, j)) + F.Eb3(n1, j);
+    F.B3(n1, j) = lambda * (F.B3(n1, j) - F.Bb3(n1, j)) + F.Bb3(n1, j);
+  }
+}
+
+// The same two boundaries with one thread per cell of the two bands of each
+// theta row: columns [0, g0) (stellar) and the last damping_length columns
+// (outflow). Every assignment of either loop reads and writes only its own
+// cell (and the background fields), so the cells are independent as long as
+// the bands do not overlap (n0 - damping_length >= g0, checked by the
+// launch). Consecutive threads take consecutive columns of a row, so a warp
+// reads and writes contiguous memory instead of 32 rows a pitch apart.
+__global__ void k_ls_bnd_radial_cells(LsGeo G, LsFields F, float omega, int damping_length,
+                                      float damping_coef) {
+  const int w = G.g0 + damping_length;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w * G.n1) return;
+  const int j = t / w, k = t - j * w;
+  if (k < G.g0) {
+    const int i = k;
+    const float theta_s = pos1(G, j, 1.0f);
+    const float theta = pos1(G, j, 0.5f);
+    const float r_s = expf(pos0(G, i, 1.0f));
+    const float r = expf(pos0(G, i, 0.5f));
+    const float omega_LT = 0.4f * omega * G.compactness;
+    F.B1(i, j) = F.Bb1(i, j);
+    F.E2(i, j) = -(omega - omega_LT) * sinf(theta) * F.Bb1(i, j) / alpha_gr(r_s) / r_s / r_s +
+                 F.Eb2(i, j);
+    F.E1(i, j) = (omega - omega_LT) * sinf(theta_s) * F.Bb2(i, j) / alpha_gr(r_s) / r / r +
+                 F.Eb1(i, j);
+    F.B2(i, j) = F.Bb2(i, j);
+    F.B3(i, j) = F.Bb3(i, j);
+  } else {
+    const int i = k - G.g0;
     const int n1 = G.n0 - damping_length + i;
     const float q = (float)i / (float)damping_length;
     const float lambda = 1.0f - damping_coef * (q * q);
@@ -659,8 +722,16 @@ cudaError_t launch_ls_inject(Ctx &c, int inj, float p1, float w, uint64_t seed, 
 cudaError_t launch_ls_field_boundary(Ctx &c, float omega) {
   const LsGeo G = make_ls_geo(c);
   const LsFields F = make_ls_fields(c);
-  k_ls_bnd_radial<<<(G.n1 + 127) / 128, 128, 0, c.stream>>>(G, F, omega, c.lsp.damping_length,
-                                                            c.lsp.damping_coef);
+  const int dl = c.lsp.damping_length;
+  if (dl >= 0 && G.n0 - dl >= G.g0) {
+    const int cells = (G.g0 + dl) * G.n1;
+    if (cells > 0)
+      k_ls_bnd_radial_cells<<<(cells + 255) / 256, 256, 0, c.stream>>>(G, F, omega, dl,
+                                                                       c.lsp.damping_coef);
+  } else {
+    k_ls_bnd_radial<<<(G.n1 + 127) / 128, 128, 0, c.stream>>>(G, F, omega, dl,
+                                                              c.lsp.damping_coef);
+  }
   k_ls_bnd_axis<<<(G.n0 + 127) / 128, 128, 0, c.stream>>>(G, F);
   c.launches += 2;
   return cudaGetLastError();

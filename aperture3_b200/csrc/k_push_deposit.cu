@@ -476,11 +476,12 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
             const float r1 = mesh_pos(P.m.lower[0], P.m.delta[0], c1, g0, x1);
             const float exp_r1 = expf(r1);
             const float r2 = mesh_pos(P.m.lower[1], P.m.delta[1], c2, g1, x2);
-            v3 = v3 - beta_phi(P.ls_compactness, P.ls_omega, exp_r1, r2);
-            float x = exp_r1 * sinf(r2) * cosf(x3);
-            float y = exp_r1 * sinf(r2) * sinf(x3);
-            float z = exp_r1 * cosf(r2);
-            logsph2cart(v1, v2, v3, r2, x3);
+            const float2 sc2 = sin_cos_ool(r2), sc3 = sin_cos_ool(x3);
+            v3 = v3 - beta_phi_s(P.ls_compactness, P.ls_omega, exp_r1, sc2.x);
+            float x = exp_r1 * sc2.x * sc3.y;
+            float y = exp_r1 * sc2.x * sc3.x;
+            float z = exp_r1 * sc2.y;
+            logsph2cart_sc(v1, v2, v3, sc2.y, sc2.x, sc3.y, sc3.x);
             x += 1.0f * v1 * P.dt;  // alpha_gr(r) = 1
             y += 1.0f * v2 * P.dt;
             z += 1.0f * v3 * P.dt;
@@ -489,10 +490,11 @@ __device__ __forceinline__ void push_deposit_tiles(const PushDepositParams &P0,
             const float exp_r1p = r1p;
             r1p = logf(r1p);
             const float r3p = atan2f(y, x);
-            cart2logsph(v1, v2, v3, r2p, r3p);
+            const float2 sp2 = sin_cos_ool(r2p), sp3 = sin_cos_ool(r3p);
+            cart2logsph_sc(v1, v2, v3, sp2.y, sp2.x, sp3.y, sp3.x);
             p1 = v1 * gamma;
             p2 = v2 * gamma;
-            p3 = (v3 + beta_phi(P.ls_compactness, P.ls_omega, exp_r1p, r2p)) * gamma;
+            p3 = (v3 + beta_phi_s(P.ls_compactness, P.ls_omega, exp_r1p, sp2.x)) * gamma;
             nx1 = x1 + (r1p - r1) / P.m.delta[0];
             nx2 = x2 + (r2p - r2) / P.m.delta[1];
             dc1 = (int)floorf(nx1);

@@ -58,7 +58,8 @@ def parse():
                     help="batched workload: keep every run's tile shape")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="box workload: skip the bounded runs of the other configurations")
+                    help="box workload: skip the bounded runs of the other configurations; "
+                         "logsph workload: skip the FP64 error run and the radiation passes")
     ap.add_argument("--cpu-budget", type=float, default=20.0,
                     help="seconds of CPU work for the cpu_baseline sample")
     ap.add_argument("--workload", default="box",
@@ -1058,7 +1059,7 @@ def run_logsph(args, emit=True, fp64_error=True):
                                 "also evaluates the reference's move in Cartesian space (sinf, "
                                 "cosf, expf, logf, acosf, atan2f) in the reference's order"}
     env.close()
-    if fp64_error:
+    if fp64_error and not args.no_extras:
         line["fp64_error_after_2000_steps"] = logsph_fp64_error()
         line["radiation"] = logsph_radiation(args)
     if emit:

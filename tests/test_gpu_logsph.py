@@ -230,9 +230,14 @@ def test_field_update(compactness):
     case.close()
 
 
-def test_field_boundary():
-    """Stellar surface, outflow damping and axis boundaries."""
-    case = LsCase((64, 32), 10, 8, compactness=0.3, damping_length=12, damping_coef=0.3)
+@pytest.mark.parametrize("damping_length", [12, 67])
+def test_field_boundary(damping_length):
+    """Stellar surface, outflow damping and axis boundaries. 12: the bands
+    of the stellar and the damped columns are apart (one thread per cell);
+    67 of the 68 columns: the damped band reaches into the stellar one and
+    each row is processed in the reference's order (stellar first)."""
+    case = LsCase((64, 32), 10, 8, compactness=0.3, damping_length=damping_length,
+                  damping_coef=0.3)
     case.step_fields(omega=0.07)
     g = case.data.fields_host()
     for key in ("E", "B"):
