@@ -101,6 +101,20 @@ __host__ __device__ constexpr int stag_y(int k) {
 // float arguments); these are the same functions, with their CUDA
 // accuracy, so only the transcendentals differ from an FP32 CPU run.
 
+// (t % n, t / n) of a flat cell index: one 32-bit division when t fits in
+// 32 bits (every grid of realistic size), else the 64-bit forms, which are
+// long instruction sequences that cost more than a cell's memory traffic.
+__device__ __forceinline__ void split_index(size_t t, int n, int &x, int &y) {
+  if (t <= 0xffffffffull) {
+    const unsigned tu = (unsigned)t, q = tu / (unsigned)n;
+    x = (int)(tu - q * (unsigned)n);
+    y = (int)q;
+  } else {
+    x = (int)(t % (size_t)n);
+    y = (int)(t / (size_t)n);
+  }
+}
+
 // Quadmesh::pos(i, n, pos_in_cell) (quadmesh.h:144-150).
 __device__ __forceinline__ float mesh_pos(float lower, float delta, int n, int guard, float x) {
   return lower + delta * ((float)(n - guard) + x);

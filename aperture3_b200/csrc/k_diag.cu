@@ -105,7 +105,10 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_fields(const DiagParams P
   double en = 0.0, mrho = 0.0, mres = 0.0, mj = 0.0;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
-    const int i = P.g0 + (int)(t % r0), j = g1 + (int)(t / r0);
+    int i, j;
+    split_index(t, r0, i, j);
+    i += P.g0;
+    j += g1;
     double s = 0.0;
     for (int k = 0; k < 3; ++k) {
       const double e = P.E[k].ptr[(size_t)j * P.E[k].pitch + i];
@@ -143,7 +146,8 @@ __global__ void __launch_bounds__(kDiagThreads) k_rho_snapshot(const ContParams 
   const size_t total = (size_t)P.n0 * P.n1;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % P.n0), j = (int)(t / P.n0);
+    int i, j;
+    split_index(t, P.n0, i, j);
     double rho = 0.0;
     for (int sp = 0; sp < P.num_species; ++sp)
       rho += P.Rho[sp].ptr[(size_t)j * P.Rho[sp].pitch + i];
@@ -165,7 +169,10 @@ __global__ void __launch_bounds__(kDiagThreads) k_continuity(const ContParams P)
   double mres = 0.0;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
-    const int i = P.g0 + (int)(t % r0), j = g1 + (int)(t / r0);
+    int i, j;
+    split_index(t, r0, i, j);
+    i += P.g0;
+    j += g1;
     double rho = 0.0;
     for (int sp = 0; sp < P.num_species; ++sp)
       rho += P.Rho[sp].ptr[(size_t)j * P.Rho[sp].pitch + i];

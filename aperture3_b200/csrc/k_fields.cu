@@ -10,6 +10,7 @@
 // produces -- without a separate pass.
 #include <cuda_runtime.h>
 
+#include "ap_device.cuh"
 #include "ap_internal.h"
 
 namespace apb {
@@ -268,8 +269,11 @@ __global__ void k_finalize(Geo G, const unsigned long long *__restrict__ acc, in
   const unsigned long long *a = acc + comp * acc_comp;
   const double inv = ldexp(1.0, -fmt->S);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
-       t += (size_t)gridDim.x * blockDim.x)
-    finalize_cell(G, a, acc_pitch, inv, out, (int)(t % G.n0), (int)(t / G.n0));
+       t += (size_t)gridDim.x * blockDim.x) {
+    int x, y;
+    split_index(t, G.n0, x, y);
+    finalize_cell(G, a, acc_pitch, inv, out, x, y);
+  }
 }
 
 Geo make_geo(const Ctx &c) {

@@ -136,47 +136,57 @@ __device__ __forceinline__ float pos1(const LsGeo &G, int n, float x) {
 }
 __device__ __forceinline__ float alpha_gr(float) { return 1.0f; }
 
-// compute_b_update_logsph (field_solver_logsph.cu:117-185). The three new
-// values are computed before any of them is stored: the arrays are distinct,
-// but the compiler cannot know that, and a store between two expressions
-// would make it reload the second one's inputs after the store instead of
-// issuing all loads up front.
+// compute_b_update_logsph (field_solver_logsph.cu:117-185). Every input is
+// loaded into a register before the first division or transcendental: the
+// slow paths of those sit behind branches, and global loads written inside
+// the expressions are not moved above a branch, so they would go out in
+// several dependent rounds. The expressions are the reference's, in its
+// order; the new values are stored once all three are computed.
 __global__ void k_ls_update_b(LsGeo G, LsFields F, LsCoef K, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0 || n2 >= G.n1 - G.g1) return;
   const Arr &l1e = K.c[AP_COEF_L1E], &l2e = K.c[AP_COEF_L2E], &l3e = K.c[AP_COEF_L3E];
+  const Arr &A1b = K.c[AP_COEF_A1B], &A2b = K.c[AP_COEF_A2B], &A3b = K.c[AP_COEF_A3B];
+  const float b1 = F.B1(n1, n2), b2 = F.B2(n1, n2), b3 = F.B3(n1, n2);
+  const float e1 = F.E1(n1, n2), eb1 = F.Eb1(n1, n2);
+  const float e1_jm = F.E1(n1, n2 - 1), eb1_jm = F.Eb1(n1, n2 - 1);
+  const float e2 = F.E2(n1, n2), eb2 = F.Eb2(n1, n2);
+  const float e2_im = F.E2(n1 - 1, n2), eb2_im = F.Eb2(n1 - 1, n2);
+  const float e3 = F.E3(n1, n2), eb3 = F.Eb3(n1, n2);
+  const float e3_jm = F.E3(n1, n2 - 1), eb3_jm = F.Eb3(n1, n2 - 1);
+  const float e3_im = F.E3(n1 - 1, n2), eb3_im = F.Eb3(n1 - 1, n2);
+  const float bb1 = F.Bb1(n1, n2), bb1_im = F.Bb1(n1 - 1, n2);
+  const float bb2 = F.Bb2(n1, n2), bb2_jm = F.Bb2(n1, n2 - 1);
+  const float l1 = l1e(n1, n2), l1_jm = l1e(n1, n2 - 1);
+  const float l2 = l2e(n1, n2), l2_im = l2e(n1 - 1, n2);
+  const float l3 = l3e(n1, n2), l3_jm = l3e(n1, n2 - 1), l3_im = l3e(n1 - 1, n2);
+  const float a1 = A1b(n1, n2), a2 = A2b(n1, n2), a3 = A3b(n1, n2);
   const float r1 = expf(pos0(G, n1, 1.0f));
   const float r0 = expf(pos0(G, n1 - 1, 1.0f));
   const float r = expf(pos0(G, n1, 0.5f));
-  const float v1 =
-      F.B1(n1, n2) +
-      -dt *
-          ((F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2) -
-           (F.E3(n1, n2 - 1) - F.Eb3(n1, n2 - 1)) * alpha_gr(r1) * l3e(n1, n2 - 1)) /
-          K.c[AP_COEF_A1B](n1, n2);
-  const float v2 =
-      F.B2(n1, n2) +
-      -dt *
-          ((F.E3(n1 - 1, n2) - F.Eb3(n1 - 1, n2)) * alpha_gr(r0) * l3e(n1 - 1, n2) -
-           (F.E3(n1, n2) - F.Eb3(n1, n2)) * alpha_gr(r1) * l3e(n1, n2)) /
-          K.c[AP_COEF_A2B](n1, n2);
+  const float v1 = b1 + -dt *
+                            ((e3 - eb3) * alpha_gr(r1) * l3 -
+                             (e3_jm - eb3_jm) * alpha_gr(r1) * l3_jm) /
+                            a1;
+  const float v2 = b2 + -dt *
+                            ((e3_im - eb3_im) * alpha_gr(r0) * l3_im -
+                             (e3 - eb3) * alpha_gr(r1) * l3) /
+                            a2;
   const float v3 =
-      F.B3(n1, n2) +
-      -dt *
-          ((((F.E2(n1, n2) - F.Eb2(n1, n2)) * alpha_gr(r1) +
-             F.Bb1(n1, n2) * beta_phi(G.compactness, G.omega, r1, pos1(G, n2, 0.5f))) *
-                l2e(n1, n2) -
-            ((F.E2(n1 - 1, n2) - F.Eb2(n1 - 1, n2)) * alpha_gr(r0) +
-             F.Bb1(n1 - 1, n2) * beta_phi(G.compactness, G.omega, r0, pos1(G, n2, 0.5f))) *
-                l2e(n1 - 1, n2) +
-            ((F.E1(n1, n2 - 1) - F.Eb1(n1, n2 - 1)) * alpha_gr(r) -
-             F.Bb2(n1, n2 - 1) * beta_phi(G.compactness, G.omega, r, pos1(G, n2 - 1, 1.0f))) *
-                l1e(n1, n2 - 1) -
-            ((F.E1(n1, n2) - F.Eb1(n1, n2)) * alpha_gr(r) -
-             F.Bb2(n1, n2) * beta_phi(G.compactness, G.omega, r, pos1(G, n2, 1.0f))) *
-                l1e(n1, n2)) /
-           K.c[AP_COEF_A3B](n1, n2));
+      b3 + -dt * ((((e2 - eb2) * alpha_gr(r1) +
+                    bb1 * beta_phi(G.compactness, G.omega, r1, pos1(G, n2, 0.5f))) *
+                       l2 -
+                   ((e2_im - eb2_im) * alpha_gr(r0) +
+                    bb1_im * beta_phi(G.compactness, G.omega, r0, pos1(G, n2, 0.5f))) *
+                       l2_im +
+                   ((e1_jm - eb1_jm) * alpha_gr(r) -
+                    bb2_jm * beta_phi(G.compactness, G.omega, r, pos1(G, n2 - 1, 1.0f))) *
+                       l1_jm -
+                   ((e1 - eb1) * alpha_gr(r) -
+                    bb2 * beta_phi(G.compactness, G.omega, r, pos1(G, n2, 1.0f))) *
+                       l1) /
+                  a3);
   F.B1(n1, n2) = v1;
   F.B2(n1, n2) = v2;
   F.B3(n1, n2) = v3;
@@ -188,43 +198,48 @@ __global__ void k_ls_update_b(LsGeo G, LsFields F, LsCoef K, float dt) {
   }
 }
 
-// compute_e_update_logsph (field_solver_logsph.cu:29-114); the new values
-// are computed before any is stored, as in k_ls_update_b.
+// compute_e_update_logsph (field_solver_logsph.cu:29-114), with the inputs
+// loaded first as in k_ls_update_b (both branches' inputs of E1).
 __global__ void k_ls_update_e(LsGeo G, LsFields F, LsCoef K, float dt) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0 || n2 >= G.n1 - G.g1) return;
   const Arr &l1b = K.c[AP_COEF_L1B], &l2b = K.c[AP_COEF_L2B], &l3b = K.c[AP_COEF_L3B];
+  const Arr &A1e = K.c[AP_COEF_A1E], &A2e = K.c[AP_COEF_A2E], &A3e = K.c[AP_COEF_A3E];
+  const float e1 = F.E1(n1, n2), e2 = F.E2(n1, n2), e3 = F.E3(n1, n2);
+  const float j1 = F.J1(n1, n2), j2 = F.J2(n1, n2), j3 = F.J3(n1, n2);
+  const float b1 = F.B1(n1, n2), bb1 = F.Bb1(n1, n2);
+  const float b1_jp = F.B1(n1, n2 + 1), bb1_jp = F.Bb1(n1, n2 + 1);
+  const float b2 = F.B2(n1, n2), bb2 = F.Bb2(n1, n2);
+  const float b2_ip = F.B2(n1 + 1, n2), bb2_ip = F.Bb2(n1 + 1, n2);
+  const float b3 = F.B3(n1, n2), bb3 = F.Bb3(n1, n2);
+  const float b3_jp = F.B3(n1, n2 + 1), bb3_jp = F.Bb3(n1, n2 + 1);
+  const float b3_ip = F.B3(n1 + 1, n2), bb3_ip = F.Bb3(n1 + 1, n2);
+  const float l1 = l1b(n1, n2), l1_jp = l1b(n1, n2 + 1);
+  const float l2 = l2b(n1, n2), l2_ip = l2b(n1 + 1, n2);
+  const float l3 = l3b(n1, n2), l3_jp = l3b(n1, n2 + 1), l3_ip = l3b(n1 + 1, n2);
+  const float a1 = A1e(n1, n2), a2 = A2e(n1, n2), a3 = A3e(n1, n2);
   const float r = expf(pos0(G, n1, 1.0f));
   const float r1 = expf(pos0(G, n1 + 1, 0.5f));
   const float r0 = expf(pos0(G, n1, 0.5f));
   float v1;
   if (fabs((double)pos1(G, n2, 1.0f) - kPi) < 1.0e-5) {
-    v1 = F.E1(n1, n2) + dt * (-4.0f * (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) /
-                                  (G.d1 * r0) -
-                              F.J1(n1, n2));
+    v1 = e1 + dt * (-4.0f * (b3 - bb3) * alpha_gr(r0) / (G.d1 * r0) - j1);
   } else {
-    v1 = F.E1(n1, n2) + dt * (((F.B3(n1, n2 + 1) - F.Bb3(n1, n2 + 1)) * alpha_gr(r0) *
-                                   l3b(n1, n2 + 1) -
-                               (F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2)) /
-                                  K.c[AP_COEF_A1E](n1, n2) -
-                              F.J1(n1, n2));
+    v1 = e1 + dt * (((b3_jp - bb3_jp) * alpha_gr(r0) * l3_jp - (b3 - bb3) * alpha_gr(r0) * l3) /
+                        a1 -
+                    j1);
   }
   const float v2 =
-      F.E2(n1, n2) + dt * (((F.B3(n1, n2) - F.Bb3(n1, n2)) * alpha_gr(r0) * l3b(n1, n2) -
-                            (F.B3(n1 + 1, n2) - F.Bb3(n1 + 1, n2)) * alpha_gr(r1) *
-                                l3b(n1 + 1, n2)) /
-                               K.c[AP_COEF_A2E](n1, n2) -
-                           F.J2(n1, n2));
-  const float v3 =
-      F.E3(n1, n2) + dt * (((F.B2(n1 + 1, n2) - F.Bb2(n1 + 1, n2)) * alpha_gr(r1) *
-                                l2b(n1 + 1, n2) -
-                            (F.B2(n1, n2) - F.Bb2(n1, n2)) * alpha_gr(r0) * l2b(n1, n2) +
-                            (F.B1(n1, n2) - F.Bb1(n1, n2)) * alpha_gr(r) * l1b(n1, n2) -
-                            (F.B1(n1, n2 + 1) - F.Bb1(n1, n2 + 1)) * alpha_gr(r) *
-                                l1b(n1, n2 + 1)) /
-                               K.c[AP_COEF_A3E](n1, n2) -
-                           F.J3(n1, n2));
+      e2 + dt * (((b3 - bb3) * alpha_gr(r0) * l3 - (b3_ip - bb3_ip) * alpha_gr(r1) * l3_ip) /
+                     a2 -
+                 j2);
+  const float v3 = e3 + dt * (((b2_ip - bb2_ip) * alpha_gr(r1) * l2_ip -
+                               (b2 - bb2) * alpha_gr(r0) * l2 +
+                               (b1 - bb1) * alpha_gr(r) * l1 -
+                               (b1_jp - bb1_jp) * alpha_gr(r) * l1_jp) /
+                                  a3 -
+                              j3);
   F.E1(n1, n2) = v1;
   F.E2(n1, n2) = v2;
   F.E3(n1, n2) = v3;
@@ -238,35 +253,43 @@ __global__ void k_ls_update_e(LsGeo G, LsFields F, LsCoef K, float dt) {
   }
 }
 
-// compute_divs_logsph (field_solver_logsph.cu:188-250); both values are
-// computed before either is stored, as in k_ls_update_b.
+// compute_divs_logsph (field_solver_logsph.cu:188-250), with the inputs
+// loaded first as in k_ls_update_b.
 __global__ void k_ls_divs(LsGeo G, LsFields F, LsCoef K) {
   const int n1 = G.g0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int n2 = G.g1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (n1 >= G.n0 - G.g0 || n2 >= G.n1 - G.g1) return;
   const Arr &A1e = K.c[AP_COEF_A1E], &A2e = K.c[AP_COEF_A2E];
   const Arr &A1b = K.c[AP_COEF_A1B], &A2b = K.c[AP_COEF_A2B], &dV = K.c[AP_COEF_DV];
+  const float e1 = F.E1(n1, n2), eb1 = F.Eb1(n1, n2);
+  const float e1_ip = F.E1(n1 + 1, n2), eb1_ip = F.Eb1(n1 + 1, n2);
+  const float e2 = F.E2(n1, n2), eb2 = F.Eb2(n1, n2);
+  const float e2_jp = F.E2(n1, n2 + 1), eb2_jp = F.Eb2(n1, n2 + 1);
+  const float b1 = F.B1(n1, n2), bb1 = F.Bb1(n1, n2);
+  const float b1_im = F.B1(n1 - 1, n2), bb1_im = F.Bb1(n1 - 1, n2);
+  const float b2 = F.B2(n1, n2), bb2 = F.Bb2(n1, n2);
+  const float b2_jm = F.B2(n1, n2 - 1), bb2_jm = F.Bb2(n1, n2 - 1);
+  const float a1e = A1e(n1, n2), a1e_ip = A1e(n1 + 1, n2);
+  const float a2e = A2e(n1, n2), a2e_jp = A2e(n1, n2 + 1);
+  const float a1b = A1b(n1, n2), a1b_im = A1b(n1 - 1, n2);
+  const float a2b = A2b(n1, n2), a2b_jm = A2b(n1, n2 - 1);
+  const float dv = dV(n1, n2);
   const bool has_e = pos0(G, n1, 1.0f) > G.d0;
   float de = 0.0f;
   if (has_e) {
     if (fabsf(pos1(G, n2, 1.0f) - G.size1 + G.lower1) < 1.0e-5) {
-      de = (float)(((double)((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
-                             (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2)) -
-                    2.0 * (double)(F.E2(n1, n2) - F.Eb2(n1, n2)) * (double)A2e(n1, n2)) /
-                   (double)(dV(n1, n2) * G.d0 * G.d1));
+      de = (float)(((double)((e1_ip - eb1_ip) * a1e_ip - (e1 - eb1) * a1e) -
+                    2.0 * (double)(e2 - eb2) * (double)a2e) /
+                   (double)(dv * G.d0 * G.d1));
     } else {
-      de = ((F.E1(n1 + 1, n2) - F.Eb1(n1 + 1, n2)) * A1e(n1 + 1, n2) -
-            (F.E1(n1, n2) - F.Eb1(n1, n2)) * A1e(n1, n2) +
-            (F.E2(n1, n2 + 1) - F.Eb2(n1, n2 + 1)) * A2e(n1, n2 + 1) -
-            (F.E2(n1, n2) - F.Eb2(n1, n2)) * A2e(n1, n2)) /
-           (dV(n1, n2) * G.d0 * G.d1);
+      de = ((e1_ip - eb1_ip) * a1e_ip - (e1 - eb1) * a1e + (e2_jp - eb2_jp) * a2e_jp -
+            (e2 - eb2) * a2e) /
+           (dv * G.d0 * G.d1);
     }
   }
-  const float db = ((F.B1(n1, n2) - F.Bb1(n1, n2)) * A1b(n1, n2) -
-                    (F.B1(n1 - 1, n2) - F.Bb1(n1 - 1, n2)) * A1b(n1 - 1, n2) +
-                    (F.B2(n1, n2) - F.Bb2(n1, n2)) * A2b(n1, n2) -
-                    (F.B2(n1, n2 - 1) - F.Bb2(n1, n2 - 1)) * A2b(n1, n2 - 1)) /
-                   (dV(n1, n2) * G.d0 * G.d1);
+  const float db =
+      ((b1 - bb1) * a1b - (b1_im - bb1_im) * a1b_im + (b2 - bb2) * a2b - (b2_jm - bb2_jm) * a2b_jm) /
+      (dv * G.d0 * G.d1);
   if (has_e) F.divE(n1, n2) = de;
   F.divB(n1, n2) = db;
   // the reference tests |pos| - delta here (not |pos - delta|)
@@ -380,6 +403,8 @@ struct LsOut {
   Arr a[3 + AP_MAX_SPECIES];
 };
 
+constexpr int kFinU = 4;  // cells per thread and loop pass, loads issued together
+
 __global__ void k_ls_finalize(LsGeo G, const unsigned long long *__restrict__ acc,
                               size_t acc_comp, const FixedFmt *fmt, int ncomp, int do_rho,
                               int zero_axis, float w, LsOut out, Arr A1e, Arr A2e, Arr dV) {
@@ -389,21 +414,42 @@ __global__ void k_ls_finalize(LsGeo G, const unsigned long long *__restrict__ ac
   const unsigned long long *a = acc + comp * acc_comp;
   const double inv = ldexp(1.0, -fmt->S);
   const bool summed = comp < 3 || do_rho;
+  const Arr cA = comp == 0 ? A1e : comp == 1 ? A2e : dV;  // unused for J3
+  const bool has_coef = comp != 2;
   const size_t total = (size_t)G.n0 * G.n1;
   const int jl = G.n1 - G.g1;
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
-       t += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(t % G.n0), y = (int)(t / G.n0);
-    float v = summed ? (float)((double)(long long)a[t] * inv) : 0.0f;
-    if (comp == 0)
-      v *= w / A1e(x, y);
-    else if (comp == 1)
-      v *= w / A2e(x, y);
-    else if (comp == 2) {
-      if (zero_axis && (y == G.g1 - 1 || y == G.g1 || y == jl - 1 || y == jl)) v = 0.0f;
-    } else
-      v /= dV(x, y);
-    o(x, y) = v;
+  const size_t stride = (size_t)gridDim.x * blockDim.x * kFinU;
+  for (size_t t0 = (size_t)blockIdx.x * blockDim.x * kFinU + threadIdx.x; t0 < total;
+       t0 += stride) {
+    long long raw[kFinU];
+    float cf[kFinU];
+    int xs[kFinU], ys[kFinU];
+#pragma unroll
+    for (int k = 0; k < kFinU; ++k) {
+      const size_t t = t0 + (size_t)k * blockDim.x;
+      raw[k] = 0;
+      cf[k] = 1.0f;
+      xs[k] = ys[k] = 0;
+      if (t < total) {
+        split_index(t, G.n0, xs[k], ys[k]);
+        if (summed) raw[k] = (long long)a[t];
+        if (has_coef) cf[k] = cA(xs[k], ys[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kFinU; ++k) {
+      const size_t t = t0 + (size_t)k * blockDim.x;
+      if (t >= total) break;
+      const int x = xs[k], y = ys[k];
+      float v = summed ? (float)((double)raw[k] * inv) : 0.0f;
+      if (comp == 0 || comp == 1)
+        v *= w / cf[k];
+      else if (comp == 2) {
+        if (zero_axis && (y == G.g1 - 1 || y == G.g1 || y == jl - 1 || y == jl)) v = 0.0f;
+      } else
+        v /= cf[k];
+      o(x, y) = v;
+    }
   }
 }
 
@@ -543,8 +589,8 @@ cudaError_t launch_ls_finalize(Ctx &c, float dt, bool do_rho, bool zero_axis) {
   volatile float d01 = c.mesh.delta[0] * c.mesh.delta[1];
   const float w = d01 / dt;
   const size_t total = (size_t)G.n0 * G.n1;
-  int gx = (int)((total + 255) / 256);
-  if (gx > c.num_sms * 4) gx = c.num_sms * 4;
+  int gx = (int)((total + 256 * kFinU - 1) / (256 * kFinU));
+  if (gx > c.num_sms * 8) gx = c.num_sms * 8;
   dim3 grid(gx, ncomp);
   k_ls_finalize<<<grid, 256, 0, c.stream>>>(G, c.acc, c.acc_comp, c.fx_used, ncomp,
                                             do_rho ? 1 : 0, zero_axis ? 1 : 0, w, out,

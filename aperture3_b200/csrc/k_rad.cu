@@ -517,10 +517,12 @@ __global__ void k_rad_move_logsph(MeshK m, PhK ph, size_t num, float dt, float r
       continue;
     }
     const float r2 = mpos(m, 1, c2, old_x2);
-    float x = exp_r1 * sinf(r2) * cosf(old_x3);
-    float y = exp_r1 * sinf(r2) * sinf(old_x3);
-    float z = exp_r1 * cosf(r2);
-    logsph2cart(v1, v2, v3, r2, old_x3);
+    // sines and cosines from one out-of-line copy, as in the particle move
+    const float2 sc2 = sin_cos_ool(r2), sc3 = sin_cos_ool(old_x3);
+    float x = exp_r1 * sc2.x * sc3.y;
+    float y = exp_r1 * sc2.x * sc3.x;
+    float z = exp_r1 * sc2.y;
+    logsph2cart_sc(v1, v2, v3, sc2.y, sc2.x, sc3.y, sc3.x);
     x += v1 * dt;
     y += v2 * dt;
     z += v3 * dt;
@@ -528,7 +530,8 @@ __global__ void k_rad_move_logsph(MeshK m, PhK ph, size_t num, float dt, float r
     const float r2p = acosf(z / r1p);
     r1p = logf(r1p);
     const float r3p = atan2f(y, x);
-    cart2logsph(v1, v2, v3, r2p, r3p);
+    const float2 sp2 = sin_cos_ool(r2p), sp3 = sin_cos_ool(r3p);
+    cart2logsph_sc(v1, v2, v3, sp2.y, sp2.x, sp3.y, sp3.x);
     ph.p1[idx] = v1 * E;
     ph.p2[idx] = v2 * E;
     ph.p3[idx] = v3 * E;
