@@ -143,14 +143,22 @@ class ApRadParams(C.Structure):
                 ("r_cutoff", C.c_float), ("track_percent", C.c_float), ("e_curv", C.c_float),
                 ("l_curv", C.c_float), ("BQ", C.c_float), ("omega", C.c_float),
                 ("seed", C.c_uint64), ("first_photon_id", C.c_uint64),
-                ("first_particle_id", C.c_uint64)]
+                ("first_particle_id", C.c_uint64), ("e_min", C.c_float),
+                ("ic_path", C.c_float), ("n_gamma", C.c_int), ("n_ep", C.c_int)]
+
+
+class ApSpectrum(C.Structure):
+    """ap_spectrum: a background photon spectrum (AP_SPEC_*)."""
+    _fields_ = [("kind", C.c_int), ("p", C.c_float * 5)]
 
 
 class ApRadCounts(C.Structure):
     _fields_ = [("marked", C.c_uint64), ("written", C.c_uint64), ("dropped", C.c_uint64)]
 
 
-RAD_DEFAULT, RAD_PULSAR = 0, 1
+RAD_DEFAULT, RAD_PULSAR, RAD_GR1D = 0, 1, 2
+SPEC_POWER_LAW_HARD, SPEC_POWER_LAW_SOFT, SPEC_BROKEN_POWER_LAW = 0, 1, 2
+SPEC_BLACK_BODY, SPEC_MONO_ENERGETIC = 3, 4
 
 COEF_NAMES = ("l1_e", "l2_e", "l3_e", "l1_b", "l2_b", "l3_b",
               "A1_e", "A2_e", "A3_e", "A1_b", "A2_b", "A3_b", "dV")
@@ -232,6 +240,8 @@ SIGNATURES = {
     "ap_emit_photons": (_i, [_vp, ApArray, C.POINTER(ApRadCounts)]),
     "ap_produce_pairs": (_i, [_vp, ApArray, C.POINTER(ApRadCounts)]),
     "ap_move_photons": (_i, [_vp, C.c_double]),
+    "ap_ic_init": (_i, [_vp, C.POINTER(ApSpectrum), C.c_double, C.c_double, C.c_double, _i, _i]),
+    "ap_ic_tables": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ap_update_particles_1d_noalloc": (_i, [C.POINTER(ApMesh), C.POINTER(ApParams),
                                             C.POINTER(ApParticles), C.c_size_t,
                                             C.POINTER(ApFields), C.c_double, C.c_uint32, _vp]),

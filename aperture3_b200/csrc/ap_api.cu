@@ -327,6 +327,7 @@ AP_API int ap_ctx_destroy(ap_ctx *c) {
   cudaFree(c->diag_dev);
   cudaFree(c->rho_prev);
   rad_free(*c);
+  ic_free(*c);
   if (c->status_host) cudaFreeHost(c->status_host);
   if (c->diag_host) cudaFreeHost(c->diag_host);
   for (int i = 0; i < c->ev_cap; ++i) {
@@ -543,7 +544,11 @@ int update_particles_gap(Ctx *c, double dt, uint32_t step) {
 // ptc_updater_1dgr::update_particles (ptc_updater_1dgr.cu:418-473).
 int update_particles_gr(Ctx *c, double dt, uint32_t step) {
   const ap_params &pr = c->params;
-  if (c->number == 0) return finish(c);  // nothing at all without particles (:422)
+  if (c->number == 0) {
+    // without particles nothing but the photons moves (:422, :492-499)
+    if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt, step));
+    return finish(c);
+  }
   const int ncomp = 3 + pr.num_species;
   const int n = c->mesh.dims[0];
   const int bl = !pr.periodic[0], bu = !pr.periodic[0];  // is_boundary(0), (1)
@@ -620,6 +625,8 @@ int update_particles_gr(Ctx *c, double dt, uint32_t step) {
   }
   c->rho_is_zero = false;
   phase_end(c, ph);
+  // the photons after the particles (:492-499)
+  if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt, step));
   if (!c->sync) return AP_OK;
   return check_status(c);  // AP_ERR_MOVED_FAR
 }
@@ -894,7 +901,7 @@ AP_API int ap_update_particles(ap_ctx *c, double dt, uint32_t step) {
   AP_TRY_ST(update_complete(c, dt, step, has_work));
   // photons move after the particles (ptc_updater.cu:814-833,
   // ptc_updater_logsph.cu:793-803)
-  if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt));
+  if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt, step));
   if (!c->sync) return AP_OK;
   return check_status(c);
 }
@@ -1248,7 +1255,7 @@ AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitte
 
 AP_API int ap_bind_photons(ap_ctx *c, const ap_photons *ph, size_t number, size_t capacity) {
   if (!c || !ph) return AP_ERR_INVALID;
-  if (c->coord != 0 && c->coord != 1) return fail(c, AP_ERR_UNSUPPORTED);
+  if (c->coord != 0 && c->coord != 1 && c->coord != 3) return fail(c, AP_ERR_UNSUPPORTED);
   if (number > capacity || capacity >= (size_t)UINT32_MAX) return fail(c, AP_ERR_CAPACITY);
   if (!ph->x1 || !ph->x2 || !ph->x3 || !ph->p1 || !ph->p2 || !ph->p3 || !ph->E ||
       !ph->weight || !ph->path_left || !ph->cell || !ph->id || !ph->flag)
@@ -1268,16 +1275,68 @@ AP_API int ap_get_photon_number(const ap_ctx *c, size_t *n) {
 
 AP_API int ap_set_rad_params(ap_ctx *c, const ap_rad_params *rp) {
   if (!c || !rp) return AP_ERR_INVALID;
-  if (rp->model != AP_RAD_DEFAULT && rp->model != AP_RAD_PULSAR) return fail(c, AP_ERR_INVALID);
+  if (rp->model != AP_RAD_DEFAULT && rp->model != AP_RAD_PULSAR && rp->model != AP_RAD_GR1D)
+    return fail(c, AP_ERR_INVALID);
   // the pulsar lab's functions read (ln r, theta) positions and Rho[0], Rho[1]
   if (rp->model == AP_RAD_PULSAR && (c->coord != 1 || c->params.num_species < 2))
     return fail(c, AP_ERR_UNSUPPORTED);
-  if (c->coord != 0 && c->coord != 1) return fail(c, AP_ERR_UNSUPPORTED);
+  // the 1D GR lab's read Grid_1dGR's arrays; its photons move with the GR
+  // mover, the others' with the Cartesian or log-spherical one
+  if ((rp->model == AP_RAD_GR1D) != (c->coord == 3)) return fail(c, AP_ERR_UNSUPPORTED);
+  if (c->coord != 0 && c->coord != 1 && c->coord != 3) return fail(c, AP_ERR_UNSUPPORTED);
+  if (rp->model == AP_RAD_GR1D) {
+    // user_rt_init (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh:
+    // 191-203): broken_power_law(1.25, 1.1, e_min, 1e-10, 0.1) over
+    // [emin(), emax()] with n0 = 1.5e24 / ic_path
+    if (!(rp->ic_path > 0.0f) || !(rp->e_min > 0.0f)) return fail(c, AP_ERR_INVALID);
+    ap_spectrum sp{};
+    sp.kind = AP_SPEC_BROKEN_POWER_LAW;
+    sp.p[0] = 1.25f;
+    sp.p[1] = 1.1f;
+    sp.p[2] = rp->e_min;
+    sp.p[3] = 1.0e-10f;
+    sp.p[4] = 0.1f;
+    const double n0 = 1.50e24 / rp->ic_path;
+    const bool same = c->ic_ready && c->ic_n_gamma == rp->n_gamma && c->ic_n_ep == rp->n_ep &&
+                      std::memcmp(&c->ic_spec, &sp, sizeof(sp)) == 0 && c->ic_n0 == n0 &&
+                      c->ic_emin == (double)sp.p[3] && c->ic_emax == (double)sp.p[4];
+    if (!same) AP_TRY_ST(ic_init(*c, sp, sp.p[3], sp.p[4], n0, rp->n_gamma, rp->n_ep));
+  }
   c->rad = *rp;
   c->rad_on = true;
   c->rad_emit_calls = c->rad_pair_calls = 0;
   c->rad_next_photon_id = rp->first_photon_id;
   c->rad_next_ptc_id = rp->first_particle_id;
+  return AP_OK;
+}
+
+AP_API int ap_ic_init(ap_ctx *c, const ap_spectrum *sp, double emin, double emax, double n0,
+                      int n_gamma, int n_ep) {
+  if (!c || !sp || sp->kind < AP_SPEC_POWER_LAW_HARD || sp->kind > AP_SPEC_MONO_ENERGETIC ||
+      !(emin > 0.0) || !(emax > emin))
+    return AP_ERR_INVALID;
+  AP_TRY_ST(ic_init(*c, *sp, emin, emax, n0, n_gamma, n_ep));
+  return finish(c);
+}
+
+AP_API int ap_ic_tables(ap_ctx *c, float *ic_rate, float *gg_rate, float *gammas, float *dNde,
+                        float *dNde_thomson, float *steps) {
+  if (!c || !c->ic_ready) return AP_ERR_INVALID;
+  const size_t ng = (size_t)c->ic_n_gamma, ne = (size_t)c->ic_n_ep;
+  const float *src[5] = {c->ic_buf, c->ic_buf + ng, c->ic_buf + 2 * ng, c->ic_buf + 3 * ng,
+                         c->ic_buf + 3 * ng + ng * ne};
+  float *dst[5] = {ic_rate, gg_rate, gammas, dNde, dNde_thomson};
+  const size_t len[5] = {ng, ng, ng, ng * ne, ng * ne};
+  for (int k = 0; k < 5; ++k)
+    if (dst[k])
+      AP_TRY(cudaMemcpyAsync(dst[k], src[k], len[k] * sizeof(float), cudaMemcpyDeviceToHost,
+                             c->stream));
+  AP_TRY(cudaStreamSynchronize(c->stream));
+  if (steps) {
+    steps[0] = c->ic_dep;
+    steps[1] = c->ic_dg;
+    steps[2] = c->ic_dlep;
+  }
   return AP_OK;
 }
 
@@ -1312,7 +1371,7 @@ AP_API int ap_produce_pairs(ap_ctx *c, ap_array produced, ap_rad_counts *out) {
 
 AP_API int ap_move_photons(ap_ctx *c, double dt) {
   if (!c || !c->ph_bound) return AP_ERR_INVALID;
-  AP_TRY_ST(rad_move_photons(*c, (float)dt));
+  AP_TRY_ST(rad_move_photons(*c, (float)dt, 0));
   return finish(c);
 }
 

@@ -288,6 +288,13 @@ struct Ctx {
   uint32_t *rad_chunks = nullptr;  // per-chunk counts, offsets, then the total
   size_t rad_chunks_cap = 0;
   uint32_t *rad_total_host = nullptr;  // pinned: marked count of the last pass
+  // inverse-Compton tables (ap_ic_init; k_ic.cu), device arrays
+  float *ic_buf = nullptr;  // ic_rate, gg_rate, gammas, dNde, dNde_thomson
+  int ic_n_gamma = 0, ic_n_ep = 0;
+  float ic_dep = 0.0f, ic_dg = 0.0f, ic_dlep = 0.0f;
+  bool ic_ready = false;
+  ap_spectrum ic_spec{};     // what the tables were built for
+  double ic_emin = 0.0, ic_emax = 0.0, ic_n0 = 0.0;
 
   // per-phase event timing (ap_set_profiling)
   bool profiling = false;
@@ -354,10 +361,14 @@ cudaError_t launch_continuity(Ctx &c, double *out);
 // photons and pair production (k_rad.cu): the photon move of an update, and
 // the emit / produce passes; *marked receives the emitters of the pass
 // (waits for the stream).
-int rad_move_photons(Ctx &c, float dt);
+int rad_move_photons(Ctx &c, float dt, uint32_t step);
 int rad_emit_photons(Ctx &c, ap_array produced, ap_rad_counts *out);
 int rad_produce_pairs(Ctx &c, ap_array produced, ap_rad_counts *out);
 void rad_free(Ctx &c);
+// inverse_compton (k_ic.cu): builds the tables on the device; frees them
+int ic_init(Ctx &c, const ap_spectrum &s, double emin, double emax, double n0, int n_gamma,
+            int n_ep);
+void ic_free(Ctx &c);
 
 // pair injection (k_pairs.cu): enqueue mark / scan / append on the device
 // count (no host synchronisation); refresh_number reads the device state

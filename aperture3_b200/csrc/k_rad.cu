@@ -1,7 +1,7 @@
 // Photons and pair production: the photon movers of the particle updaters
-// and radiative_transfer's emit_photons / produce_pairs with the default or
-// the pulsar lab's user radiative functions (semantics in aperture_b200.h,
-// ap_rad_params). Each pass is three launches in slot order, so its result
+// and radiative_transfer's emit_photons / produce_pairs with the default,
+// the pulsar lab's or the 1D GR lab's user radiative functions (semantics
+// in aperture_b200.h, ap_rad_params). Each pass is three launches in slot order, so its result
 // does not depend on scheduling:
 //   1. mark:   per slot, the model's check (a Philox draw where the model
 //              draws one); per-chunk counts; per-cell produced weights,
@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "ap_device.cuh"
+#include "ap_ic.cuh"
 #include "ap_internal.h"
 
 namespace apb {
@@ -46,6 +47,10 @@ struct RadK {
   FieldArr B[3];
   FieldArr Rho[2];
   FieldArr produced;  // ptr null: not accumulated
+  // 1D GR model: Grid_1dGR's per-cell arrays, spin, omega, IC tables
+  const float *alpha, *D1, *D2, *D3, *B3B1, *grr, *gff, *beta_phi;
+  float a, gr_omega;
+  IcK ic;
 };
 
 // The four uniforms in (0, 1] of one particle (tag 1) or photon (tag 2):
@@ -111,11 +116,101 @@ __device__ float rho_c(float r, float theta) {
                  (double)(3.0f * s * (1.0f + c2)));
 }
 
+// ---- The 1D GR lab's functions (labs/1dgr/src/cuda/radiation/
+// user_radiative_functions.cuh:19-189). A metric array at x1 of cell c is
+// interpolated between c - 1 and c. Draws: u0 the emission / conversion
+// test, u1 the photon energy.
+__device__ __forceinline__ float gr_at(const float *a, uint32_t c, float x1) {
+  return a[c] * x1 + a[c - 1] * (1.0f - x1);
+}
+__device__ __forceinline__ float sgnf(float v) { return (float)((0.0f < v) - (v < 0.0f)); }
+
+// Boyer-Lindquist r of the tortoise coordinate xi (the division in double
+// as the reference writes it).
+__device__ __forceinline__ float gr_r(float xi, float a) {
+  const float rp = 1.0f + sqrtf(1.0f - a * a);
+  const float rm = 1.0f - sqrtf(1.0f - a * a);
+  const float exp_xi = expf(xi * (rp - rm));
+  return (float)((rp - rm * exp_xi) / (1.0 - exp_xi));
+}
+
+__device__ bool check_emit_gr(const RadK &K, const PtcK &p, size_t tid, uint32_t cell,
+                              const float u[4]) {
+  const float alpha = gr_at(K.alpha, cell, p.x1[tid]);
+  const float gamma = alpha * p.E[tid];
+  return u[0] < ic_rate(K.ic, gamma) * alpha * K.delta_t;
+}
+
+__device__ void emit_photon_gr(const RadK &K, const PtcK &p, size_t tid, const PhK &ph,
+                               size_t off, const float u[4]) {
+  const float x1 = p.x1[tid], p1 = p.p1[tid], u0_ptc = p.E[tid];
+  const uint32_t c = p.cell[tid];
+  const float xi = mpos(K.m, 0, c1_of(K.m, c), x1);
+  const float a = K.a;
+  const float r = gr_r(xi, a);
+  const float Delta = (float)(r * r - 2.0 * r + a * a);
+  const float alpha = gr_at(K.alpha, c, x1), D1 = gr_at(K.D1, c, x1);
+  const float D2 = gr_at(K.D2, c, x1), D3 = gr_at(K.D3, c, x1);
+  const float B3B1 = gr_at(K.B3B1, c, x1), g11 = gr_at(K.grr, c, x1);
+  const float g33 = gr_at(K.gff, c, x1), beta = gr_at(K.beta_phi, c, x1);
+  const float ur_ptc = u0_ptc * Delta * (p1 / u0_ptc - D1) / D2;
+  const float gamma = alpha * u0_ptc;
+  const float Eph = ic_photon_e(K.ic, gamma, u[1]);
+  const float En = (gamma - Eph) / alpha;
+  p.E[tid] = En;
+  float np1 = sgnf(p1) * sqrtf(En * En * (D2 * (alpha * alpha - D3) + D1 * D1) - D2);
+  if (np1 != np1) np1 = 0.0f;
+  p.p1[tid] = np1;
+  if (fabsf(Eph) < 50.0f) return;  // the energy is taken, no photon kept
+  ph.x1[off] = x1;
+  ph.x2[off] = ph.x3[off] = 0.0f;
+  ph.p1[off] = Delta * (Eph / gamma) * ur_ptc / g11;
+  ph.p2[off] = 0.0f;
+  ph.p3[off] = (Eph / gamma) * (u0_ptc * (K.gr_omega + beta) + B3B1 * ur_ptc) / g33;
+  ph.E[off] = Eph / alpha;
+  ph.w[off] = p.w[tid];
+  ph.path[off] = 0.0f;
+  ph.cell[off] = c;
+}
+
+__device__ bool check_pair_gr(const RadK &K, const PhK &ph, size_t tid, uint32_t cell,
+                              const float u[4]) {
+  const float alpha = gr_at(K.alpha, cell, ph.x1[tid]);
+  const float u0_hat = alpha * fabsf(ph.E[tid]);
+  const float prob = gg_rate(K.ic, u0_hat) * alpha * K.delta_t;
+  return u[1] < prob;
+}
+
+__device__ void produce_pair_gr(const RadK &K, const PhK &ph, size_t tid, const PtcK &p,
+                                size_t off) {
+  const float u0 = 0.5f * fabsf(ph.E[tid]);
+  const uint32_t c = ph.cell[tid];
+  const float x1 = ph.x1[tid];
+  ph.cell[tid] = AP_MAX_CELL;
+  const float alpha = gr_at(K.alpha, c, x1), D1 = gr_at(K.D1, c, x1);
+  const float D2 = gr_at(K.D2, c, x1), D3 = gr_at(K.D3, c, x1);
+  float p1 = sgnf(ph.p1[tid]) * sqrtf(u0 * u0 * (D2 * (alpha * alpha - D3) + D1 * D1) - D2);
+  if (p1 != p1) p1 = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const size_t o = off + (size_t)k;
+    p.x1[o] = x1;
+    p.x2[o] = p.x3[o] = 0.0f;
+    p.p1[o] = p1;
+    p.p2[o] = p.p3[o] = 0.0f;
+    p.E[o] = u0;
+    p.w[o] = ph.w[tid];
+    p.cell[o] = c;
+    p.flag[o] = kSecondary | ((uint32_t)k << 29);
+  }
+}
+
 // check_emit_photon (default :13-17; pulsar :26-53).
 __device__ bool check_emit(const RadK &K, const PtcK &p, size_t tid, uint32_t cell,
                            const float u[4]) {
   const float gamma = p.E[tid];
   if (K.model == AP_RAD_DEFAULT) return gamma > K.gamma_thr;
+  if (K.model == AP_RAD_GR1D) return check_emit_gr(K, p, tid, cell, u);
   const int c1 = c1_of(K.m, cell), c2 = c2_of(K.m, cell);
   const float r = expf(mpos(K.m, 0, c1, p.x1[tid]));
   if (r > 0.6f / K.omega) return false;
@@ -132,6 +227,10 @@ __device__ bool check_emit(const RadK &K, const PtcK &p, size_t tid, uint32_t ce
 // energy and the photon goes to slot off, or the slot stays empty.
 __device__ void emit_photon(const RadK &K, const PtcK &p, size_t tid, const PhK &ph, size_t off,
                             const float u[4]) {
+  if (K.model == AP_RAD_GR1D) {
+    emit_photon_gr(K, p, tid, ph, off, u);
+    return;
+  }
   const uint32_t c = p.cell[tid];
   const int c1 = c1_of(K.m, c), c2 = c2_of(K.m, c);
   const float p1 = p.p1[tid], p2 = p.p2[tid], p3 = p.p3[tid];
@@ -405,7 +504,15 @@ __global__ void __launch_bounds__(kRadThreads)
       uint32_t cell = AP_MAX_CELL;
       if (idx < number) {
         cell = ph.cell[idx];
-        if (cell != AP_MAX_CELL && in_bulk(K.m, cell)) e = check_pair(K, ph, idx, cell);
+        if (cell != AP_MAX_CELL && in_bulk(K.m, cell)) {
+          if (K.model == AP_RAD_GR1D) {
+            float u[4];
+            uniforms(K, 2u, ph.id[idx], u);
+            e = check_pair_gr(K, ph, idx, cell, u);
+          } else {
+            e = check_pair(K, ph, idx, cell);
+          }
+        }
         mark[idx] = e ? 1 : 0;
       }
       if (K.produced.ptr) add_produced(K, cell, e ? ph.w[idx] : 0.0f, e);
@@ -437,7 +544,10 @@ __global__ void __launch_bounds__(kRadThreads)
       uniforms(K, 2u, ph.id[idx], u);
       p.cell[off] = p.cell[off + 1] = AP_MAX_CELL;
       p.flag[off] = p.flag[off + 1] = 0u;
-      produce_pair(ph, idx, p, off);
+      if (K.model == AP_RAD_GR1D)
+        produce_pair_gr(K, ph, idx, p, off);
+      else
+        produce_pair(ph, idx, p, off);
       const bool tracked = u[0] < K.track_percent;
 #pragma unroll
       for (int m = 0; m < 2; ++m) {
@@ -492,6 +602,69 @@ __global__ void k_rad_move_cart(MeshK m, PhK ph, size_t num, float dt, int per0,
                         wrap_coord(n2, m.guard[1], m.dims[1], m.red[1], per1);
       ph.cell[idx] = keep ? (uint32_t)(n1 + n2 * m.dims[0]) : AP_MAX_CELL;
     }
+  }
+}
+
+// update_photon_1dgr (ptc_updater_1dgr.cu:301-400): photons outside the
+// bulk are removed; the others get the GR force on p1 and move in x1, and
+// tracked ones keep the lower u_0 in p2 when step % data_interval == 0.
+// The reference fixes the spin to 0.99 here (:322).
+struct GrPhK {
+  const float *alpha, *grr, *gff, *beta_phi, *theta;
+  float inv_delta, dt;
+  uint32_t step, data_interval;
+};
+__global__ void k_rad_move_gr(MeshK m, PhK ph, size_t num, GrPhK G) {
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < num;
+       idx += (size_t)blockDim.x * gridDim.x) {
+    const uint32_t c = ph.cell[idx];
+    if (c == AP_MAX_CELL) continue;
+    if (!in_bulk(m, c)) {
+      ph.cell[idx] = AP_MAX_CELL;
+      continue;
+    }
+    float p1 = ph.p1[idx];
+    const float p3 = ph.p3[idx], x1 = ph.x1[idx];
+    float u0 = fabsf(ph.E[idx]);
+    const float nx1 = 1.0f - x1;
+    const float xi = mpos(m, 0, (int)c, x1);
+    const float a = 0.99f;
+    const float r = gr_r(xi, a);
+    const float alpha = G.alpha[c] * x1 + G.alpha[c - 1] * nx1;
+    const float gamma11 = G.grr[c] * x1 + G.grr[c - 1] * nx1;
+    const float gamma33 = G.gff[c] * x1 + G.gff[c - 1] * nx1;
+    const float dDelta_dr = 2.0f * r - 2.0f;
+    const float dl = r * r - 2.0f * r + a * a;
+    const float Delta_sqr = dl * dl;
+    u0 = sqrtf(gamma11 * p1 * p1 / Delta_sqr + gamma33 * p3 * p3) / alpha;
+    const float da2dr = (G.alpha[c] * G.alpha[c] - G.alpha[c - 1] * G.alpha[c - 1]) * G.inv_delta;
+    const float dgamma11dxi = (G.grr[c] - G.grr[c - 1]) * G.inv_delta;
+    const float dgamma33dxi = (G.gff[c] - G.gff[c - 1]) * G.inv_delta;
+    const float dbetadxi = (G.beta_phi[c] - G.beta_phi[c - 1]) * G.inv_delta;
+    const float gr_term =
+        (-0.5f * u0 * da2dr -
+         (p1 * p1 * dgamma11dxi / Delta_sqr + p3 * p3 * dgamma33dxi) * 0.5f / u0 +
+         p3 * dbetadxi + gamma11 * p1 * p1 * dDelta_dr / (Delta_sqr * u0)) *
+        G.dt;
+    p1 += gr_term;
+    u0 = sqrtf(gamma11 * p1 * p1 / Delta_sqr + gamma33 * p3 * p3) / alpha;
+    ph.p1[idx] = p1;
+    ph.E[idx] = u0;
+    const float vr = gamma11 * p1 / (Delta_sqr * u0);
+    if (G.step % G.data_interval == 0 && (ph.flag[idx] & kTracked)) {
+      const float theta = G.theta[c] * x1 + G.theta[c - 1] * nx1;
+      const float ct = cosf(theta);
+      const float Sigma = (r * r + a * a * (ct * ct));
+      const float Delta = (r * r - 2.0f * r + a * a);
+      const float g_00 = -(1.0f + 2.0f * r * (r * r + a * a) / Sigma / Delta);
+      const float g_03 = -2.0f * r * a / Sigma / Delta;
+      ph.p2[idx] = (u0 - g_03 * p3) / g_00;
+    }
+    float new_x1 = x1 + vr * G.dt * G.inv_delta;
+    const int dc1 = (int)floorf(new_x1);
+    new_x1 -= (float)dc1;
+    ph.cell[idx] = c + (uint32_t)dc1;
+    ph.x1[idx] = new_x1;
   }
 }
 
@@ -592,6 +765,34 @@ RadK radk_of(const Ctx &c, ap_array produced, uint32_t call) {
   for (int s = 0; s < 2; ++s)
     K.Rho[s] = s < c.params.num_species ? field_of(c.fields.Rho[s]) : FieldArr{nullptr, 0};
   K.produced = field_of(produced);
+  K.alpha = K.D1 = K.D2 = K.D3 = K.B3B1 = K.grr = K.gff = K.beta_phi = nullptr;
+  K.a = K.gr_omega = 0.0f;
+  K.ic = IcK{};
+  if (c.coord == 3) {
+    K.alpha = coef_array(c, AP_GR_ALPHA).ptr;
+    K.D1 = coef_array(c, AP_GR_D1).ptr;
+    K.D2 = coef_array(c, AP_GR_D2).ptr;
+    K.D3 = coef_array(c, AP_GR_D3).ptr;
+    K.B3B1 = coef_array(c, AP_GR_B3B1).ptr;
+    K.grr = coef_array(c, AP_GR_GAMMA_RR).ptr;
+    K.gff = coef_array(c, AP_GR_GAMMA_FF).ptr;
+    K.beta_phi = coef_array(c, AP_GR_BETA_PHI).ptr;
+    K.a = (float)c.gr.a;
+    K.gr_omega = (float)c.gr.omega;
+  }
+  if (c.ic_ready) {
+    const int ng = c.ic_n_gamma, ne = c.ic_n_ep;
+    K.ic.ic_rate = c.ic_buf;
+    K.ic.gg_rate = c.ic_buf + ng;
+    K.ic.gammas = c.ic_buf + 2 * ng;
+    K.ic.dNde = c.ic_buf + 3 * ng;
+    K.ic.dNde_th = c.ic_buf + 3 * ng + (size_t)ng * ne;
+    K.ic.n_gamma = ng;
+    K.ic.n_ep = ne;
+    K.ic.dep = c.ic_dep;
+    K.ic.dg = c.ic_dg;
+    K.ic.dlep = c.ic_dlep;
+  }
   return K;
 }
 
@@ -627,10 +828,22 @@ uint32_t grid_of(const Ctx &c, uint32_t nchunks) {
 
 }  // namespace
 
-int rad_move_photons(Ctx &c, float dt) {
+int rad_move_photons(Ctx &c, float dt, uint32_t step) {
   if (!c.ph_bound || c.ph_number == 0) return AP_OK;
   const uint32_t grid = (uint32_t)c.num_sms * 4;
-  if (c.coord == 1)
+  if (c.coord == 3) {
+    GrPhK G;
+    G.alpha = coef_array(c, AP_GR_ALPHA).ptr;
+    G.grr = coef_array(c, AP_GR_GAMMA_RR).ptr;
+    G.gff = coef_array(c, AP_GR_GAMMA_FF).ptr;
+    G.beta_phi = coef_array(c, AP_GR_BETA_PHI).ptr;
+    G.theta = coef_array(c, AP_GR_THETA).ptr;
+    G.inv_delta = c.mesh.inv_delta[0];
+    G.dt = dt;
+    G.step = step;
+    G.data_interval = (uint32_t)c.params.data_interval;
+    k_rad_move_gr<<<grid, 256, 0, c.stream>>>(c.mk, phk_of(c), c.ph_number, G);
+  } else if (c.coord == 1)
     k_rad_move_logsph<<<grid, 256, 0, c.stream>>>(c.mk, phk_of(c), c.ph_number, dt,
                                                     c.rad.r_cutoff);
   else

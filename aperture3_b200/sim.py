@@ -77,10 +77,12 @@ class SimParams:
     damping_coef: float = 0.002
     # 1D GR lab (coord_system "1DGR"): black hole spin (src/sim_params.h:63)
     a: float = 0.0
-    # photons and pair production (src/sim_params.h:23, 50-83); rad_model
+    # photons and pair production (src/sim_params.h:23, 50-88); rad_model
     # selects the user radiative functions: "default" (src/cuda/radiation/
-    # user_radiative_functions.cu) or "pulsar" (the pulsar lab's); rad_seed
-    # keys the counter-based random stream that replaces cuRAND
+    # user_radiative_functions.cu), "pulsar" (the pulsar lab's) or "gr1d"
+    # (the 1D GR lab's, with the inverse-Compton tables of e_min, ic_path,
+    # n_gamma, n_ep); rad_seed keys the counter-based random stream that
+    # replaces cuRAND
     max_photon_number: int = 100
     create_pairs: bool = False
     gamma_thr: float = 20.0
@@ -91,6 +93,10 @@ class SimParams:
     r_cutoff: float = 4.0
     l_curv: float = 6.0
     e_curv: float = 6.4e-9
+    e_min: float = 1.0e-3
+    ic_path: float = 1.0
+    n_gamma: int = 600
+    n_ep: int = 600
     rad_model: str = "default"
     rad_seed: int = 1
 
@@ -862,10 +868,12 @@ class radiative_transfer:
     """radiative_transfer (src/radiation/radiative_transfer.h:11-29): photon
     emission and pair production with the user radiative functions that
     SimParams.rad_model names ("default": src/cuda/radiation/
-    user_radiative_functions.cu; "pulsar": the pulsar lab's). The photon
-    move itself is part of update_particles, as in the reference."""
+    user_radiative_functions.cu; "pulsar": the pulsar lab's; "gr1d": the 1D
+    GR lab's, whose inverse-Compton tables are built here as its
+    user_rt_init builds them). The photon move itself is part of
+    update_particles, as in the reference."""
 
-    MODELS = {"default": _lib.RAD_DEFAULT, "pulsar": _lib.RAD_PULSAR}
+    MODELS = {"default": _lib.RAD_DEFAULT, "pulsar": _lib.RAD_PULSAR, "gr1d": _lib.RAD_GR1D}
 
     def __init__(self, env: SimEnvironment, first_photon_id: int = 1 << 60,
                  first_particle_id: int = (1 << 60) + (1 << 59)):
@@ -886,6 +894,10 @@ class radiative_transfer:
         rp.seed = int(pr.rad_seed)
         rp.first_photon_id = int(first_photon_id)
         rp.first_particle_id = int(first_particle_id)
+        rp.e_min = pr.e_min
+        rp.ic_path = pr.ic_path
+        rp.n_gamma = int(pr.n_gamma)
+        rp.n_ep = int(pr.n_ep)
         check(env._lib.ap_set_rad_params(env.ctx, C.byref(rp)), "ap_set_rad_params")
         self.last: Dict[str, int] = {}
 
@@ -911,6 +923,46 @@ class radiative_transfer:
         data.refresh_number()
         self.last = self._counts(cnt)
         return self.last
+
+
+class inverse_compton:
+    """inverse_compton (src/cuda/radiation/rt_ic.h, rt_ic.cu): the rate and
+    photon-energy tables for a background spectrum, built on the device of
+    an environment. `spectrum` is one of SPECTRA with its constructor's
+    arguments, e.g. ("broken_power_law", 1.25, 1.1, 1e-3, 1e-10, 0.1)."""
+
+    SPECTRA = {"power_law_hard": _lib.SPEC_POWER_LAW_HARD,
+               "power_law_soft": _lib.SPEC_POWER_LAW_SOFT,
+               "broken_power_law": _lib.SPEC_BROKEN_POWER_LAW,
+               "black_body": _lib.SPEC_BLACK_BODY,
+               "mono_energetic": _lib.SPEC_MONO_ENERGETIC}
+
+    def __init__(self, env: SimEnvironment):
+        self.env = env
+        self.n_gamma = int(env.params.n_gamma)
+        self.n_ep = int(env.params.n_ep)
+
+    def init(self, spectrum, emin: float, emax: float, n0: float):
+        sp = _lib.ApSpectrum()
+        sp.kind = self.SPECTRA[spectrum[0]]
+        for k, v in enumerate(spectrum[1:]):
+            sp.p[k] = float(v)
+        check(self.env._lib.ap_ic_init(self.env.ctx, C.byref(sp), float(emin), float(emax),
+                                       float(n0), self.n_gamma, self.n_ep), "ap_ic_init")
+
+    def tables(self) -> Dict[str, np.ndarray]:
+        """ic_rate, gg_rate, gammas (n_gamma), dNde, dNde_thomson (n_gamma x
+        n_ep) and the steps dep, dg, dlep."""
+        ng, ne = self.n_gamma, self.n_ep
+        out = {k: np.zeros(ng, np.float32) for k in ("ic_rate", "gg_rate", "gammas")}
+        out.update({k: np.zeros((ng, ne), np.float32) for k in ("dNde", "dNde_thomson")})
+        steps = np.zeros(3, np.float32)
+        check(self.env._lib.ap_ic_tables(
+            self.env.ctx, *[out[k].ctypes.data for k in ("ic_rate", "gg_rate", "gammas", "dNde",
+                                                          "dNde_thomson")],
+            steps.ctypes.data), "ap_ic_tables")
+        out["dep"], out["dg"], out["dlep"] = (float(x) for x in steps)
+        return out
 
 
 # Python-style aliases

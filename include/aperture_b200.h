@@ -487,13 +487,18 @@ AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32
  * Photons and pair production: radiative_transfer (src/radiation/
  * radiative_transfer.h:11-29, src/cuda/radiation/radiative_transfer.cu)
  * with the user radiative functions of the framework
- * (src/cuda/radiation/user_radiative_functions.cu, AP_RAD_DEFAULT) or of
+ * (src/cuda/radiation/user_radiative_functions.cu, AP_RAD_DEFAULT), of
  * the pulsar lab (labs/pulsar/src/cuda/radiation/
- * user_radiative_functions.cu, AP_RAD_PULSAR), and the photon movers of
- * the particle updaters (ptc_updater.cu:627-690, ptc_updater_logsph.cu:
- * 58-131), which ap_update_particles runs after the particles when photons
- * are bound, followed by the exchange: photons leaving the bulk wrap
- * through periodic sides (Cartesian) or are removed.
+ * user_radiative_functions.cu, AP_RAD_PULSAR) or of the 1D GR lab
+ * (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh, AP_RAD_GR1D,
+ * which samples inverse-Compton emission and gamma-gamma conversion from the
+ * tables of ap_ic_init), and the photon movers of the particle updaters
+ * (ptc_updater.cu:627-690, ptc_updater_logsph.cu:58-131,
+ * ptc_updater_1dgr.cu:301-400), which ap_update_particles runs after the
+ * particles when photons are bound, followed by the exchange: photons
+ * leaving the bulk wrap through periodic sides (Cartesian) or are removed
+ * (the 1D GR mover removes photons outside the bulk before moving them, as
+ * the reference's does).
  *
  * Each pass ranks its emitters in slot order and appends: photon k of an
  * emit_photons call at slot number + k (the photon count then grows by the
@@ -512,6 +517,7 @@ AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32
  * (a photon the model does not keep) have cell = MAX_CELL. */
 #define AP_RAD_DEFAULT 0
 #define AP_RAD_PULSAR 1
+#define AP_RAD_GR1D 2
 typedef struct {
   float *x1, *x2, *x3;
   float *p1, *p2, *p3;
@@ -535,12 +541,50 @@ typedef struct {
   uint64_t seed;
   uint64_t first_photon_id;
   uint64_t first_particle_id;
+  /* AP_RAD_GR1D (user_rt_init, labs/1dgr/src/cuda/radiation/
+     user_radiative_functions.cuh:191-203): tables of n_gamma x n_ep
+     entries for the background broken_power_law(1.25, 1.1, e_min, 1e-10,
+     0.1) with photon density 1.5e24 / ic_path; the spin and omega are the
+     1D GR context's (ap_gr_params).                                        */
+  float e_min;          /* SimParams::e_min (default 1e-3)                 */
+  float ic_path;        /* SimParams::ic_path (default 1)                  */
+  int n_gamma, n_ep;    /* SimParams::n_gamma, n_ep (default 600, 600)     */
 } ap_rad_params;
 typedef struct {
   uint64_t marked;   /* particles (photons) that passed the model's check  */
   uint64_t written;  /* appended within the capacity                      */
   uint64_t dropped;  /* over the capacity                                 */
 } ap_rad_counts;
+
+/* Background photon spectra of inverse_compton::init (src/radiation/
+ * spectra.h); p[] holds the constructor's arguments in order. */
+#define AP_SPEC_POWER_LAW_HARD 0   /* delta, emin, emax                 */
+#define AP_SPEC_POWER_LAW_SOFT 1   /* alpha, emin, emax                 */
+#define AP_SPEC_BROKEN_POWER_LAW 2 /* alpha, delta, epeak, emin, emax   */
+#define AP_SPEC_BLACK_BODY 3       /* kT                                */
+#define AP_SPEC_MONO_ENERGETIC 4   /* e0, de                            */
+typedef struct {
+  int kind;
+  float p[5];
+} ap_spectrum;
+
+/* inverse_compton's constructor and init(n_e, emin, emax, n0)
+ * (src/cuda/radiation/rt_ic.cu:207-435): for n_gamma Lorentz factors
+ * log-spaced over [1.01, 1e15], the scattering rate and the gamma-gamma
+ * pair rate in the background n0 * n_e, and the cumulative, normalised
+ * distributions of the scattered photon energy over n_ep linear (dNde) and
+ * n_ep log-spaced (dNde_thomson) fractions of gamma. The reference
+ * integrates on the host (100 angles x 800 energies per entry, one entry
+ * after the other); here one GPU pass per table, with the same integrands
+ * in double and the same float rounding of the stored values and of the
+ * cumulative sums. The tables stay on the device for AP_RAD_GR1D. */
+AP_API int ap_ic_init(ap_ctx *ctx, const ap_spectrum *spectrum, double emin, double emax,
+                      double n0, int n_gamma, int n_ep);
+/* Copies the tables to host arrays (each may be NULL): ic_rate, gg_rate,
+ * gammas of n_gamma floats; dNde, dNde_thomson of n_gamma x n_ep floats,
+ * row n for gammas[n]; steps = {dep, dg, dlep}. */
+AP_API int ap_ic_tables(ap_ctx *ctx, float *ic_rate, float *gg_rate, float *gammas,
+                        float *dNde, float *dNde_thomson, float *steps);
 
 /* Binds caller-owned photon arrays of `capacity` slots, `number` in use. */
 AP_API int ap_bind_photons(ap_ctx *ctx, const ap_photons *ph, size_t number, size_t capacity);
@@ -558,7 +602,8 @@ AP_API int ap_emit_photons(ap_ctx *ctx, ap_array photon_produced, ap_rad_counts 
  * Waits for the stream. */
 AP_API int ap_produce_pairs(ap_ctx *ctx, ap_array pair_produced, ap_rad_counts *out);
 /* The photon move of one update (also run by ap_update_particles when
- * photons are bound). */
+ * photons are bound; the 1D GR mover records the lower u_0 of tracked
+ * photons as on step 0 when called here). */
 AP_API int ap_move_photons(ap_ctx *ctx, double dt);
 
 /* Device time per phase of the update, from CUDA events recorded on the

@@ -3,10 +3,14 @@
  *
  * Restates, in FP32 with the reference's operation order (compiled with
  * -ffp-contract=off), the photon movers of the particle updaters and the
- * radiative_transfer module with its two user-function sets:
+ * radiative_transfer module with its three user-function sets:
  *   - the framework's default: src/cuda/radiation/user_radiative_functions.cu
  *   - the pulsar lab's:        labs/pulsar/src/cuda/radiation/
  *                              user_radiative_functions.cu
+ *   - the 1D GR lab's:         labs/1dgr/src/cuda/radiation/
+ *                              user_radiative_functions.cuh (with the
+ *                              inverse-Compton tables of ap_ic.c), and the
+ *                              1D GR photon mover
  * The float transcendentals are the C library's expf, sinf, cosf, acosf,
  * logf, atan2f (the reference's device code calls the float overloads);
  * rho_c's pow and chi's square root take double arguments there and here.
@@ -18,7 +22,8 @@
  *     counter (pass, id, tag), so the result does not depend on scheduling.
  *     The draws are used as: default model u0 = photon energy, u1 = free
  *     path, u2 = tracking; pulsar model u0 = emission test, u2 = tracking;
- *     pair production u0 = tracking;
+ *     1D GR model u0 = emission test, u1 = photon energy, u2 = tracking;
+ *     pair production u0 = tracking (1D GR: u1 = conversion test);
  *   - order: emitters are ranked in slot order (the reference ranks them by
  *     block and shared-memory atomic order);
  *   - ids: every new photon and particle gets an id from the counter
@@ -251,11 +256,158 @@ static float rho_c(float r, float theta) {
                  (double)(3.0f * s * (1.0f + c2)));
 }
 
+/* ---- the 1D GR lab's functions (labs/1dgr/src/cuda/radiation/
+ * user_radiative_functions.cuh:19-189). A metric array at x1 in cell c is
+ * interpolated between c - 1 and c. The photon energy draw is u1; the
+ * emission and conversion tests draw u0 and u1. */
+static inline float gr_at(const float *a, uint32_t c, float x1) {
+  return a[c] * x1 + a[c - 1] * (1.0f - x1);
+}
+static inline float sgnf(float v) { return (float)((0.0f < v) - (v < 0.0f)); }
+
+/* The Boyer-Lindquist r of the tortoise coordinate xi and Delta
+ * (:38-45); r takes the reference's double division. */
+static inline float gr_r(float xi, float a) {
+  const float rp = 1.0f + sqrtf(1.0f - a * a);
+  const float rm = 1.0f - sqrtf(1.0f - a * a);
+  const float exp_xi = expf(xi * (rp - rm));
+  return (float)((rp - rm * exp_xi) / (1.0 - exp_xi));
+}
+
+static int check_emit_gr(const or_rad_params *rp, const or_ptc *p, size_t tid, const float u[4]) {
+  const or_rad_gr *g = rp->gr;
+  const float alpha = gr_at(g->alpha, p->cell[tid], p->x1[tid]);
+  const float gamma = alpha * p->E[tid];
+  return u[0] < or_ic_rate(g->ic, gamma) * alpha * rp->delta_t;
+}
+
+static void emit_photon_gr(const or_mesh *m, const or_rad_params *rp, or_ptc *p, size_t tid,
+                           or_photons *ph, size_t off, const float u[4]) {
+  const or_rad_gr *g = rp->gr;
+  const float x1 = p->x1[tid], p1 = p->p1[tid], u0_ptc = p->E[tid];
+  const uint32_t c = p->cell[tid];
+  const float xi = mpos(m, 0, c1_of(m, c), x1);
+  const float a = g->a;
+  const float r = gr_r(xi, a);
+  const float Delta = (float)(r * r - 2.0 * r + a * a);
+  const float alpha = gr_at(g->alpha, c, x1), D1 = gr_at(g->D1, c, x1);
+  const float D2 = gr_at(g->D2, c, x1), D3 = gr_at(g->D3, c, x1);
+  const float B3B1 = gr_at(g->B3B1, c, x1), g11 = gr_at(g->gamma_rr, c, x1);
+  const float g33 = gr_at(g->gamma_ff, c, x1), beta = gr_at(g->beta_phi, c, x1);
+  const float ur_ptc = u0_ptc * Delta * (p1 / u0_ptc - D1) / D2;
+  const float gamma = alpha * p->E[tid];
+  const float Eph = or_ic_photon_e(g->ic, gamma, u[1]);
+  p->E[tid] = (gamma - Eph) / alpha;
+  const float En = p->E[tid];
+  float np1 = sgnf(p1) * sqrtf(En * En * (D2 * (alpha * alpha - D3) + D1 * D1) - D2);
+  if (np1 != np1) np1 = 0.0f;
+  p->p1[tid] = np1;
+  if (fabsf(Eph) < 50.0f) return; /* energy taken, no photon kept */
+  ph->x1[off] = x1;
+  ph->x2[off] = ph->x3[off] = 0.0f;
+  ph->p1[off] = Delta * (Eph / gamma) * ur_ptc / g11;
+  ph->p2[off] = 0.0f;
+  ph->p3[off] = (Eph / gamma) * (u0_ptc * (g->omega + beta) + B3B1 * ur_ptc) / g33;
+  ph->E[off] = Eph / alpha;
+  ph->weight[off] = p->weight[tid];
+  ph->path_left[off] = 0.0f;
+  ph->cell[off] = c;
+}
+
+static int check_pair_gr(const or_rad_params *rp, const or_photons *ph, size_t tid,
+                         const float u[4]) {
+  const or_rad_gr *g = rp->gr;
+  const float alpha = gr_at(g->alpha, ph->cell[tid], ph->x1[tid]);
+  const float u0_hat = alpha * fabsf(ph->E[tid]);
+  const float prob = or_gg_rate(g->ic, u0_hat) * alpha * rp->delta_t;
+  return u[1] < prob;
+}
+
+static void produce_pair_gr(const or_rad_params *rp, or_photons *ph, size_t tid, or_ptc *p,
+                            size_t off) {
+  const or_rad_gr *g = rp->gr;
+  const float u0 = 0.5f * fabsf(ph->E[tid]);
+  const uint32_t c = ph->cell[tid];
+  const float x1 = ph->x1[tid];
+  ph->cell[tid] = OR_MAX_CELL;
+  const float alpha = gr_at(g->alpha, c, x1), D1 = gr_at(g->D1, c, x1);
+  const float D2 = gr_at(g->D2, c, x1), D3 = gr_at(g->D3, c, x1);
+  float p1 = sgnf(ph->p1[tid]) * sqrtf(u0 * u0 * (D2 * (alpha * alpha - D3) + D1 * D1) - D2);
+  if (p1 != p1) p1 = 0.0f;
+  for (int k = 0; k < 2; ++k) {
+    const size_t o = off + (size_t)k;
+    p->x1[o] = x1;
+    p->x2[o] = p->x3[o] = 0.0f;
+    p->p1[o] = p1;
+    p->p2[o] = p->p3[o] = 0.0f;
+    p->E[o] = u0;
+    p->weight[o] = ph->weight[tid];
+    p->cell[o] = c;
+    p->flag[o] = FLAG_SECONDARY | ((uint32_t)k << 29);
+  }
+}
+
+void or_move_photons_gr(const or_mesh *m, const or_rad_gr *g, or_photons *ph, size_t num,
+                        float dt, uint32_t step, int data_interval) {
+  const float inv = m->inv_delta[0];
+  for (size_t idx = 0; idx < num; ++idx) {
+    const uint32_t c = ph->cell[idx];
+    if (c == OR_MAX_CELL) continue;
+    if (!in_bulk(m, c)) {
+      ph->cell[idx] = OR_MAX_CELL;
+      continue;
+    }
+    float p1 = ph->p1[idx];
+    const float p3 = ph->p3[idx], x1 = ph->x1[idx];
+    float u0 = fabsf(ph->E[idx]);
+    const float nx1 = 1.0f - x1;
+    const float xi = mpos(m, 0, (int)c, x1);
+    const float a = 0.99f; /* the reference fixes the spin here (:322) */
+    const float r = gr_r(xi, a);
+    const float alpha = g->alpha[c] * x1 + g->alpha[c - 1] * nx1;
+    const float gamma11 = g->gamma_rr[c] * x1 + g->gamma_rr[c - 1] * nx1;
+    const float gamma33 = g->gamma_ff[c] * x1 + g->gamma_ff[c - 1] * nx1;
+    const float dDelta_dr = 2.0f * r - 2.0f;
+    const float dl = r * r - 2.0f * r + a * a;
+    const float Delta_sqr = dl * dl;
+    u0 = sqrtf(gamma11 * p1 * p1 / Delta_sqr + gamma33 * p3 * p3) / alpha;
+    const float da2dr = (g->alpha[c] * g->alpha[c] - g->alpha[c - 1] * g->alpha[c - 1]) * inv;
+    const float dgamma11dxi = (g->gamma_rr[c] - g->gamma_rr[c - 1]) * inv;
+    const float dgamma33dxi = (g->gamma_ff[c] - g->gamma_ff[c - 1]) * inv;
+    const float dbetadxi = (g->beta_phi[c] - g->beta_phi[c - 1]) * inv;
+    const float gr_term =
+        (-0.5f * u0 * da2dr - (p1 * p1 * dgamma11dxi / Delta_sqr + p3 * p3 * dgamma33dxi) *
+                                  0.5f / u0 +
+         p3 * dbetadxi + gamma11 * p1 * p1 * dDelta_dr / (Delta_sqr * u0)) *
+        dt;
+    p1 += gr_term;
+    u0 = sqrtf(gamma11 * p1 * p1 / Delta_sqr + gamma33 * p3 * p3) / alpha;
+    ph->p1[idx] = p1;
+    ph->E[idx] = u0;
+    const float vr = gamma11 * p1 / (Delta_sqr * u0);
+    if (step % (uint32_t)data_interval == 0 && (ph->flag[idx] & FLAG_TRACKED)) {
+      const float theta = g->theta[c] * x1 + g->theta[c - 1] * nx1;
+      const float ct = cosf(theta);
+      const float Sigma = (r * r + a * a * (ct * ct));
+      const float Delta = (r * r - 2.0f * r + a * a);
+      const float g_00 = -(1.0f + 2.0f * r * (r * r + a * a) / Sigma / Delta);
+      const float g_03 = -2.0f * r * a / Sigma / Delta;
+      ph->p2[idx] = (u0 - g_03 * ph->p3[idx]) / g_00;
+    }
+    float new_x1 = x1 + vr * dt * inv;
+    const int dc1 = (int)floorf(new_x1);
+    new_x1 -= (float)dc1;
+    ph->cell[idx] = c + (uint32_t)dc1;
+    ph->x1[idx] = new_x1;
+  }
+}
+
 /* check_emit_photon of the model (default :13-17; pulsar :26-53). */
 static int check_emit(const or_mesh *m, const or_rad_params *rp, const or_ptc *p, size_t tid,
                       const float u[4]) {
   const float gamma = p->E[tid];
   if (rp->model == OR_RAD_DEFAULT) return gamma > rp->gamma_thr;
+  if (rp->model == OR_RAD_GR1D) return check_emit_gr(rp, p, tid, u);
   const uint32_t c = p->cell[tid];
   const int c1 = c1_of(m, c), c2 = c2_of(m, c);
   const float r = expf(mpos(m, 0, c1, p->x1[tid]));
@@ -273,6 +425,10 @@ static int check_emit(const or_mesh *m, const or_rad_params *rp, const or_ptc *p
  * parent and writes the photon at slot off, or leaves the slot a hole. */
 static void emit_photon(const or_mesh *m, const or_rad_params *rp, or_ptc *p, size_t tid,
                         or_photons *ph, size_t off, const or_fields *f, const float u[4]) {
+  if (rp->model == OR_RAD_GR1D) {
+    emit_photon_gr(m, rp, p, tid, ph, off, u);
+    return;
+  }
   const uint32_t c = p->cell[tid];
   const int c1 = c1_of(m, c), c2 = c2_of(m, c);
   const float p1 = p->p1[tid], p2 = p->p2[tid], p3 = p->p3[tid];
@@ -434,7 +590,13 @@ void or_produce_pairs(const or_mesh *m, const or_rad_params *rp, or_photons *ph,
   for (size_t tid = 0; tid < ph_num; ++tid) {
     const uint32_t cell = ph->cell[tid];
     if (cell == OR_MAX_CELL || !in_bulk(m, cell)) continue;
-    if (!check_pair(m, rp, ph, tid, f)) continue;
+    if (rp->model == OR_RAD_GR1D) {
+      float ug[4];
+      or_rad_uniforms(rp->seed, 2u, call, ph->id[tid], ug);
+      if (!check_pair_gr(rp, ph, tid, ug)) continue;
+    } else if (!check_pair(m, rp, ph, tid, f)) {
+      continue;
+    }
     if (pair_produced) AT2(pair_produced, c1_of(m, cell), c2_of(m, cell)) += ph->weight[tid];
     const size_t off = base + 2 * rank;
     const uint64_t id = first_id + 2 * (uint64_t)rank;
@@ -447,7 +609,10 @@ void or_produce_pairs(const or_mesh *m, const or_rad_params *rp, or_photons *ph,
     or_rad_uniforms(rp->seed, 2u, call, ph->id[tid], u);
     p->cell[off] = p->cell[off + 1] = OR_MAX_CELL;
     p->flag[off] = p->flag[off + 1] = 0u;
-    produce_pair(ph, tid, p, off);
+    if (rp->model == OR_RAD_GR1D)
+      produce_pair_gr(rp, ph, tid, p, off);
+    else
+      produce_pair(ph, tid, p, off);
     const int tracked = u[0] < rp->track_percent;
     for (int k = 0; k < 2; ++k) {
       if (tracked) p->flag[off + k] |= FLAG_TRACKED;

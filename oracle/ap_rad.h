@@ -6,6 +6,7 @@
 #ifndef AP_RAD_H_
 #define AP_RAD_H_
 
+#include "ap_ic.h"
 #include "ap_oracle.h"
 
 #ifdef __cplusplus
@@ -22,10 +23,20 @@ typedef struct {
   uint32_t *flag;
 } or_photons;
 
-/* The two emission / conversion models: the framework's default
- * (src/cuda/radiation/user_radiative_functions.cu) and the pulsar lab's
- * (labs/pulsar/src/cuda/radiation/user_radiative_functions.cu). */
-enum { OR_RAD_DEFAULT = 0, OR_RAD_PULSAR = 1 };
+/* The emission / conversion models: the framework's default
+ * (src/cuda/radiation/user_radiative_functions.cu), the pulsar lab's
+ * (labs/pulsar/src/cuda/radiation/user_radiative_functions.cu) and the 1D
+ * GR lab's (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh). */
+enum { OR_RAD_DEFAULT = 0, OR_RAD_PULSAR = 1, OR_RAD_GR1D = 2 };
+
+/* What the 1D GR lab's functions read besides SimParams: Grid_1dGR's
+ * per-cell arrays (grid_1dgr.h mesh_ptrs), the spin a, omega, and the
+ * inverse-Compton tables. */
+typedef struct {
+  const float *alpha, *D1, *D2, *D3, *B3B1, *gamma_rr, *gamma_ff, *beta_phi, *theta;
+  float a, omega;
+  const or_ic_tables *ic;
+} or_rad_gr;
 
 /* The SimParams members the radiation functions read (src/sim_params.h:
  * 17-123), the random key and the id counters. */
@@ -34,6 +45,7 @@ typedef struct {
   float delta_t, gamma_thr, E_secondary, photon_path, r_cutoff, track_percent;
   float e_curv, l_curv, BQ, omega;
   uint64_t seed;
+  const or_rad_gr *gr; /* OR_RAD_GR1D only */
 } or_rad_params;
 
 /* Counts of one emission or conversion pass. */
@@ -59,6 +71,13 @@ void or_move_photons_cart(const or_mesh *m, or_photons *ph, size_t num, float dt
  * grid: photons outside the bulk are removed. */
 void or_move_photons_logsph(const or_mesh *m, const or_rad_params *rp, or_photons *ph,
                             size_t num, float dt);
+
+/* update_photon_1dgr (src/cuda/algorithms/ptc_updater_1dgr.cu:301-400):
+ * photons outside the bulk are removed, the others get the GR force on p1
+ * and move in x1; tracked photons keep the lower u_0 in p2 on steps with
+ * step % data_interval == 0. */
+void or_move_photons_gr(const or_mesh *m, const or_rad_gr *g, or_photons *ph, size_t num,
+                        float dt, uint32_t step, int data_interval);
 
 /* radiative_transfer::emit_photons (src/cuda/radiation/radiative_transfer.cu:
  * 28-97, 196-243) with the model's check_emit_photon / emit_photon: parents

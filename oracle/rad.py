@@ -1,8 +1,9 @@
 """CPU oracle for photons and pair production -- TEST INFRASTRUCTURE ONLY.
 
 Wraps ``ap_rad.c`` of ``liboracle.so`` (the restatement of the photon movers
-and of ``radiative_transfer`` with the default and the pulsar lab's user
-radiative functions) and the pin library ``_ref/libapref_rad.so`` that runs
+and of ``radiative_transfer`` with the default, the pulsar lab's and the 1D
+GR lab's user radiative functions), ``ap_ic.c`` (the inverse-Compton tables
+of ``src/cuda/radiation/rt_ic.cu``) and the pin library ``_ref/libapref_rad.so`` that runs
 the reference's own user functions on the host (built by
 ``ref_build/Makefile`` when the reference tree is present), plus the photon
 movers of ``_ref/libapref.so`` and ``_ref/libapref_ls.so``.
@@ -28,7 +29,9 @@ PH_FIELDS = (
     ("cell", np.uint32), ("id", np.uint64), ("flag", np.uint32),
 )
 
-RAD_DEFAULT, RAD_PULSAR = 0, 1
+RAD_DEFAULT, RAD_PULSAR, RAD_GR1D = 0, 1, 2
+SPEC_POWER_LAW_HARD, SPEC_POWER_LAW_SOFT, SPEC_BROKEN_POWER_LAW = 0, 1, 2
+SPEC_BLACK_BODY, SPEC_MONO_ENERGETIC = 3, 4
 
 
 class Photons(C.Structure):
@@ -41,8 +44,27 @@ class RadParams(C.Structure):
         ("model", C.c_int), ("delta_t", C.c_float), ("gamma_thr", C.c_float),
         ("E_secondary", C.c_float), ("photon_path", C.c_float), ("r_cutoff", C.c_float),
         ("track_percent", C.c_float), ("e_curv", C.c_float), ("l_curv", C.c_float),
-        ("BQ", C.c_float), ("omega", C.c_float), ("seed", C.c_uint64),
+        ("BQ", C.c_float), ("omega", C.c_float), ("seed", C.c_uint64), ("gr", C.c_void_p),
     ]
+
+
+class Spectrum(C.Structure):
+    """or_spectrum (ap_ic.h)."""
+    _fields_ = [("kind", C.c_int), ("p", C.c_float * 5)]
+
+
+class IcTablesS(C.Structure):
+    """or_ic_tables (ap_ic.h)."""
+    _fields_ = [("n_gamma", C.c_int), ("n_ep", C.c_int), ("dep", C.c_float), ("dg", C.c_float),
+                ("dlep", C.c_float), ("ic_rate", C.c_void_p), ("gg_rate", C.c_void_p),
+                ("gammas", C.c_void_p), ("dNde", C.c_void_p), ("dNde_thomson", C.c_void_p)]
+
+
+class RadGr(C.Structure):
+    """or_rad_gr (ap_rad.h)."""
+    _fields_ = [(n, C.c_void_p) for n in ("alpha", "D1", "D2", "D3", "B3B1", "gamma_rr",
+                                          "gamma_ff", "beta_phi", "theta")] + [
+        ("a", C.c_float), ("omega", C.c_float), ("ic", C.c_void_p)]
 
 
 class RadCounts(C.Structure):
@@ -54,7 +76,71 @@ def rad_params(model=RAD_DEFAULT, delta_t=0.01, gamma_thr=20.0, E_secondary=4.0,
                BQ=1.0, omega=0.2, seed=1):
     """RadParams with the reference's SimParams defaults (sim_params.h:50-83)."""
     return RadParams(model, delta_t, gamma_thr, E_secondary, photon_path, r_cutoff,
-                     track_percent, e_curv, l_curv, BQ, omega, seed)
+                     track_percent, e_curv, l_curv, BQ, omega, seed, None)
+
+
+def spectrum(kind, *p):
+    s = Spectrum()
+    s.kind = kind
+    for k, v in enumerate(p):
+        s.p[k] = v
+    return s
+
+
+class IcTables:
+    """inverse_compton's tables for one spectrum (or_ic_init): numpy arrays
+    ic_rate, gg_rate, gammas (n_gamma) and dNde, dNde_thomson (n_gamma x
+    n_ep), and the steps dep, dg, dlep."""
+
+    def __init__(self, spec, emin, emax, n0, n_gamma=600, n_ep=600):
+        self.ic_rate = np.zeros(n_gamma, np.float32)
+        self.gg_rate = np.zeros(n_gamma, np.float32)
+        self.gammas = np.zeros(n_gamma, np.float32)
+        self.dNde = np.zeros((n_gamma, n_ep), np.float32)
+        self.dNde_thomson = np.zeros((n_gamma, n_ep), np.float32)
+        self.s = IcTablesS(n_gamma, n_ep, 0.0, 0.0, 0.0, self.ic_rate.ctypes.data,
+                           self.gg_rate.ctypes.data, self.gammas.ctypes.data,
+                           self.dNde.ctypes.data, self.dNde_thomson.ctypes.data)
+        lib.or_ic_init(C.byref(spec), float(emin), float(emax), float(n0), C.byref(self.s))
+        self.dep, self.dg, self.dlep = self.s.dep, self.s.dg, self.s.dlep
+
+    def rate(self, gamma):
+        return lib.or_ic_rate(C.byref(self.s), float(gamma))
+
+    def gg(self, eph):
+        return lib.or_gg_rate(C.byref(self.s), float(eph))
+
+    def photon_e(self, gamma, u):
+        return lib.or_ic_photon_e(C.byref(self.s), float(gamma), float(u))
+
+
+def gr1d_spectrum(e_min):
+    """The 1D GR lab's background (user_rt_init, labs/1dgr/src/cuda/
+    radiation/user_radiative_functions.cuh:191-203): broken_power_law(1.25,
+    1.1, e_min, 1e-10, 0.1); tables over [1e-10, 0.1] with n0 = 1.5e24 /
+    ic_path."""
+    return spectrum(SPEC_BROKEN_POWER_LAW, 1.25, 1.1, e_min, 1e-10, 0.1)
+
+
+class GrRad:
+    """or_rad_gr over the 15 Grid_1dGR arrays of oracle.gr_coef and an
+    IcTables (kept alive with it)."""
+
+    NAMES = ("alpha", "D1", "D2", "D3", "B3B1", "gamma_rr", "gamma_ff", "beta_phi", "theta")
+
+    def __init__(self, co, a, omega, ic):
+        from . import GR_COEF_NAMES
+        self.arrs = [np.ascontiguousarray(co[GR_COEF_NAMES.index(n)], np.float32)
+                     for n in self.NAMES]
+        self.ic = ic
+        self.s = RadGr(*[x.ctypes.data for x in self.arrs], float(a), float(omega),
+                       C.addressof(ic.s))
+
+
+def gr_rad_params(gr, delta_t, track_percent=0.2, seed=1):
+    rp = rad_params(model=RAD_GR1D, delta_t=delta_t, track_percent=track_percent, seed=seed)
+    rp.gr = C.addressof(gr.s)
+    return rp
 
 
 for _name, _res, _args in [
@@ -65,6 +151,11 @@ for _name, _res, _args in [
                                C.c_uint64, _vp]),
     ("or_produce_pairs", None, [_vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, C.c_uint32,
                                 C.c_uint64, _vp]),
+    ("or_move_photons_gr", None, [_vp, _vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int]),
+    ("or_ic_init", None, [_vp, C.c_double, C.c_double, C.c_double, _vp]),
+    ("or_ic_rate", C.c_float, [_vp, C.c_float]),
+    ("or_gg_rate", C.c_float, [_vp, C.c_float]),
+    ("or_ic_photon_e", C.c_float, [_vp, C.c_float, C.c_float]),
 ]:
     _f = getattr(lib, _name)
     _f.restype = _res
@@ -109,6 +200,11 @@ def move_photons_cart(m, ph, num, dt, periodic):
 def move_photons_logsph(m, rp, ph, num, dt):
     s = photons_struct(ph)
     lib.or_move_photons_logsph(C.byref(m), C.byref(rp), C.byref(s), num, dt)
+
+
+def move_photons_gr(m, gr, ph, num, dt, step, data_interval):
+    s = photons_struct(ph)
+    lib.or_move_photons_gr(C.byref(m), C.byref(gr.s), C.byref(s), num, dt, step, data_interval)
 
 
 def emit_photons(m, rp, p, ptc_num, ph, ph_num, ph_cap, f, photon_produced, call, first_id):

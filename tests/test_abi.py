@@ -44,6 +44,10 @@ def test_struct_layouts_match_header():
     assert C.sizeof(ApParams) == 4 * (1 + 1 + 1 + 3 + 8 + 8 + 2 + 1)
     assert C.sizeof(ApParticles) == 8 * 11
     assert C.sizeof(ApFields) == 16 * (3 * 5 + 8 + 2)
+    from aperture3_b200._lib import ApRadParams, ApSpectrum
+    # model, 10 floats, padding, 3 x uint64, e_min, ic_path, n_gamma, n_ep
+    assert C.sizeof(ApRadParams) == 4 + 40 + 4 + 24 + 16
+    assert C.sizeof(ApSpectrum) == 4 + 20
 
 
 def test_invalid_arguments_are_rejected_without_a_device():
