@@ -410,6 +410,13 @@ class SimData:
               "ap_get_photon_number")
         return int(n.value)
 
+    def photons_modified(self, number: int):
+        """The photon count after the photon arrays were written on the
+        device (slots [0, number) in use)."""
+        if self.photons is None:
+            raise _lib.ApError(1, "photons_modified: no photon storage")
+        self._bind_photons(int(number))
+
     def set_photons(self, host: Dict[str, np.ndarray]):
         """Copies host photon arrays into slots [0, n)."""
         if self.photons is None:

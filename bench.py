@@ -1128,6 +1128,126 @@ def logsph_radiation(args, passes=4):
     }
 
 
+def gr_radiation(passes=4):
+    """The 1D GR lab's radiative transfer: inverse_compton's tables at the
+    reference's default size (n_gamma = n_ep = 600; its user_rt_init
+    spectrum) built on the GPU, against the oracle's sequential C
+    restatement of the reference's host loops on a bounded sample (one
+    host thread, 40 Lorentz factors x 40 energies, scaled by integrand
+    evaluations); then emission and conversion passes on a 16384-cell GR
+    grid with 4 M particles (gamma up to ~1e5) and 2 M photons: device
+    time of each pass (CUDA events), the first pass untimed."""
+    import time as _t
+
+    import numpy as np
+    import torch
+
+    from aperture3_b200 import SimData, SimEnvironment, SimParams, radiative_transfer
+
+    # a synthetic field-line table (the lab reads one from coef.h5), spin
+    # 0.9 and omega 0.2: B^3 / B^1 large enough that u_0 is real everywhere
+    a_s, om = 0.9, 0.2
+    r = np.geomspace(1.15, 14.0, 600)
+    th = 0.3 + 0.2 / r
+    Sg, Dl = r * r + a_s * a_s * np.cos(th) ** 2, r * r - 2 * r + a_s * a_s
+    A = (r * r + a_s * a_s) ** 2 - Dl * a_s * a_s * np.sin(th) ** 2
+    w = 2 * a_s * r / A
+    g11, g33, al2 = Sg / Dl, A * np.sin(th) ** 2 / Sg, Dl * Sg / A
+    b31 = 1.5 * np.sqrt(np.maximum(0.0, g11 * (g33 * (om - w) ** 2 - al2) / (g33 * al2))) + 0.1
+    tab = {k: v.astype(np.float32) for k, v in {
+        "r": r, "B1": 1.0 / r ** 2, "B3": b31 / r ** 2, "jr": 0.5 / r ** 2, "rho": 0.2 / r ** 2,
+        "theta": th, "dpsidth": 0.5 * np.sin(th)}.items()}
+    N, n, n_ph, guard = 16384, 4 << 20, 2 << 20, 3
+    delta = float(np.float32(6.138) / np.float32(N))
+    dt = float(np.float32(0.25 * delta))
+    cap, ph_cap = n + 4 * n_ph + (1 << 20), n_ph + 2 * n + (1 << 20)
+    params = SimParams(N=(N, 1, 1), guard=(3, 0, 0), lower=(-6.273, 0.0, 0.0),
+                       size=(6.138, 1.0, 1.0), delta_t=dt, q_e=1.2, num_species=2,
+                       periodic_boundary=(False, False, False), data_interval=4,
+                       coord_system="1DGR", a=a_s, omega=om, B0=1.0, max_ptc_number=cap,
+                       create_pairs=True, max_photon_number=ph_cap, rad_model="gr1d", rad_seed=3,
+                       e_min=1e-3, ic_path=0.004, n_gamma=600, n_ep=600)
+    env = SimEnvironment(params, gr_table=tab)
+    dev = torch.device("cuda", 0)
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    rt = radiative_transfer(env)  # builds the 600 x 600 tables
+    torch.cuda.synchronize()
+    table_s = _t.perf_counter() - t0
+    # the reference's host loops, sequential, on a sample (the oracle's C
+    # restatement: the CPU baseline of this line)
+    from oracle import rad
+    ng_s, ne_s = 40, 40
+    t0 = _t.perf_counter()
+    rad.IcTables(rad.gr1d_spectrum(1e-3), 1e-10, 0.1, 1.5e24 / 0.004, ng_s, ne_s)
+    cpu_s = _t.perf_counter() - t0
+    evals = lambda ng, ne: ng * 2 * 100 * 800 + 2 * ng * ne * 800  # noqa: E731
+    cpu_full_s = cpu_s * evals(600, 600) / evals(ng_s, ne_s)
+    # a GR state on the device
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    data = SimData(env)
+    dims = N + 2 * guard
+    cells = torch.randint(guard + 2, dims - guard - 2, (n,), generator=g, device=dev)
+    x1 = torch.rand(n, generator=g, device=dev)
+    p1 = 3000.0 * torch.randn(n, generator=g, device=dev)
+    cot = [torch.from_numpy(np.asarray(env.gr_coef(k), np.float32)).to(dev) for k in range(4)]
+    nx = 1.0 - x1
+    it = lambda k: cot[k][cells] * x1 + cot[k][cells - 1] * nx  # noqa: E731
+    D1, D2, D3, al = it(0), it(1), it(2), it(3)
+    u0 = torch.sqrt((D2 + p1 * p1) / (D2 * (al * al - D3) + D1 * D1))
+    ptc = {"x1": x1, "x2": torch.zeros(n, device=dev), "x3": torch.zeros(n, device=dev),
+           "p1": p1, "p2": torch.zeros(n, device=dev), "p3": torch.zeros(n, device=dev),
+           "E": u0, "weight": torch.ones(n, device=dev), "cell": cells,
+           "id": torch.arange(n, device=dev),
+           "flag": (torch.arange(n, device=dev) % 2) << 29}
+    data.set_particles_device(ptc)
+    pc = torch.randint(guard + 2, dims - guard - 2, (n_ph,), generator=g, device=dev)
+    E = torch.exp(np.log(10.0) + torch.rand(n_ph, generator=g, device=dev) * np.log(1e6))
+    phs = {"x1": torch.rand(n_ph, generator=g, device=dev), "p1": E * (2 * torch.rand(
+        n_ph, generator=g, device=dev) - 1), "p3": 0.1 * E * torch.randn(n_ph, generator=g,
+                                                                          device=dev),
+           "E": E, "weight": torch.ones(n_ph, device=dev), "cell": pc,
+           "id": torch.arange(n_ph, device=dev) + (1 << 40)}
+    for k, v in phs.items():
+        dst = data.photons[k][:n_ph]
+        dst.copy_(v.to(dst.dtype) if k not in ("cell", "id") else v.to(torch.int64).to(dst.dtype))
+    data.photons_modified(n_ph)
+    rows = []
+    stream = torch.cuda.Stream()
+    env.set_stream(stream)
+    with torch.cuda.stream(stream):
+        for r in range(passes + 1):
+            n_ptc, n_ph_in = data.number, data.photon_number
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            em = rt.emit_photons(data)
+            e[1].record(stream)
+            pr = rt.produce_pairs(data)
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            data.sort_particles()
+            if r == 0:
+                continue
+            rows.append({"particles": n_ptc, "photons_in": n_ph_in, "emitters": em["marked"],
+                         "written": em["written"], "pairs": pr["written"],
+                         "emit_ms": e[0].elapsed_time(e[1]), "pairs_ms": e[1].elapsed_time(e[2])})
+    env.close()
+    emit_ms = sum(r["emit_ms"] for r in rows) / len(rows)
+    pair_ms = sum(r["pairs_ms"] for r in rows) / len(rows)
+    return {
+        "model": "1D GR lab (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh), "
+                 "IC tables of user_rt_init (broken power law, e_min 1e-3), ic_path 0.004",
+        "ic_tables_600x600_s": table_s,
+        "ic_tables_cpu_sample": {"n_gamma": ng_s, "n_ep": ne_s, "seconds": cpu_s, "threads": 1,
+                                 "kind": "port",
+                                 "projected_600x600_s": cpu_full_s},
+        "passes": rows, "emit_ms": emit_ms, "produce_ms": pair_ms,
+        "emit_particles_per_s": sum(r["particles"] for r in rows) / len(rows) / (emit_ms / 1e3),
+        "produce_photons_per_s": sum(r["photons_in"] for r in rows) / len(rows) / (pair_ms / 1e3),
+    }
+
+
 def run_served(args, emit=True):
     """Served stream of 1D gap runs: `runs` requests with Poisson arrivals
     (50/s), 512-16384 cells, 32-256 particles per cell, 200-5000 steps
@@ -1258,8 +1378,10 @@ def run_extras(args):
     configuration (its own roofline, CPU baseline and e2e), the
     log-spherical grid (throughput at 1024^2 over 20 steps, and the error
     against the FP64 build after 2000 steps on a reduced grid), the batched
-    boxes (24 runs, 20 timed steps) and the served stream (24 requests,
-    p50/p99 completion latency against one at a time)."""
+    boxes (24 runs, 20 timed steps), the served stream (24 requests,
+    p50/p99 completion latency against one at a time) and the 1D GR lab's
+    radiative transfer (inverse-Compton tables, emission and conversion
+    passes)."""
     import copy
     out = {}
     t0 = time.perf_counter()
@@ -1284,6 +1406,7 @@ def run_extras(args):
     asv = copy.copy(a)
     asv.runs, asv.steps_scale, asv.hbm_budget = 24, 1.0, 60.0
     timed("served", lambda: run_served(asv, emit=False))
+    timed("gr_radiation", gr_radiation)
     out["seconds"] = time.perf_counter() - t0
     return out
 

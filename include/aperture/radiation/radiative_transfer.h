@@ -35,6 +35,10 @@ class radiative_transfer {
     rp.seed = p.rad_seed;
     rp.first_photon_id = 1ull << 60;
     rp.first_particle_id = (1ull << 60) + (1ull << 59);
+    rp.e_min = p.e_min;
+    rp.ic_path = p.ic_path;
+    rp.n_gamma = p.n_gamma;
+    rp.n_ep = p.n_ep;
     ap_check(ap_set_rad_params(m_env.ctx(), &rp), "radiative_transfer");
   }
 

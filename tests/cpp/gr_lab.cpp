@@ -2,8 +2,9 @@
 // reference's 1dgr lab uses its algorithm classes (labs/1dgr/src/main.cpp):
 // the field-line table the reference reads from coef.h5 (a synthetic one
 // here), pairs from fill_multiplicity, then update_particles /
-// update_fields with a periodic sort. Exits 0 and prints "gr_lab ok" when
-// the run is healthy.
+// update_fields, the lab's radiative transfer (inverse-Compton emission and
+// gamma-gamma conversion from its tables) and a periodic sort. Exits 0 and
+// prints "gr_lab ok" when the run is healthy.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -11,6 +12,7 @@
 
 #include "aperture/algorithms/field_solver_1dgr.h"
 #include "aperture/algorithms/ptc_updater_1dgr.h"
+#include "aperture/radiation/radiative_transfer.h"
 
 using namespace Aperture;
 
@@ -33,6 +35,13 @@ int main(int argc, char **argv) {
   params.a = 0.99f;
   params.omega = 0.211765f;
   params.periodic_boundary[0] = false;
+  // labs/1dgr/src/main.cpp: radiative_transfer with the lab's functions
+  params.create_pairs = true;
+  params.rad_model = AP_RAD_GR1D;
+  params.max_photon_number = 4096 * 8;
+  params.ic_path = 1.0e-3f;
+  params.n_gamma = 200;
+  params.n_ep = 200;
   // a field-line table: B^3 / B^1 large enough near the horizon that u_0
   // is real everywhere
   const int nt = 600;
@@ -64,21 +73,29 @@ int main(int argc, char **argv) {
     sim_data data(env);
     field_solver_1dgr solver(env);
     ptc_updater_1dgr pusher(env);
+    radiative_transfer rad(env);
     data.E.initialize(0, [](double x, double, double) { return 0.05 * std::sin(3.0 * x); });
     data.fill_multiplicity(1.0f, 2);
     const size_t n0 = data.particles.number();
+    uint64_t emitters = 0;
     for (uint32_t step = 0; step < (uint32_t)steps; ++step) {
-      pusher.update_particles(data, params.delta_t, step);
+      pusher.update_particles(data, params.delta_t, step);  // and the photons
       solver.update_fields(data, params.delta_t, step * params.delta_t);
+      if (params.create_pairs) {
+        rad.emit_photons(data);
+        emitters += rad.last_counts().marked;
+        rad.produce_pairs(data);
+      }
       if (step % params.sort_interval == 0 && step != 0) data.sort_particles();
     }
     ap_diag d{};
     ap_check(ap_diagnostics(env.ctx(), &d), "diagnostics");
     const bool ok = n0 == (size_t)4096 * 4 && data.particles.number() > n0 / 2 &&
                     std::isfinite(d.kinetic) && std::isfinite(d.field_energy) &&
-                    std::isfinite(d.max_abs_j) && d.max_abs_j > 0.0;
-    std::printf("particles %zu of %zu field_energy %.6e max|J| %.6e\n",
-                data.particles.number(), n0, d.field_energy, d.max_abs_j);
+                    std::isfinite(d.max_abs_j) && d.max_abs_j > 0.0 && emitters > 0;
+    std::printf("particles %zu of %zu field_energy %.6e max|J| %.6e emitters %llu\n",
+                data.particles.number(), n0, d.field_energy, d.max_abs_j,
+                (unsigned long long)emitters);
     std::printf(ok ? "gr_lab ok\n" : "gr_lab FAILED\n");
     return ok ? 0 : 1;
   } catch (const ap_error &e) {
