@@ -636,6 +636,8 @@ def load_ref_gr(build=True):
     r.ref_gr_filter.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_int]
     r.ref_gr_update_e.restype = None
     r.ref_gr_update_e.argtypes = [_vp, _vp, _vp, _vp, C.c_float]
+    r.ref_gr_move_photons.restype = None
+    r.ref_gr_move_photons.argtypes = [_vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int, _vp]
     ref_gr = r
     return ref_gr
 

@@ -3,7 +3,8 @@
 Wraps ``ap_rad.c`` of ``liboracle.so`` (the restatement of the photon movers
 and of ``radiative_transfer`` with the default, the pulsar lab's and the 1D
 GR lab's user radiative functions), ``ap_ic.c`` (the inverse-Compton tables
-of ``src/cuda/radiation/rt_ic.cu``) and the pin library ``_ref/libapref_rad.so`` that runs
+of ``src/cuda/radiation/rt_ic.cu``), the pin library ``_ref/libapref_rad_gr.so``
+that runs the 1D GR lab's own user radiative functions on the host and the pin library ``_ref/libapref_rad.so`` that runs
 the reference's own user functions on the host (built by
 ``ref_build/Makefile`` when the reference tree is present), plus the photon
 movers of ``_ref/libapref.so`` and ``_ref/libapref_ls.so``.
@@ -301,3 +302,57 @@ def ref_move_photons_logsph(m, r_cutoff, ph, num, dt):
 
 def ref_available():
     return (ref_tree_present() or os.path.exists(_REF_PATH)) and load_ref() is not None
+
+
+_REF_GR_PATH = os.path.join(_HERE, "_ref", "libapref_rad_gr.so")
+ref_gr = None
+
+
+def load_ref_gr(build=True):
+    """The 1D GR lab's own user radiative functions on the host (with the
+    oracle's inverse-Compton lookups), or None."""
+    global ref_gr
+    if ref_gr is not None:
+        return ref_gr
+    if not os.path.exists(_REF_GR_PATH) and build and ref_tree_present():
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_rad_gr.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_GR_PATH):
+        return None
+    r = C.CDLL(_REF_GR_PATH)
+    r.ref_gr_emit_photons.restype = C.c_int
+    r.ref_gr_emit_photons.argtypes = [_vp, _vp, C.c_float, C.c_float, _vp, _sz, _vp, _vp, _sz,
+                                      _vp, C.c_uint64, _vp]
+    r.ref_gr_produce_pairs.restype = C.c_int
+    r.ref_gr_produce_pairs.argtypes = [_vp, _vp, C.c_float, C.c_float, _vp, _sz, _vp, _vp, _sz,
+                                       _vp, C.c_uint64, _vp]
+    ref_gr = r
+    return ref_gr
+
+
+def ref_gr_emit_photons(m, rp, p, ptc_num, ph, ph_num, ph_cap, call, first_id):
+    """The lab's check_emit_photon / emit_photon in the build's pass;
+    rp is gr_rad_params(...). Returns (new photon number, RadCounts)."""
+    u4 = uniforms(rp.seed, 1, call, p["id"][:ptc_num])
+    sp, sph = ptc_struct(p), photons_struct(ph)
+    n = C.c_size_t(ph_num)
+    cnt = RadCounts()
+    rc = load_ref_gr().ref_gr_emit_photons(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
+                                           C.byref(sp), ptc_num, C.byref(sph), C.byref(n),
+                                           ph_cap, _p(u4), first_id, C.byref(cnt))
+    assert rc == 0, "a user function drew more uniforms than the build gives it"
+    return n.value, cnt
+
+
+def ref_gr_produce_pairs(m, rp, ph, ph_num, p, ptc_num, ptc_cap, call, first_id):
+    u4 = uniforms(rp.seed, 2, call, ph["id"][:ph_num])
+    sp, sph = ptc_struct(p), photons_struct(ph)
+    n = C.c_size_t(ptc_num)
+    cnt = RadCounts()
+    rc = load_ref_gr().ref_gr_produce_pairs(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
+                                            C.byref(sph), ph_num, C.byref(sp), C.byref(n),
+                                            ptc_cap, _p(u4), first_id, C.byref(cnt))
+    assert rc == 0, "a user function drew more uniforms than the build gives it"
+    return n.value, cnt

@@ -2,8 +2,8 @@
  * Oracle pin build (TEST INFRASTRUCTURE ONLY): the 1D GR lab's kernels and
  * its coefficient computation run on the host.
  *
- * The Makefile copies update_ptc_1dgr and filter_current1d from
- * src/cuda/algorithms/ptc_updater_1dgr.cu and update_e_1dgr from
+ * The Makefile copies update_ptc_1dgr, filter_current1d and
+ * update_photon_1dgr from src/cuda/algorithms/ptc_updater_1dgr.cu and update_e_1dgr from
  * field_solver_1dgr.cu into oracle/_ref/ (extract_kernels.py; the rest of
  * that Kernels namespace draws its initial conditions from cuRAND) and
  * includes them unmodified behind the host stand-ins of shim/.
@@ -164,6 +164,30 @@ void ref_gr_update_e(const ref_mesh *m, float *E1, float *J1, const float *const
   set_mesh(dev_mesh, m);
   one_thread();
   Kernels::update_e_1dgr(pp(E1, m), pp(E1, m), pp(J1, m), mesh_ptrs_of(co), dt);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* Same layout as or_photons (oracle/ap_rad.h). */
+typedef struct {
+  float *x1, *x2, *x3, *p1, *p2, *p3, *E, *weight, *path_left;
+  uint32_t *cell; uint64_t *id; uint32_t *flag;
+} ref_photons;
+
+/* update_photon_1dgr (ptc_updater_1dgr.cu:301-400) as one thread. */
+void ref_gr_move_photons(const ref_mesh *m, const ref_photons *ph, size_t num, float dt,
+                         uint32_t step, int data_interval, const float *const co[15]) {
+  set_mesh(dev_mesh, m);
+  dev_params.data_interval = data_interval;
+  photon_data d;
+  d.x1 = ph->x1; d.x2 = ph->x2; d.x3 = ph->x3;
+  d.p1 = ph->p1; d.p2 = ph->p2; d.p3 = ph->p3;
+  d.E = ph->E; d.weight = ph->weight; d.path_left = ph->path_left;
+  d.cell = ph->cell; d.id = ph->id; d.flag = ph->flag;
+  one_thread();
+  Kernels::update_photon_1dgr(d, num, mesh_ptrs_of(co), dt, step);
 }
 
 }  // extern "C"
