@@ -11,10 +11,13 @@
  * -ffp-contract=off. The library computes the same sums on the GPU with
  * CUDA's functions, so the two agree to the last bits of those functions.
  *
- * Parity unpinned: the reference's init is host code in a .cu file that
- * needs its CUDA array classes and launches kernels, so it is not built
- * here; this restatement is checked by the properties of the tables
- * (tests/test_ic_oracle.py) and against the library.
+ * Pinned: oracle/ref_build compiles the reference's own integrands and
+ * inverse_compton::init for the host (libapref_ic.so, with the
+ * constructor's few grid lines restated around them), and
+ * tests/test_ic_oracle.py requires every table entry to be equal bit for
+ * bit for each spectrum; the lookups are pinned through the 1D GR pin
+ * (tests/test_rad_gr_pin.py), which runs the reference's own find_ic_rate,
+ * find_gg_rate and gen_photon_e.
  */
 #include "ap_ic.h"
 

@@ -356,3 +356,42 @@ def ref_gr_produce_pairs(m, rp, ph, ph_num, p, ptc_num, ptc_cap, call, first_id)
                                             ptc_cap, _p(u4), first_id, C.byref(cnt))
     assert rc == 0, "a user function drew more uniforms than the build gives it"
     return n.value, cnt
+
+
+_REF_IC_PATH = os.path.join(_HERE, "_ref", "libapref_ic.so")
+ref_ic = None
+
+
+def load_ref_ic(build=True):
+    """The reference's own inverse_compton::init on the host, or None."""
+    global ref_ic
+    if ref_ic is not None:
+        return ref_ic
+    if not os.path.exists(_REF_IC_PATH) and build and ref_tree_present():
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_ic.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_IC_PATH):
+        return None
+    r = C.CDLL(_REF_IC_PATH)
+    r.ref_ic_init.restype = C.c_int
+    r.ref_ic_init.argtypes = [C.c_int, _vp, C.c_float, C.c_float, C.c_double, C.c_int, C.c_int,
+                              _vp, _vp, _vp, _vp, _vp, _vp]
+    ref_ic = r
+    return ref_ic
+
+
+def ref_ic_tables(spec, emin, emax, n0, n_gamma, n_ep):
+    """The tables of the reference's inverse_compton::init, as a dict."""
+    out = {k: np.zeros(n_gamma, np.float32) for k in ("ic_rate", "gg_rate", "gammas")}
+    out.update({k: np.zeros((n_gamma, n_ep), np.float32) for k in ("dNde", "dNde_thomson")})
+    steps = np.zeros(3, np.float32)
+    p = np.array(list(spec.p), np.float32)
+    rc = load_ref_ic().ref_ic_init(spec.kind, p.ctypes.data, float(emin), float(emax), float(n0),
+                                   n_gamma, n_ep, *[out[k].ctypes.data for k in (
+                                       "ic_rate", "gg_rate", "gammas", "dNde", "dNde_thomson")],
+                                   steps.ctypes.data)
+    assert rc == 0
+    out["dep"], out["dg"], out["dlep"] = steps
+    return out

@@ -1,7 +1,9 @@
-"""Oracle pin build helper: copies the named __global__ / HD functions of a
-reference source file (verbatim, in file order) into an include file under
-oracle/_ref/. Used for files whose Kernels namespace also holds code that
-does not build on the host (curand initial conditions)."""
+"""Oracle pin build helper: copies the named __global__ / __device__ /
+HD_INLINE / HOST_DEVICE functions of a reference source file (verbatim, in file order)
+into an include file under oracle/_ref/, and member-function templates
+named Class::member (from their "template <...>" line). Used for files
+whose other code does not build on the host (curand initial conditions,
+kernel launches, device arrays)."""
 import re
 import sys
 
@@ -16,8 +18,12 @@ def extract(src, names):
         # a definition starts with a qualifier line followed by "name(" or
         # with "qualifier type name(" on one line
         head = "".join(lines[i:i + 2])
-        m = re.match(r"\s*(__global__|HD_INLINE)\b[^\n]*\n?\s*([A-Za-z_]\w*)\s*\(", head)
-        if m and m.group(2) in names:
+        m = re.match(r"\s*(__global__|__device__|HD_INLINE|HOST_DEVICE)\b[^\n]*\n?\s*([A-Za-z_]\w*)\s*\(",
+                     head)
+        head3 = "".join(lines[i:i + 3])
+        mt = re.match(r"\s*template\s*<[^>]*>\s*\n\s*\w+\s*\n\s*([A-Za-z_]\w*::[A-Za-z_]\w*)\s*\(",
+                      head3)
+        if (m and m.group(2) in names) or (mt and mt.group(1) in names):
             depth, j, started = 0, i, False
             while j < len(lines):
                 code = lines[j].split("//", 1)[0]  # braces in comments do not count
@@ -36,7 +42,7 @@ def extract(src, names):
 if __name__ == "__main__":
     src, dst, names = sys.argv[1], sys.argv[2], set(sys.argv[3:])
     body = extract(src, names)
-    found = set(re.findall(r"\b(" + "|".join(names) + r")\s*\(", body))
+    found = set(re.findall(r"(" + "|".join(re.escape(n) for n in names) + r")\s*\(", body))
     missing = names - found
     if missing:
         sys.exit(f"not found in {src}: {sorted(missing)}")

@@ -6,18 +6,20 @@
  * unmodified behind shim_rgr/ (CudaRng with its m_local_state, a no-op
  * inverse_compton for user_rt_init, which the pin never calls) and the
  * 1D GR shims; src/grids/grid_1dgr.cpp is the second translation unit, as
- * in the GR pin. The functions' inverse-Compton lookups (find_ic_rate,
- * find_gg_rate, gen_photon_e, declared in src/cuda/radiation/rt_ic_dev.h)
- * are served by the oracle's restatement (oracle/ap_ic.c) on the tables
- * the driver is given, with gen_photon_e drawing from the same queue of
- * uniforms as CudaRng. So this pins the user functions; the tables and
- * lookups are the oracle's.
+ * in the GR pin. The functions' inverse-Compton lookups are the reference's
+ * own device functions (find_n_gamma, binary_search, gen_photon_e,
+ * find_ic_rate, find_gg_rate, copied from src/cuda/radiation/rt_ic.cu into
+ * oracle/_ref/ic_dev.inc by the Makefile), reading the tables the driver is
+ * given (the oracle's, which tests/test_ic_oracle.py pins bit for bit to
+ * the reference's own inverse_compton::init) through host stand-ins for
+ * their __constant__ symbols; gen_photon_e draws from the same queue of
+ * uniforms as CudaRng.
  *
  * The drivers restate the passes of radiative_transfer.cu as the rad pin
  * does (ref_rad_shim.cpp), with the build's draw order: emission test u0,
  * photon energy u1, tracking u2; conversion test u1, tracking u0.
  */
-#include "ls_host_math.h"
+#include "rgr_host_math.h"
 #include "cuda_builtins_host.h"
 #include "core/constant_defs.h"
 #include "core/typedefs.h"
@@ -60,14 +62,19 @@ int ap_ref_rng_underflow = 0;
 #include "cuda/cudarng.h"
 #include "grids/grid_1dgr.h"
 
+#include "cuda/radiation/rt_ic_dev.h"
+
+#define MIN_GAMMA 1.01f  /* rt_ic.cu:14-18 */
+#define MAX_GAMMA 1.0e15
+#define MIN_EP 1.0e-10
+
 namespace Aperture {
 namespace Kernels {
-static const or_ic_tables *g_ic = nullptr;
-Scalar find_ic_rate(Scalar gamma) { return or_ic_rate(g_ic, gamma); }
-Scalar find_gg_rate(Scalar eph) { return or_gg_rate(g_ic, eph); }
-Scalar gen_photon_e(Scalar gamma, curandState *) {
-  return or_ic_photon_e(g_ic, gamma, ap_ref_next_uniform());
-}
+/* host stand-ins for rt_ic.cu's __constant__ table symbols */
+Scalar dev_ic_dep, dev_ic_dg, dev_ic_dlep;
+cudaPitchedPtr dev_ic_dNde, dev_ic_dNde_thomson;
+Scalar *dev_ic_rate, *dev_gg_rate, *dev_gammas;
+#include "ic_dev.inc"
 }  // namespace Kernels
 }  // namespace Aperture
 
@@ -138,7 +145,22 @@ static void set_state(const ref_mesh *m, const ref_gr *g, float delta_t, float t
   mp.gamma_ff = g->gamma_ff;
   mp.beta_phi = g->beta_phi;
   mp.theta = g->theta;
-  Kernels::g_ic = g->ic;
+  const or_ic_tables *t = g->ic;
+  dev_params.n_gamma = t->n_gamma;
+  Kernels::dev_ic_dep = t->dep;
+  Kernels::dev_ic_dg = t->dg;
+  Kernels::dev_ic_dlep = t->dlep;
+  Kernels::dev_ic_rate = t->ic_rate;
+  Kernels::dev_gg_rate = t->gg_rate;
+  Kernels::dev_gammas = t->gammas;
+  /* multi_array<Scalar> rows of n_ep entries (get_cudaPitchedPtr; the
+     reference's binary_search takes xsize as the entry count) */
+  Kernels::dev_ic_dNde.ptr = t->dNde;
+  Kernels::dev_ic_dNde.pitch = (size_t)t->n_ep * sizeof(float);
+  Kernels::dev_ic_dNde.xsize = (size_t)t->n_ep;
+  Kernels::dev_ic_dNde.ysize = (size_t)t->n_gamma;
+  Kernels::dev_ic_dNde_thomson = Kernels::dev_ic_dNde;
+  Kernels::dev_ic_dNde_thomson.ptr = t->dNde_thomson;
   Kernels::ap_ref_rng_underflow = 0;
 }
 

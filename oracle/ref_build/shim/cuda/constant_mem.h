@@ -18,6 +18,7 @@ struct ap_ref_params {
   /* radiative transfer (user_radiative_functions.cu of src/ and of the
    * pulsar lab) */
   float delta_t, gamma_thr, E_secondary, photon_path, l_curv, e_curv, BQ;
+  int n_gamma;  /* inverse-Compton table size (rt_ic.cu find_n_gamma) */
 };
 extern Quadmesh dev_mesh;
 extern ap_ref_params dev_params;

@@ -1,2 +1,2 @@
-/* Oracle pin build: curandState and curand_uniform come from ls_host_math.h. */
-#include "ls_host_math.h"
+/* Oracle pin build: curandState and curand_uniform come from rgr_host_math.h. */
+#include "rgr_host_math.h"

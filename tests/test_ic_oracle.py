@@ -1,9 +1,7 @@
-"""The inverse-Compton oracle (oracle/ap_ic.c) against properties of the
-tables that inverse_compton::init builds (src/cuda/radiation/rt_ic.cu) and
-of the lookups that sample them. The reference's init is host code inside
-a .cu file that needs its CUDA array classes, so it is not built here; the
-restatement is checked by these properties and, on the GPU, against the
-library (tests/test_gpu_rad_gr.py)."""
+"""The inverse-Compton oracle (oracle/ap_ic.c) pinned bit for bit to the
+reference's own inverse_compton::init (src/cuda/radiation/rt_ic.cu,
+compiled for the host by oracle/ref_build as libapref_ic.so), and checked
+against properties of the tables and of the lookups that sample them."""
 import math
 
 import numpy as np
@@ -85,3 +83,29 @@ def test_spectra():
     e = 2e-4
     kT = float(np.float32(1e-4))
     assert abs(ne(bb, e) - 1.75464e30 * e * e / math.expm1(e / kT)) < 1e-12 * ne(bb, e)
+
+
+SPECTRA = [
+    (rad.SPEC_BROKEN_POWER_LAW, (1.25, 1.1, 1e-3, 1e-10, 0.1), 1e-10, 0.1, 1.5e24),
+    (rad.SPEC_BLACK_BODY, (3e-6,), 3e-16, 3e-3, 1e-6),
+    (rad.SPEC_POWER_LAW_HARD, (0.5, 1e-6, 1e-2), 1e-6, 1e-2, 1e20),
+    (rad.SPEC_POWER_LAW_SOFT, (2.0, 1e-6, 1e-2), 1e-6, 1e-2, 1e20),
+    (rad.SPEC_MONO_ENERGETIC, (1e-3, 1e-4), 1e-5, 1e-1, 1e18),
+]
+
+
+@pytest.mark.skipif(rad.load_ref_ic() is None, reason="reference tree not present")
+@pytest.mark.parametrize("kind,p,emin,emax,n0", SPECTRA)
+def test_tables_bit_exact_against_reference(kind, p, emin, emax, n0):
+    """Every table entry and step of the oracle equals the reference's own
+    init on the same grid, for each of its spectra."""
+    ng, ne = 24, 20
+    spec = rad.spectrum(kind, *p)
+    ref = rad.ref_ic_tables(spec, emin, emax, n0, ng, ne)
+    got = rad.IcTables(spec, emin, emax, n0, ng, ne)
+    for k in ("dep", "dg", "dlep"):
+        assert np.float32(getattr(got, k)) == np.float32(ref[k]), k
+    for k in ("ic_rate", "gg_rate", "gammas", "dNde", "dNde_thomson"):
+        a, b = getattr(got, k), ref[k]
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (k, np.flatnonzero(
+            a.view(np.uint32).ravel() != b.view(np.uint32).ravel())[:5])

@@ -1,10 +1,11 @@
 """The oracle's 1D GR radiative transfer (oracle/ap_rad.c, model GR1D) pinned
 bit for bit to the 1D GR lab's own user radiative functions
 (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh), compiled for
-the host by oracle/ref_build (libapref_rad_gr.so). Both sides use the
-oracle's inverse-Compton tables and lookups (oracle/ap_ic.c, unpinned), so
-this pins the functions' metric interpolation, energy loss, photon and pair
-momenta, flags and the draw order. The oracle's GR photon mover is pinned
+the host by oracle/ref_build (libapref_rad_gr.so) together with the
+reference's own inverse-Compton lookups (find_ic_rate, find_gg_rate,
+gen_photon_e of rt_ic.cu) on the oracle's tables (pinned to the reference's
+init by tests/test_ic_oracle.py): this pins the oracle's lookups, metric
+interpolation, energy loss, photon and pair momenta, flags and draw order. The oracle's GR photon mover is pinned
 to the reference's update_photon_1dgr (ptc_updater_1dgr.cu:301-400), which
 the 1D GR pin library (libapref_gr.so) compiles for the host."""
 import numpy as np
