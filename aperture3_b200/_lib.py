@@ -156,7 +156,7 @@ class ApRadCounts(C.Structure):
     _fields_ = [("marked", C.c_uint64), ("written", C.c_uint64), ("dropped", C.c_uint64)]
 
 
-RAD_DEFAULT, RAD_PULSAR, RAD_GR1D = 0, 1, 2
+RAD_DEFAULT, RAD_PULSAR, RAD_GR1D, RAD_GAP1D = 0, 1, 2, 3
 SPEC_POWER_LAW_HARD, SPEC_POWER_LAW_SOFT, SPEC_BROKEN_POWER_LAW = 0, 1, 2
 SPEC_BLACK_BODY, SPEC_MONO_ENERGETIC = 3, 4
 

@@ -473,10 +473,12 @@ namespace apb {
 
 // ptc_updater_1dgap::update_particles (ptc_updater_1dgap.cu:219-272).
 int update_particles_gap(Ctx *c, double dt, uint32_t step) {
-  (void)step;
   const ap_params &pr = c->params;
-  // the reference does nothing at all without particles (:226)
-  if (c->number == 0) return finish(c);
+  // without particles nothing but the photons moves (:226, :272-278)
+  if (c->number == 0) {
+    if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt, step));
+    return finish(c);
+  }
   const int ncomp = 3 + pr.num_species;
   const int n = c->mesh.dims[0];
   const int bl = !pr.periodic[0], bu = !pr.periodic[0];  // is_boundary(0), (1)
@@ -538,6 +540,8 @@ int update_particles_gap(Ctx *c, double dt, uint32_t step) {
   }
   c->rho_is_zero = false;
   phase_end(c, ph);
+  // the photons after the particles (:272-278)
+  if (c->ph_bound) AP_TRY_ST(rad_move_photons(*c, (float)dt, step));
   return finish(c);
 }
 
@@ -1255,7 +1259,6 @@ AP_API int ap_inject_pairs(ap_ctx *c, double dt, uint32_t step, uint64_t *emitte
 
 AP_API int ap_bind_photons(ap_ctx *c, const ap_photons *ph, size_t number, size_t capacity) {
   if (!c || !ph) return AP_ERR_INVALID;
-  if (c->coord != 0 && c->coord != 1 && c->coord != 3) return fail(c, AP_ERR_UNSUPPORTED);
   if (number > capacity || capacity >= (size_t)UINT32_MAX) return fail(c, AP_ERR_CAPACITY);
   if (!ph->x1 || !ph->x2 || !ph->x3 || !ph->p1 || !ph->p2 || !ph->p3 || !ph->E ||
       !ph->weight || !ph->path_left || !ph->cell || !ph->id || !ph->flag)
@@ -1275,7 +1278,8 @@ AP_API int ap_get_photon_number(const ap_ctx *c, size_t *n) {
 
 AP_API int ap_set_rad_params(ap_ctx *c, const ap_rad_params *rp) {
   if (!c || !rp) return AP_ERR_INVALID;
-  if (rp->model != AP_RAD_DEFAULT && rp->model != AP_RAD_PULSAR && rp->model != AP_RAD_GR1D)
+  if (rp->model != AP_RAD_DEFAULT && rp->model != AP_RAD_PULSAR && rp->model != AP_RAD_GR1D &&
+      rp->model != AP_RAD_GAP1D)
     return fail(c, AP_ERR_INVALID);
   // the pulsar lab's functions read (ln r, theta) positions and Rho[0], Rho[1]
   if (rp->model == AP_RAD_PULSAR && (c->coord != 1 || c->params.num_species < 2))
@@ -1283,11 +1287,13 @@ AP_API int ap_set_rad_params(ap_ctx *c, const ap_rad_params *rp) {
   // the 1D GR lab's read Grid_1dGR's arrays; its photons move with the GR
   // mover, the others' with the Cartesian or log-spherical one
   if ((rp->model == AP_RAD_GR1D) != (c->coord == 3)) return fail(c, AP_ERR_UNSUPPORTED);
-  if (c->coord != 0 && c->coord != 1 && c->coord != 3) return fail(c, AP_ERR_UNSUPPORTED);
-  if (rp->model == AP_RAD_GR1D) {
-    // user_rt_init (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh:
-    // 191-203): broken_power_law(1.25, 1.1, e_min, 1e-10, 0.1) over
-    // [emin(), emax()] with n0 = 1.5e24 / ic_path
+  // the 1D gap lab's functions, with its photon mover, on a 1D gap context
+  if ((rp->model == AP_RAD_GAP1D) != (c->coord == 2)) return fail(c, AP_ERR_UNSUPPORTED);
+  if (rp->model == AP_RAD_GR1D || rp->model == AP_RAD_GAP1D) {
+    // user_rt_init of either lab (labs/1dgr/src/cuda/radiation/
+    // user_radiative_functions.cuh:191-203, labs/1dgap/...:135-144):
+    // broken_power_law(1.25, 1.1, e_min, 1e-10, 0.1) over [emin(), emax()]
+    // with n0 = 1.5e24 / ic_path
     if (!(rp->ic_path > 0.0f) || !(rp->e_min > 0.0f)) return fail(c, AP_ERR_INVALID);
     ap_spectrum sp{};
     sp.kind = AP_SPEC_BROKEN_POWER_LAW;

@@ -51,6 +51,7 @@ struct RadK {
   const float *alpha, *D1, *D2, *D3, *B3B1, *grr, *gff, *beta_phi;
   float a, gr_omega;
   IcK ic;
+  float e_min;  // 1D gap model: photons below 0.001 / e_min are not kept
 };
 
 // The four uniforms in (0, 1] of one particle (tag 1) or photon (tag 2):
@@ -205,12 +206,73 @@ __device__ void produce_pair_gr(const RadK &K, const PhK &ph, size_t tid, const 
   }
 }
 
+// ---- The 1D gap lab's functions (labs/1dgap/src/cuda/radiation/
+// user_radiative_functions.cuh:17-131): the same tables on a flat line.
+// Draws: u0 the emission / conversion test, u1 the photon energy.
+__device__ __forceinline__ bool check_emit_gap(const RadK &K, const PtcK &p, size_t tid,
+                                               const float u[4]) {
+  return u[0] < ic_rate(K.ic, p.E[tid]) * K.delta_t;
+}
+
+__device__ void emit_photon_gap(const RadK &K, const PtcK &p, size_t tid, const PhK &ph,
+                                size_t off, const float u[4]) {
+  const float x1 = p.x1[tid], p1 = p.p1[tid];
+  const uint32_t c = p.cell[tid];
+  const float gamma = p.E[tid];
+  float Eph = ic_photon_e(K.ic, gamma, u[1]);
+  if (Eph >= gamma - 1.01f) Eph = gamma - 1.01f;
+  const float En = gamma - Eph;
+  p.E[tid] = En;
+  float np1 = En * p1 / gamma;
+  if (np1 != np1) np1 = 0.0f;
+  p.p1[tid] = np1;
+  if (fabsf(Eph) < 0.001f / K.e_min) return;  // the energy is taken, no photon kept
+  ph.x1[off] = x1;
+  ph.x2[off] = ph.x3[off] = 0.0f;
+  ph.p1[off] = sgnf(p1) * Eph;
+  ph.p2[off] = ph.p3[off] = 0.0f;
+  ph.E[off] = Eph;
+  ph.w[off] = p.w[tid];
+  ph.path[off] = 0.0f;
+  ph.cell[off] = c;
+}
+
+__device__ __forceinline__ bool check_pair_gap(const RadK &K, const PhK &ph, size_t tid,
+                                               const float u[4]) {
+  return u[1] < gg_rate(K.ic, ph.E[tid]) * K.delta_t;
+}
+
+__device__ void produce_pair_gap(const RadK &K, const PhK &ph, size_t tid, const PtcK &p,
+                                 size_t off) {
+  const float Eph = fabsf(ph.p1[tid]);
+  const uint32_t c = ph.cell[tid];
+  const float x1 = ph.x1[tid];
+  ph.cell[tid] = AP_MAX_CELL;
+  float p1 = sgnf(ph.p1[tid]) * sqrtf(0.25f * Eph * Eph - 1.0f);
+  if (p1 != p1) p1 = 0.0f;
+  const float beta = mpos(K.m, 0, c1_of(K.m, c), x1);
+  const float E = sqrtf(1.0f + p1 * p1 + beta * beta);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const size_t o = off + (size_t)k;
+    p.x1[o] = x1;
+    p.x2[o] = p.x3[o] = 0.0f;
+    p.p1[o] = p1;
+    p.p2[o] = p.p3[o] = 0.0f;
+    p.E[o] = E;
+    p.w[o] = ph.w[tid];
+    p.cell[o] = c;
+    p.flag[o] = kSecondary | ((uint32_t)k << 29);
+  }
+}
+
 // check_emit_photon (default :13-17; pulsar :26-53).
 __device__ bool check_emit(const RadK &K, const PtcK &p, size_t tid, uint32_t cell,
                            const float u[4]) {
   const float gamma = p.E[tid];
   if (K.model == AP_RAD_DEFAULT) return gamma > K.gamma_thr;
   if (K.model == AP_RAD_GR1D) return check_emit_gr(K, p, tid, cell, u);
+  if (K.model == AP_RAD_GAP1D) return check_emit_gap(K, p, tid, u);
   const int c1 = c1_of(K.m, cell), c2 = c2_of(K.m, cell);
   const float r = expf(mpos(K.m, 0, c1, p.x1[tid]));
   if (r > 0.6f / K.omega) return false;
@@ -229,6 +291,10 @@ __device__ void emit_photon(const RadK &K, const PtcK &p, size_t tid, const PhK 
                             const float u[4]) {
   if (K.model == AP_RAD_GR1D) {
     emit_photon_gr(K, p, tid, ph, off, u);
+    return;
+  }
+  if (K.model == AP_RAD_GAP1D) {
+    emit_photon_gap(K, p, tid, ph, off, u);
     return;
   }
   const uint32_t c = p.cell[tid];
@@ -505,10 +571,11 @@ __global__ void __launch_bounds__(kRadThreads)
       if (idx < number) {
         cell = ph.cell[idx];
         if (cell != AP_MAX_CELL && in_bulk(K.m, cell)) {
-          if (K.model == AP_RAD_GR1D) {
+          if (K.model == AP_RAD_GR1D || K.model == AP_RAD_GAP1D) {
             float u[4];
             uniforms(K, 2u, ph.id[idx], u);
-            e = check_pair_gr(K, ph, idx, cell, u);
+            e = K.model == AP_RAD_GR1D ? check_pair_gr(K, ph, idx, cell, u)
+                                       : check_pair_gap(K, ph, idx, u);
           } else {
             e = check_pair(K, ph, idx, cell);
           }
@@ -546,6 +613,8 @@ __global__ void __launch_bounds__(kRadThreads)
       p.flag[off] = p.flag[off + 1] = 0u;
       if (K.model == AP_RAD_GR1D)
         produce_pair_gr(K, ph, idx, p, off);
+      else if (K.model == AP_RAD_GAP1D)
+        produce_pair_gap(K, ph, idx, p, off);
       else
         produce_pair(ph, idx, p, off);
       const bool tracked = u[0] < K.track_percent;
@@ -668,6 +737,26 @@ __global__ void k_rad_move_gr(MeshK m, PhK ph, size_t num, GrPhK G) {
   }
 }
 
+// update_photon_1dgap (ptc_updater_1dgap.cu:163-192): photons outside the
+// bulk are removed, the others move one light step along the sign of p1.
+__global__ void k_rad_move_gap(MeshK m, PhK ph, size_t num, float dt) {
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < num;
+       idx += (size_t)blockDim.x * gridDim.x) {
+    const uint32_t c = ph.cell[idx];
+    if (c == AP_MAX_CELL) continue;
+    if (!in_bulk(m, c)) {
+      ph.cell[idx] = AP_MAX_CELL;
+      continue;
+    }
+    const float p1 = ph.p1[idx], x1 = ph.x1[idx];
+    float new_x1 = x1 + sgnf(p1) * dt * m.inv_delta[0];
+    const int dc1 = (int)floorf(new_x1);
+    new_x1 -= (float)dc1;
+    ph.cell[idx] = c + (uint32_t)dc1;
+    ph.x1[idx] = new_x1;
+  }
+}
+
 // move_photons (ptc_updater_logsph.cu:58-131), then send_particles and
 // clear_guard_cells: photons outside the bulk are removed. The cell is
 // taken before the axis reflection, as the reference does.
@@ -768,6 +857,7 @@ RadK radk_of(const Ctx &c, ap_array produced, uint32_t call) {
   K.alpha = K.D1 = K.D2 = K.D3 = K.B3B1 = K.grr = K.gff = K.beta_phi = nullptr;
   K.a = K.gr_omega = 0.0f;
   K.ic = IcK{};
+  K.e_min = c.rad.e_min;
   if (c.coord == 3) {
     K.alpha = coef_array(c, AP_GR_ALPHA).ptr;
     K.D1 = coef_array(c, AP_GR_D1).ptr;
@@ -843,6 +933,8 @@ int rad_move_photons(Ctx &c, float dt, uint32_t step) {
     G.step = step;
     G.data_interval = (uint32_t)c.params.data_interval;
     k_rad_move_gr<<<grid, 256, 0, c.stream>>>(c.mk, phk_of(c), c.ph_number, G);
+  } else if (c.coord == 2) {
+    k_rad_move_gap<<<grid, 256, 0, c.stream>>>(c.mk, phk_of(c), c.ph_number, dt);
   } else if (c.coord == 1)
     k_rad_move_logsph<<<grid, 256, 0, c.stream>>>(c.mk, phk_of(c), c.ph_number, dt,
                                                     c.rad.r_cutoff);

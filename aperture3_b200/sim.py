@@ -79,10 +79,10 @@ class SimParams:
     a: float = 0.0
     # photons and pair production (src/sim_params.h:23, 50-88); rad_model
     # selects the user radiative functions: "default" (src/cuda/radiation/
-    # user_radiative_functions.cu), "pulsar" (the pulsar lab's) or "gr1d"
-    # (the 1D GR lab's, with the inverse-Compton tables of e_min, ic_path,
-    # n_gamma, n_ep); rad_seed keys the counter-based random stream that
-    # replaces cuRAND
+    # user_radiative_functions.cu), "pulsar" (the pulsar lab's), "gr1d" (the
+    # 1D GR lab's) or "gap1d" (the 1D gap lab's), the last two with the
+    # inverse-Compton tables of e_min, ic_path, n_gamma, n_ep; rad_seed keys
+    # the counter-based random stream that replaces cuRAND
     max_photon_number: int = 100
     create_pairs: bool = False
     gamma_thr: float = 20.0
@@ -875,12 +875,13 @@ class radiative_transfer:
     """radiative_transfer (src/radiation/radiative_transfer.h:11-29): photon
     emission and pair production with the user radiative functions that
     SimParams.rad_model names ("default": src/cuda/radiation/
-    user_radiative_functions.cu; "pulsar": the pulsar lab's; "gr1d": the 1D
-    GR lab's, whose inverse-Compton tables are built here as its
-    user_rt_init builds them). The photon move itself is part of
+    user_radiative_functions.cu; "pulsar": the pulsar lab's; "gr1d" and
+    "gap1d": the 1D GR and gap labs', whose inverse-Compton tables are built
+    here as their user_rt_init builds them). The photon move itself is part of
     update_particles, as in the reference."""
 
-    MODELS = {"default": _lib.RAD_DEFAULT, "pulsar": _lib.RAD_PULSAR, "gr1d": _lib.RAD_GR1D}
+    MODELS = {"default": _lib.RAD_DEFAULT, "pulsar": _lib.RAD_PULSAR, "gr1d": _lib.RAD_GR1D,
+              "gap1d": _lib.RAD_GAP1D}
 
     def __init__(self, env: SimEnvironment, first_photon_id: int = 1 << 60,
                  first_particle_id: int = (1 << 60) + (1 << 59)):

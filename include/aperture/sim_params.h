@@ -50,16 +50,16 @@ struct SimParams {
   float r_cutoff = 4.0;
   float l_curv = 6.0;
   float e_curv = 6.4e-9;
-  // background photons and table sizes of the 1D GR lab's inverse-Compton
-  // tables (src/sim_params.h:69-88)
+  // background photons and table sizes of the 1D GR and gap labs'
+  // inverse-Compton tables (src/sim_params.h:69-88)
   float e_min = 1.0e-3;
   float ic_path = 1.0;
   int n_gamma = 600;
   int n_ep = 600;
   // which user radiative functions (AP_RAD_DEFAULT: src/cuda/radiation/
   // user_radiative_functions.cu; AP_RAD_PULSAR: the pulsar lab's;
-  // AP_RAD_GR1D: the 1D GR lab's; the reference picks them at build time by
-  // lab shadowing) and the key of the counter-based random stream that
+  // AP_RAD_GR1D: the 1D GR lab's; AP_RAD_GAP1D: the 1D gap lab's; the
+  // reference picks them at build time by lab shadowing) and the key of the counter-based random stream that
   // replaces cuRAND
   int rad_model = 0;
   uint64_t rad_seed = 1;

@@ -489,16 +489,18 @@ AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32
  * with the user radiative functions of the framework
  * (src/cuda/radiation/user_radiative_functions.cu, AP_RAD_DEFAULT), of
  * the pulsar lab (labs/pulsar/src/cuda/radiation/
- * user_radiative_functions.cu, AP_RAD_PULSAR) or of the 1D GR lab
- * (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh, AP_RAD_GR1D,
- * which samples inverse-Compton emission and gamma-gamma conversion from the
- * tables of ap_ic_init), and the photon movers of the particle updaters
- * (ptc_updater.cu:627-690, ptc_updater_logsph.cu:58-131,
- * ptc_updater_1dgr.cu:301-400), which ap_update_particles runs after the
+ * user_radiative_functions.cu, AP_RAD_PULSAR), of the 1D GR lab
+ * (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh, AP_RAD_GR1D)
+ * or of the 1D gap lab (labs/1dgap/.../user_radiative_functions.cuh,
+ * AP_RAD_GAP1D) -- the last two sample inverse-Compton emission and
+ * gamma-gamma conversion from the tables of ap_ic_init -- and the photon
+ * movers of the particle updaters (ptc_updater.cu:627-690,
+ * ptc_updater_logsph.cu:58-131, ptc_updater_1dgr.cu:301-400,
+ * ptc_updater_1dgap.cu:163-192), which ap_update_particles runs after the
  * particles when photons are bound, followed by the exchange: photons
  * leaving the bulk wrap through periodic sides (Cartesian) or are removed
- * (the 1D GR mover removes photons outside the bulk before moving them, as
- * the reference's does).
+ * (the 1D GR and gap movers remove photons outside the bulk before moving
+ * them, as the reference's do).
  *
  * Each pass ranks its emitters in slot order and appends: photon k of an
  * emit_photons call at slot number + k (the photon count then grows by the
@@ -518,6 +520,7 @@ AP_API int ap_batch_inject_pairs(ap_batch *batch, const double *dt, const uint32
 #define AP_RAD_DEFAULT 0
 #define AP_RAD_PULSAR 1
 #define AP_RAD_GR1D 2
+#define AP_RAD_GAP1D 3
 typedef struct {
   float *x1, *x2, *x3;
   float *p1, *p2, *p3;
@@ -541,11 +544,12 @@ typedef struct {
   uint64_t seed;
   uint64_t first_photon_id;
   uint64_t first_particle_id;
-  /* AP_RAD_GR1D (user_rt_init, labs/1dgr/src/cuda/radiation/
-     user_radiative_functions.cuh:191-203): tables of n_gamma x n_ep
-     entries for the background broken_power_law(1.25, 1.1, e_min, 1e-10,
-     0.1) with photon density 1.5e24 / ic_path; the spin and omega are the
-     1D GR context's (ap_gr_params).                                        */
+  /* AP_RAD_GR1D and AP_RAD_GAP1D (user_rt_init of either lab, e.g.
+     labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh:191-203):
+     tables of n_gamma x n_ep entries for the background
+     broken_power_law(1.25, 1.1, e_min, 1e-10, 0.1) with photon density
+     1.5e24 / ic_path; the gap lab keeps photons above 0.001 / e_min; the
+     spin and omega are the 1D GR context's (ap_gr_params).                  */
   float e_min;          /* SimParams::e_min (default 1e-3)                 */
   float ic_path;        /* SimParams::ic_path (default 1)                  */
   int n_gamma, n_ep;    /* SimParams::n_gamma, n_ep (default 600, 600)     */

@@ -129,7 +129,7 @@ def _load_oracle():
     path = os.path.join(_HERE, "liboracle.so")
     srcs = [os.path.join(_HERE, n) for n in ("ap_oracle.c", "ap_oracle.h", "ap_logsph.c",
                                               "ap_logsph.h", "ap_gr.c", "ap_gr.h", "ap_rad.c",
-                                              "ap_rad.h")]
+                                              "ap_rad.h", "ap_ic.c", "ap_ic.h")]
     if not os.path.exists(path) or any(os.path.getmtime(path) < os.path.getmtime(s)
                                        for s in srcs):
         _build(_HERE, "liboracle.so")
@@ -603,6 +603,8 @@ def load_ref_gap(build=True):
     r.ref_gap_filter.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int]
     r.ref_gap_update_e.restype = None
     r.ref_gap_update_e.argtypes = [_vp, _vp, _vp, C.c_float, C.c_float]
+    r.ref_gap_move_photons.restype = None
+    r.ref_gap_move_photons.argtypes = [_vp, _vp, _sz, C.c_float, C.c_uint32]
     ref_gap = r
     return ref_gap
 

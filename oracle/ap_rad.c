@@ -11,6 +11,9 @@
  *                              user_radiative_functions.cuh (with the
  *                              inverse-Compton tables of ap_ic.c), and the
  *                              1D GR photon mover
+ *   - the 1D gap lab's:        labs/1dgap/src/cuda/radiation/
+ *                              user_radiative_functions.cuh (the same
+ *                              tables), and the 1D gap photon mover
  * The float transcendentals are the C library's expf, sinf, cosf, acosf,
  * logf, atan2f (the reference's device code calls the float overloads);
  * rho_c's pow and chi's square root take double arguments there and here.
@@ -22,8 +25,9 @@
  *     counter (pass, id, tag), so the result does not depend on scheduling.
  *     The draws are used as: default model u0 = photon energy, u1 = free
  *     path, u2 = tracking; pulsar model u0 = emission test, u2 = tracking;
- *     1D GR model u0 = emission test, u1 = photon energy, u2 = tracking;
- *     pair production u0 = tracking (1D GR: u1 = conversion test);
+ *     1D GR and gap models u0 = emission test, u1 = photon energy,
+ *     u2 = tracking; pair production u0 = tracking (1D GR and gap: u1 =
+ *     conversion test);
  *   - order: emitters are ranked in slot order (the reference ranks them by
  *     block and shared-memory atomic order);
  *   - ids: every new photon and particle gets an id from the counter
@@ -402,12 +406,89 @@ void or_move_photons_gr(const or_mesh *m, const or_rad_gr *g, or_photons *ph, si
   }
 }
 
+/* ---- the 1D gap lab's functions (labs/1dgap/src/cuda/radiation/
+ * user_radiative_functions.cuh:17-131): the 1D GR lab's tables on a flat
+ * line. Draws as for the 1D GR model. */
+static int check_emit_gap(const or_rad_params *rp, const or_ptc *p, size_t tid,
+                          const float u[4]) {
+  return u[0] < or_ic_rate(rp->gr->ic, p->E[tid]) * rp->delta_t;
+}
+
+static void emit_photon_gap(const or_rad_params *rp, or_ptc *p, size_t tid, or_photons *ph,
+                            size_t off, const float u[4]) {
+  const float x1 = p->x1[tid], p1 = p->p1[tid];
+  const uint32_t c = p->cell[tid];
+  const float gamma = p->E[tid];
+  float Eph = or_ic_photon_e(rp->gr->ic, gamma, u[1]);
+  if (Eph >= gamma - 1.01f) Eph = gamma - 1.01f;
+  const float En = gamma - Eph;
+  p->E[tid] = En;
+  float np1 = En * p1 / gamma;
+  if (np1 != np1) np1 = 0.0f;
+  p->p1[tid] = np1;
+  if (fabsf(Eph) < 0.001f / rp->e_min) return; /* energy taken, no photon kept */
+  ph->x1[off] = x1;
+  ph->x2[off] = ph->x3[off] = 0.0f;
+  ph->p1[off] = sgnf(p1) * Eph;
+  ph->p2[off] = ph->p3[off] = 0.0f;
+  ph->E[off] = Eph;
+  ph->weight[off] = p->weight[tid];
+  ph->path_left[off] = 0.0f;
+  ph->cell[off] = c;
+}
+
+static int check_pair_gap(const or_rad_params *rp, const or_photons *ph, size_t tid,
+                          const float u[4]) {
+  return u[1] < or_gg_rate(rp->gr->ic, ph->E[tid]) * rp->delta_t;
+}
+
+static void produce_pair_gap(const or_mesh *m, or_photons *ph, size_t tid, or_ptc *p,
+                             size_t off) {
+  const float Eph = fabsf(ph->p1[tid]);
+  const uint32_t c = ph->cell[tid];
+  const float x1 = ph->x1[tid];
+  ph->cell[tid] = OR_MAX_CELL;
+  float p1 = sgnf(ph->p1[tid]) * sqrtf(0.25f * Eph * Eph - 1.0f);
+  if (p1 != p1) p1 = 0.0f;
+  const float beta = mpos(m, 0, c1_of(m, c), x1);
+  const float E = sqrtf(1.0f + p1 * p1 + beta * beta);
+  for (int k = 0; k < 2; ++k) {
+    const size_t o = off + (size_t)k;
+    p->x1[o] = x1;
+    p->x2[o] = p->x3[o] = 0.0f;
+    p->p1[o] = p1;
+    p->p2[o] = p->p3[o] = 0.0f;
+    p->E[o] = E;
+    p->weight[o] = ph->weight[tid];
+    p->cell[o] = c;
+    p->flag[o] = FLAG_SECONDARY | ((uint32_t)k << 29);
+  }
+}
+
+void or_move_photons_gap(const or_mesh *m, or_photons *ph, size_t num, float dt) {
+  for (size_t idx = 0; idx < num; ++idx) {
+    const uint32_t c = ph->cell[idx];
+    if (c == OR_MAX_CELL) continue;
+    if (!in_bulk(m, c)) {
+      ph->cell[idx] = OR_MAX_CELL;
+      continue;
+    }
+    const float p1 = ph->p1[idx], x1 = ph->x1[idx];
+    float new_x1 = x1 + sgnf(p1) * dt * m->inv_delta[0];
+    const int dc1 = (int)floorf(new_x1);
+    new_x1 -= (float)dc1;
+    ph->cell[idx] = c + (uint32_t)dc1;
+    ph->x1[idx] = new_x1;
+  }
+}
+
 /* check_emit_photon of the model (default :13-17; pulsar :26-53). */
 static int check_emit(const or_mesh *m, const or_rad_params *rp, const or_ptc *p, size_t tid,
                       const float u[4]) {
   const float gamma = p->E[tid];
   if (rp->model == OR_RAD_DEFAULT) return gamma > rp->gamma_thr;
   if (rp->model == OR_RAD_GR1D) return check_emit_gr(rp, p, tid, u);
+  if (rp->model == OR_RAD_GAP1D) return check_emit_gap(rp, p, tid, u);
   const uint32_t c = p->cell[tid];
   const int c1 = c1_of(m, c), c2 = c2_of(m, c);
   const float r = expf(mpos(m, 0, c1, p->x1[tid]));
@@ -427,6 +508,10 @@ static void emit_photon(const or_mesh *m, const or_rad_params *rp, or_ptc *p, si
                         or_photons *ph, size_t off, const or_fields *f, const float u[4]) {
   if (rp->model == OR_RAD_GR1D) {
     emit_photon_gr(m, rp, p, tid, ph, off, u);
+    return;
+  }
+  if (rp->model == OR_RAD_GAP1D) {
+    emit_photon_gap(rp, p, tid, ph, off, u);
     return;
   }
   const uint32_t c = p->cell[tid];
@@ -590,10 +675,12 @@ void or_produce_pairs(const or_mesh *m, const or_rad_params *rp, or_photons *ph,
   for (size_t tid = 0; tid < ph_num; ++tid) {
     const uint32_t cell = ph->cell[tid];
     if (cell == OR_MAX_CELL || !in_bulk(m, cell)) continue;
-    if (rp->model == OR_RAD_GR1D) {
+    if (rp->model == OR_RAD_GR1D || rp->model == OR_RAD_GAP1D) {
       float ug[4];
       or_rad_uniforms(rp->seed, 2u, call, ph->id[tid], ug);
-      if (!check_pair_gr(rp, ph, tid, ug)) continue;
+      if (!(rp->model == OR_RAD_GR1D ? check_pair_gr(rp, ph, tid, ug)
+                                     : check_pair_gap(rp, ph, tid, ug)))
+        continue;
     } else if (!check_pair(m, rp, ph, tid, f)) {
       continue;
     }
@@ -611,6 +698,8 @@ void or_produce_pairs(const or_mesh *m, const or_rad_params *rp, or_photons *ph,
     p->flag[off] = p->flag[off + 1] = 0u;
     if (rp->model == OR_RAD_GR1D)
       produce_pair_gr(rp, ph, tid, p, off);
+    else if (rp->model == OR_RAD_GAP1D)
+      produce_pair_gap(m, ph, tid, p, off);
     else
       produce_pair(ph, tid, p, off);
     const int tracked = u[0] < rp->track_percent;

@@ -25,9 +25,11 @@ typedef struct {
 
 /* The emission / conversion models: the framework's default
  * (src/cuda/radiation/user_radiative_functions.cu), the pulsar lab's
- * (labs/pulsar/src/cuda/radiation/user_radiative_functions.cu) and the 1D
- * GR lab's (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh). */
-enum { OR_RAD_DEFAULT = 0, OR_RAD_PULSAR = 1, OR_RAD_GR1D = 2 };
+ * (labs/pulsar/src/cuda/radiation/user_radiative_functions.cu), the 1D GR
+ * lab's (labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh) and the
+ * 1D gap lab's (labs/1dgap/src/cuda/radiation/user_radiative_functions.cuh;
+ * of or_rad_gr it reads only the tables). */
+enum { OR_RAD_DEFAULT = 0, OR_RAD_PULSAR = 1, OR_RAD_GR1D = 2, OR_RAD_GAP1D = 3 };
 
 /* What the 1D GR lab's functions read besides SimParams: Grid_1dGR's
  * per-cell arrays (grid_1dgr.h mesh_ptrs), the spin a, omega, and the
@@ -45,7 +47,8 @@ typedef struct {
   float delta_t, gamma_thr, E_secondary, photon_path, r_cutoff, track_percent;
   float e_curv, l_curv, BQ, omega;
   uint64_t seed;
-  const or_rad_gr *gr; /* OR_RAD_GR1D only */
+  const or_rad_gr *gr; /* OR_RAD_GR1D, OR_RAD_GAP1D */
+  float e_min;         /* OR_RAD_GAP1D: photons below 0.001 / e_min not kept */
 } or_rad_params;
 
 /* Counts of one emission or conversion pass. */
@@ -78,6 +81,11 @@ void or_move_photons_logsph(const or_mesh *m, const or_rad_params *rp, or_photon
  * step % data_interval == 0. */
 void or_move_photons_gr(const or_mesh *m, const or_rad_gr *g, or_photons *ph, size_t num,
                         float dt, uint32_t step, int data_interval);
+
+/* update_photon_1dgap (src/cuda/algorithms/ptc_updater_1dgap.cu:163-192):
+ * photons outside the bulk are removed, the others move dt along the sign
+ * of p1. */
+void or_move_photons_gap(const or_mesh *m, or_photons *ph, size_t num, float dt);
 
 /* radiative_transfer::emit_photons (src/cuda/radiation/radiative_transfer.cu:
  * 28-97, 196-243) with the model's check_emit_photon / emit_photon: parents

@@ -30,7 +30,7 @@ PH_FIELDS = (
     ("cell", np.uint32), ("id", np.uint64), ("flag", np.uint32),
 )
 
-RAD_DEFAULT, RAD_PULSAR, RAD_GR1D = 0, 1, 2
+RAD_DEFAULT, RAD_PULSAR, RAD_GR1D, RAD_GAP1D = 0, 1, 2, 3
 SPEC_POWER_LAW_HARD, SPEC_POWER_LAW_SOFT, SPEC_BROKEN_POWER_LAW = 0, 1, 2
 SPEC_BLACK_BODY, SPEC_MONO_ENERGETIC = 3, 4
 
@@ -46,6 +46,7 @@ class RadParams(C.Structure):
         ("E_secondary", C.c_float), ("photon_path", C.c_float), ("r_cutoff", C.c_float),
         ("track_percent", C.c_float), ("e_curv", C.c_float), ("l_curv", C.c_float),
         ("BQ", C.c_float), ("omega", C.c_float), ("seed", C.c_uint64), ("gr", C.c_void_p),
+        ("e_min", C.c_float),
     ]
 
 
@@ -77,7 +78,7 @@ def rad_params(model=RAD_DEFAULT, delta_t=0.01, gamma_thr=20.0, E_secondary=4.0,
                BQ=1.0, omega=0.2, seed=1):
     """RadParams with the reference's SimParams defaults (sim_params.h:50-83)."""
     return RadParams(model, delta_t, gamma_thr, E_secondary, photon_path, r_cutoff,
-                     track_percent, e_curv, l_curv, BQ, omega, seed, None)
+                     track_percent, e_curv, l_curv, BQ, omega, seed, None, 1e-3)
 
 
 def spectrum(kind, *p):
@@ -138,6 +139,26 @@ class GrRad:
                        C.addressof(ic.s))
 
 
+class GapRad:
+    """or_rad_gr carrying only the tables, for the 1D gap lab's model."""
+
+    def __init__(self, ic):
+        self.ic = ic
+        self.s = RadGr(*([None] * 9), 0.0, 0.0, C.addressof(ic.s))
+
+
+def gap_rad_params(gap, delta_t, e_min=1e-3, track_percent=0.2, seed=1):
+    rp = rad_params(model=RAD_GAP1D, delta_t=delta_t, track_percent=track_percent, seed=seed)
+    rp.gr = C.addressof(gap.s)
+    rp.e_min = e_min
+    return rp
+
+
+def move_photons_gap(m, ph, num, dt):
+    s = photons_struct(ph)
+    lib.or_move_photons_gap(C.byref(m), C.byref(s), num, dt)
+
+
 def gr_rad_params(gr, delta_t, track_percent=0.2, seed=1):
     rp = rad_params(model=RAD_GR1D, delta_t=delta_t, track_percent=track_percent, seed=seed)
     rp.gr = C.addressof(gr.s)
@@ -153,6 +174,7 @@ for _name, _res, _args in [
     ("or_produce_pairs", None, [_vp, _vp, _vp, _sz, _vp, _vp, _sz, _vp, _vp, C.c_uint32,
                                 C.c_uint64, _vp]),
     ("or_move_photons_gr", None, [_vp, _vp, _vp, _sz, C.c_float, C.c_uint32, C.c_int]),
+    ("or_move_photons_gap", None, [_vp, _vp, _sz, C.c_float]),
     ("or_ic_init", None, [_vp, C.c_double, C.c_double, C.c_double, _vp]),
     ("or_ic_rate", C.c_float, [_vp, C.c_float]),
     ("or_gg_rate", C.c_float, [_vp, C.c_float]),
@@ -321,25 +343,61 @@ def load_ref_gr(build=True):
             return None
     if not os.path.exists(_REF_GR_PATH):
         return None
-    r = C.CDLL(_REF_GR_PATH)
+    ref_gr = _rgr_lib(_REF_GR_PATH)
+    return ref_gr
+
+
+def _rgr_lib(path):
+    r = C.CDLL(path)
+    r.ref_rgr_set_e_min.restype = None
+    r.ref_rgr_set_e_min.argtypes = [C.c_float]
     r.ref_gr_emit_photons.restype = C.c_int
     r.ref_gr_emit_photons.argtypes = [_vp, _vp, C.c_float, C.c_float, _vp, _sz, _vp, _vp, _sz,
                                       _vp, C.c_uint64, _vp]
     r.ref_gr_produce_pairs.restype = C.c_int
     r.ref_gr_produce_pairs.argtypes = [_vp, _vp, C.c_float, C.c_float, _vp, _sz, _vp, _vp, _sz,
                                        _vp, C.c_uint64, _vp]
-    ref_gr = r
-    return ref_gr
+    return r
+
+
+_REF_GAP_RAD_PATH = os.path.join(_HERE, "_ref", "libapref_rad_gap.so")
+ref_gap_rad = None
+
+
+def load_ref_gap_rad(build=True):
+    """The 1D gap lab's own user radiative functions on the host (the same
+    driver as load_ref_gr), or None."""
+    global ref_gap_rad
+    if ref_gap_rad is not None:
+        return ref_gap_rad
+    if not os.path.exists(_REF_GAP_RAD_PATH) and build and ref_tree_present():
+        try:
+            _build(os.path.join(_HERE, "ref_build"), "../_ref/libapref_rad_gap.so")
+        except Exception:
+            return None
+    if not os.path.exists(_REF_GAP_RAD_PATH):
+        return None
+    ref_gap_rad = _rgr_lib(_REF_GAP_RAD_PATH)
+    return ref_gap_rad
+
+
+def _ref_lib_of(rp):
+    if rp.model == RAD_GAP1D:
+        r = load_ref_gap_rad()
+        r.ref_rgr_set_e_min(rp.e_min)
+        return r
+    return load_ref_gr()
 
 
 def ref_gr_emit_photons(m, rp, p, ptc_num, ph, ph_num, ph_cap, call, first_id):
-    """The lab's check_emit_photon / emit_photon in the build's pass;
-    rp is gr_rad_params(...). Returns (new photon number, RadCounts)."""
+    """The lab's check_emit_photon / emit_photon in the build's pass, of the
+    1D GR lab (rp from gr_rad_params) or of the 1D gap lab (gap_rad_params).
+    Returns (new photon number, RadCounts)."""
     u4 = uniforms(rp.seed, 1, call, p["id"][:ptc_num])
     sp, sph = ptc_struct(p), photons_struct(ph)
     n = C.c_size_t(ph_num)
     cnt = RadCounts()
-    rc = load_ref_gr().ref_gr_emit_photons(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
+    rc = _ref_lib_of(rp).ref_gr_emit_photons(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
                                            C.byref(sp), ptc_num, C.byref(sph), C.byref(n),
                                            ph_cap, _p(u4), first_id, C.byref(cnt))
     assert rc == 0, "a user function drew more uniforms than the build gives it"
@@ -351,7 +409,7 @@ def ref_gr_produce_pairs(m, rp, ph, ph_num, p, ptc_num, ptc_cap, call, first_id)
     sp, sph = ptc_struct(p), photons_struct(ph)
     n = C.c_size_t(ptc_num)
     cnt = RadCounts()
-    rc = load_ref_gr().ref_gr_produce_pairs(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
+    rc = _ref_lib_of(rp).ref_gr_produce_pairs(C.byref(m), rp.gr, rp.delta_t, rp.track_percent,
                                             C.byref(sph), ph_num, C.byref(sp), C.byref(n),
                                             ptc_cap, _p(u4), first_id, C.byref(cnt))
     assert rc == 0, "a user function drew more uniforms than the build gives it"

@@ -2,7 +2,8 @@
  * Oracle pin build (TEST INFRASTRUCTURE ONLY): the 1D gap lab's kernels run
  * on the host.
  *
- * The Makefile copies update_ptc_1dgap, filter_current1d and beta_phi from
+ * The Makefile copies update_ptc_1dgap, filter_current1d, beta_phi and
+ * update_photon_1dgap from
  * src/cuda/algorithms/ptc_updater_1dgap.cu and update_e_1dgap from
  * field_solver_1dgap.cu into oracle/_ref/ (extract_kernels.py; the rest of
  * that Kernels namespace draws its initial conditions from cuRAND) and
@@ -116,6 +117,29 @@ void ref_gap_update_e(const ref_mesh *m, float *E1, float *J1, float j0, float d
   set_mesh(m);
   one_thread();
   Kernels::update_e_1dgap(pp(E1, m), pp(J1, m), j0, dt);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* Same layout as or_photons (oracle/ap_rad.h). */
+typedef struct {
+  float *x1, *x2, *x3, *p1, *p2, *p3, *E, *weight, *path_left;
+  uint32_t *cell; uint64_t *id; uint32_t *flag;
+} ref_photons;
+
+/* update_photon_1dgap (ptc_updater_1dgap.cu:163-192) as one thread. */
+void ref_gap_move_photons(const ref_mesh *m, const ref_photons *ph, size_t num, float dt,
+                          uint32_t step) {
+  set_mesh(m);
+  photon_data d;
+  d.x1 = ph->x1; d.x2 = ph->x2; d.x3 = ph->x3;
+  d.p1 = ph->p1; d.p2 = ph->p2; d.p3 = ph->p3;
+  d.E = ph->E; d.weight = ph->weight; d.path_left = ph->path_left;
+  d.cell = ph->cell; d.id = ph->id; d.flag = ph->flag;
+  one_thread();
+  Kernels::update_photon_1dgap(d, num, dt, step);
 }
 
 }  // extern "C"

@@ -1,6 +1,8 @@
 /*
  * Oracle pin build, 1D GR radiation (TEST INFRASTRUCTURE ONLY): runs the
- * 1D GR lab's own user radiative functions on the host.
+ * 1D GR lab's own user radiative functions on the host; built a second time
+ * with AP_REF_GAP for the 1D gap lab's (labs/1dgap/src/cuda/radiation/
+ * user_radiative_functions.cuh, which includes the same headers).
  *
  * labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh is compiled
  * unmodified behind shim_rgr/ (CudaRng with its m_local_state, a no-op
@@ -78,7 +80,11 @@ Scalar *dev_ic_rate, *dev_gg_rate, *dev_gammas;
 }  // namespace Kernels
 }  // namespace Aperture
 
+#ifdef AP_REF_GAP
+#include "labs/1dgap/src/cuda/radiation/user_radiative_functions.cuh"
+#else
 #include "labs/1dgr/src/cuda/radiation/user_radiative_functions.cuh"
+#endif
 
 namespace Aperture {
 Grid &sim_environment::local_grid() {
@@ -134,6 +140,7 @@ static void set_state(const ref_mesh *m, const ref_gr *g, float delta_t, float t
   dev_params.track_percent = track_percent;
   dev_params.a = g->a;
   dev_params.omega = g->omega;
+#ifndef AP_REF_GAP
   Grid_1dGR::mesh_ptrs &mp = Kernels::dev_mesh_ptrs_1dgr;
   mp = Grid_1dGR::mesh_ptrs();
   mp.alpha = g->alpha;
@@ -145,6 +152,7 @@ static void set_state(const ref_mesh *m, const ref_gr *g, float delta_t, float t
   mp.gamma_ff = g->gamma_ff;
   mp.beta_phi = g->beta_phi;
   mp.theta = g->theta;
+#endif
   const or_ic_tables *t = g->ic;
   dev_params.n_gamma = t->n_gamma;
   Kernels::dev_ic_dep = t->dep;
@@ -185,6 +193,9 @@ static void queue(const float *u, int n) {
 static const uint32_t kTracked = 1u << 1;
 
 extern "C" {
+
+/* SimParams::e_min, which the 1D gap lab's emit_photon reads. */
+void ref_rgr_set_e_min(float e_min) { dev_params.e_min = e_min; }
 
 /* emit_photons with the lab's check_emit_photon / emit_photon, parents in
  * slot order; u4 holds the build's four uniforms of every particle slot.

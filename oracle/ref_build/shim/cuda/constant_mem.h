@@ -19,6 +19,7 @@ struct ap_ref_params {
    * pulsar lab) */
   float delta_t, gamma_thr, E_secondary, photon_path, l_curv, e_curv, BQ;
   int n_gamma;  /* inverse-Compton table size (rt_ic.cu find_n_gamma) */
+  float e_min;  /* 1D gap lab: photons below 0.001 / e_min not kept */
 };
 extern Quadmesh dev_mesh;
 extern ap_ref_params dev_params;

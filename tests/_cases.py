@@ -279,3 +279,37 @@ def rad_rho(f, rng, frac_dense=0.3):
     dense = rng.random(shape) < frac_dense
     f["Rho"][0][:] = (-a).astype(np.float32)
     f["Rho"][1][:] = np.where(dense, a * (1 + 1e-3), a * 3.0).astype(np.float32)
+
+
+def gap_rad_case(ng, ne, n=6000, n_ph=6000, ic_path=0.004, seed=13):
+    """The 1D gap lab's radiative transfer: a 512-cell gap grid with hot
+    particles (gamma log-uniform in [2, 1e5]), photons of energy 10 .. 1e6,
+    inverse-Compton tables of ng x ng entries and the oracle's parameters
+    (model, tables, e_min 1e-3). Returns (mesh, params, tables holder,
+    particles, photons, n, n_ph, capacity, photon capacity)."""
+    from oracle import rad
+    rng = np.random.default_rng(seed)
+    m = oracle.make_mesh((512, 1, 1), (2, 0, 0), lower=(0.0, 0, 0), size=(1.0, 1, 1))
+    cap, ph_cap = 4 * n + 1024, 3 * n_ph + 1024
+    p = empty_ptc(cap)
+    p["cell"][:n] = rng.integers(m.guard[0], m.dims[0] - m.guard[0], n).astype(np.uint32)
+    p["cell"][n:] = oracle.MAX_CELL
+    p["x1"][:n] = rng.random(n, dtype=np.float32)
+    g = np.exp(np.log(2.0) + rng.random(n) * np.log(5e4))
+    p["E"][:n] = g.astype(np.float32)
+    p["p1"][:n] = (np.where(rng.random(n) < 0.5, -1, 1) * np.sqrt(g * g - 1)).astype(np.float32)
+    p["weight"][:n] = (0.5 + rng.random(n)).astype(np.float32)
+    p["flag"][:n] = (rng.integers(0, 2, n).astype(np.uint32) << np.uint32(29))
+    p["id"][:n] = np.arange(n, dtype=np.uint64) + 31
+    ph = rad.new_photons(ph_cap)
+    ph["cell"][:n_ph] = rng.integers(m.guard[0], m.dims[0] - m.guard[0], n_ph).astype(np.uint32)
+    ph["x1"][:n_ph] = rng.random(n_ph, dtype=np.float32)
+    E = np.exp(np.log(10.0) + rng.random(n_ph) * np.log(1e5))
+    ph["p1"][:n_ph] = (np.where(rng.random(n_ph) < 0.5, -1, 1) * E).astype(np.float32)
+    ph["E"][:n_ph] = E.astype(np.float32)
+    ph["weight"][:n_ph] = (0.5 + rng.random(n_ph)).astype(np.float32)
+    ph["id"][:n_ph] = np.arange(n_ph, dtype=np.uint64) + 700_000
+    tables = rad.IcTables(rad.gr1d_spectrum(1e-3), 1e-10, 0.1, 1.5e24 / ic_path, ng, ne)
+    gap = rad.GapRad(tables)
+    rp = rad.gap_rad_params(gap, 2e-3, e_min=1e-3, track_percent=0.3, seed=9)
+    return m, rp, gap, p, ph, n, n_ph, cap, ph_cap

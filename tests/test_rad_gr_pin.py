@@ -13,7 +13,7 @@ import pytest
 
 import oracle
 from oracle import rad
-from _cases import GR_A, GR_OMEGA, empty_ptc, gr_dt, gr_mesh, gr_particles, gr_table
+from _cases import GR_A, GR_OMEGA, empty_ptc, gap_rad_case, gr_dt, gr_mesh, gr_particles, gr_table
 
 pytestmark = pytest.mark.skipif(rad.load_ref_gr() is None,
                                 reason="reference tree not present and no prebuilt pin library")
@@ -119,3 +119,50 @@ def test_gr_photon_mover_bit_exact():
                                                  rp.delta_t, step, 2, ptrs)
     _same(a, b, "photons")
     assert (a["cell"][:n_ph] == oracle.MAX_CELL).sum() >= 20
+
+
+# ---- the 1D gap lab (labs/1dgap/src/cuda/radiation/user_radiative_functions.cuh)
+
+gap_pin = pytest.mark.skipif(rad.load_ref_gap_rad() is None, reason="no 1D gap radiation pin")
+
+
+@gap_pin
+@pytest.mark.parametrize("call", [0, 4])
+def test_gap_emission_bit_exact(call):
+    m, rp, gap, p, ph, n, n_ph, cap, ph_cap = gap_rad_case(NG, NE)
+    po, pho = oracle.copy_ptc(p), rad.copy_photons(ph)
+    pr, phr = oracle.copy_ptc(p), rad.copy_photons(ph)
+    f = oracle.new_fields(m, 2)
+    n1, c1 = rad.emit_photons(m, rp, po, n, pho, n_ph, ph_cap, f, None, call, 1 << 40)
+    n2, c2 = rad.ref_gr_emit_photons(m, rp, pr, n, phr, n_ph, ph_cap, call, 1 << 40)
+    assert (n1, c1.marked, c1.written) == (n2, c2.marked, c2.written)
+    assert c1.marked > 200
+    _same(po, pr, "particles")
+    _same(pho, phr, "photons")
+
+
+@gap_pin
+def test_gap_conversion_bit_exact():
+    m, rp, gap, p, ph, n, n_ph, cap, ph_cap = gap_rad_case(NG, NE, ic_path=0.0005)
+    po, pho = oracle.copy_ptc(p), rad.copy_photons(ph)
+    pr, phr = oracle.copy_ptc(p), rad.copy_photons(ph)
+    f = oracle.new_fields(m, 2)
+    n1, c1 = rad.produce_pairs(m, rp, pho, n_ph, po, n, cap, f, None, 1, 1 << 41)
+    n2, c2 = rad.ref_gr_produce_pairs(m, rp, phr, n_ph, pr, n, cap, 1, 1 << 41)
+    assert (n1, c1.marked, c1.written) == (n2, c2.marked, c2.written)
+    assert c1.marked > 100
+    _same(po, pr, "particles")
+    _same(pho, phr, "photons")
+
+
+@pytest.mark.skipif(oracle.load_ref_gap() is None, reason="no 1D gap pin library")
+def test_gap_photon_mover_bit_exact():
+    import ctypes as C
+    m, rp, gap, p, ph, n, n_ph, cap, ph_cap = gap_rad_case(NG, NE)
+    ph["cell"][:10] = np.uint32(0)  # in the guard: removed first
+    a, b = rad.copy_photons(ph), rad.copy_photons(ph)
+    for step in range(4):
+        rad.move_photons_gap(m, a, n_ph, 2e-3)
+        oracle.load_ref_gap().ref_gap_move_photons(C.byref(m), C.byref(rad.photons_struct(b)),
+                                                   n_ph, 2e-3, step)
+    _same(a, b, "photons")
