@@ -404,6 +404,10 @@ def run_ours(args, rank, world, local_rank):
                 # the north star quotes the fraction against ~8 TB/s as well
                 "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": achieved / NOMINAL_HBM_GBS,
                 "traffic": (tpp * n if tpp is not None else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                  "launch, mean of four launches of the 1024^2 x 64 ppc "
+                                  "benchmark (profiles/k_push_deposit_2d_box.md), in B per "
+                                  "particle x this run's particles",
                 "kernel": "k_push_deposit_2d", "kernel_ms": k_ms,
                 "phases_ms_per_step": {
                     "push_deposit": pt.push_deposit_ms / args.steps,
