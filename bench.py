@@ -170,14 +170,14 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per particle of the fused kernel from the committed ncu
-    summary (line 'dram_bytes_per_particle: X'), or None."""
-    path = os.path.join(ROOT, "profiles", "k_push_deposit_2d_box.md")
+def profiled_traffic(name="k_push_deposit_2d_box.md", key="dram_bytes_per_particle"):
+    """A DRAM traffic figure of a fused kernel from its committed ncu summary
+    under profiles/ (line '<key>: X'), or None."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
             for line in f:
-                if line.strip().startswith("dram_bytes_per_particle:"):
+                if line.strip().startswith(key + ":"):
                     return float(line.split(":")[1])
     except Exception:
         pass
@@ -1057,7 +1057,12 @@ def run_logsph(args, emit=True, fp64_error=True):
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_source": peak_kind,
                         "peak_nominal": NOMINAL_HBM_GBS,
-                        "frac_nominal": achieved / NOMINAL_HBM_GBS, "traffic": None,
+                        "frac_nominal": achieved / NOMINAL_HBM_GBS,
+                        "traffic": profiled_traffic("k_push_deposit_2d_logsph.md",
+                                                    "dram_bytes_per_launch"),
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                          "mean of four launches of this workload "
+                                          "(profiles/k_push_deposit_2d_logsph.md)",
                         "kernel": "k_push_deposit_2d (log-spherical)", "kernel_ms": k_ms,
                         "note": "algorithmic bytes as for the Cartesian box; each particle "
                                 "also evaluates the reference's move in Cartesian space (sinf, "
