@@ -800,7 +800,13 @@ def run_box1d(args, emit=True):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": achieved / NOMINAL_HBM_GBS,
-                     "traffic": None, "kernel": "k_push_deposit_1d", "kernel_ms": k_ms},
+                     "traffic": profiled_traffic("k_push_deposit_1d_config1.md",
+                                                 "dram_bytes_per_launch"),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean "
+                                       "of four launches of this configuration "
+                                       "(profiles/k_push_deposit_1d_config1.md); the store is "
+                                       "L2-resident",
+                     "kernel": "k_push_deposit_1d", "kernel_ms": k_ms},
         "phases_ms_per_step": {"push_deposit": pt.push_deposit_ms / steps,
                                "finalize": pt.finalize_ms / steps,
                                "fields": pt.fields_ms / steps},
